@@ -1,0 +1,166 @@
+/*
+ * illume_gpu.h — C ABI of the B200 ray-query / path-tracing library.
+ *
+ * This is the drop-in boundary for rs_illume's aggregate.  In the reference
+ * every aggregate implements `trait Primitive` (src/core/primitive/mod.rs:9-20):
+ *   world_bound()  -> Box<dyn Bounding3<Float>>
+ *   intersect(&Ray) -> Option<SurfaceInteraction>
+ *   intersect_p(&Ray) -> bool
+ * and `BVHAccel` (src/accelerators/bvh.rs:24-93, 540-663) is the CPU
+ * implementation this library replaces.  A GPU aggregate is one context plus
+ * one accel id; the batch entry points below are the intended path, and a
+ * single-ray `Primitive::intersect` is a batch of one.
+ *
+ * Conventions
+ *  - Every function returns int32_t status: ILM_OK (0) or a negative ILM_ERR_*.
+ *    No exception or abort crosses this boundary; ilm_last_error_string()
+ *    describes the last failure on a context.
+ *  - Ray/hit pointers may be device memory (stream-ordered, asynchronous) or
+ *    host memory (pageable or pinned; the call stages through device buffers
+ *    and returns when the results are back in host memory).
+ *  - `stream` is a cudaStream_t passed as void*; NULL selects the context's
+ *    own stream.
+ *  - Primitive ids: meshes and sphere sets passed to ilm_accel_build are
+ *    numbered in list order; triangles of a mesh (or spheres of a set) take
+ *    consecutive ids.  This matches BVHAccel's `primitives` vector order.
+ *  - One context per host thread, or external serialisation.
+ */
+#ifndef ILLUME_GPU_H
+#define ILLUME_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ----------------------------------------------------------------- status */
+enum {
+    ILM_OK = 0,
+    ILM_ERR_INVALID_ARGUMENT = -1,   /* null/misaligned pointer, bad size/id */
+    ILM_ERR_OUT_OF_MEMORY = -2,
+    ILM_ERR_CUDA = -3,               /* a CUDA runtime call failed */
+    ILM_ERR_TRAVERSAL_LIMIT = -4,    /* a ray overflowed the traversal stack or
+                                        iteration cap; its record is flagged */
+    ILM_ERR_TIMEOUT = -5,            /* host watchdog gave up waiting */
+    ILM_ERR_NOT_FOUND = -6,          /* unknown mesh / accel id */
+    ILM_ERR_NO_DEVICE = -7           /* no CUDA device or the kernels are missing */
+};
+
+/* ----------------------------------------------------------------- records */
+/* Ray record, 32 bytes: replaces geometry/ray.rs:11-19 (o, d, t_max; the
+ * time/medium/differential fields are not used on this path). */
+typedef struct { float o[3]; float tmin; float d[3]; float tmax; } ilm_ray;
+/* Closest-hit record, 16 bytes: primitive id (ILM_MISS on a miss), t, and
+ * (u, v).  Triangles: u = b1, v = b2, so the hit point is
+ * b0*p0 + b1*p1 + b2*p2 with b0 = 1-u-v (shapes/triangle.rs:232-236).
+ * Spheres: the parametric (u, v) of shapes/sphere.rs:191-193. */
+typedef struct { uint32_t prim; float t; float u; float v; } ilm_hit;
+#define ILM_MISS 0xFFFFFFFFu
+
+/* Sphere shape: mirrors Sphere::new (shapes/sphere.rs:50-75).  Transforms are
+ * row-major 4x4, m[i][j] at [4*i + j]; world_to_object must be the inverse. */
+typedef struct {
+    float object_to_world[16];
+    float world_to_object[16];
+    float radius, z_min, z_max, phi_max_deg;
+    int32_t reverse_orientation;
+} ilm_sphere_desc;
+
+typedef struct {
+    int32_t device;        /* CUDA device ordinal */
+    int32_t stack_depth;   /* traversal stack entries per ray, <= 64 (0 = 64) */
+    int32_t block_size;    /* threads per block for traversal (0 = default) */
+    int32_t flags;         /* ILM_FLAG_* */
+    uint32_t max_iterations; /* per-ray traversal loop cap (0 = 2^20) */
+} ilm_config;
+/* Validate host-resident rays (finite origin/direction, non-zero direction,
+ * tmax >= 0) before any launch; an invalid ray fails the call with
+ * ILM_ERR_INVALID_ARGUMENT. */
+#define ILM_FLAG_VALIDATE_RAYS 1
+
+typedef struct {
+    int32_t width;             /* 2 (the reference's binary layout), 4 or 8 */
+    int32_t max_prims_in_node; /* BVHAccel::new max_prims_in_node (4 in all configs) */
+} ilm_build_opts;
+
+typedef struct {
+    uint32_t n_prims;
+    uint32_t n_binary_nodes;   /* nodes of the SAH binary tree (bvh.rs layout) */
+    uint32_t n_nodes;          /* nodes of the device layout for `width` */
+    uint32_t width;
+    uint64_t device_bytes;     /* nodes + primitive records in HBM */
+    double build_seconds;      /* host SAH build + collapse + upload */
+} ilm_accel_info;
+
+typedef uint32_t ilm_mesh_id;
+typedef uint32_t ilm_accel_id;
+typedef struct ilm_context ilm_context;
+
+/* ----------------------------------------------------------------- context */
+int32_t ilm_context_create(ilm_context** out, const ilm_config* cfg);
+int32_t ilm_context_destroy(ilm_context* ctx);
+/* Last error message on ctx (static string for ctx == NULL). Never NULL. */
+const char* ilm_last_error_string(const ilm_context* ctx);
+
+/* ----------------------------------------------------------------- shapes */
+/* TriangleMesh::new (shapes/triangle.rs:36-73) with world-space vertices:
+ * xyz holds 3*nv floats, idx holds 3*nt vertex indices.  Host memory is
+ * copied; the caller keeps ownership. */
+int32_t ilm_mesh_upload(ilm_context* ctx, const float* xyz, uint32_t nv,
+                        const uint32_t* idx, uint32_t nt, ilm_mesh_id* out);
+/* A set of spheres (shapes/sphere.rs). */
+int32_t ilm_spheres_upload(ilm_context* ctx, const ilm_sphere_desc* spheres, uint32_t n,
+                           ilm_mesh_id* out);
+
+/* ----------------------------------------------------------------- accel */
+/* BVHAccel::new (accelerators/bvh.rs:32-93): SAH recursive build with 12
+ * buckets (bvh.rs:95-247), flattened depth-first (bvh.rs:504-537), then laid
+ * out for `width` (2 = the reference's 32-byte nodes; 4/8 = compressed wide
+ * nodes collapsed from the same binary tree). */
+int32_t ilm_accel_build(ilm_context* ctx, const ilm_mesh_id* meshes, uint32_t n_meshes,
+                        const ilm_build_opts* opts, ilm_accel_id* out);
+int32_t ilm_accel_destroy(ilm_context* ctx, ilm_accel_id accel);
+/* Primitive::world_bound for BVHAccel (bvh.rs:555-561): {min xyz, max xyz}. */
+int32_t ilm_accel_world_bound(ilm_context* ctx, ilm_accel_id accel, float out[6]);
+int32_t ilm_accel_get_info(ilm_context* ctx, ilm_accel_id accel, ilm_accel_info* out);
+/* Copies of the SAH binary tree (32-byte nodes as bvh.rs:665-673) and the
+ * ordered primitive ids, for inspection. */
+int32_t ilm_accel_binary_nodes(ilm_context* ctx, ilm_accel_id accel, void* out_nodes,
+                               uint32_t* out_prim_order);
+
+/* Host-only build of the same structure, for inspection and tests (no GPU
+ * needed): one triangle mesh followed by one sphere set.  ilm_host_layout_copy
+ * fills any non-NULL output: binary nodes (32 B each), ordered primitive ids,
+ * the device node array (n_nodes * 32/64/80 B for width 2/4/8), the 48-byte
+ * primitive records, and the world bound (6 floats). */
+typedef struct ilm_host_layout ilm_host_layout;
+int32_t ilm_host_layout_build(const float* xyz, uint32_t nv, const uint32_t* idx, uint32_t nt,
+                              const ilm_sphere_desc* spheres, uint32_t ns, const ilm_build_opts* opts,
+                              ilm_host_layout** out);
+int32_t ilm_host_layout_info(const ilm_host_layout* layout, ilm_accel_info* out);
+int32_t ilm_host_layout_copy(const ilm_host_layout* layout, void* bin_nodes, uint32_t* prim_order, void* nodes,
+                             void* records, float* bound);
+int32_t ilm_host_layout_destroy(ilm_host_layout* layout);
+
+/* ----------------------------------------------------------------- queries */
+/* Primitive::intersect for BVHAccel (bvh.rs:563-612), batched: one closest
+ * hit per ray.  Ties at equal t resolve to the smaller primitive id. */
+int32_t ilm_intersect_closest(ilm_context* ctx, ilm_accel_id accel, const ilm_ray* rays,
+                              uint64_t n, ilm_hit* hits, void* stream);
+/* Primitive::intersect_p for BVHAccel (bvh.rs:614-662), batched:
+ * occluded[i] = 1 when any primitive is hit with 0 < t <= rays[i].tmax. */
+int32_t ilm_intersect_any(ilm_context* ctx, ilm_accel_id accel, const ilm_ray* rays,
+                          uint64_t n, uint32_t* occluded, void* stream);
+
+/* Device error word accumulated by the kernels since the last reset
+ * (bit 0: traversal stack overflow, bit 1: iteration cap).  Synchronises. */
+int32_t ilm_device_errors(ilm_context* ctx, uint32_t* out_flags, int32_t reset);
+/* Waits for `stream` (NULL = context stream) for at most timeout_s seconds;
+ * ILM_ERR_TIMEOUT if it is still busy. */
+int32_t ilm_synchronize(ilm_context* ctx, void* stream, double timeout_s);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,199 @@
+"""CPU oracle (test infrastructure only).
+
+ctypes wrapper of ``oracle/liboracle.so``, a scalar C++ restatement of
+rs_illume's ray-query hot path (see oracle/oracle.h for the file:line map and
+the D1..D24 repairs).  Only tests/, ``__graft_entry__.smoke()`` and bench.py's
+CPU-baseline / reference legs use it, as the checker; the product library never
+links or calls it.
+
+Parity status: unpinned by the reference's own tests -- the reference has no
+tests, golden vectors or fixtures for this path and cannot be compiled here.
+The restatement is pinned to analytic known-answer cases instead
+(tests/test_oracle_kat.py).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "liboracle.so")
+
+RAY_DTYPE = np.dtype([("o", "<f4", (3,)), ("tmin", "<f4"), ("d", "<f4", (3,)), ("tmax", "<f4")])
+HIT_DTYPE = np.dtype([("prim", "<u4"), ("t", "<f4"), ("u", "<f4"), ("v", "<f4")])
+BIN_NODE_DTYPE = np.dtype([("bmin", "<f4", (3,)), ("bmax", "<f4", (3,)), ("offset", "<i4"),
+                           ("n_prims", "<u2"), ("axis", "u1"), ("pad", "u1")])
+
+
+class orc_sphere_desc(ctypes.Structure):
+    _fields_ = [("object_to_world", ctypes.c_float * 16), ("world_to_object", ctypes.c_float * 16),
+                ("radius", ctypes.c_float), ("z_min", ctypes.c_float), ("z_max", ctypes.c_float),
+                ("phi_max_deg", ctypes.c_float), ("reverse_orientation", ctypes.c_int32)]
+
+
+_P = ctypes.c_void_p
+_SIG = {
+    "orc_gamma": (ctypes.c_float, [ctypes.c_int]),
+    "orc_next_float_up": (ctypes.c_float, [ctypes.c_float]),
+    "orc_next_float_down": (ctypes.c_float, [ctypes.c_float]),
+    "orc_rng_u32": (None, [ctypes.c_uint64, ctypes.c_uint64, _P]),
+    "orc_rng_floats": (None, [ctypes.c_uint64, ctypes.c_uint64, _P]),
+    "orc_rng_floats_advanced": (None, [ctypes.c_uint64, ctypes.c_int64, ctypes.c_uint64, _P]),
+    "orc_scene_create": (_P, [_P, ctypes.c_uint32, _P, ctypes.c_uint32, _P, ctypes.c_uint32, ctypes.c_int]),
+    "orc_scene_destroy": (None, [_P]),
+    "orc_scene_node_count": (ctypes.c_uint32, [_P]),
+    "orc_scene_nodes": (None, [_P, _P]),
+    "orc_scene_prim_order": (None, [_P, _P]),
+    "orc_scene_world_bound": (None, [_P, _P]),
+    "orc_scene_build_seconds": (ctypes.c_double, [_P]),
+    "orc_intersect": (ctypes.c_int64, [_P, _P, ctypes.c_uint64, _P, _P, _P, ctypes.c_int]),
+    "orc_intersect_p": (ctypes.c_int64, [_P, _P, ctypes.c_uint64, _P, _P, _P, ctypes.c_int]),
+    "orc_triangle_intersect": (ctypes.c_int, [_P, _P, _P, _P, ctypes.c_int, _P]),
+    "orc_sphere_intersect": (ctypes.c_int, [_P, _P, ctypes.c_int, _P]),
+    "orc_sphere_world_bound": (None, [_P, _P]),
+    "orc_last_trace_seconds": (ctypes.c_double, []),
+}
+
+_lib = None
+
+
+def load():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: build it with `make -C oracle`")
+        lib = ctypes.CDLL(LIB_PATH)
+        for k, (r, a) in _SIG.items():
+            f = getattr(lib, k)
+            f.restype = r
+            f.argtypes = a
+        _lib = lib
+    return _lib
+
+
+def _p(a):
+    if a is None:
+        return None
+    assert a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data
+
+
+def gamma(n: int) -> float:
+    return load().orc_gamma(n)
+
+
+def rng_floats(seq: int, n: int, advance: int = 0) -> np.ndarray:
+    out = np.empty(n, np.float32)
+    if advance:
+        load().orc_rng_floats_advanced(seq, advance, n, _p(out))
+    else:
+        load().orc_rng_floats(seq, n, _p(out))
+    return out
+
+
+def rng_u32(seq: int, n: int) -> np.ndarray:
+    out = np.empty(n, np.uint32)
+    load().orc_rng_u32(seq, n, _p(out))
+    return out
+
+
+def sphere_desc(radius: float, translate=(0.0, 0.0, 0.0), scale: float = 1.0, z_min=None, z_max=None,
+                phi_max_deg: float = 360.0, reverse: bool = False) -> orc_sphere_desc:
+    d = orc_sphere_desc()
+    tx, ty, tz = translate
+    m = [scale, 0, 0, tx, 0, scale, 0, ty, 0, 0, scale, tz, 0, 0, 0, 1]
+    inv = [1.0 / scale, 0, 0, -tx / scale, 0, 1.0 / scale, 0, -ty / scale, 0, 0, 1.0 / scale, -tz / scale, 0, 0, 0, 1]
+    for i in range(16):
+        d.object_to_world[i] = m[i]
+        d.world_to_object[i] = inv[i]
+    d.radius = radius
+    d.z_min = -radius if z_min is None else z_min
+    d.z_max = radius if z_max is None else z_max
+    d.phi_max_deg = phi_max_deg
+    d.reverse_orientation = int(reverse)
+    return d
+
+
+class Scene:
+    """BVHAccel over triangles (ids 0..nt-1) followed by spheres."""
+
+    def __init__(self, xyz, idx, spheres=(), max_prims_in_node: int = 4):
+        lib = load()
+        self._xyz = np.ascontiguousarray(xyz, np.float32).reshape(-1, 3)
+        self._idx = np.ascontiguousarray(idx, np.uint32).reshape(-1, 3)
+        sph = (orc_sphere_desc * max(1, len(spheres)))(*spheres)
+        self.n_prims = len(self._idx) + len(spheres)
+        self.h = lib.orc_scene_create(_p(self._xyz), len(self._xyz), _p(self._idx), len(self._idx),
+                                      ctypes.addressof(sph), len(spheres), max_prims_in_node)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            load().orc_scene_destroy(self.h)
+            self.h = None
+
+    @property
+    def build_seconds(self) -> float:
+        return load().orc_scene_build_seconds(self.h)
+
+    def nodes(self) -> np.ndarray:
+        n = load().orc_scene_node_count(self.h)
+        out = np.zeros(n, BIN_NODE_DTYPE)
+        load().orc_scene_nodes(self.h, _p(out))
+        return out
+
+    def prim_order(self) -> np.ndarray:
+        out = np.zeros(self.n_prims, np.uint32)
+        load().orc_scene_prim_order(self.h, _p(out))
+        return out
+
+    def world_bound(self) -> np.ndarray:
+        out = np.zeros(6, np.float32)
+        load().orc_scene_world_bound(self.h, _p(out))
+        return out
+
+    def intersect(self, rays: np.ndarray, threads: int = 0, counters: bool = False):
+        rays = np.ascontiguousarray(rays)
+        hits = np.empty(len(rays), HIT_DTYPE)
+        nv = np.empty(len(rays), np.uint32) if counters else None
+        nt = np.empty(len(rays), np.uint32) if counters else None
+        ovf = load().orc_intersect(self.h, _p(rays), len(rays), _p(hits), _p(nv), _p(nt), threads)
+        assert ovf == 0, f"{ovf} rays overflowed the 64-entry traversal stack"
+        return (hits, nv, nt) if counters else hits
+
+    def intersect_p(self, rays: np.ndarray, threads: int = 0, counters: bool = False):
+        rays = np.ascontiguousarray(rays)
+        occ = np.empty(len(rays), np.uint8)
+        nv = np.empty(len(rays), np.uint32) if counters else None
+        nt = np.empty(len(rays), np.uint32) if counters else None
+        ovf = load().orc_intersect_p(self.h, _p(rays), len(rays), _p(occ), _p(nv), _p(nt), threads)
+        assert ovf == 0, f"{ovf} rays overflowed the 64-entry traversal stack"
+        return (occ, nv, nt) if counters else occ
+
+
+def last_trace_seconds() -> float:
+    return load().orc_last_trace_seconds()
+
+
+def triangle_intersect(p0, p1, p2, o, d, tmax=float("inf"), closest=True):
+    """Returns (t, b0, b1, b2) or None."""
+    r = np.zeros(1, RAY_DTYPE)
+    r["o"][0] = o
+    r["d"][0] = d
+    r["tmax"][0] = tmax
+    pts = [np.asarray(p, np.float32) for p in (p0, p1, p2)]
+    out = np.zeros(4, np.float32)
+    ok = load().orc_triangle_intersect(_p(pts[0]), _p(pts[1]), _p(pts[2]), _p(r), int(closest), _p(out))
+    return tuple(float(x) for x in out) if ok else None
+
+
+def sphere_intersect(desc: orc_sphere_desc, o, d, tmax=float("inf")):
+    """Returns (t, u, v) or None."""
+    r = np.zeros(1, RAY_DTYPE)
+    r["o"][0] = o
+    r["d"][0] = d
+    r["tmax"][0] = tmax
+    out = np.zeros(3, np.float32)
+    ok = load().orc_sphere_intersect(ctypes.byref(desc), _p(r), 1, _p(out))
+    return tuple(float(x) for x in out) if ok else None

@@ -1,0 +1,809 @@
+// CPU oracle: scalar restatement of rs_illume's ray-query hot path.
+// TEST INFRASTRUCTURE ONLY (see oracle.h).  Built with -ffp-contract=off
+// -fno-fast-math so every float expression rounds exactly as the Rust source
+// (Rust never fuses multiply-add).  All citations are paths inside the
+// rs_illume repository.
+#include "oracle.h"
+
+#include <atomic>
+#include <chrono>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <limits>
+#include <thread>
+#include <vector>
+
+namespace orc {
+
+// ---------------------------------------------------------------- pbrt.rs
+// MACHINE_EPSILON = f32::EPSILON * 0.5 (core/pbrt.rs:23)
+static const float kMachineEps = std::numeric_limits<float>::epsilon() * 0.5f;
+static const float kPi = 3.14159265358979323846f;
+
+// gamma(n) (core/pbrt.rs:172-174)
+static float gamma(int n) {
+    return ((float)n * kMachineEps) / (1.0f - (float)n * kMachineEps);
+}
+
+static inline uint32_t f2u(float f) { uint32_t u; std::memcpy(&u, &f, 4); return u; }
+static inline float u2f(uint32_t u) { float f; std::memcpy(&f, &u, 4); return f; }
+
+// next_float_up (core/pbrt.rs:129-147)
+static float next_float_up(float v) {
+    if (std::isinf(v) && v > 0.0f) return v;
+    float nv = (v == -0.0f) ? 0.0f : v;   // -0.0 == 0.0, so both zeros map to +0
+    uint32_t ui = f2u(nv);
+    if (nv >= 0.0f) ++ui; else --ui;
+    return u2f(ui);
+}
+// next_float_down (core/pbrt.rs:151-169)
+static float next_float_down(float v) {
+    if (std::isinf(v) && v < 0.0f) return v;
+    float nv = (v == 0.0f) ? -0.0f : v;
+    uint32_t ui = f2u(nv);
+    if (nv > 0.0f) --ui; else ++ui;
+    return u2f(ui);
+}
+
+// ---------------------------------------------------------------- rng.rs
+// PCG32 (core/rng.rs:9-63); advance() with D18 repaired (loop while delta>0,
+// wrapping arithmetic).
+struct Rng {
+    uint64_t state = 0x853c49e6748fea9bULL, inc = 0xda3e39cb94b95bdbULL;
+    static constexpr uint64_t kMult = 0x5851f42d4c957f2dULL;
+    explicit Rng(uint64_t seq) { set_sequence(seq); }
+    void set_sequence(uint64_t initseq) {          // rng.rs:30-36
+        state = 0;
+        inc = (initseq << 1) | 1;
+        uniform_u32();
+        state += 0x853c49e6748fea9bULL;
+        uniform_u32();
+    }
+    uint32_t uniform_u32() {                       // rng.rs:38-49
+        uint64_t old = state;
+        state = old * kMult + inc;
+        uint32_t xorshifted = (uint32_t)(((old >> 18) ^ old) >> 27);
+        uint32_t rot = (uint32_t)(old >> 59);
+        return (xorshifted >> rot) | (xorshifted << ((~rot + 1u) & 31));
+    }
+    float uniform_float() {                        // rng.rs:60-63
+        float f = (float)uniform_u32() * 0x1p-32f;
+        const float one_minus_eps = 0x1.fffffep-1f;
+        return f < one_minus_eps ? f : one_minus_eps;
+    }
+    void advance(int64_t idelta) {                 // rng.rs:65-82, D18
+        uint64_t cur_mult = kMult, cur_plus = inc, acc_mult = 1, acc_plus = 0;
+        uint64_t delta = (uint64_t)idelta;
+        while (delta > 0) {
+            if (delta & 1) { acc_mult *= cur_mult; acc_plus = acc_plus * cur_mult + cur_plus; }
+            cur_plus = (cur_mult + 1) * cur_plus;
+            cur_mult *= cur_mult;
+            delta /= 2;
+        }
+        state = acc_mult * state + acc_plus;
+    }
+};
+
+// ---------------------------------------------------------------- geometry
+struct V3 { float x, y, z; };
+static inline float comp(const V3& v, int i) { return i == 0 ? v.x : (i == 1 ? v.y : v.z); }
+static inline V3 sub(const V3& a, const V3& b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+// Vector3::cross evaluates in f64 and rounds to f32 (geometry/vector3.rs:67-82)
+static inline V3 cross64(const V3& a, const V3& b) {
+    double ax = a.x, ay = a.y, az = a.z, bx = b.x, by = b.y, bz = b.z;
+    return {(float)((ay * bz) - (az * by)), (float)((az * bx) - (ax * bz)),
+            (float)((ax * by) - (ay * bx))};
+}
+// Vector3::length_squared (vector3.rs:43-48)
+static inline float length_sq(const V3& v) { return v.x * v.x + v.y * v.y + v.z * v.z; }
+
+// Bounds3<f32> with Default min=MAX, max=MIN (geometry/bounds3.rs:357-368)
+struct B3 {
+    V3 mn{std::numeric_limits<float>::max(), std::numeric_limits<float>::max(),
+          std::numeric_limits<float>::max()};
+    V3 mx{-std::numeric_limits<float>::max(), -std::numeric_limits<float>::max(),
+          -std::numeric_limits<float>::max()};
+};
+// Point3::min / max (geometry/point3.rs:70-92)
+static inline V3 pmin(const V3& a, const V3& b) {
+    return {a.x < b.x ? a.x : b.x, a.y < b.y ? a.y : b.y, a.z < b.z ? a.z : b.z};
+}
+static inline V3 pmax(const V3& a, const V3& b) {
+    return {a.x > b.x ? a.x : b.x, a.y > b.y ? a.y : b.y, a.z > b.z ? a.z : b.z};
+}
+// Bounding3::union (bounds3.rs:37-47)
+static inline B3 bunion(const B3& a, const B3& b) { B3 r; r.mn = pmin(a.mn, b.mn); r.mx = pmax(a.mx, b.mx); return r; }
+static inline B3 bunion_pt(const B3& a, const V3& p) { B3 r; r.mn = pmin(a.mn, p); r.mx = pmax(a.mx, p); return r; }
+// Bounding3::maximum_extent (bounds3.rs:53-56)
+static inline int maximum_extent(const B3& b) {
+    V3 d = sub(b.mx, b.mn);
+    if (d.x > d.y && d.x > d.z) return 0;
+    if (d.y > d.z) return 1;
+    return 2;
+}
+// Bounding3::surface_area (bounds3.rs:59-62)
+static inline float surface_area(const B3& b) {
+    V3 d = sub(b.mx, b.mn);
+    return 2.0f * (d.x * d.y + d.x * d.z + d.y * d.z);
+}
+// Bounds3::centroid (bounds3.rs:238-242)
+static inline V3 centroid(const B3& b) {
+    return {b.mn.x * 0.5f + b.mx.x * 0.5f, b.mn.y * 0.5f + b.mx.y * 0.5f, b.mn.z * 0.5f + b.mx.z * 0.5f};
+}
+// Bounds3::offset (bounds3.rs:178-193)
+static inline V3 offset(const B3& b, const V3& p) {
+    V3 o = sub(p, b.mn);
+    if (b.mx.x > b.mn.x) o.x /= b.mx.x - b.mn.x;
+    if (b.mx.y > b.mn.y) o.y /= b.mx.y - b.mn.y;
+    if (b.mx.z > b.mn.z) o.z /= b.mx.z - b.mn.z;
+    return o;
+}
+
+struct Ray { V3 o, d; float t_max; };
+
+// Bounding3::intersect_p with precomputed inv_dir (bounds3.rs:284-318)
+static inline bool box_intersect_p(const orc_bvh_node& n, const Ray& ray, const V3& inv_dir,
+                                   const int dir_is_neg[3]) {
+    const float* mm[2] = {n.bmin, n.bmax};
+    const float robust = 1.0f + 2.0f * gamma(3);
+    float t_min = (mm[dir_is_neg[0]][0] - ray.o.x) * inv_dir.x;
+    float t_max = (mm[1 - dir_is_neg[0]][0] - ray.o.x) * inv_dir.x;
+    float ty_min = (mm[dir_is_neg[1]][1] - ray.o.y) * inv_dir.y;
+    float ty_max = (mm[1 - dir_is_neg[1]][1] - ray.o.y) * inv_dir.y;
+    t_max *= robust;
+    ty_max *= robust;
+    if (t_min > ty_max || ty_min > t_max) return false;
+    if (ty_min > t_min) t_min = ty_min;
+    if (ty_max < t_max) t_max = ty_max;
+    float tz_min = (mm[dir_is_neg[2]][2] - ray.o.z) * inv_dir.z;
+    float tz_max = (mm[1 - dir_is_neg[2]][2] - ray.o.z) * inv_dir.z;
+    tz_max *= robust;
+    if (t_min > tz_max || tz_min > t_max) return false;
+    if (tz_min > t_min) t_min = tz_min;
+    if (tz_max < t_max) t_max = tz_max;
+    return (t_min < ray.t_max) && (t_max > 0.0f);
+}
+
+// ---------------------------------------------------------------- triangle.rs
+// Watertight ray-triangle test, Triangle::intersect (triangle.rs:142-262,
+// 281-289) and Triangle::intersect_p (triangle.rs:421-541).  `closest`
+// selects intersect(), which additionally rejects triangles whose geometric
+// normal (p2-p0)x(p1-p0) has zero squared length (triangle.rs:281-289; D14
+// makes the uv-determinant branch unreachable, so this is the check that
+// runs).  D11 (3-element permute) and D12 (true max_component) repaired.
+static bool triangle_test(const V3& p0, const V3& p1, const V3& p2, const Ray& ray,
+                          bool closest, float* t_out, float* b_out) {
+    // translate (157-159)
+    V3 p0t = sub(p0, ray.o), p1t = sub(p1, ray.o), p2t = sub(p2, ray.o);
+    // permute (162-174); max_dimension (vector3.rs:140-150)
+    V3 ad{std::fabs(ray.d.x), std::fabs(ray.d.y), std::fabs(ray.d.z)};
+    int kz = (ad.x > ad.y) ? (ad.x > ad.z ? 0 : 2) : (ad.y > ad.z ? 1 : 2);
+    int kx = kz + 1; if (kx == 3) kx = 0;
+    int ky = kx + 1; if (ky == 3) ky = 0;
+    V3 d{comp(ray.d, kx), comp(ray.d, ky), comp(ray.d, kz)};
+    p0t = {comp(p0t, kx), comp(p0t, ky), comp(p0t, kz)};
+    p1t = {comp(p1t, kx), comp(p1t, ky), comp(p1t, kz)};
+    p2t = {comp(p2t, kx), comp(p2t, ky), comp(p2t, kz)};
+    // shear (177-185)
+    float sx = -d.x / d.z, sy = -d.y / d.z, sz = 1.0f / d.z;
+    p0t.x += sx * p0t.z; p0t.y += sy * p0t.z;
+    p1t.x += sx * p1t.z; p1t.y += sy * p1t.z;
+    p2t.x += sx * p2t.z; p2t.y += sy * p2t.z;
+    // edge functions (188-190)
+    float e0 = p1t.x * p2t.y - p1t.y * p2t.x;
+    float e1 = p2t.x * p0t.y - p2t.y * p0t.x;
+    float e2 = p0t.x * p1t.y - p0t.y * p1t.x;
+    // f64 fallback at edges (193-204)
+    if (e0 == 0.0f || e1 == 0.0f || e2 == 0.0f) {
+        double p2txp1ty = (double)p2t.x * (double)p1t.y;
+        double p2typ1tx = (double)p2t.y * (double)p1t.x;
+        e0 = (float)(p2typ1tx - p2txp1ty);
+        double p0txp2ty = (double)p0t.x * (double)p2t.y;
+        double p0typ2tx = (double)p0t.y * (double)p2t.x;
+        e1 = (float)(p0typ2tx - p0txp2ty);
+        double p1txp0ty = (double)p1t.x * (double)p0t.y;
+        double p1typ0tx = (double)p1t.y * (double)p0t.x;
+        e2 = (float)(p1typ0tx - p1txp0ty);
+    }
+    // edge and determinant tests (207-215)
+    if ((e0 < 0.0f || e1 < 0.0f || e2 < 0.0f) && (e0 > 0.0f || e1 > 0.0f || e2 > 0.0f)) return false;
+    float det = e0 + e1 + e2;
+    if (det == 0.0f) return false;
+    // scaled hit distance and range test (218-229)
+    p0t.z *= sz; p1t.z *= sz; p2t.z *= sz;
+    float t_scaled = e0 * p0t.z + e1 * p1t.z + e2 * p2t.z;
+    if (det < 0.0f && (t_scaled >= 0.0f || t_scaled < ray.t_max * det)) return false;
+    else if (det > 0.0f && (t_scaled <= 0.0f || t_scaled > ray.t_max * det)) return false;
+    // barycentrics and t (232-236)
+    float inv_det = 1.0f / det;
+    float b0 = e0 * inv_det, b1 = e1 * inv_det, b2 = e2 * inv_det;
+    float t = t_scaled * inv_det;
+    // conservative t > 0 (241-262), max_component repaired (D12)
+    auto max3 = [](float a, float b, float c) { float m = a > b ? a : b; return m > c ? m : c; };
+    float max_zt = max3(std::fabs(p0t.z), std::fabs(p1t.z), std::fabs(p2t.z));
+    float delta_z = gamma(3) * max_zt;
+    float max_xt = max3(std::fabs(p0t.x), std::fabs(p1t.x), std::fabs(p2t.x));
+    float max_yt = max3(std::fabs(p0t.y), std::fabs(p1t.y), std::fabs(p2t.y));
+    float delta_x = gamma(5) * (max_xt + max_zt);
+    float delta_y = gamma(5) * (max_yt + max_zt);
+    float delta_e = 2.0f * (gamma(2) * max_xt * max_yt + delta_y * max_xt + delta_x * max_yt);
+    float max_e = max3(std::fabs(e0), std::fabs(e1), std::fabs(e2));
+    float delta_t = 3.0f * (gamma(3) * max_e * max_zt + delta_e * max_zt + delta_z * max_e) *
+                    std::fabs(inv_det);
+    if (t <= delta_t) return false;
+    if (closest) {
+        // degenerate-triangle rejection (281-289)
+        V3 ng = cross64(sub(p2, p0), sub(p1, p0));
+        if (length_sq(ng) == 0.0f) return false;
+    }
+    *t_out = t;
+    b_out[0] = b0; b_out[1] = b1; b_out[2] = b2;
+    return true;
+}
+
+// ---------------------------------------------------------------- efloat.rs
+// EFloat interval arithmetic (core/efloat.rs:5-257).  D23: the scalar
+// operators (Add/Sub/Mul/Div<f32>, Mul<EFloat> for f32, efloat.rs:123-195)
+// build EFloat::new(rhs, rhs), i.e. an error equal to the value itself, which
+// turns `* -0.5` into an interval with low > high and trips check(); repaired
+// to an exact constant EFloat::new(rhs, 0.0) as pbrt-v3 does.
+struct EF {
+    float v, low, high;
+};
+static inline EF ef_new(float v, float err) {        // efloat.rs:12-29
+    if (err == 0.0f) return {v, v, v};
+    return {v, next_float_down(v - err), next_float_up(v + err)};
+}
+static inline EF ef_add(EF a, EF b) {                 // efloat.rs:108-118
+    return {a.v + b.v, next_float_down(a.low + b.low), next_float_up(a.high + b.high)};
+}
+static inline EF ef_sub(EF a, EF b) {                 // efloat.rs:127-137
+    return {a.v - b.v, next_float_down(a.low - b.low), next_float_up(a.high - b.high)};
+}
+static inline EF ef_mul(EF a, EF b) {                 // efloat.rs:146-162
+    float p0 = a.low * b.low, p1 = a.high * b.low, p2 = a.low * b.high, p3 = a.high * b.high;
+    float lo = std::fmin(std::fmin(std::fmin(p0, p1), p2), p3);
+    float hi = std::fmax(std::fmax(std::fmax(p0, p1), p2), p3);
+    return {a.v * b.v, next_float_down(lo), next_float_up(hi)};
+}
+static inline EF ef_div(EF a, EF b) {                 // efloat.rs:180-205
+    if (b.low < 0.0f && b.high > 0.0f)
+        return {a.v / b.v, -std::numeric_limits<float>::infinity(), std::numeric_limits<float>::infinity()};
+    float d0 = a.low / b.low, d1 = a.high / b.low, d2 = a.low / b.high, d3 = a.high / b.high;
+    float lo = std::fmin(std::fmin(std::fmin(d0, d1), d2), d3);
+    float hi = std::fmax(std::fmax(std::fmax(d0, d1), d2), d3);
+    return {a.v / b.v, next_float_down(lo), next_float_up(hi)};
+}
+// quadratic (efloat.rs:232-257)
+static bool ef_quadratic(EF a, EF b, EF c, EF* t0, EF* t1) {
+    double discrim = (double)b.v * (double)b.v - 4.0 * (double)a.v * (double)c.v;
+    if (discrim < 0.0) return false;
+    double root = std::sqrt(discrim);
+    EF froot = ef_new((float)root, kMachineEps * (float)root);
+    EF q = (b.v < 0.0f) ? ef_mul(ef_sub(b, froot), ef_new(-0.5f, 0.0f))
+                        : ef_mul(ef_add(b, froot), ef_new(-0.5f, 0.0f));
+    *t0 = ef_div(q, a);
+    *t1 = ef_div(c, q);
+    if (t0->v > t1->v) { EF s = *t0; *t0 = *t1; *t1 = s; }
+    return true;
+}
+
+// ---------------------------------------------------------------- sphere.rs
+struct Sphere {
+    float m[16], mi[16];   // object_to_world, world_to_object (row-major)
+    float radius, z_min, z_max, theta_min, theta_max, phi_max;
+    bool reverse;
+};
+// Sphere::new (sphere.rs:50-75; D22: made public)
+static Sphere sphere_new(const orc_sphere_desc& d) {
+    Sphere s;
+    std::memcpy(s.m, d.object_to_world, sizeof s.m);
+    std::memcpy(s.mi, d.world_to_object, sizeof s.mi);
+    float mn = std::fmin(d.z_min, d.z_max), mx = std::fmax(d.z_min, d.z_max);
+    auto clamp = [](float v, float lo, float hi) { return v < lo ? lo : (v > hi ? hi : v); };
+    s.radius = d.radius;
+    s.z_min = clamp(mn, -d.radius, d.radius);
+    s.z_max = clamp(mx, -d.radius, d.radius);
+    s.theta_min = std::acos(clamp(mn / d.radius, -1.0f, 1.0f));
+    s.theta_max = std::acos(clamp(mx / d.radius, -1.0f, 1.0f));
+    // radians(): FRAC_PI_180 * deg (pbrt.rs:51-53)
+    s.phi_max = (kPi / 180.0f) * clamp(d.phi_max_deg, 0.0f, 360.0f);
+    s.reverse = d.reverse_orientation != 0;
+    return s;
+}
+// Transform::transform_bounds -> Bounds3::transform (bounds3.rs:320-356)
+static B3 sphere_world_bound(const Sphere& s) {
+    B3 ob;
+    ob.mn = {-s.radius, -s.radius, s.z_min};
+    ob.mx = {s.radius, s.radius, s.z_max};
+    float bmin[3] = {s.m[3], s.m[7], s.m[11]}, bmax[3] = {s.m[3], s.m[7], s.m[11]};
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) {
+            float a = s.m[4 * i + j] * comp(ob.mn, j);
+            float b = s.m[4 * i + j] * comp(ob.mx, j);
+            if (a < b) { bmin[i] += a; bmax[i] += b; } else { bmin[i] += b; bmax[i] += a; }
+        }
+    B3 r;
+    r.mn = {bmin[0], bmin[1], bmin[2]};
+    r.mx = {bmax[0], bmax[1], bmax[2]};
+    return r;
+}
+// Transform::transform_ray_with_error (transform.rs:392-435), using
+// transform_point_with_error (224-247) and transform_vector_with_error (296-309).
+static void transform_ray_with_error(const float* m, const Ray& r, V3* o, V3* d, V3* oe, V3* de) {
+    float x = r.o.x, y = r.o.y, z = r.o.z;
+    float xp = (m[0] * x + m[1] * y) + (m[2] * z + m[3]);
+    float yp = (m[4] * x + m[5] * y) + (m[6] * z + m[7]);
+    float zp = (m[8] * x + m[9] * y) + (m[10] * z + m[11]);
+    float wp = (m[12] * x + m[13] * y) + (m[14] * z + m[15]);
+    float xs = std::fabs(m[0] * x) + std::fabs(m[1] * y) + std::fabs(m[2] * z) + std::fabs(m[3]);
+    float ys = std::fabs(m[4] * x) + std::fabs(m[5] * y) + std::fabs(m[6] * z) + std::fabs(m[7]);
+    float zs = std::fabs(m[8] * x) + std::fabs(m[9] * y) + std::fabs(m[10] * z) + std::fabs(m[11]);
+    float g3 = gamma(3);
+    *oe = {xs * g3, ys * g3, zs * g3};
+    if (wp == 1.0f) *o = {xp, yp, zp}; else *o = {xp / wp, yp / wp, zp / wp};
+    x = r.d.x; y = r.d.y; z = r.d.z;
+    de->x = g3 * (std::fabs(m[0] * x) + std::fabs(m[1] * y) + std::fabs(m[2] * z));
+    de->y = g3 * (std::fabs(m[4] * x) + std::fabs(m[5] * y) + std::fabs(m[6] * z));
+    de->z = g3 * (std::fabs(m[8] * x) + std::fabs(m[9] * y) + std::fabs(m[10] * z));
+    *d = {m[0] * x + m[1] * y + m[2] * z, m[4] * x + m[5] * y + m[6] * z, m[8] * x + m[9] * y + m[10] * z};
+    float ls = length_sq(*d);
+    if (ls > 0.0f) {
+        float dt = (std::fabs(d->x) * oe->x + std::fabs(d->y) * oe->y + std::fabs(d->z) * oe->z) / ls;
+        o->x += d->x * dt; o->y += d->y * dt; o->z += d->z * dt;
+    }
+}
+// Sphere::intersect / intersect_p (sphere.rs:105-188 and 238-323).  D24:
+// Point3::distance (point3.rs:62-66) returns sqrt(p.o) instead of |p-o|, so
+// the refine step would divide by zero; repaired to the Euclidean distance.
+static bool sphere_test(const Sphere& s, const Ray& world_ray, float* t_out, float* uv_out) {
+    V3 o, d, oe, de;
+    transform_ray_with_error(s.mi, world_ray, &o, &d, &oe, &de);
+    float t_max = world_ray.t_max;
+    EF ox = ef_new(o.x, oe.x), oy = ef_new(o.y, oe.y), oz = ef_new(o.z, oe.z);
+    EF dx = ef_new(d.x, de.x), dy = ef_new(d.y, de.y), dz = ef_new(d.z, de.z);
+    EF a = ef_add(ef_add(ef_mul(dx, dx), ef_mul(dy, dy)), ef_mul(dz, dz));
+    EF b = ef_mul(ef_add(ef_add(ef_mul(dx, ox), ef_mul(dy, oy)), ef_mul(dz, oz)), ef_new(2.0f, 0.0f));
+    EF rr = ef_new(s.radius, 0.0f);
+    EF c = ef_sub(ef_add(ef_add(ef_mul(ox, ox), ef_mul(oy, oy)), ef_mul(oz, oz)), ef_mul(rr, rr));
+    EF t0, t1;
+    if (!ef_quadratic(a, b, c, &t0, &t1)) return false;
+    if (t0.high > t_max || t1.low <= 0.0f) return false;
+    EF th = t0;
+    if (th.low <= 0.0f) {
+        th = t1;
+        if (th.high > t_max) return false;
+    }
+    auto hit_point = [&](float t, V3* p, float* phi) {
+        *p = {o.x + d.x * t, o.y + d.y * t, o.z + d.z * t};
+        float dist = std::sqrt(p->x * p->x + p->y * p->y + p->z * p->z);  // D24
+        float k = s.radius / dist;
+        p->x *= k; p->y *= k; p->z *= k;
+        if (p->x == 0.0f && p->y == 0.0f) p->x = 1e-5f * s.radius;
+        *phi = std::atan2(p->y, p->x);
+        if (*phi < 0.0f) *phi += 2.0f * kPi;
+    };
+    V3 p; float phi;
+    hit_point(th.v, &p, &phi);
+    auto clipped = [&](const V3& q, float ph) {
+        return (s.z_min > -s.radius && q.z < s.z_min) || (s.z_max < s.radius && q.z > s.z_max) ||
+               ph > s.phi_max;
+    };
+    if (clipped(p, phi)) {
+        if (th.v == t1.v) return false;
+        if (t1.high > t_max) return false;
+        th = t1;
+        hit_point(th.v, &p, &phi);
+        if (clipped(p, phi)) return false;
+    }
+    // parametric (u, v) (sphere.rs:191-193)
+    float u = phi / s.phi_max;
+    float zr = p.z / s.radius;
+    zr = zr < -1.0f ? -1.0f : (zr > 1.0f ? 1.0f : zr);
+    float theta = std::acos(zr);
+    float v = (theta - s.theta_min) / (s.theta_max - s.theta_min);
+    *t_out = th.v;
+    uv_out[0] = u; uv_out[1] = v;
+    return true;
+}
+
+// ---------------------------------------------------------------- bvh.rs
+struct PrimInfo { uint32_t prim; B3 bounds; V3 centroid; };
+struct BuildNode {
+    B3 bounds;
+    int child[2] = {-1, -1};
+    int split_axis = 0;
+    uint32_t first_prim_offset = 0, n_primitives = 0;
+};
+struct BucketInfo { uint32_t count = 0; B3 bounds; };
+
+struct Builder {
+    int max_prims;
+    std::vector<PrimInfo>& info;
+    std::vector<BuildNode> nodes;
+    std::vector<uint32_t> ordered;
+    Builder(int mp, std::vector<PrimInfo>& pi) : max_prims(mp), info(pi) {}
+
+    int make_leaf(uint32_t start, uint32_t end, const B3& bounds) {
+        BuildNode n;
+        n.first_prim_offset = (uint32_t)ordered.size();
+        for (uint32_t i = start; i < end; ++i) ordered.push_back(info[i].prim);
+        n.n_primitives = end - start;
+        n.bounds = bounds;
+        nodes.push_back(n);
+        return (int)nodes.size() - 1;
+    }
+    // SAH bucket of a centroid; D2 (bvh.rs:176,219): cast after multiplying.
+    static int bucket_of(const B3& cb, const V3& c, int dim) {
+        int b = (int)(12.0f * comp(offset(cb, c), dim));
+        if (b == 12) b = 11;
+        return b;
+    }
+    // recursive_build (bvh.rs:95-247), SAH path; D1 (centroid bounds are a
+    // union of centroids), D2, D3 (argmin, first minimum wins) repaired; D7
+    // (leaf on zero centroid extent) and D8 (split criterion) kept.
+    int build(uint32_t start, uint32_t end) {
+        B3 bounds;
+        for (uint32_t i = start; i < end; ++i) bounds = bunion(bounds, info[i].bounds);
+        uint32_t n = end - start;
+        if (n == 1) return make_leaf(start, end, bounds);
+        B3 cb;
+        for (uint32_t i = start; i < end; ++i) cb = bunion_pt(cb, info[i].centroid);
+        int dim = maximum_extent(cb);
+        uint32_t mid = (start + end) / 2;
+        if (comp(cb.mx, dim) == comp(cb.mn, dim)) return make_leaf(start, end, bounds);
+        if (n <= 2) {
+            // partial_sort(mid) of two elements (slice_extension.rs:45-72): one
+            // pivot pass that swaps iff c[1] < c[0].
+            if (comp(info[start + 1].centroid, dim) < comp(info[start].centroid, dim))
+                std::swap(info[start], info[start + 1]);
+        } else {
+            BucketInfo buckets[12];
+            for (uint32_t i = start; i < end; ++i) {
+                int b = bucket_of(cb, info[i].centroid, dim);
+                buckets[b].count += 1;
+                buckets[b].bounds = bunion(buckets[b].bounds, info[i].bounds);
+            }
+            float cost[11];
+            for (int i = 0; i < 11; ++i) {
+                B3 b0, b1;
+                uint32_t c0 = 0, c1 = 0;
+                for (int j = 0; j <= i; ++j) { b0 = bunion(b0, buckets[j].bounds); c0 += buckets[j].count; }
+                for (int j = i + 1; j < 12; ++j) { b1 = bunion(b1, buckets[j].bounds); c1 += buckets[j].count; }
+                cost[i] = 1.0f + ((float)c0 * surface_area(b0) + (float)c1 * surface_area(b1)) /
+                                     surface_area(bounds);
+            }
+            float min_cost = cost[0];
+            int split = 0;
+            for (int i = 1; i < 11; ++i)
+                if (cost[i] < min_cost) { min_cost = cost[i]; split = i; }
+            float leaf_cost = (float)n;
+            if (n > (uint32_t)max_prims || min_cost < leaf_cost) {
+                // SliceExtension::partition (slice_extension.rs:20-43)
+                uint32_t first = end;
+                for (uint32_t i = start; i < end; ++i)
+                    if (!(bucket_of(cb, info[i].centroid, dim) <= split)) { first = i; break; }
+                if (first != end) {
+                    for (uint32_t i = first; i < end; ++i)
+                        if (bucket_of(cb, info[i].centroid, dim) <= split) { std::swap(info[i], info[first]); ++first; }
+                }
+                mid = first;
+            } else {
+                return make_leaf(start, end, bounds);
+            }
+        }
+        int self = (int)nodes.size();
+        nodes.push_back(BuildNode());
+        int c0 = build(start, mid);
+        int c1 = build(mid, end);
+        // init_interior (bvh.rs:707-719)
+        nodes[self].bounds = bunion(nodes[c0].bounds, nodes[c1].bounds);
+        nodes[self].split_axis = dim;
+        nodes[self].child[0] = c0;
+        nodes[self].child[1] = c1;
+        nodes[self].n_primitives = 0;
+        return self;
+    }
+};
+
+// flatten_bvh_tree (bvh.rs:504-537): depth-first, first child adjacent.
+static uint32_t flatten(const std::vector<BuildNode>& bn, int node, std::vector<orc_bvh_node>& out, uint32_t* offset) {
+    uint32_t my = (*offset)++;
+    const BuildNode& b = bn[node];
+    orc_bvh_node ln;
+    std::memset(&ln, 0, sizeof ln);
+    ln.bmin[0] = b.bounds.mn.x; ln.bmin[1] = b.bounds.mn.y; ln.bmin[2] = b.bounds.mn.z;
+    ln.bmax[0] = b.bounds.mx.x; ln.bmax[1] = b.bounds.mx.y; ln.bmax[2] = b.bounds.mx.z;
+    if (b.n_primitives > 0) {
+        ln.offset = (int32_t)b.first_prim_offset;
+        ln.n_prims = (uint16_t)b.n_primitives;
+        out[my] = ln;
+    } else {
+        flatten(bn, b.child[0], out, offset);
+        ln.offset = (int32_t)flatten(bn, b.child[1], out, offset);
+        ln.axis = (uint8_t)b.split_axis;
+        out[my] = ln;
+    }
+    return my;
+}
+
+struct Scene {
+    std::vector<V3> verts;
+    std::vector<uint32_t> idx;
+    uint32_t nt = 0;
+    std::vector<Sphere> spheres;
+    std::vector<orc_bvh_node> nodes;
+    std::vector<uint32_t> prims;      // ordered primitive ids
+    double build_seconds = 0;
+};
+
+static B3 tri_bound(const Scene& s, uint32_t t) {
+    // Triangle::world_bound (triangle.rs:126-132)
+    const V3& p0 = s.verts[s.idx[3 * t]];
+    const V3& p1 = s.verts[s.idx[3 * t + 1]];
+    const V3& p2 = s.verts[s.idx[3 * t + 2]];
+    B3 b;
+    b.mn = pmin(p0, p1);
+    b.mx = pmax(p0, p1);
+    return bunion_pt(b, p2);
+}
+
+// Test one primitive; returns hit and fills t / uv (u=b1, v=b2 for triangles).
+static bool prim_test(const Scene& s, uint32_t prim, const Ray& ray, bool closest, float* t, float* uv) {
+    if (prim < s.nt) {
+        float b[3];
+        bool h = triangle_test(s.verts[s.idx[3 * prim]], s.verts[s.idx[3 * prim + 1]],
+                               s.verts[s.idx[3 * prim + 2]], ray, closest, t, b);
+        if (h) { uv[0] = b[1]; uv[1] = b[2]; }
+        return h;
+    }
+    return sphere_test(s.spheres[prim - s.nt], ray, t, uv);
+}
+
+// BVHAccel::intersect (bvh.rs:563-612).  D4: the far child is pushed in both
+// branches.  D5: the traversal owns a mutable t_max that every primitive test
+// sees and that shrinks on each accepted hit.  Ties: a hit is accepted when
+// t < best or (t == best and its primitive id is smaller), so the result does
+// not depend on visit order except for near-ties.
+static int trace_closest(const Scene& s, const orc_ray& r, orc_hit* hit, uint32_t* nv, uint32_t* nt) {
+    hit->prim = 0xFFFFFFFFu; hit->t = r.tmax; hit->u = 0; hit->v = 0;
+    uint32_t visits = 0, tests = 0;
+    int overflow = 0;
+    if (!s.nodes.empty()) {
+        Ray ray{{r.o[0], r.o[1], r.o[2]}, {r.d[0], r.d[1], r.d[2]}, r.tmax};
+        V3 inv{1.0f / ray.d.x, 1.0f / ray.d.y, 1.0f / ray.d.z};
+        int neg[3] = {inv.x < 0.0f, inv.y < 0.0f, inv.z < 0.0f};
+        uint32_t stack[64];
+        int sp = 0;
+        uint32_t cur = 0;
+        for (;;) {
+            const orc_bvh_node& n = s.nodes[cur];
+            ++visits;
+            if (box_intersect_p(n, ray, inv, neg)) {
+                if (n.n_prims > 0) {
+                    for (uint32_t i = 0; i < n.n_prims; ++i) {
+                        uint32_t prim = s.prims[n.offset + i];
+                        float t, uv[2];
+                        ++tests;
+                        if (prim_test(s, prim, ray, true, &t, uv) &&
+                            (t < ray.t_max || (t == ray.t_max && prim < hit->prim))) {
+                            ray.t_max = t;
+                            hit->prim = prim; hit->t = t; hit->u = uv[0]; hit->v = uv[1];
+                        }
+                    }
+                    if (sp == 0) break;
+                    cur = stack[--sp];
+                } else {
+                    if (sp == 64) { overflow = 1; break; }
+                    if (neg[n.axis]) { stack[sp++] = cur + 1; cur = (uint32_t)n.offset; }
+                    else { stack[sp++] = (uint32_t)n.offset; cur = cur + 1; }
+                }
+            } else {
+                if (sp == 0) break;
+                cur = stack[--sp];
+            }
+        }
+    }
+    if (hit->prim == 0xFFFFFFFFu) hit->t = r.tmax;
+    if (nv) *nv = visits;
+    if (nt) *nt = tests;
+    return overflow;
+}
+
+// BVHAccel::intersect_p (bvh.rs:614-662), D4 repaired.
+static int trace_any(const Scene& s, const orc_ray& r, uint8_t* occ, uint32_t* nv, uint32_t* nt) {
+    uint32_t visits = 0, tests = 0;
+    int overflow = 0;
+    *occ = 0;
+    if (!s.nodes.empty()) {
+        Ray ray{{r.o[0], r.o[1], r.o[2]}, {r.d[0], r.d[1], r.d[2]}, r.tmax};
+        V3 inv{1.0f / ray.d.x, 1.0f / ray.d.y, 1.0f / ray.d.z};
+        int neg[3] = {inv.x < 0.0f, inv.y < 0.0f, inv.z < 0.0f};
+        uint32_t stack[64];
+        int sp = 0;
+        uint32_t cur = 0;
+        for (;;) {
+            const orc_bvh_node& n = s.nodes[cur];
+            ++visits;
+            if (box_intersect_p(n, ray, inv, neg)) {
+                if (n.n_prims > 0) {
+                    bool found = false;
+                    for (uint32_t i = 0; i < n.n_prims; ++i) {
+                        float t, uv[2];
+                        ++tests;
+                        if (prim_test(s, s.prims[n.offset + i], ray, false, &t, uv)) { found = true; break; }
+                    }
+                    if (found) { *occ = 1; break; }
+                    if (sp == 0) break;
+                    cur = stack[--sp];
+                } else {
+                    if (sp == 64) { overflow = 1; break; }
+                    if (neg[n.axis]) { stack[sp++] = cur + 1; cur = (uint32_t)n.offset; }
+                    else { stack[sp++] = (uint32_t)n.offset; cur = cur + 1; }
+                }
+            } else {
+                if (sp == 0) break;
+                cur = stack[--sp];
+            }
+        }
+    }
+    if (nv) *nv = visits;
+    if (nt) *nt = tests;
+    return overflow;
+}
+
+static double g_last_trace_seconds = 0.0;
+
+template <class F>
+static int64_t parallel_rays(uint64_t n, int nthreads, F&& fn) {
+    if (nthreads <= 0) nthreads = (int)std::thread::hardware_concurrency();
+    if (nthreads <= 0) nthreads = 1;
+    std::atomic<uint64_t> next{0};
+    std::atomic<int64_t> overflow{0};
+    const uint64_t chunk = 256;
+    auto worker = [&]() {
+        int64_t local = 0;
+        for (;;) {
+            uint64_t b = next.fetch_add(chunk);
+            if (b >= n) break;
+            uint64_t e = b + chunk < n ? b + chunk : n;
+            for (uint64_t i = b; i < e; ++i) local += fn(i);
+        }
+        overflow += local;
+    };
+    auto t0 = std::chrono::steady_clock::now();
+    if (nthreads == 1) worker();
+    else {
+        std::vector<std::thread> th;
+        for (int i = 0; i < nthreads; ++i) th.emplace_back(worker);
+        for (auto& t : th) t.join();
+    }
+    g_last_trace_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    return overflow.load();
+}
+
+}  // namespace orc
+
+using namespace orc;
+
+extern "C" {
+
+float orc_gamma(int n) { return gamma(n); }
+float orc_next_float_up(float v) { return next_float_up(v); }
+float orc_next_float_down(float v) { return next_float_down(v); }
+
+void orc_rng_u32(uint64_t seq, uint64_t n, uint32_t* out) {
+    Rng r(seq);
+    for (uint64_t i = 0; i < n; ++i) out[i] = r.uniform_u32();
+}
+void orc_rng_floats(uint64_t seq, uint64_t n, float* out) {
+    Rng r(seq);
+    for (uint64_t i = 0; i < n; ++i) out[i] = r.uniform_float();
+}
+void orc_rng_floats_advanced(uint64_t seq, int64_t delta, uint64_t n, float* out) {
+    Rng r(seq);
+    r.advance(delta);
+    for (uint64_t i = 0; i < n; ++i) out[i] = r.uniform_float();
+}
+
+void* orc_scene_create(const float* verts, uint32_t nv, const uint32_t* idx, uint32_t nt,
+                       const orc_sphere_desc* spheres, uint32_t ns, int max_prims_in_node) {
+    auto t0 = std::chrono::steady_clock::now();
+    Scene* s = new Scene();
+    s->verts.resize(nv);
+    for (uint32_t i = 0; i < nv; ++i) s->verts[i] = {verts[3 * i], verts[3 * i + 1], verts[3 * i + 2]};
+    s->idx.assign(idx, idx + 3 * (size_t)nt);
+    s->nt = nt;
+    for (uint32_t i = 0; i < ns; ++i) s->spheres.push_back(sphere_new(spheres[i]));
+    uint32_t np = nt + ns;
+    if (np > 0) {
+        // BVHPrimitiveInfo per primitive (bvh.rs:50-53, 730-737)
+        std::vector<PrimInfo> info(np);
+        for (uint32_t i = 0; i < np; ++i) {
+            info[i].prim = i;
+            info[i].bounds = (i < nt) ? tri_bound(*s, i) : sphere_world_bound(s->spheres[i - nt]);
+            info[i].centroid = centroid(info[i].bounds);
+        }
+        Builder b(max_prims_in_node, info);
+        b.nodes.reserve(2 * (size_t)np);
+        b.ordered.reserve(np);
+        int root = b.build(0, np);
+        s->nodes.resize(b.nodes.size());
+        uint32_t off = 0;
+        flatten(b.nodes, root, s->nodes, &off);
+        s->prims = std::move(b.ordered);
+    }
+    s->build_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    return s;
+}
+void orc_scene_destroy(void* scene) { delete (Scene*)scene; }
+uint32_t orc_scene_node_count(void* scene) { return (uint32_t)((Scene*)scene)->nodes.size(); }
+void orc_scene_nodes(void* scene, orc_bvh_node* out) {
+    Scene* s = (Scene*)scene;
+    if (!s->nodes.empty()) std::memcpy(out, s->nodes.data(), s->nodes.size() * sizeof(orc_bvh_node));
+}
+void orc_scene_prim_order(void* scene, uint32_t* out) {
+    Scene* s = (Scene*)scene;
+    if (!s->prims.empty()) std::memcpy(out, s->prims.data(), s->prims.size() * 4);
+}
+void orc_scene_world_bound(void* scene, float out[6]) {
+    // BVHAccel::world_bound (bvh.rs:555-561)
+    Scene* s = (Scene*)scene;
+    B3 b;
+    if (!s->nodes.empty()) {
+        b.mn = {s->nodes[0].bmin[0], s->nodes[0].bmin[1], s->nodes[0].bmin[2]};
+        b.mx = {s->nodes[0].bmax[0], s->nodes[0].bmax[1], s->nodes[0].bmax[2]};
+    }
+    out[0] = b.mn.x; out[1] = b.mn.y; out[2] = b.mn.z;
+    out[3] = b.mx.x; out[4] = b.mx.y; out[5] = b.mx.z;
+}
+double orc_scene_build_seconds(void* scene) { return ((Scene*)scene)->build_seconds; }
+
+int64_t orc_intersect(void* scene, const orc_ray* rays, uint64_t n, orc_hit* hits,
+                      uint32_t* node_visits, uint32_t* prim_tests, int nthreads) {
+    const Scene& s = *(Scene*)scene;
+    return parallel_rays(n, nthreads, [&](uint64_t i) {
+        return trace_closest(s, rays[i], &hits[i], node_visits ? &node_visits[i] : nullptr,
+                             prim_tests ? &prim_tests[i] : nullptr);
+    });
+}
+int64_t orc_intersect_p(void* scene, const orc_ray* rays, uint64_t n, uint8_t* occluded,
+                        uint32_t* node_visits, uint32_t* prim_tests, int nthreads) {
+    const Scene& s = *(Scene*)scene;
+    return parallel_rays(n, nthreads, [&](uint64_t i) {
+        return trace_any(s, rays[i], &occluded[i], node_visits ? &node_visits[i] : nullptr,
+                         prim_tests ? &prim_tests[i] : nullptr);
+    });
+}
+
+int orc_triangle_intersect(const float* p0, const float* p1, const float* p2, const orc_ray* r,
+                           int closest, float* out) {
+    Ray ray{{r->o[0], r->o[1], r->o[2]}, {r->d[0], r->d[1], r->d[2]}, r->tmax};
+    float t, b[3];
+    if (!triangle_test({p0[0], p0[1], p0[2]}, {p1[0], p1[1], p1[2]}, {p2[0], p2[1], p2[2]}, ray,
+                       closest != 0, &t, b))
+        return 0;
+    out[0] = t; out[1] = b[0]; out[2] = b[1]; out[3] = b[2];
+    return 1;
+}
+
+int orc_sphere_intersect(const orc_sphere_desc* sd, const orc_ray* r, int closest, float* out) {
+    (void)closest;
+    Sphere s = sphere_new(*sd);
+    Ray ray{{r->o[0], r->o[1], r->o[2]}, {r->d[0], r->d[1], r->d[2]}, r->tmax};
+    float t, uv[2];
+    if (!sphere_test(s, ray, &t, uv)) return 0;
+    out[0] = t; out[1] = uv[0]; out[2] = uv[1];
+    return 1;
+}
+
+void orc_sphere_world_bound(const orc_sphere_desc* sd, float out[6]) {
+    B3 b = sphere_world_bound(sphere_new(*sd));
+    out[0] = b.mn.x; out[1] = b.mn.y; out[2] = b.mn.z;
+    out[3] = b.mx.x; out[4] = b.mx.y; out[5] = b.mx.z;
+}
+
+double orc_last_trace_seconds(void) { return g_last_trace_seconds; }
+
+}  // extern "C"

@@ -1,0 +1,96 @@
+/*
+ * CPU oracle for the ray-query / path-tracing hot path of rs_illume.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This library is a scalar C++ restatement of the
+ * reference's Rust code (rs_illume, a pbrt-v3 port).  It exists so that the
+ * GPU product can be checked against it and so that the CPU baseline can be
+ * timed.  The product library (rs_illume_b200) never links or calls it; only
+ * tests/, __graft_entry__.smoke() and bench.py's CPU legs do.
+ *
+ * Parity status: the reference crate ships no test, golden vector or fixture
+ * for this path and cannot be compiled (no Rust toolchain; the crate itself
+ * has compile errors), so parity with the reference is UNPINNED by the
+ * reference's own tests.  The restatement is pinned instead to analytic
+ * known-answer cases (tests/test_oracle_kat.py) and follows the cited lines.
+ * Where the reference is wrong or does not compile, the repair is applied and
+ * numbered (D1..D24); the product applies the same repairs.
+ */
+#ifndef ILLUME_ORACLE_H
+#define ILLUME_ORACLE_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* 32-byte ray record: origin, t_min (unused, 0), direction, t_max. */
+typedef struct { float o[3]; float tmin; float d[3]; float tmax; } orc_ray;
+/* 16-byte hit record: primitive id (0xFFFFFFFF = miss), t, u (=b1), v (=b2). */
+typedef struct { uint32_t prim; float t; float u; float v; } orc_hit;
+
+/* Sphere shape (shapes/sphere.rs:15-75): object_to_world / world_to_object
+ * are row-major 4x4 (m[i][j] at [4*i+j]). */
+typedef struct {
+    float object_to_world[16];
+    float world_to_object[16];
+    float radius, z_min, z_max, phi_max_deg;
+    int32_t reverse_orientation;
+} orc_sphere_desc;
+
+/* 32-byte flattened BVH node (accelerators/bvh.rs:665-673, 32 B per D6). */
+typedef struct {
+    float bmin[3], bmax[3];
+    int32_t offset;      /* leaf: first primitive; interior: second child */
+    uint16_t n_prims;    /* 0 = interior */
+    uint8_t axis;
+    uint8_t pad;
+} orc_bvh_node;
+
+/* Constants of core/pbrt.rs (gamma(n), SHADOW_EPSILON). */
+float orc_gamma(int n);
+float orc_next_float_up(float v);
+float orc_next_float_down(float v);
+
+/* PCG32 (core/rng.rs:15-63). Writes n draws of Rng::new(seq). */
+void orc_rng_u32(uint64_t seq, uint64_t n, uint32_t* out);
+void orc_rng_floats(uint64_t seq, uint64_t n, float* out);
+/* Rng::new(seq) advanced by delta draws (D18 repaired), then n draws. */
+void orc_rng_floats_advanced(uint64_t seq, int64_t delta, uint64_t n, float* out);
+
+/* Scene = triangles (world-space vertices + 3 indices each) followed by
+ * spheres.  Primitive ids: triangles 0..nt-1, spheres nt..nt+ns-1.
+ * Builds the SAH BVHAccel (bvh.rs:32-93) with max_prims_in_node. */
+void* orc_scene_create(const float* verts, uint32_t nv, const uint32_t* idx,
+                       uint32_t nt, const orc_sphere_desc* spheres, uint32_t ns,
+                       int max_prims_in_node);
+void orc_scene_destroy(void* scene);
+uint32_t orc_scene_node_count(void* scene);
+void orc_scene_nodes(void* scene, orc_bvh_node* out);
+void orc_scene_prim_order(void* scene, uint32_t* out);
+void orc_scene_world_bound(void* scene, float out[6]);
+double orc_scene_build_seconds(void* scene);
+
+/* BVHAccel::intersect over a ray batch (bvh.rs:563-612 with D4/D5).
+ * node_visits / prim_tests may be NULL; otherwise per-ray counters.
+ * Returns number of rays whose 64-entry stack overflowed (0 expected). */
+int64_t orc_intersect(void* scene, const orc_ray* rays, uint64_t n, orc_hit* hits,
+                      uint32_t* node_visits, uint32_t* prim_tests, int nthreads);
+/* BVHAccel::intersect_p (bvh.rs:614-662 with D4). */
+int64_t orc_intersect_p(void* scene, const orc_ray* rays, uint64_t n, uint8_t* occluded,
+                        uint32_t* node_visits, uint32_t* prim_tests, int nthreads);
+
+/* Single-shape tests for known-answer checks.  out = {t, b0, b1, b2}. */
+int orc_triangle_intersect(const float* p0, const float* p1, const float* p2,
+                           const orc_ray* r, int closest, float* out);
+/* out = {t, u, v}. */
+int orc_sphere_intersect(const orc_sphere_desc* s, const orc_ray* r, int closest, float* out);
+void orc_sphere_world_bound(const orc_sphere_desc* s, float out[6]);
+
+/* Wall-clock seconds spent by the last orc_intersect/_p call (traversal only). */
+double orc_last_trace_seconds(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

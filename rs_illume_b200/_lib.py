@@ -1,0 +1,145 @@
+"""ctypes binding of libillume_gpu.so (include/illume_gpu.h, include/illume_workloads.h).
+
+The shared library is built in-tree by ``rs_illume_b200/csrc/Makefile``.  There
+is no fallback: if the library is missing or cannot run on the device, every
+GPU entry point raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libillume_gpu.so")
+
+ILM_OK = 0
+ILM_ERR_INVALID_ARGUMENT = -1
+ILM_ERR_OUT_OF_MEMORY = -2
+ILM_ERR_CUDA = -3
+ILM_ERR_TRAVERSAL_LIMIT = -4
+ILM_ERR_TIMEOUT = -5
+ILM_ERR_NOT_FOUND = -6
+ILM_ERR_NO_DEVICE = -7
+ILM_MISS = 0xFFFFFFFF
+ILM_TRAVERSAL_ERROR = 0xFFFFFFFE
+
+STATUS_NAMES = {
+    ILM_OK: "ILM_OK",
+    ILM_ERR_INVALID_ARGUMENT: "ILM_ERR_INVALID_ARGUMENT",
+    ILM_ERR_OUT_OF_MEMORY: "ILM_ERR_OUT_OF_MEMORY",
+    ILM_ERR_CUDA: "ILM_ERR_CUDA",
+    ILM_ERR_TRAVERSAL_LIMIT: "ILM_ERR_TRAVERSAL_LIMIT",
+    ILM_ERR_TIMEOUT: "ILM_ERR_TIMEOUT",
+    ILM_ERR_NOT_FOUND: "ILM_ERR_NOT_FOUND",
+    ILM_ERR_NO_DEVICE: "ILM_ERR_NO_DEVICE",
+}
+
+# numpy views of the C records
+RAY_DTYPE = np.dtype([("o", "<f4", (3,)), ("tmin", "<f4"), ("d", "<f4", (3,)), ("tmax", "<f4")])
+HIT_DTYPE = np.dtype([("prim", "<u4"), ("t", "<f4"), ("u", "<f4"), ("v", "<f4")])
+BIN_NODE_DTYPE = np.dtype([("bmin", "<f4", (3,)), ("bmax", "<f4", (3,)), ("offset", "<i4"),
+                           ("n_prims", "<u2"), ("axis", "u1"), ("pad", "u1")])
+PRIM_REC_DTYPE = np.dtype([("p0", "<f4", (3,)), ("prim", "<u4"), ("p1", "<f4", (3,)), ("flags", "<u4"),
+                           ("p2", "<f4", (3,)), ("aux", "<u4")])
+assert RAY_DTYPE.itemsize == 32 and HIT_DTYPE.itemsize == 16
+assert BIN_NODE_DTYPE.itemsize == 32 and PRIM_REC_DTYPE.itemsize == 48
+
+
+class ilm_config(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int32), ("stack_depth", ctypes.c_int32),
+                ("block_size", ctypes.c_int32), ("flags", ctypes.c_int32), ("max_iterations", ctypes.c_uint32)]
+
+
+class ilm_build_opts(ctypes.Structure):
+    _fields_ = [("width", ctypes.c_int32), ("max_prims_in_node", ctypes.c_int32)]
+
+
+class ilm_accel_info(ctypes.Structure):
+    _fields_ = [("n_prims", ctypes.c_uint32), ("n_binary_nodes", ctypes.c_uint32),
+                ("n_nodes", ctypes.c_uint32), ("width", ctypes.c_uint32),
+                ("device_bytes", ctypes.c_uint64), ("build_seconds", ctypes.c_double)]
+
+
+class ilm_sphere_desc(ctypes.Structure):
+    _fields_ = [("object_to_world", ctypes.c_float * 16), ("world_to_object", ctypes.c_float * 16),
+                ("radius", ctypes.c_float), ("z_min", ctypes.c_float), ("z_max", ctypes.c_float),
+                ("phi_max_deg", ctypes.c_float), ("reverse_orientation", ctypes.c_int32)]
+
+
+_P = ctypes.c_void_p
+_U32 = ctypes.c_uint32
+_U64 = ctypes.c_uint64
+_I32 = ctypes.c_int32
+_F = ctypes.c_float
+
+# name -> (restype, argtypes)
+SIGNATURES = {
+    "ilm_context_create": (_I32, [ctypes.POINTER(_P), ctypes.POINTER(ilm_config)]),
+    "ilm_context_destroy": (_I32, [_P]),
+    "ilm_last_error_string": (ctypes.c_char_p, [_P]),
+    "ilm_mesh_upload": (_I32, [_P, _P, _U32, _P, _U32, ctypes.POINTER(_U32)]),
+    "ilm_spheres_upload": (_I32, [_P, _P, _U32, ctypes.POINTER(_U32)]),
+    "ilm_accel_build": (_I32, [_P, _P, _U32, ctypes.POINTER(ilm_build_opts), ctypes.POINTER(_U32)]),
+    "ilm_accel_destroy": (_I32, [_P, _U32]),
+    "ilm_accel_world_bound": (_I32, [_P, _U32, _P]),
+    "ilm_accel_get_info": (_I32, [_P, _U32, ctypes.POINTER(ilm_accel_info)]),
+    "ilm_accel_binary_nodes": (_I32, [_P, _U32, _P, _P]),
+    "ilm_host_layout_build": (_I32, [_P, _U32, _P, _U32, _P, _U32, ctypes.POINTER(ilm_build_opts),
+                                     ctypes.POINTER(_P)]),
+    "ilm_host_layout_info": (_I32, [_P, ctypes.POINTER(ilm_accel_info)]),
+    "ilm_host_layout_copy": (_I32, [_P, _P, _P, _P, _P, _P]),
+    "ilm_host_layout_destroy": (_I32, [_P]),
+    "ilm_intersect_closest": (_I32, [_P, _U32, _P, _U64, _P, _P]),
+    "ilm_intersect_any": (_I32, [_P, _U32, _P, _U64, _P, _P]),
+    "ilm_device_errors": (_I32, [_P, ctypes.POINTER(_U32), _I32]),
+    "ilm_synchronize": (_I32, [_P, _P, ctypes.c_double]),
+    # workloads
+    "ilm_wl_rng_floats": (None, [_U64, _U64, _P]),
+    "ilm_wl_rng_u32": (None, [_U64, _U64, _P]),
+    "ilm_wl_soup": (None, [_U64, _U32, _F, _P, _P]),
+    "ilm_wl_icosphere_counts": (None, [_U32, ctypes.POINTER(_U32), ctypes.POINTER(_U32)]),
+    "ilm_wl_icosphere": (None, [_U32, _U64, _F, _F, _P, _P, _P]),
+    "ilm_wl_camera_rays": (None, [_U32, _U32, _P, _F, _P]),
+    "ilm_wl_ball_rays": (None, [_U64, _U64, _U64, _U64, _F, _F, _F, _P]),
+}
+
+_lib = None
+
+
+class IllumeError(RuntimeError):
+    def __init__(self, status: int, where: str, detail: str = ""):
+        self.status = status
+        name = STATUS_NAMES.get(status, str(status))
+        super().__init__(f"{where} failed with {name}" + (f": {detail}" if detail else ""))
+
+
+def load() -> ctypes.CDLL:
+    """Loads the library (once).  Raises if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: build it with `make -C rs_illume_b200/csrc` "
+                               "(or __graft_entry__.build())")
+        lib = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = lib
+    return _lib
+
+
+def ptr(a) -> int:
+    """Address of a C-contiguous numpy array (or a raw integer address)."""
+    if a is None:
+        return None
+    if isinstance(a, int):
+        return a
+    if isinstance(a, np.ndarray):
+        assert a.flags["C_CONTIGUOUS"], "array must be C-contiguous"
+        return a.ctypes.data
+    if hasattr(a, "data_ptr"):      # torch tensor (device or host)
+        return a.data_ptr()
+    raise TypeError(f"cannot take the address of {type(a)}")

@@ -1,0 +1,458 @@
+// C ABI of the ray-query library (include/illume_gpu.h).
+#include "illume_gpu.h"
+
+#include <cuda_runtime.h>
+
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "builder.h"
+#include "context.h"
+#include "kernels.h"
+
+using namespace ilm;
+
+namespace ilm {
+
+void set_error(ilm_context* ctx, const std::string& msg) {
+    if (ctx) ctx->last_error = msg;
+}
+
+int32_t cuda_fail(ilm_context* ctx, cudaError_t e, const char* what) {
+    char buf[256];
+    std::snprintf(buf, sizeof buf, "%s: %s", what, cudaGetErrorString(e));
+    set_error(ctx, buf);
+    return e == cudaErrorMemoryAllocation ? ILM_ERR_OUT_OF_MEMORY : ILM_ERR_CUDA;
+}
+
+DeviceBuffer::~DeviceBuffer() {
+    if (ptr) cudaFree(ptr);
+}
+
+cudaError_t DeviceBuffer::reserve(size_t n) {
+    if (n <= bytes) return cudaSuccess;
+    if (ptr) { cudaFree(ptr); ptr = nullptr; bytes = 0; }
+    cudaError_t e = cudaMalloc(&ptr, n);
+    if (e == cudaSuccess) bytes = n;
+    return e;
+}
+
+PtrKind classify(const void* p) {
+    cudaPointerAttributes attr;
+    cudaError_t e = cudaPointerGetAttributes(&attr, p);
+    if (e != cudaSuccess) { cudaGetLastError(); return PtrKind::kHost; }
+    if (attr.type == cudaMemoryTypeDevice || attr.type == cudaMemoryTypeManaged) return PtrKind::kDevice;
+    return PtrKind::kHost;
+}
+
+Accel* find_accel(ilm_context* ctx, ilm_accel_id id) {
+    auto it = ctx->accels.find(id);
+    return it == ctx->accels.end() ? nullptr : it->second.get();
+}
+
+}  // namespace ilm
+
+#define ILM_CHECK_CTX(ctx)                                   \
+    do {                                                     \
+        if (!(ctx)) return ILM_ERR_INVALID_ARGUMENT;         \
+        cudaError_t _e = cudaSetDevice((ctx)->device);       \
+        if (_e != cudaSuccess) return cuda_fail((ctx), _e, "cudaSetDevice"); \
+    } while (0)
+
+#define ILM_CUDA(ctx, call, what)                            \
+    do {                                                     \
+        cudaError_t _e = (call);                             \
+        if (_e != cudaSuccess) return cuda_fail((ctx), _e, what); \
+    } while (0)
+
+extern "C" {
+
+const char* ilm_last_error_string(const ilm_context* ctx) {
+    if (!ctx) return "no context";
+    return ctx->last_error.c_str();
+}
+
+int32_t ilm_context_create(ilm_context** out, const ilm_config* cfg) {
+    if (!out) return ILM_ERR_INVALID_ARGUMENT;
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return ILM_ERR_NO_DEVICE;
+    }
+    int dev = cfg ? cfg->device : 0;
+    if (dev < 0 || dev >= ndev) return ILM_ERR_INVALID_ARGUMENT;
+    if (cfg && (cfg->stack_depth < 0 || cfg->stack_depth > 64 || cfg->block_size < 0 || cfg->block_size > 1024))
+        return ILM_ERR_INVALID_ARGUMENT;
+    std::unique_ptr<ilm_context> ctx(new ilm_context());
+    ctx->device = dev;
+    ctx->stack_depth = (cfg && cfg->stack_depth) ? cfg->stack_depth : 64;
+    ctx->block_size = (cfg && cfg->block_size) ? cfg->block_size : 128;
+    ctx->flags = cfg ? cfg->flags : 0;
+    if (cfg && cfg->max_iterations) ctx->max_iter = cfg->max_iterations;
+    if (cudaSetDevice(dev) != cudaSuccess) return ILM_ERR_NO_DEVICE;
+    // Fail early when this build's kernels cannot run on the device.
+    cudaFuncAttributes fa;
+    if (!kernels_loadable(&fa)) {
+        cudaGetLastError();
+        return ILM_ERR_NO_DEVICE;
+    }
+    if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) return ILM_ERR_CUDA;
+    for (auto& s : ctx->pipe)
+        if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) return ILM_ERR_CUDA;
+    if (cudaEventCreateWithFlags(&ctx->fence, cudaEventDisableTiming) != cudaSuccess) return ILM_ERR_CUDA;
+    if (ctx->err_word.reserve(sizeof(uint32_t)) != cudaSuccess) return ILM_ERR_OUT_OF_MEMORY;
+    if (cudaMemset(ctx->err_word.ptr, 0, sizeof(uint32_t)) != cudaSuccess) return ILM_ERR_CUDA;
+    *out = ctx.release();
+    return ILM_OK;
+}
+
+int32_t ilm_context_destroy(ilm_context* ctx) {
+    if (!ctx) return ILM_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(ctx->device);
+    cudaDeviceSynchronize();
+    ctx->accels.clear();
+    for (auto& st : ctx->stage) { st.rays.release(); st.out.release(); }
+    ctx->err_word.release();
+    ctx->scratch_release();
+    if (ctx->fence) cudaEventDestroy(ctx->fence);
+    for (auto& s : ctx->pipe) if (s) cudaStreamDestroy(s);
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+    return ILM_OK;
+}
+
+int32_t ilm_mesh_upload(ilm_context* ctx, const float* xyz, uint32_t nv, const uint32_t* idx, uint32_t nt,
+                        ilm_mesh_id* out) {
+    if (!ctx || !out) return ILM_ERR_INVALID_ARGUMENT;
+    if ((nv > 0 && !xyz) || (nt > 0 && !idx)) {
+        set_error(ctx, "ilm_mesh_upload: null vertex or index pointer");
+        return ILM_ERR_INVALID_ARGUMENT;
+    }
+    for (uint64_t i = 0; i < 3ull * nv; ++i)
+        if (!std::isfinite(xyz[i])) {
+            set_error(ctx, "ilm_mesh_upload: non-finite vertex coordinate");
+            return ILM_ERR_INVALID_ARGUMENT;
+        }
+    for (uint64_t i = 0; i < 3ull * nt; ++i)
+        if (idx[i] >= nv) {
+            set_error(ctx, "ilm_mesh_upload: vertex index out of range");
+            return ILM_ERR_INVALID_ARGUMENT;
+        }
+    auto m = std::make_unique<Mesh>();
+    m->is_spheres = false;
+    m->xyz.assign(xyz, xyz + 3ull * nv);
+    m->idx.assign(idx, idx + 3ull * nt);
+    m->n_prims = nt;
+    ilm_mesh_id id = ctx->next_mesh++;
+    ctx->meshes[id] = std::move(m);
+    *out = id;
+    return ILM_OK;
+}
+
+int32_t ilm_spheres_upload(ilm_context* ctx, const ilm_sphere_desc* spheres, uint32_t n, ilm_mesh_id* out) {
+    if (!ctx || !out || (n > 0 && !spheres)) return ILM_ERR_INVALID_ARGUMENT;
+    auto m = std::make_unique<Mesh>();
+    m->is_spheres = true;
+    for (uint32_t i = 0; i < n; ++i) {
+        const ilm_sphere_desc& d = spheres[i];
+        if (!(d.radius > 0.0f) || !std::isfinite(d.radius)) {
+            set_error(ctx, "ilm_spheres_upload: radius must be positive and finite");
+            return ILM_ERR_INVALID_ARGUMENT;
+        }
+        SphereInput in;
+        std::memcpy(in.o2w, d.object_to_world, sizeof in.o2w);
+        std::memcpy(in.w2o, d.world_to_object, sizeof in.w2o);
+        in.radius = d.radius; in.z_min = d.z_min; in.z_max = d.z_max; in.phi_max_deg = d.phi_max_deg;
+        in.reverse = d.reverse_orientation;
+        m->spheres.push_back(make_sphere(in));
+    }
+    m->n_prims = n;
+    ilm_mesh_id id = ctx->next_mesh++;
+    ctx->meshes[id] = std::move(m);
+    *out = id;
+    return ILM_OK;
+}
+
+int32_t ilm_accel_build(ilm_context* ctx, const ilm_mesh_id* meshes, uint32_t n_meshes, const ilm_build_opts* opts,
+                        ilm_accel_id* out) {
+    ILM_CHECK_CTX(ctx);
+    if (!out || (n_meshes > 0 && !meshes)) return ILM_ERR_INVALID_ARGUMENT;
+    int width = opts ? opts->width : 8;
+    int max_prims = opts ? opts->max_prims_in_node : 4;
+    auto t0 = std::chrono::steady_clock::now();
+    std::vector<MeshView> views;
+    for (uint32_t k = 0; k < n_meshes; ++k) {
+        auto it = ctx->meshes.find(meshes[k]);
+        if (it == ctx->meshes.end()) {
+            set_error(ctx, "ilm_accel_build: unknown mesh id");
+            return ILM_ERR_NOT_FOUND;
+        }
+        const Mesh& m = *it->second;
+        views.push_back({m.is_spheres, m.xyz.data(), m.idx.data(), m.spheres.data(), m.n_prims});
+    }
+    auto acc = std::make_unique<Accel>();
+    std::string msg = build_layout(views, width, max_prims, (int)std::thread::hardware_concurrency(), acc->host);
+    if (!msg.empty()) {
+        set_error(ctx, "ilm_accel_build: " + msg);
+        return ILM_ERR_INVALID_ARGUMENT;
+    }
+    const HostLayout& h = acc->host;
+    if (!h.node_bytes.empty()) {
+        ILM_CUDA(ctx, acc->d_nodes.reserve(h.node_bytes.size()), "cudaMalloc(nodes)");
+        ILM_CUDA(ctx, cudaMemcpy(acc->d_nodes.ptr, h.node_bytes.data(), h.node_bytes.size(), cudaMemcpyHostToDevice),
+                 "cudaMemcpy(nodes)");
+    }
+    size_t rb = h.records.size() * sizeof(PrimRec);
+    if (rb) {
+        ILM_CUDA(ctx, acc->d_prims.reserve(rb), "cudaMalloc(prims)");
+        ILM_CUDA(ctx, cudaMemcpy(acc->d_prims.ptr, h.records.data(), rb, cudaMemcpyHostToDevice), "cudaMemcpy(prims)");
+    }
+    size_t sb = h.spheres.size() * sizeof(SphereRec);
+    if (sb) {
+        ILM_CUDA(ctx, acc->d_spheres.reserve(sb), "cudaMalloc(spheres)");
+        ILM_CUDA(ctx, cudaMemcpy(acc->d_spheres.ptr, h.spheres.data(), sb, cudaMemcpyHostToDevice),
+                 "cudaMemcpy(spheres)");
+    }
+    acc->device_bytes = h.node_bytes.size() + rb + sb;
+    acc->build_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    ilm_accel_id id = ctx->next_accel++;
+    ctx->accels[id] = std::move(acc);
+    *out = id;
+    return ILM_OK;
+}
+
+int32_t ilm_accel_destroy(ilm_context* ctx, ilm_accel_id accel) {
+    ILM_CHECK_CTX(ctx);
+    auto it = ctx->accels.find(accel);
+    if (it == ctx->accels.end()) return ILM_ERR_NOT_FOUND;
+    cudaDeviceSynchronize();
+    ctx->accels.erase(it);
+    return ILM_OK;
+}
+
+int32_t ilm_accel_world_bound(ilm_context* ctx, ilm_accel_id accel, float out[6]) {
+    if (!ctx || !out) return ILM_ERR_INVALID_ARGUMENT;
+    Accel* a = find_accel(ctx, accel);
+    if (!a) return ILM_ERR_NOT_FOUND;
+    std::memcpy(out, a->host.bound, sizeof a->host.bound);
+    return ILM_OK;
+}
+
+int32_t ilm_accel_get_info(ilm_context* ctx, ilm_accel_id accel, ilm_accel_info* out) {
+    if (!ctx || !out) return ILM_ERR_INVALID_ARGUMENT;
+    Accel* a = find_accel(ctx, accel);
+    if (!a) return ILM_ERR_NOT_FOUND;
+    out->n_prims = a->host.n_prims;
+    out->n_binary_nodes = (uint32_t)a->host.bin_nodes.size();
+    out->n_nodes = a->host.n_nodes;
+    out->width = (uint32_t)a->host.width;
+    out->device_bytes = a->device_bytes;
+    out->build_seconds = a->build_seconds;
+    return ILM_OK;
+}
+
+int32_t ilm_accel_binary_nodes(ilm_context* ctx, ilm_accel_id accel, void* out_nodes, uint32_t* out_prim_order) {
+    if (!ctx) return ILM_ERR_INVALID_ARGUMENT;
+    Accel* a = find_accel(ctx, accel);
+    if (!a) return ILM_ERR_NOT_FOUND;
+    if (out_nodes && !a->host.bin_nodes.empty())
+        std::memcpy(out_nodes, a->host.bin_nodes.data(), a->host.bin_nodes.size() * sizeof(BinNode));
+    if (out_prim_order && !a->host.prim_order.empty())
+        std::memcpy(out_prim_order, a->host.prim_order.data(), a->host.prim_order.size() * 4);
+    return ILM_OK;
+}
+
+static int32_t intersect_impl(ilm_context* ctx, ilm_accel_id accel, const ilm_ray* rays, uint64_t n, ilm_hit* hits,
+                              uint32_t* occ, void* stream) {
+    ILM_CHECK_CTX(ctx);
+    void* out = occ ? (void*)occ : (void*)hits;
+    if (n == 0) return ILM_OK;
+    if (!rays || !out) {
+        set_error(ctx, "null ray or result pointer");
+        return ILM_ERR_INVALID_ARGUMENT;
+    }
+    if (((uintptr_t)rays & 15u) || (!occ && ((uintptr_t)hits & 15u)) || (occ && ((uintptr_t)occ & 3u))) {
+        set_error(ctx, "ray/hit buffers must be 16-byte aligned (occlusion flags 4-byte aligned)");
+        return ILM_ERR_INVALID_ARGUMENT;
+    }
+    Accel* a = find_accel(ctx, accel);
+    if (!a) {
+        set_error(ctx, "unknown accel id");
+        return ILM_ERR_NOT_FOUND;
+    }
+    DeviceAccel da = a->view();
+    LaunchParams lp{ctx->stack_depth, ctx->block_size, ctx->max_iter};
+    uint32_t* err = static_cast<uint32_t*>(ctx->err_word.ptr);
+    cudaStream_t user = stream ? static_cast<cudaStream_t>(stream) : ctx->stream;
+    PtrKind kr = classify(rays), ko = classify(out);
+    if (kr != ko) {
+        set_error(ctx, "rays and results must both be device memory or both host memory");
+        return ILM_ERR_INVALID_ARGUMENT;
+    }
+    if (kr == PtrKind::kDevice) {
+        ILM_CUDA(ctx, launch_trace(da, rays, n, hits, occ, err, lp, user), "trace launch");
+        return ILM_OK;
+    }
+    if (ctx->flags & ILM_FLAG_VALIDATE_RAYS) {
+        for (uint64_t i = 0; i < n; ++i) {
+            const ilm_ray& r = rays[i];
+            bool ok = std::isfinite(r.o[0]) && std::isfinite(r.o[1]) && std::isfinite(r.o[2]) &&
+                      std::isfinite(r.d[0]) && std::isfinite(r.d[1]) && std::isfinite(r.d[2]) &&
+                      !(r.d[0] == 0.0f && r.d[1] == 0.0f && r.d[2] == 0.0f) && !(r.tmax < 0.0f) &&
+                      !std::isnan(r.tmax);
+            if (!ok) {
+                char buf[128];
+                std::snprintf(buf, sizeof buf, "ray %llu is invalid (non-finite, zero direction or tmax < 0)",
+                              (unsigned long long)i);
+                set_error(ctx, buf);
+                return ILM_ERR_INVALID_ARGUMENT;
+            }
+        }
+    }
+    // Host buffers: pipelined chunks over three streams (copy-in, trace,
+    // copy-out of consecutive chunks overlap).
+    const uint64_t chunk = ctx->stage_chunk;
+    const size_t out_rec = occ ? sizeof(uint32_t) : sizeof(ilm_hit);
+    for (auto& st : ctx->stage) {
+        ILM_CUDA(ctx, st.rays.reserve(chunk * sizeof(ilm_ray)), "cudaMalloc(stage rays)");
+        ILM_CUDA(ctx, st.out.reserve(chunk * sizeof(ilm_hit)), "cudaMalloc(stage out)");
+    }
+    ILM_CUDA(ctx, cudaEventRecord(ctx->fence, user), "cudaEventRecord");
+    for (auto& s : ctx->pipe) ILM_CUDA(ctx, cudaStreamWaitEvent(s, ctx->fence, 0), "cudaStreamWaitEvent");
+    uint64_t c = 0;
+    for (uint64_t off = 0; off < n; off += chunk, ++c) {
+        uint64_t cnt = n - off < chunk ? n - off : chunk;
+        int slot = (int)(c % kPipeDepth);
+        cudaStream_t s = ctx->pipe[slot];
+        Stage& st = ctx->stage[slot];
+        ILM_CUDA(ctx, cudaMemcpyAsync(st.rays.ptr, rays + off, cnt * sizeof(ilm_ray), cudaMemcpyHostToDevice, s),
+                 "cudaMemcpyAsync(rays)");
+        ILM_CUDA(ctx,
+                 launch_trace(da, static_cast<const ilm_ray*>(st.rays.ptr), cnt,
+                              occ ? nullptr : static_cast<ilm_hit*>(st.out.ptr),
+                              occ ? static_cast<uint32_t*>(st.out.ptr) : nullptr, err, lp, s),
+                 "trace launch");
+        void* dst = occ ? (void*)(occ + off) : (void*)(hits + off);
+        ILM_CUDA(ctx, cudaMemcpyAsync(dst, st.out.ptr, cnt * out_rec, cudaMemcpyDeviceToHost, s),
+                 "cudaMemcpyAsync(results)");
+    }
+    for (auto& s : ctx->pipe) ILM_CUDA(ctx, cudaStreamSynchronize(s), "cudaStreamSynchronize");
+    return ILM_OK;
+}
+
+int32_t ilm_intersect_closest(ilm_context* ctx, ilm_accel_id accel, const ilm_ray* rays, uint64_t n, ilm_hit* hits,
+                              void* stream) {
+    if (!ctx) return ILM_ERR_INVALID_ARGUMENT;
+    if (n > 0 && !hits) { set_error(ctx, "null hit pointer"); return ILM_ERR_INVALID_ARGUMENT; }
+    return intersect_impl(ctx, accel, rays, n, hits, nullptr, stream);
+}
+
+int32_t ilm_intersect_any(ilm_context* ctx, ilm_accel_id accel, const ilm_ray* rays, uint64_t n, uint32_t* occluded,
+                          void* stream) {
+    if (!ctx) return ILM_ERR_INVALID_ARGUMENT;
+    if (n > 0 && !occluded) { set_error(ctx, "null occlusion pointer"); return ILM_ERR_INVALID_ARGUMENT; }
+    return intersect_impl(ctx, accel, rays, n, nullptr, occluded, stream);
+}
+
+struct ilm_host_layout {
+    ilm::HostLayout h;
+    double seconds = 0.0;
+};
+
+int32_t ilm_host_layout_build(const float* xyz, uint32_t nv, const uint32_t* idx, uint32_t nt,
+                              const ilm_sphere_desc* spheres, uint32_t ns, const ilm_build_opts* opts,
+                              ilm_host_layout** out) {
+    if (!out || (nv > 0 && !xyz) || (nt > 0 && !idx) || (ns > 0 && !spheres)) return ILM_ERR_INVALID_ARGUMENT;
+    for (uint64_t i = 0; i < 3ull * nt; ++i)
+        if (idx[i] >= nv) return ILM_ERR_INVALID_ARGUMENT;
+    for (uint64_t i = 0; i < 3ull * nv; ++i)
+        if (!std::isfinite(xyz[i])) return ILM_ERR_INVALID_ARGUMENT;
+    std::vector<SphereRec> sph;
+    for (uint32_t i = 0; i < ns; ++i) {
+        const ilm_sphere_desc& d = spheres[i];
+        if (!(d.radius > 0.0f) || !std::isfinite(d.radius)) return ILM_ERR_INVALID_ARGUMENT;
+        SphereInput in;
+        std::memcpy(in.o2w, d.object_to_world, sizeof in.o2w);
+        std::memcpy(in.w2o, d.world_to_object, sizeof in.w2o);
+        in.radius = d.radius; in.z_min = d.z_min; in.z_max = d.z_max; in.phi_max_deg = d.phi_max_deg;
+        in.reverse = d.reverse_orientation;
+        sph.push_back(make_sphere(in));
+    }
+    std::vector<MeshView> views;
+    if (nt > 0) views.push_back({false, xyz, idx, nullptr, nt});
+    if (ns > 0) views.push_back({true, nullptr, nullptr, sph.data(), ns});
+    auto t0 = std::chrono::steady_clock::now();
+    std::unique_ptr<ilm_host_layout> hl(new ilm_host_layout());
+    std::string msg = build_layout(views, opts ? opts->width : 8, opts ? opts->max_prims_in_node : 4,
+                                   (int)std::thread::hardware_concurrency(), hl->h);
+    if (!msg.empty()) return ILM_ERR_INVALID_ARGUMENT;
+    hl->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    *out = hl.release();
+    return ILM_OK;
+}
+
+int32_t ilm_host_layout_info(const ilm_host_layout* hl, ilm_accel_info* out) {
+    if (!hl || !out) return ILM_ERR_INVALID_ARGUMENT;
+    const HostLayout& h = hl->h;
+    out->n_prims = h.n_prims;
+    out->n_binary_nodes = (uint32_t)h.bin_nodes.size();
+    out->n_nodes = h.n_nodes;
+    out->width = (uint32_t)h.width;
+    out->device_bytes = h.node_bytes.size() + h.records.size() * sizeof(PrimRec) + h.spheres.size() * sizeof(SphereRec);
+    out->build_seconds = hl->seconds;
+    return ILM_OK;
+}
+
+int32_t ilm_host_layout_copy(const ilm_host_layout* hl, void* bin_nodes, uint32_t* prim_order, void* nodes,
+                             void* records, float* bound) {
+    if (!hl) return ILM_ERR_INVALID_ARGUMENT;
+    const HostLayout& h = hl->h;
+    if (bin_nodes && !h.bin_nodes.empty()) std::memcpy(bin_nodes, h.bin_nodes.data(), h.bin_nodes.size() * sizeof(BinNode));
+    if (prim_order && !h.prim_order.empty()) std::memcpy(prim_order, h.prim_order.data(), h.prim_order.size() * 4);
+    if (nodes && !h.node_bytes.empty()) std::memcpy(nodes, h.node_bytes.data(), h.node_bytes.size());
+    if (records && !h.records.empty()) std::memcpy(records, h.records.data(), h.records.size() * sizeof(PrimRec));
+    if (bound) std::memcpy(bound, h.bound, sizeof h.bound);
+    return ILM_OK;
+}
+
+int32_t ilm_host_layout_destroy(ilm_host_layout* hl) {
+    if (!hl) return ILM_ERR_INVALID_ARGUMENT;
+    delete hl;
+    return ILM_OK;
+}
+
+int32_t ilm_device_errors(ilm_context* ctx, uint32_t* out_flags, int32_t reset) {
+    ILM_CHECK_CTX(ctx);
+    if (!out_flags) return ILM_ERR_INVALID_ARGUMENT;
+    ILM_CUDA(ctx, cudaDeviceSynchronize(), "cudaDeviceSynchronize");
+    ILM_CUDA(ctx, cudaMemcpy(out_flags, ctx->err_word.ptr, sizeof(uint32_t), cudaMemcpyDeviceToHost), "cudaMemcpy(err)");
+    if (reset) ILM_CUDA(ctx, cudaMemset(ctx->err_word.ptr, 0, sizeof(uint32_t)), "cudaMemset(err)");
+    return ILM_OK;
+}
+
+int32_t ilm_synchronize(ilm_context* ctx, void* stream, double timeout_s) {
+    ILM_CHECK_CTX(ctx);
+    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : ctx->stream;
+    auto t0 = std::chrono::steady_clock::now();
+    for (;;) {
+        cudaError_t e = cudaStreamQuery(s);
+        if (e == cudaSuccess) return ILM_OK;
+        if (e != cudaErrorNotReady) return cuda_fail(ctx, e, "cudaStreamQuery");
+        double el = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        if (el > timeout_s) {
+            set_error(ctx, "ilm_synchronize: timed out");
+            return ILM_ERR_TIMEOUT;
+        }
+        std::this_thread::sleep_for(std::chrono::microseconds(50));
+    }
+}
+
+}  // extern "C"

@@ -1,0 +1,85 @@
+// Host-side acceleration-structure construction.
+#pragma once
+#include <stdint.h>
+#include <string>
+#include <vector>
+
+#include "layout.h"
+
+namespace ilm {
+
+struct Box {
+    float mn[3], mx[3];
+};
+Box empty_box();                  // Bounds3::default (min = MAX, max = -MAX)
+
+struct BuildPrim {
+    uint32_t prim;                // primitive id
+    Box bounds;
+    float centroid[3];
+};
+
+// SAH binary build with 12 buckets and BVHAccel's leaf rule (bvh.rs:95-247,
+// with the centroid-bound, bucket-index and argmin repairs), flattened
+// depth-first as flatten_bvh_tree (bvh.rs:504-537).  On return `prims` is in
+// leaf order (the order of BVHAccel's ordered_prims) and leaf offsets index it.
+// Subtrees are built on up to `threads` host threads; the result does not
+// depend on the thread count.
+void sah_build(std::vector<BuildPrim>& prims, int max_prims_in_node, int threads,
+               std::vector<BinNode>& nodes);
+
+// Collapses the binary tree into W-wide compressed nodes (W = 4 or 8).
+// `prims` is the leaf-ordered list from sah_build (for per-primitive boxes).
+// Outputs the node array (raw bytes, node 0 = root) and, for each primitive
+// record slot of the wide layout, the index into `prims` it holds.
+void collapse_wide(const std::vector<BinNode>& bin, const std::vector<BuildPrim>& prims, int width,
+                   std::vector<uint8_t>& node_bytes, uint32_t* n_nodes,
+                   std::vector<uint32_t>& record_order);
+
+// Triangle bound as Triangle::world_bound (shapes/triangle.rs:126-132).
+Box triangle_bound(const float* p0, const float* p1, const float* p2);
+// Centroid as Bounds3::centroid (geometry/bounds3.rs:238-242).
+void box_centroid(const Box& b, float c[3]);
+// (p2-p0)x(p1-p0) evaluated as Vector3::cross (f64, rounded) has zero
+// squared length (shapes/triangle.rs:281-289).
+bool triangle_degenerate(const float* p0, const float* p1, const float* p2);
+// Sphere::new derived values and world bound (shapes/sphere.rs:50-75;
+// geometry/bounds3.rs:320-356).
+struct SphereInput {
+    float o2w[16], w2o[16];
+    float radius, z_min, z_max, phi_max_deg;
+    int32_t reverse;
+};
+SphereRec make_sphere(const SphereInput& in);
+Box sphere_bound(const SphereRec& s);
+
+// One shape list entry: a triangle mesh (world-space vertices) or a sphere set.
+struct MeshView {
+    bool is_spheres;
+    const float* xyz;
+    const uint32_t* idx;
+    const SphereRec* spheres;
+    uint32_t n_prims;
+};
+
+// Everything the device needs for one acceleration structure, built on the
+// host: the SAH binary tree, the layout for `width`, and primitive records in
+// traversal order.
+struct HostLayout {
+    int width = 8;
+    uint32_t n_prims = 0;
+    std::vector<BinNode> bin_nodes;
+    std::vector<uint32_t> prim_order;   // BVHAccel ordered_prims as primitive ids
+    std::vector<uint8_t> node_bytes;
+    uint32_t n_nodes = 0;
+    std::vector<PrimRec> records;
+    std::vector<SphereRec> spheres;
+    float bound[6];
+};
+
+// BVHAccel::new (bvh.rs:32-93) followed by the device layout.  Returns an
+// empty string on success or a description of the failure.
+std::string build_layout(const std::vector<MeshView>& meshes, int width, int max_prims_in_node, int threads,
+                         HostLayout& out);
+
+}  // namespace ilm

@@ -1,0 +1,96 @@
+// Library-internal state behind the opaque ilm_context handle.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "builder.h"
+#include "illume_gpu.h"
+#include "kernels.h"
+#include "layout.h"
+
+namespace ilm {
+
+struct DeviceBuffer {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+    DeviceBuffer() = default;
+    DeviceBuffer(const DeviceBuffer&) = delete;
+    DeviceBuffer& operator=(const DeviceBuffer&) = delete;
+    ~DeviceBuffer();
+    cudaError_t reserve(size_t n);   // grows (discarding contents) when too small
+    void release() {
+        if (ptr) cudaFree(ptr);
+        ptr = nullptr;
+        bytes = 0;
+    }
+};
+
+struct Mesh {
+    bool is_spheres = false;
+    std::vector<float> xyz;          // world-space vertices
+    std::vector<uint32_t> idx;
+    std::vector<SphereRec> spheres;
+    uint32_t n_prims = 0;
+};
+
+struct Accel {
+    HostLayout host;                 // SAH tree, prim order, bound (device copies below)
+    DeviceBuffer d_nodes, d_prims, d_spheres;
+    uint64_t device_bytes = 0;
+    double build_seconds = 0.0;
+
+    DeviceAccel view() const {
+        DeviceAccel a;
+        a.width = host.width;
+        a.nodes = d_nodes.ptr;
+        a.n_nodes = host.n_nodes;
+        a.prims = static_cast<const PrimRec*>(d_prims.ptr);
+        a.n_records = (uint32_t)host.records.size();
+        a.spheres = static_cast<const SphereRec*>(d_spheres.ptr);
+        return a;
+    }
+};
+
+constexpr int kPipeDepth = 3;
+
+struct Stage {
+    DeviceBuffer rays, out;
+};
+
+enum class PtrKind { kHost, kDevice };
+
+}  // namespace ilm
+
+struct ilm_context {
+    int device = 0;
+    int stack_depth = 64;
+    int block_size = 128;
+    int flags = 0;
+    uint32_t max_iter = 1u << 20;
+    cudaStream_t stream = nullptr;
+    cudaStream_t pipe[ilm::kPipeDepth] = {nullptr, nullptr, nullptr};
+    cudaEvent_t fence = nullptr;
+    ilm::Stage stage[ilm::kPipeDepth];
+    uint64_t stage_chunk = 1ull << 18;
+    ilm::DeviceBuffer err_word;
+    std::string last_error;
+    std::map<ilm_mesh_id, std::unique_ptr<ilm::Mesh>> meshes;
+    std::map<ilm_accel_id, std::unique_ptr<ilm::Accel>> accels;
+    ilm_mesh_id next_mesh = 1;
+    ilm_accel_id next_accel = 1;
+    void scratch_release() {}
+};
+
+namespace ilm {
+void set_error(ilm_context* ctx, const std::string& msg);
+int32_t cuda_fail(ilm_context* ctx, cudaError_t e, const char* what);
+PtrKind classify(const void* p);
+Accel* find_accel(ilm_context* ctx, ilm_accel_id id);
+// True when this library's kernels have an image for the current device.
+bool kernels_loadable(cudaFuncAttributes* attr);
+}  // namespace ilm

@@ -1,0 +1,265 @@
+"""Host-side mirror of rs_illume's aggregate interface for the GPU path.
+
+``GpuBVHAccel`` stands where ``BVHAccel`` (src/accelerators/bvh.rs:24-93)
+stands in the reference: it implements the ``Primitive`` surface
+(src/core/primitive/mod.rs:9-20) -- ``world_bound``, ``intersect``,
+``intersect_p`` and the material/area-light queries that an aggregate answers
+with an error (bvh.rs:540-553) -- on top of the C ABI in include/illume_gpu.h.
+Batched calls (``intersect_batch`` / ``intersect_p_batch``) are the intended
+path; the single-ray methods are batches of one.  ``Scene`` mirrors
+src/core/scene.rs:10-53.
+"""
+from __future__ import annotations
+
+import ctypes
+import logging
+from dataclasses import dataclass
+from typing import Optional, Sequence
+
+import numpy as np
+
+from . import _lib
+from ._lib import (HIT_DTYPE, ILM_MISS, RAY_DTYPE, IllumeError, ilm_accel_info, ilm_build_opts,
+                   ilm_config, ilm_sphere_desc, ptr)
+
+log = logging.getLogger("rs_illume_b200")
+
+SPLIT_METHODS = ("SAH", "HLBVH", "Middle", "EqualCounts")   # bvh.rs:16-22
+
+
+@dataclass
+class Bounds3f:
+    """geometry/bounds3.rs:74-77."""
+    min: np.ndarray
+    max: np.ndarray
+
+
+@dataclass
+class Ray:
+    """geometry/ray.rs:11-19 (o, d, t_max; time/medium/differential unused here)."""
+    o: Sequence[float]
+    d: Sequence[float]
+    t_max: float = float("inf")
+
+
+@dataclass
+class Hit:
+    """Closest-hit result: the primitive, t and (u, v); for triangles u = b1 and
+    v = b2 of the watertight test (shapes/triangle.rs:232-236)."""
+    prim: int
+    t: float
+    u: float
+    v: float
+
+    def point(self, ray: Ray) -> np.ndarray:
+        """Ray::point_at_time (ray.rs:35-37)."""
+        return np.asarray(ray.o, np.float32) + np.asarray(ray.d, np.float32) * np.float32(self.t)
+
+
+def rays_array(rays: Sequence[Ray]) -> np.ndarray:
+    a = np.zeros(len(rays), RAY_DTYPE)
+    for i, r in enumerate(rays):
+        a["o"][i] = r.o
+        a["d"][i] = r.d
+        a["tmax"][i] = r.t_max
+    return a
+
+
+class Context:
+    """One ilm_context (device, streams, staging buffers, error word)."""
+
+    def __init__(self, device: int = 0, stack_depth: int = 0, block_size: int = 0, validate_rays: bool = False,
+                 max_iterations: int = 0):
+        self._lib = _lib.load()
+        cfg = ilm_config(device, stack_depth, block_size, 1 if validate_rays else 0, max_iterations)
+        h = ctypes.c_void_p()
+        st = self._lib.ilm_context_create(ctypes.byref(h), ctypes.byref(cfg))
+        if st != _lib.ILM_OK:
+            raise IllumeError(st, "ilm_context_create")
+        self.handle = h
+
+    def check(self, status: int, where: str) -> None:
+        if status != _lib.ILM_OK:
+            detail = self._lib.ilm_last_error_string(self.handle)
+            raise IllumeError(status, where, detail.decode() if detail else "")
+
+    def device_errors(self, reset: bool = True) -> int:
+        flags = ctypes.c_uint32()
+        self.check(self._lib.ilm_device_errors(self.handle, ctypes.byref(flags), int(reset)), "ilm_device_errors")
+        return flags.value
+
+    def synchronize(self, stream=None, timeout_s: float = 60.0) -> None:
+        self.check(self._lib.ilm_synchronize(self.handle, stream, timeout_s), "ilm_synchronize")
+
+    def close(self) -> None:
+        if getattr(self, "handle", None):
+            self._lib.ilm_context_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class TriangleMesh:
+    """TriangleMesh (shapes/triangle.rs:17-74) with world-space vertices."""
+
+    def __init__(self, ctx: Context, xyz: np.ndarray, idx: np.ndarray):
+        xyz = np.ascontiguousarray(xyz, np.float32).reshape(-1, 3)
+        idx = np.ascontiguousarray(idx, np.uint32).reshape(-1, 3)
+        mid = ctypes.c_uint32()
+        ctx.check(ctx._lib.ilm_mesh_upload(ctx.handle, ptr(xyz), len(xyz), ptr(idx), len(idx), ctypes.byref(mid)),
+                  "ilm_mesh_upload")
+        self.id = mid.value
+        self.n_prims = len(idx)
+
+
+def sphere_desc(radius: float, translate=(0.0, 0.0, 0.0), scale: float = 1.0, z_min: Optional[float] = None,
+                z_max: Optional[float] = None, phi_max_deg: float = 360.0, reverse: bool = False) -> ilm_sphere_desc:
+    """Sphere::new arguments (shapes/sphere.rs:50-75) for a translate*scale placement."""
+    d = ilm_sphere_desc()
+    tx, ty, tz = translate
+    m = [scale, 0, 0, tx, 0, scale, 0, ty, 0, 0, scale, tz, 0, 0, 0, 1]
+    inv = [1.0 / scale, 0, 0, -tx / scale, 0, 1.0 / scale, 0, -ty / scale, 0, 0, 1.0 / scale, -tz / scale, 0, 0, 0, 1]
+    for i in range(16):
+        d.object_to_world[i] = m[i]
+        d.world_to_object[i] = inv[i]
+    d.radius = radius
+    d.z_min = -radius if z_min is None else z_min
+    d.z_max = radius if z_max is None else z_max
+    d.phi_max_deg = phi_max_deg
+    d.reverse_orientation = int(reverse)
+    return d
+
+
+class Spheres:
+    """A set of Sphere shapes (shapes/sphere.rs)."""
+
+    def __init__(self, ctx: Context, descs: Sequence[ilm_sphere_desc]):
+        arr = (ilm_sphere_desc * len(descs))(*descs)
+        mid = ctypes.c_uint32()
+        ctx.check(ctx._lib.ilm_spheres_upload(ctx.handle, ctypes.addressof(arr), len(descs), ctypes.byref(mid)),
+                  "ilm_spheres_upload")
+        self.id = mid.value
+        self.n_prims = len(descs)
+        self.descs = list(descs)
+
+
+class GpuBVHAccel:
+    """GPU drop-in for BVHAccel: same SAH tree, queries on the B200."""
+
+    def __init__(self, ctx: Context, shapes: Sequence, max_prims_in_node: int = 4, split_method: str = "SAH",
+                 width: int = 8):
+        if split_method not in SPLIT_METHODS:
+            raise ValueError(f"unknown split method {split_method!r}")
+        if split_method != "SAH":
+            raise NotImplementedError("only the SAH split method is built on the GPU path")
+        self.ctx = ctx
+        ids = (ctypes.c_uint32 * len(shapes))(*[s.id for s in shapes])
+        opts = ilm_build_opts(width, max_prims_in_node)
+        aid = ctypes.c_uint32()
+        ctx.check(ctx._lib.ilm_accel_build(ctx.handle, ids, len(shapes), ctypes.byref(opts), ctypes.byref(aid)),
+                  "ilm_accel_build")
+        self.id = aid.value
+        self.width = width
+        self.n_prims = sum(s.n_prims for s in shapes)
+
+    # -- Primitive surface (primitive/mod.rs:9-20) -------------------------
+    def world_bound(self) -> Bounds3f:
+        b = np.zeros(6, np.float32)
+        self.ctx.check(self.ctx._lib.ilm_accel_world_bound(self.ctx.handle, self.id, ptr(b)), "ilm_accel_world_bound")
+        return Bounds3f(b[:3].copy(), b[3:].copy())
+
+    def intersect(self, ray: Ray) -> Optional[Hit]:
+        h = self.intersect_batch(rays_array([ray]))[0]
+        if h["prim"] == ILM_MISS:
+            return None
+        if h["prim"] == _lib.ILM_TRAVERSAL_ERROR:
+            raise IllumeError(_lib.ILM_ERR_TRAVERSAL_LIMIT, "intersect")
+        return Hit(int(h["prim"]), float(h["t"]), float(h["u"]), float(h["v"]))
+
+    def intersect_p(self, ray: Ray) -> bool:
+        occ = self.intersect_p_batch(rays_array([ray]))[0]
+        if occ == _lib.ILM_TRAVERSAL_ERROR:
+            raise IllumeError(_lib.ILM_ERR_TRAVERSAL_LIMIT, "intersect_p")
+        return bool(occ)
+
+    def get_area_light(self):
+        log.error("GpuBVHAccel::get_area_light() called; should have gone to GeometricPrimitive.")
+        return None
+
+    def get_material(self):
+        log.error("GpuBVHAccel::get_material() called; should have gone to GeometricPrimitive.")
+        return None
+
+    def compute_scattering_function(self, *args, **kwargs):
+        log.error("GpuBVHAccel::compute_scattering_function() called; should have gone to GeometricPrimitive.")
+
+    # -- batched path ------------------------------------------------------
+    def intersect_batch(self, rays, hits=None, stream=None):
+        """Closest hit for every ray.  `rays` is a RAY_DTYPE numpy array (host)
+        or a torch uint8/float tensor on the device holding 32-byte records;
+        `hits` likewise (16-byte records).  Host arrays return a HIT_DTYPE array."""
+        n = _count(rays, 32)
+        if hits is None:
+            if not isinstance(rays, np.ndarray):
+                raise ValueError("device rays need a device `hits` buffer")
+            hits = np.empty(n, HIT_DTYPE)
+        self.ctx.check(self.ctx._lib.ilm_intersect_closest(self.ctx.handle, self.id, ptr(rays), n, ptr(hits),
+                                                           _stream(stream)), "ilm_intersect_closest")
+        return hits
+
+    def intersect_p_batch(self, rays, occluded=None, stream=None):
+        n = _count(rays, 32)
+        if occluded is None:
+            if not isinstance(rays, np.ndarray):
+                raise ValueError("device rays need a device `occluded` buffer")
+            occluded = np.empty(n, np.uint32)
+        self.ctx.check(self.ctx._lib.ilm_intersect_any(self.ctx.handle, self.id, ptr(rays), n, ptr(occluded),
+                                                       _stream(stream)), "ilm_intersect_any")
+        return occluded
+
+    def info(self) -> dict:
+        inf = ilm_accel_info()
+        self.ctx.check(self.ctx._lib.ilm_accel_get_info(self.ctx.handle, self.id, ctypes.byref(inf)),
+                       "ilm_accel_get_info")
+        return {k: getattr(inf, k) for k, _ in inf._fields_}
+
+    def binary_nodes(self):
+        inf = self.info()
+        nodes = np.zeros(inf["n_binary_nodes"], _lib.BIN_NODE_DTYPE)
+        order = np.zeros(inf["n_prims"], np.uint32)
+        self.ctx.check(self.ctx._lib.ilm_accel_binary_nodes(self.ctx.handle, self.id, ptr(nodes), ptr(order)),
+                       "ilm_accel_binary_nodes")
+        return nodes, order
+
+
+class Scene:
+    """Scene (core/scene.rs:10-53): an aggregate plus lights."""
+
+    def __init__(self, aggregate: GpuBVHAccel, lights: Sequence = ()):
+        self.aggregate = aggregate
+        self.lights = list(lights)
+        self.world_bound = aggregate.world_bound()
+
+    def intersect(self, ray: Ray) -> Optional[Hit]:
+        return self.aggregate.intersect(ray)
+
+    def intersect_p(self, ray: Ray) -> bool:
+        return self.aggregate.intersect_p(ray)
+
+
+def _count(buf, rec: int) -> int:
+    if isinstance(buf, np.ndarray):
+        return buf.nbytes // rec
+    return buf.numel() * buf.element_size() // rec
+
+
+def _stream(stream):
+    if stream is None:
+        return None
+    if isinstance(stream, int):
+        return stream
+    return stream.cuda_stream     # torch.cuda.Stream

@@ -1,0 +1,85 @@
+"""Seeded synthetic inputs for the benchmark configurations.
+
+The reference ships no benchmark inputs, so scenes and rays are generated
+procedurally with the reference's PCG32 (src/core/rng.rs) by the C++ generators
+in csrc/workloads.cpp (declared in include/illume_workloads.h).
+
+  coherent      32,768-triangle soup in the unit cube (centre ~ U[0,1]^3, vertex
+                offsets ~ U[-0.02, 0.02]^3, seed 1), 256x256 pinhole primary rays
+                from (0.5, 0.5, -1.5) looking +z, 45 degree vertical fov.
+  incoherent    displaced icosphere level 8 (1,310,720 triangles, seed 2);
+                4,194,304 rays from a radius-3 ball with uniform directions;
+                the first half closest-hit (tmax = inf), the second half shadow
+                rays with tmax ~ U[0.1, 4].
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from ._lib import RAY_DTYPE, ptr
+
+
+def rng_floats(seq: int, n: int) -> np.ndarray:
+    out = np.empty(n, np.float32)
+    _lib.load().ilm_wl_rng_floats(seq, n, ptr(out))
+    return out
+
+
+def rng_u32(seq: int, n: int) -> np.ndarray:
+    out = np.empty(n, np.uint32)
+    _lib.load().ilm_wl_rng_u32(seq, n, ptr(out))
+    return out
+
+
+def soup(seed: int = 1, n: int = 32768, spread: float = 0.02):
+    xyz = np.empty((3 * n, 3), np.float32)
+    idx = np.empty((n, 3), np.uint32)
+    _lib.load().ilm_wl_soup(seed, n, spread, ptr(xyz), ptr(idx))
+    return xyz, idx
+
+
+def icosphere_counts(level: int):
+    nv, nt = ctypes.c_uint32(), ctypes.c_uint32()
+    _lib.load().ilm_wl_icosphere_counts(level, ctypes.byref(nv), ctypes.byref(nt))
+    return nv.value, nt.value
+
+
+def icosphere(level: int, seed: int, amplitude: float = 0.05, radius: float = 1.0, centre=(0.0, 0.0, 0.0)):
+    nv, nt = icosphere_counts(level)
+    xyz = np.empty((nv, 3), np.float32)
+    idx = np.empty((nt, 3), np.uint32)
+    c = np.asarray(centre, np.float32)
+    _lib.load().ilm_wl_icosphere(level, seed, amplitude, radius, ptr(c), ptr(xyz), ptr(idx))
+    return xyz, idx
+
+
+def camera_rays(width: int = 256, height: int = 256, eye=(0.5, 0.5, -1.5), fov_deg: float = 45.0) -> np.ndarray:
+    out = np.empty(width * height, RAY_DTYPE)
+    e = np.asarray(eye, np.float32)
+    _lib.load().ilm_wl_camera_rays(width, height, ptr(e), fov_deg, ptr(out))
+    return out
+
+
+def ball_rays(seed: int = 2, skip: int = 4, n: int = 4194304, n_closest: int | None = None, radius: float = 3.0,
+              tmax_lo: float = 0.1, tmax_hi: float = 4.0) -> np.ndarray:
+    if n_closest is None:
+        n_closest = n // 2
+    out = np.empty(n, RAY_DTYPE)
+    _lib.load().ilm_wl_ball_rays(seed, skip, n, n_closest, radius, tmax_lo, tmax_hi, ptr(out))
+    return out
+
+
+def coherent_workload():
+    """32,768-triangle soup + 65,536 primary rays."""
+    xyz, idx = soup(1, 32768, 0.02)
+    return xyz, idx, camera_rays(256, 256, (0.5, 0.5, -1.5), 45.0)
+
+
+def incoherent_workload(n_rays: int = 4194304, level: int = 8):
+    """Displaced icosphere + ball rays (first half closest, second half shadow)."""
+    xyz, idx = icosphere(level, 2, 0.05, 1.0)
+    rays = ball_rays(2, 4, n_rays, n_rays // 2, 3.0, 0.1, 4.0)
+    return xyz, idx, rays
