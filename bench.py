@@ -71,7 +71,7 @@ class ClockSampler:
         try:
             self.f = open(self.path, "w")
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={gpu_index}", f"--query-gpu={q}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
                                          stdout=self.f, stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
@@ -169,7 +169,7 @@ def run_ours(args):
     dev = torch.device("cuda", local)
 
     xyz, idx, rays = wl.incoherent_workload(N_RAYS)
-    ctx = rb.Context(local)
+    ctx = rb.Context(local, grid_schedule=(args.schedule == "grid"))
     t0 = time.perf_counter()
     acc = rb.GpuBVHAccel(ctx, [rb.TriangleMesh(ctx, xyz, idx)], width=args.width)
     build_s = time.perf_counter() - t0
@@ -190,12 +190,19 @@ def run_ours(args):
             dist.barrier()
         torch.cuda.synchronize(dev)
 
-    def timed(fn, steps, warmup):
+    def timed(fn, steps, warmup, min_warm_s=0.0):
         evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
-        with torch.cuda.stream(stream):
-            for _ in range(warmup):
+        t_start = time.perf_counter()
+        k = 0
+        # at least `warmup` untimed steps, and at least min_warm_s of them so the
+        # clock sampler is running under load before the timed region
+        while k < warmup or time.perf_counter() - t_start < min_warm_s:
+            with torch.cuda.stream(stream):
                 flush.zero_()
                 fn()
+            if k % 8 == 7:
+                stream.synchronize()
+            k += 1
         barrier()
         with torch.cuda.stream(stream):
             for a, b in evs:
@@ -212,8 +219,8 @@ def run_ours(args):
     def trace_any():
         acc.intersect_p_batch(d_shadow, d_occ, stream=stream)
 
-    sampler = ClockSampler(local) if rank == 0 else None
-    ms = timed(trace_closest, args.steps, args.warmup)
+    sampler = ClockSampler(local) if rank == 0 and not args.no_clocks else None
+    ms = timed(trace_closest, args.steps, args.warmup, min_warm_s=1.0 if sampler else 0.0)
     clocks = sampler.stop() if sampler else None
     ms_any = timed(trace_any, args.steps, args.warmup)
 
@@ -260,6 +267,7 @@ def run_ours(args):
             "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded procedural scene and rays)",
             "config": {"workload": WORKLOAD, "bvh_width": args.width, "max_prims_in_node": 4,
+                       "schedule": args.schedule,
                        "l2": "flushed between steps (256 MiB write outside the timed launches)",
                        "parallelism": "replicas" if world > 1 else "single GPU"},
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
@@ -296,7 +304,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--width", type=int, default=8, choices=[2, 4, 8])
+    ap.add_argument("--schedule", default="persistent", choices=["persistent", "grid"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-clocks", action="store_true", help="skip nvidia-smi clock sampling (profiler runs)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -78,6 +78,10 @@ typedef struct {
  * tmax >= 0) before any launch; an invalid ray fails the call with
  * ILM_ERR_INVALID_ARGUMENT. */
 #define ILM_FLAG_VALIDATE_RAYS 1
+/* Wide layouts: one thread per ray instead of the default persistent schedule
+ * (warps claim rays in chunks from a per-stream device counter and refill
+ * finished lanes). */
+#define ILM_FLAG_GRID_SCHEDULE 2
 
 typedef struct {
     int32_t width;             /* 2 (the reference's binary layout), 4 or 8 */

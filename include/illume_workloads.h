@@ -49,6 +49,24 @@ void ilm_wl_camera_rays(uint32_t width, uint32_t height, const float eye[3], flo
 void ilm_wl_ball_rays(uint64_t seed, uint64_t skip, uint64_t n, uint64_t n_closest,
                       float radius, float tmax_lo, float tmax_hi, ilm_ray* out);
 
+/* Procedural Cornell box in [0,1]^3 (y up, open towards -z):
+ *   floor y=0, ceiling y=1, back wall z=1 (white 0.73), left wall x=0 (red
+ *   0.63/0.065/0.05), right wall x=1 (green 0.14/0.45/0.09), 2 triangles each;
+ *   ceiling light quad x,z in [0.375,0.625] at y=0.999, emitting 15 downwards
+ *   (both triangles' normals (p0-p2)x(p1-p2) point -y), 2 triangles;
+ *   tall box 0.3x0.6x0.3 centred (0.33, 0.3, 0.65) rotated +18 deg about y and
+ *   short box 0.3x0.3x0.3 centred (0.66, 0.15, 0.33) rotated -18 deg, white,
+ *   12 triangles each; displaced icosphere (see ilm_wl_icosphere) of
+ *   `ico_level`, radius 0.2, amplitude 0.05, phases from Rng::new(seed),
+ *   centred (0.66, 0.52, 0.33), white.
+ * Materials: 0 white, 1 red, 2 green, 3 light (albedo 0, emission 15).
+ * Camera for this scene: eye (0.5, 0.5, -1.37), looking +z, fov 40 deg.
+ * mat: one material index per triangle; albedo / emission: 4 x RGB. */
+#define ILM_CORNELL_N_MATERIALS 4
+void ilm_wl_cornell_counts(uint32_t ico_level, uint32_t* nv, uint32_t* nt);
+void ilm_wl_cornell(uint32_t ico_level, uint64_t seed, float* xyz, uint32_t* idx, uint32_t* mat,
+                    float* albedo, float* emission);
+
 #ifdef __cplusplus
 }
 #endif

@@ -54,6 +54,10 @@ _SIG = {
     "orc_sphere_intersect": (ctypes.c_int, [_P, _P, ctypes.c_int, _P]),
     "orc_sphere_world_bound": (None, [_P, _P]),
     "orc_last_trace_seconds": (ctypes.c_double, []),
+    "orc_render_pt": (ctypes.c_int, [_P, _P, _P, ctypes.c_uint32, _P, _P, _P, _P, ctypes.c_float, ctypes.c_uint32,
+                                     ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32,
+                                     ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32,
+                                     ctypes.c_uint32, ctypes.c_int, _P, _P]),
 }
 
 _lib = None
@@ -170,6 +174,25 @@ class Scene:
         ovf = load().orc_intersect_p(self.h, _p(rays), len(rays), _p(occ), _p(nv), _p(nt), threads)
         assert ovf == 0, f"{ovf} rays overflowed the 64-entry traversal stack"
         return (occ, nv, nt) if counters else occ
+
+
+def render_pt(scene: "Scene", xyz, idx, mat, albedo, emission, eye, fov_deg, width, height, spp, max_depth=8,
+              rr_depth=3, seed=3, window=None, threads=0):
+    """Path-traced image (oracle/pt.cpp).  Returns (rgb[h, w, 3], (closest rays, shadow rays))."""
+    x0, y0, x1, y1 = window if window else (0, 0, width, height)
+    xyz = np.ascontiguousarray(xyz, np.float32)
+    idx = np.ascontiguousarray(idx, np.uint32)
+    mat = np.ascontiguousarray(mat, np.uint32)
+    albedo = np.ascontiguousarray(albedo, np.float32)
+    emission = np.ascontiguousarray(emission, np.float32)
+    eye = np.asarray(eye, np.float32)
+    out = np.zeros((y1 - y0, x1 - x0, 3), np.float32)
+    counts = np.zeros(2, np.uint64)
+    st = load().orc_render_pt(scene.h, _p(xyz), _p(idx), len(idx), _p(mat), _p(albedo), _p(emission), _p(eye),
+                              fov_deg, width, height, spp, max_depth, rr_depth, seed, x0, y0, x1, y1, threads,
+                              _p(out), _p(counts))
+    assert st == 0, "invalid render arguments"
+    return out, (int(counts[0]), int(counts[1]))
 
 
 def last_trace_seconds() -> float:

@@ -87,6 +87,23 @@ int orc_triangle_intersect(const float* p0, const float* p1, const float* p2,
 int orc_sphere_intersect(const orc_sphere_desc* s, const orc_ray* r, int closest, float* out);
 void orc_sphere_world_bound(const orc_sphere_desc* s, float out[6]);
 
+/* Single-ray forms (used by the path-tracer restatement). Return 1 on stack overflow. */
+int orc_trace_closest1(void* scene, const orc_ray* ray, orc_hit* hit);
+int orc_trace_any1(void* scene, const orc_ray* ray, uint8_t* occluded);
+
+/* Path tracer (oracle/pt.cpp): renders pixels [x0,x1) x [y0,y1) of a
+ * width x height pinhole image (eye, looking +z, up +y, vertical fov) with
+ * spp stratified samples (spp must be a square), Lambertian triangles
+ * (albedo[3*material]) and one-sided diffuse emitters (emission[3*material]),
+ * max_depth bounces, Russian roulette from bounce rr_depth.  `scene` must have
+ * been created from the same triangles.  rgb_out: 3 floats per pixel, row-major
+ * over the window; ray_counts: {closest-hit rays, shadow rays}. */
+int orc_render_pt(void* scene, const float* verts, const uint32_t* idx, uint32_t nt,
+                  const uint32_t* prim_material, const float* albedo, const float* emission,
+                  const float eye[3], float fov_deg, uint32_t width, uint32_t height, uint32_t spp,
+                  uint32_t max_depth, uint32_t rr_depth, uint64_t seed, uint32_t x0, uint32_t y0,
+                  uint32_t x1, uint32_t y1, int nthreads, float* rgb_out, uint64_t* ray_counts);
+
 /* Wall-clock seconds spent by the last orc_intersect/_p call (traversal only). */
 double orc_last_trace_seconds(void);
 

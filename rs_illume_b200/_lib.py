@@ -22,6 +22,8 @@ ILM_ERR_TRAVERSAL_LIMIT = -4
 ILM_ERR_TIMEOUT = -5
 ILM_ERR_NOT_FOUND = -6
 ILM_ERR_NO_DEVICE = -7
+ILM_FLAG_VALIDATE_RAYS = 1
+ILM_FLAG_GRID_SCHEDULE = 2
 ILM_MISS = 0xFFFFFFFF
 ILM_TRAVERSAL_ERROR = 0xFFFFFFFE
 
@@ -103,6 +105,8 @@ SIGNATURES = {
     "ilm_wl_icosphere": (None, [_U32, _U64, _F, _F, _P, _P, _P]),
     "ilm_wl_camera_rays": (None, [_U32, _U32, _P, _F, _P]),
     "ilm_wl_ball_rays": (None, [_U64, _U64, _U64, _U64, _F, _F, _F, _P]),
+    "ilm_wl_cornell_counts": (None, [_U32, ctypes.POINTER(_U32), ctypes.POINTER(_U32)]),
+    "ilm_wl_cornell": (None, [_U32, _U64, _P, _P, _P, _P, _P]),
 }
 
 _lib = None

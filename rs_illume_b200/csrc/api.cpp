@@ -289,7 +289,8 @@ static int32_t intersect_impl(ilm_context* ctx, ilm_accel_id accel, const ilm_ra
         return ILM_ERR_NOT_FOUND;
     }
     DeviceAccel da = a->view();
-    LaunchParams lp{ctx->stack_depth, ctx->block_size, ctx->max_iter};
+    const int persistent = (ctx->flags & ILM_FLAG_GRID_SCHEDULE) ? 0 : 1;
+    LaunchParams lp{ctx->stack_depth, ctx->block_size, ctx->max_iter, persistent, nullptr};
     uint32_t* err = static_cast<uint32_t*>(ctx->err_word.ptr);
     cudaStream_t user = stream ? static_cast<cudaStream_t>(stream) : ctx->stream;
     PtrKind kr = classify(rays), ko = classify(out);
@@ -297,7 +298,12 @@ static int32_t intersect_impl(ilm_context* ctx, ilm_accel_id accel, const ilm_ra
         set_error(ctx, "rays and results must both be device memory or both host memory");
         return ILM_ERR_INVALID_ARGUMENT;
     }
+    auto counter = [&](cudaStream_t s) -> unsigned long long* {
+        return persistent ? ctx->counter_for(s) : nullptr;
+    };
     if (kr == PtrKind::kDevice) {
+        lp.counter = counter(user);
+        if (persistent && !lp.counter) return ILM_ERR_OUT_OF_MEMORY;
         ILM_CUDA(ctx, launch_trace(da, rays, n, hits, occ, err, lp, user), "trace launch");
         return ILM_OK;
     }
@@ -335,6 +341,8 @@ static int32_t intersect_impl(ilm_context* ctx, ilm_accel_id accel, const ilm_ra
         Stage& st = ctx->stage[slot];
         ILM_CUDA(ctx, cudaMemcpyAsync(st.rays.ptr, rays + off, cnt * sizeof(ilm_ray), cudaMemcpyHostToDevice, s),
                  "cudaMemcpyAsync(rays)");
+        lp.counter = counter(s);
+        if (persistent && !lp.counter) return ILM_ERR_OUT_OF_MEMORY;
         ILM_CUDA(ctx,
                  launch_trace(da, static_cast<const ilm_ray*>(st.rays.ptr), cnt,
                               occ ? nullptr : static_cast<ilm_hit*>(st.out.ptr),

@@ -52,6 +52,7 @@ struct Accel {
         a.prims = static_cast<const PrimRec*>(d_prims.ptr);
         a.n_records = (uint32_t)host.records.size();
         a.spheres = static_cast<const SphereRec*>(d_spheres.ptr);
+        for (int k = 0; k < 6; ++k) a.bound[k] = host.bound[k];
         return a;
     }
 };
@@ -83,7 +84,21 @@ struct ilm_context {
     std::map<ilm_accel_id, std::unique_ptr<ilm::Accel>> accels;
     ilm_mesh_id next_mesh = 1;
     ilm_accel_id next_accel = 1;
-    void scratch_release() {}
+    // Work counters of the persistent schedule, one per stream: launches on one
+    // stream run in order, so a counter is never shared by two live launches.
+    std::map<cudaStream_t, std::unique_ptr<ilm::DeviceBuffer>> counters;
+    unsigned long long* counter_for(cudaStream_t s) {
+        auto& b = counters[s];
+        if (!b) {
+            b.reset(new ilm::DeviceBuffer());
+            if (b->reserve(sizeof(unsigned long long)) != cudaSuccess) {
+                counters.erase(s);
+                return nullptr;
+            }
+        }
+        return static_cast<unsigned long long*>(b->ptr);
+    }
+    void scratch_release() { counters.clear(); }
 };
 
 namespace ilm {

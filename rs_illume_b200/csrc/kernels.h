@@ -16,16 +16,41 @@ struct DeviceAccel {
     const PrimRec* prims;      // traversal-ordered primitive records
     uint32_t n_records;
     const SphereRec* spheres;
+    float bound[6];            // world bound (root box), min xyz / max xyz
 };
 
 struct LaunchParams {
     int stack_depth;           // > 32 selects the 64-entry stack variant
     int block_size;
     uint32_t max_iter;         // per-ray loop cap
+    int persistent;            // wide layouts: persistent schedule (needs `counter`)
+    unsigned long long* counter;   // device work counter, private to the launch's stream
+};
+
+// Everything a trace kernel reads, passed by value.
+struct TraceArgs {
+    const void* nodes;
+    uint32_t n_nodes;
+    const PrimRec* prims;
+    const SphereRec* spheres;
+    const ilm_ray* rays;
+    uint64_t n;                        // ray count (upper bound when n_dev is set)
+    const unsigned long long* n_dev;   // optional device-side ray count
+    ilm_hit* hits;                     // closest hit output (any-hit: null)
+    uint32_t* occ;                     // any-hit output (closest: null)
+    uint32_t* err;
+    uint32_t max_iter;
+    unsigned long long* counter;       // persistent-schedule work counter
+    float bound[6];
 };
 
 // occ == nullptr: closest hit into `hits`; otherwise any-hit into `occ`.
+// When n_dev is non-null the kernels trace min(*n_dev, n) rays.
 cudaError_t launch_trace(const DeviceAccel& a, const ilm_ray* rays, uint64_t n, ilm_hit* hits, uint32_t* occ,
-                         uint32_t* err, const LaunchParams& lp, cudaStream_t s);
+                         uint32_t* err, const LaunchParams& lp, cudaStream_t s,
+                         const unsigned long long* n_dev = nullptr);
+
+cudaError_t launch_trace_binary(const TraceArgs& t, cudaStream_t s);
+cudaError_t launch_trace_wide(int width, const TraceArgs& t, const LaunchParams& lp, cudaStream_t s);
 
 }  // namespace ilm

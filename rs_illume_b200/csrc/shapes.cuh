@@ -167,7 +167,7 @@ __device__ __forceinline__ EF ef_div(EF a, EF b) {
 // Transform::transform_ray_with_error (core/transform.rs:392-435).  The
 // refine step uses the Euclidean distance (point3.rs:62-66 computes sqrt of a
 // dot product instead).  Returns t and the parametric (u, v).
-__device__ __noinline__ bool sphere_test(const SphereRec& s, float rox, float roy, float roz, float rdx,
+static __device__ __noinline__ bool sphere_test(const SphereRec& s, float rox, float roy, float roz, float rdx,
                                          float rdy, float rdz, float tmax, float& t_out, float& u_out,
                                          float& v_out) {
     const float* m = s.w2o;

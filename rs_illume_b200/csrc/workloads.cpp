@@ -126,6 +126,69 @@ void ilm_wl_camera_rays(uint32_t width, uint32_t height, const float eye[3], flo
         }
 }
 
+void ilm_wl_cornell_counts(uint32_t ico_level, uint32_t* nv, uint32_t* nt) {
+    uint32_t iv, it;
+    ilm_wl_icosphere_counts(ico_level, &iv, &it);
+    *nv = 5 * 4 + 4 + 2 * 8 + iv;
+    *nt = 5 * 2 + 2 + 2 * 12 + it;
+}
+
+void ilm_wl_cornell(uint32_t ico_level, uint64_t seed, float* xyz, uint32_t* idx, uint32_t* mat, float* albedo,
+                    float* emission) {
+    const float alb[4][3] = {{0.73f, 0.73f, 0.73f}, {0.63f, 0.065f, 0.05f}, {0.14f, 0.45f, 0.09f}, {0, 0, 0}};
+    const float emi[4][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}, {15.0f, 15.0f, 15.0f}};
+    for (int m = 0; m < 4; ++m)
+        for (int k = 0; k < 3; ++k) { albedo[3 * m + k] = alb[m][k]; emission[3 * m + k] = emi[m][k]; }
+    uint32_t nv = 0, nt = 0;
+    auto vert = [&](double x, double y, double z) {
+        xyz[3 * nv] = (float)x; xyz[3 * nv + 1] = (float)y; xyz[3 * nv + 2] = (float)z;
+        return nv++;
+    };
+    auto tri = [&](uint32_t a, uint32_t b, uint32_t c, uint32_t m) {
+        idx[3 * nt] = a; idx[3 * nt + 1] = b; idx[3 * nt + 2] = c;
+        mat[nt++] = m;
+    };
+    // quad a-b-c-d as triangles (a,b,c) and (a,c,d)
+    auto quad = [&](const double* a, const double* b, const double* c, const double* d, uint32_t m) {
+        uint32_t ia = vert(a[0], a[1], a[2]), ib = vert(b[0], b[1], b[2]);
+        uint32_t ic = vert(c[0], c[1], c[2]), id = vert(d[0], d[1], d[2]);
+        tri(ia, ib, ic, m);
+        tri(ia, ic, id, m);
+    };
+    const double f0[3] = {0, 0, 0}, f1[3] = {1, 0, 0}, f2[3] = {1, 0, 1}, f3[3] = {0, 0, 1};
+    const double c0[3] = {0, 1, 0}, c1[3] = {1, 1, 0}, c2[3] = {1, 1, 1}, c3[3] = {0, 1, 1};
+    quad(f0, f3, f2, f1, 0);   // floor
+    quad(c0, c1, c2, c3, 0);   // ceiling
+    quad(f3, c3, c2, f2, 0);   // back wall z = 1
+    quad(f0, c0, c3, f3, 1);   // left wall x = 0 (red)
+    quad(f1, f2, c2, c1, 2);   // right wall x = 1 (green)
+    // light: (x0,h,z0) (x1,h,z0) (x1,h,z1) (x0,h,z1) -> both normals -y
+    const double h = 0.999, lx0 = 0.375, lx1 = 0.625, lz0 = 0.375, lz1 = 0.625;
+    const double l0[3] = {lx0, h, lz0}, l1[3] = {lx1, h, lz0}, l2[3] = {lx1, h, lz1}, l3[3] = {lx0, h, lz1};
+    quad(l0, l1, l2, l3, 3);
+    auto box = [&](double cx, double cy, double cz, double sx, double sy, double sz, double deg) {
+        double a = deg * kPiD / 180.0, ca = std::cos(a), sa = std::sin(a);
+        uint32_t base = nv;
+        for (int k = 0; k < 8; ++k) {
+            double x = (k & 1 ? 0.5 : -0.5) * sx, y = (k & 2 ? 0.5 : -0.5) * sy, z = (k & 4 ? 0.5 : -0.5) * sz;
+            vert(cx + ca * x + sa * z, cy + y, cz - sa * x + ca * z);
+        }
+        const int faces[6][4] = {{0, 2, 3, 1}, {4, 5, 7, 6}, {0, 1, 5, 4}, {2, 6, 7, 3}, {0, 4, 6, 2}, {1, 3, 7, 5}};
+        for (auto& fc : faces) {
+            tri(base + fc[0], base + fc[1], base + fc[2], 0);
+            tri(base + fc[0], base + fc[2], base + fc[3], 0);
+        }
+    };
+    box(0.33, 0.3, 0.65, 0.3, 0.6, 0.3, 18.0);
+    box(0.66, 0.15, 0.33, 0.3, 0.3, 0.3, -18.0);
+    uint32_t iv, it;
+    ilm_wl_icosphere_counts(ico_level, &iv, &it);
+    const float centre[3] = {0.66f, 0.52f, 0.33f};
+    ilm_wl_icosphere(ico_level, seed, 0.05f, 0.2f, centre, xyz + 3 * (size_t)nv, idx + 3 * (size_t)nt);
+    for (uint32_t i = 0; i < 3 * it; ++i) idx[3 * (size_t)nt + i] += nv;
+    for (uint32_t i = 0; i < it; ++i) mat[nt + i] = 0;
+}
+
 void ilm_wl_ball_rays(uint64_t seed, uint64_t skip, uint64_t n, uint64_t n_closest,
                       float radius, float tmax_lo, float tmax_hi, ilm_ray* out) {
     ilm::Pcg32 r(seed);

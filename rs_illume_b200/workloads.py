@@ -72,6 +72,24 @@ def ball_rays(seed: int = 2, skip: int = 4, n: int = 4194304, n_closest: int | N
     return out
 
 
+CORNELL_CAMERA = {"eye": (0.5, 0.5, -1.37), "fov_deg": 40.0}
+
+
+def cornell(ico_level: int = 6, seed: int = 3):
+    """Procedural Cornell box (include/illume_workloads.h): returns
+    (xyz, idx, material per triangle, albedo[4,3], emission[4,3])."""
+    lib = _lib.load()
+    nv, nt = ctypes.c_uint32(), ctypes.c_uint32()
+    lib.ilm_wl_cornell_counts(ico_level, ctypes.byref(nv), ctypes.byref(nt))
+    xyz = np.empty((nv.value, 3), np.float32)
+    idx = np.empty((nt.value, 3), np.uint32)
+    mat = np.empty(nt.value, np.uint32)
+    albedo = np.empty((4, 3), np.float32)
+    emission = np.empty((4, 3), np.float32)
+    lib.ilm_wl_cornell(ico_level, seed, ptr(xyz), ptr(idx), ptr(mat), ptr(albedo), ptr(emission))
+    return xyz, idx, mat, albedo, emission
+
+
 def coherent_workload():
     """32,768-triangle soup + 65,536 primary rays."""
     xyz, idx = soup(1, 32768, 0.02)

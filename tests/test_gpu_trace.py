@@ -121,6 +121,21 @@ def test_incoherent_full_size_properties(ctx, incoherent):
     assert ctx.device_errors() == 0
 
 
+@pytest.mark.parametrize("width", [4, 8])
+def test_persistent_and_grid_schedules_agree(incoherent, width):
+    """The persistent schedule (work counter, lane refill) and one thread per
+    ray must produce byte-identical records, for closest and any hit."""
+    xyz, idx, rays, sc = incoherent
+    out = []
+    for grid in (False, True):
+        c = rb.Context(0, grid_schedule=grid, stack_depth=32 if width == 4 else 64)
+        acc = rb.GpuBVHAccel(c, [rb.TriangleMesh(c, xyz, idx)], width=width)
+        out.append((acc.intersect_batch(rays[:1 << 20]).tobytes(), acc.intersect_p_batch(rays[1 << 21:]).tobytes()))
+        assert c.device_errors() == 0
+        c.close()
+    assert out[0] == out[1]
+
+
 def sphere_scene():
     rng = np.random.default_rng(5)
     centres = rng.uniform(-1, 1, (64, 3))
@@ -166,10 +181,10 @@ def test_device_pointers_and_stream(ctx, incoherent):
     s.synchronize()
     g = d_hits.cpu().numpy().view(HIT_DTYPE)
     assert g.tobytes() == acc.intersect_batch(host).tobytes()
-    d_occ = torch.empty(n, dtype=torch.uint32, device="cuda")
+    d_occ = torch.empty(n, dtype=torch.int32, device="cuda")
     acc.intersect_p_batch(d_rays, d_occ)
     torch.cuda.synchronize()
-    assert np.array_equal(d_occ.cpu().numpy(), acc.intersect_p_batch(host))
+    assert np.array_equal(d_occ.cpu().numpy().view(np.uint32), acc.intersect_p_batch(host))
 
 
 def test_edge_cases(ctx):
