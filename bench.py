@@ -169,7 +169,8 @@ def run_ours(args):
     dev = torch.device("cuda", local)
 
     xyz, idx, rays = wl.incoherent_workload(N_RAYS)
-    ctx = rb.Context(local, grid_schedule=(args.schedule == "grid"))
+    ctx = rb.Context(local, grid_schedule=(args.schedule == "grid"), high_occupancy=args.high_occupancy,
+                     stack_depth=args.stack_depth)
     t0 = time.perf_counter()
     acc = rb.GpuBVHAccel(ctx, [rb.TriangleMesh(ctx, xyz, idx)], width=args.width)
     build_s = time.perf_counter() - t0
@@ -240,6 +241,20 @@ def run_ours(args):
             e2e_s.append(t)
     barrier()
     err = ctx.device_errors()
+    # the host link alone: plain pinned copies of the same bytes, for context
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    link = []
+    for _ in range(3):
+        ev[0].record(stream)
+        with torch.cuda.stream(stream):
+            d_closest.copy_(h_rays, non_blocking=True)
+            ev[1].record(stream)
+            h_hits.copy_(d_hits, non_blocking=True)
+            ev[2].record(stream)
+        stream.synchronize()
+        link.append((ev[0].elapsed_time(ev[1]), ev[1].elapsed_time(ev[2])))
+    h2d_ms = min(x[0] for x in link)
+    d2h_ms = min(x[1] for x in link)
 
     tot = sum(ms) / 1e3
     tot_any = sum(ms_any) / 1e3
@@ -267,7 +282,8 @@ def run_ours(args):
             "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded procedural scene and rays)",
             "config": {"workload": WORKLOAD, "bvh_width": args.width, "max_prims_in_node": 4,
-                       "schedule": args.schedule,
+                       "schedule": args.schedule, "high_occupancy": args.high_occupancy,
+                       "stack_depth": args.stack_depth,
                        "l2": "flushed between steps (256 MiB write outside the timed launches)",
                        "parallelism": "replicas" if world > 1 else "single GPU"},
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
@@ -275,7 +291,10 @@ def run_ours(args):
                          "peak_source": f"{peak_kind} hbm_gbs",
                          "bytes_per_ray": round(BYTES_PER_RAY_CLOSEST, 3)},
             "e2e": {"value": round(e2e_value, 3), "unit": UNIT, "h2d_bytes_per_step": N_CLOSEST * 32,
-                    "d2h_bytes_per_step": N_CLOSEST * 16},
+                    "d2h_bytes_per_step": N_CLOSEST * 16,
+                    "pcie_h2d_gbs": round(N_CLOSEST * 32 / h2d_ms / 1e6, 1),
+                    "pcie_d2h_gbs": round(N_CLOSEST * 16 / d2h_ms / 1e6, 1),
+                    "link_bound_mrays_s": round(N_CLOSEST / max(h2d_ms, d2h_ms) / 1e3, 1)},
             "gpu_launches": args.steps,
             "clocks": clocks,
             "anyhit": {"value": round(any_value, 3), "unit": UNIT, "rays": N_CLOSEST,
@@ -305,6 +324,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--width", type=int, default=8, choices=[2, 4, 8])
     ap.add_argument("--schedule", default="persistent", choices=["persistent", "grid"])
+    ap.add_argument("--high-occupancy", action="store_true", help="64-register persistent kernel variant")
+    ap.add_argument("--stack-depth", type=int, default=64, choices=[32, 64])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-clocks", action="store_true", help="skip nvidia-smi clock sampling (profiler runs)")
     args = ap.parse_args()

@@ -82,6 +82,9 @@ typedef struct {
  * (warps claim rays in chunks from a per-stream device counter and refill
  * finished lanes). */
 #define ILM_FLAG_GRID_SCHEDULE 2
+/* Persistent schedule compiled for 8 resident blocks per SM (64 registers per
+ * thread) instead of the compiler's register choice. */
+#define ILM_FLAG_HIGH_OCCUPANCY 4
 
 typedef struct {
     int32_t width;             /* 2 (the reference's binary layout), 4 or 8 */

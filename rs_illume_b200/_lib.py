@@ -24,6 +24,7 @@ ILM_ERR_NOT_FOUND = -6
 ILM_ERR_NO_DEVICE = -7
 ILM_FLAG_VALIDATE_RAYS = 1
 ILM_FLAG_GRID_SCHEDULE = 2
+ILM_FLAG_HIGH_OCCUPANCY = 4
 ILM_MISS = 0xFFFFFFFF
 ILM_TRAVERSAL_ERROR = 0xFFFFFFFE
 

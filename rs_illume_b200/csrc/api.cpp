@@ -290,7 +290,8 @@ static int32_t intersect_impl(ilm_context* ctx, ilm_accel_id accel, const ilm_ra
     }
     DeviceAccel da = a->view();
     const int persistent = (ctx->flags & ILM_FLAG_GRID_SCHEDULE) ? 0 : 1;
-    LaunchParams lp{ctx->stack_depth, ctx->block_size, ctx->max_iter, persistent, nullptr};
+    LaunchParams lp{ctx->stack_depth, ctx->block_size, ctx->max_iter, persistent, nullptr,
+                    (ctx->flags & ILM_FLAG_HIGH_OCCUPANCY) ? 8 : 0};
     uint32_t* err = static_cast<uint32_t*>(ctx->err_word.ptr);
     cudaStream_t user = stream ? static_cast<cudaStream_t>(stream) : ctx->stream;
     PtrKind kr = classify(rays), ko = classify(out);

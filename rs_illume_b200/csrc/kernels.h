@@ -25,6 +25,7 @@ struct LaunchParams {
     uint32_t max_iter;         // per-ray loop cap
     int persistent;            // wide layouts: persistent schedule (needs `counter`)
     unsigned long long* counter;   // device work counter, private to the launch's stream
+    int min_blocks;            // persistent kernel occupancy hint (8 = 64-register variant)
 };
 
 // Everything a trace kernel reads, passed by value.

@@ -260,8 +260,10 @@ __global__ void __launch_bounds__(128) k_trace_wide(TraceArgs a) {
 
 constexpr uint32_t kChunk = 64;
 
-template <int W, int kStack, bool kAny>
-__global__ void __launch_bounds__(128) k_trace_wide_persistent(TraceArgs a) {
+// kMinBlocks > 0 asks the compiler for that many resident 128-thread blocks
+// per SM (64 registers at 8), trading a few spills for more warps in flight.
+template <int W, int kStack, bool kAny, int kMinBlocks>
+__global__ void __launch_bounds__(128, kMinBlocks) k_trace_wide_persistent(TraceArgs a) {
     const uint64_t n = ray_count(a);
     const unsigned lane = threadIdx.x & 31u;
     const unsigned below = (1u << lane) - 1u;
@@ -303,12 +305,12 @@ __global__ void __launch_bounds__(128) k_trace_wide_persistent(TraceArgs a) {
     }
 }
 
-template <int W, int kStack>
-cudaError_t launch(const TraceArgs& t, const LaunchParams& lp, cudaStream_t s) {
+template <int W, int kStack, int kMinBlocks>
+cudaError_t launch_persistent(const TraceArgs& t, cudaStream_t s) {
     const unsigned block = 128;
-    if (lp.persistent && t.counter) {
-        auto kc = k_trace_wide_persistent<W, kStack, false>;
-        auto ka = k_trace_wide_persistent<W, kStack, true>;
+    {
+        auto kc = k_trace_wide_persistent<W, kStack, false, kMinBlocks>;
+        auto ka = k_trace_wide_persistent<W, kStack, true, kMinBlocks>;
         static int per_sm[2] = {0, 0};
         static int sms = 0;
         int which = t.occ ? 1 : 0;
@@ -329,6 +331,13 @@ cudaError_t launch(const TraceArgs& t, const LaunchParams& lp, cudaStream_t s) {
         else kc<<<(unsigned)grid, block, 0, s>>>(t);
         return cudaGetLastError();
     }
+}
+
+template <int W, int kStack>
+cudaError_t launch(const TraceArgs& t, const LaunchParams& lp, cudaStream_t s) {
+    const unsigned block = 128;
+    if (lp.persistent && t.counter)
+        return lp.min_blocks >= 8 ? launch_persistent<W, kStack, 8>(t, s) : launch_persistent<W, kStack, 1>(t, s);
     unsigned grid = (unsigned)((t.n + block - 1) / block);
     if (t.occ) k_trace_wide<W, kStack, true><<<grid, block, 0, s>>>(t);
     else k_trace_wide<W, kStack, false><<<grid, block, 0, s>>>(t);
