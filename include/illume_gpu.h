@@ -160,6 +160,26 @@ int32_t ilm_intersect_closest(ilm_context* ctx, ilm_accel_id accel, const ilm_ra
 int32_t ilm_intersect_any(ilm_context* ctx, ilm_accel_id accel, const ilm_ray* rays,
                           uint64_t n, uint32_t* occluded, void* stream);
 
+/* Closest hit without allocating (no counterpart in the reference).  For
+ * callers that must not call cudaMalloc/cudaFree once set up: a render loop
+ * with a fixed memory budget, a process whose device memory is owned by a
+ * caching allocator, or a thread that must not stall the device (cudaMalloc
+ * and cudaFree can synchronise it).  Same results as ilm_intersect_closest.
+ * Its scratch is one fixed array that the library holds on every GPU that
+ * loads it, until exit: 3 MiB + 256 B (a work counter, an error word and
+ * staging for up to ILM_NOALLOC_MAX_RAYS rays and hits).
+ *  - n > ILM_NOALLOC_MAX_RAYS fails with ILM_ERR_INVALID_ARGUMENT.
+ *  - The first call on a device resolves the array's address on that device;
+ *    make that first call before any stream capture.
+ *  - All calls share the array: calls that overlap on the GPU race.
+ *    Serialise them (one stream, or wait between calls).
+ *  - Host buffers: returns with the hits in host memory, and
+ *    ILM_ERR_TRAVERSAL_LIMIT if a ray hit the traversal limits.  Device
+ *    buffers: stream-ordered; such rays are only marked in their records. */
+#define ILM_NOALLOC_MAX_RAYS 65536
+int32_t ilm_intersect_closest_noalloc(ilm_context* ctx, ilm_accel_id accel, const ilm_ray* rays,
+                                      uint64_t n, ilm_hit* hits, void* stream);
+
 /* Device error word accumulated by the kernels since the last reset
  * (bit 0: traversal stack overflow, bit 1: iteration cap).  Synchronises. */
 int32_t ilm_device_errors(ilm_context* ctx, uint32_t* out_flags, int32_t reset);

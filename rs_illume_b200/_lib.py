@@ -96,6 +96,7 @@ SIGNATURES = {
     "ilm_host_layout_destroy": (_I32, [_P]),
     "ilm_intersect_closest": (_I32, [_P, _U32, _P, _U64, _P, _P]),
     "ilm_intersect_any": (_I32, [_P, _U32, _P, _U64, _P, _P]),
+    "ilm_intersect_closest_noalloc": (_I32, [_P, _U32, _P, _U64, _P, _P]),
     "ilm_device_errors": (_I32, [_P, ctypes.POINTER(_U32), _I32]),
     "ilm_synchronize": (_I32, [_P, _P, ctypes.c_double]),
     # workloads
