@@ -180,6 +180,50 @@ int32_t ilm_intersect_any(ilm_context* ctx, ilm_accel_id accel, const ilm_ray* r
 int32_t ilm_intersect_closest_noalloc(ilm_context* ctx, ilm_accel_id accel, const ilm_ray* rays,
                                       uint64_t n, ilm_hit* hits, void* stream);
 
+/* ----------------------------------------------------------- path tracing */
+/* Wavefront path tracer over a triangle accel: the PBR-book path loop with
+ * the reference's one-light direct lighting with MIS
+ * (core/integrator.rs:321-494), Lambertian BSDF
+ * (reflection/lambertian_reflection.rs), one-sided diffuse area lights (one
+ * per emissive triangle; Triangle::sample, shapes/triangle.rs:616-642),
+ * cosine BSDF sampling and Russian roulette.  The reference has no
+ * PathIntegrator; its render loop is core/integrator.rs:48-145. */
+typedef struct {
+    const uint32_t* prim_material;  /* material index per primitive (host memory) */
+    const float* albedo;            /* Lambertian reflectance, 3 floats per material */
+    const float* emission;          /* emitted radiance along the triangle normal
+                                       normalize((p0-p2) x (p1-p2)), 3 per material */
+    uint32_t n_materials;
+    float eye[3];                   /* pinhole camera at eye, looking +z, up +y */
+    float fov_deg;                  /* vertical field of view */
+    uint32_t width, height;
+} ilm_pt_scene_desc;
+
+typedef struct {
+    uint32_t spp;          /* samples per pixel: a perfect square, sqrt(spp)^2 jittered strata */
+    uint32_t max_depth;    /* bounces (8 in the benchmark) */
+    uint32_t rr_depth;     /* Russian roulette from this bounce on (3) */
+    uint64_t seed;
+    uint32_t wave_paths;   /* paths in flight per wave (0 = 2^21) */
+    int32_t use_graphs;    /* replay each bounce as a CUDA graph */
+} ilm_pt_opts;
+
+typedef struct {
+    uint64_t closest_rays; /* camera + continuation rays */
+    uint64_t shadow_rays;  /* light-sample and BSDF-sample visibility rays */
+    double seconds;        /* device time of the render (CUDA events) */
+    uint32_t waves;
+} ilm_pt_stats;
+
+typedef uint32_t ilm_pt_scene_id;
+/* Materials and lights for `accel` (triangle meshes only). */
+int32_t ilm_pt_scene_create(ilm_context* ctx, ilm_accel_id accel, const ilm_pt_scene_desc* desc,
+                            ilm_pt_scene_id* out);
+/* Renders width x height RGB (3 floats per pixel, row 0 at the top): the mean
+ * of spp samples per pixel.  rgb_out may be host or device memory. */
+int32_t ilm_render_pt(ilm_context* ctx, ilm_pt_scene_id scene, const ilm_pt_opts* opts, float* rgb_out,
+                      ilm_pt_stats* stats);
+
 /* Device error word accumulated by the kernels since the last reset
  * (bit 0: traversal stack overflow, bit 1: iteration cap).  Synchronises. */
 int32_t ilm_device_errors(ilm_context* ctx, uint32_t* out_flags, int32_t reset);

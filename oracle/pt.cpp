@@ -308,6 +308,10 @@ RGB li(const PtScene& s, V o, V d, Rng& rng, uint32_t max_depth, uint32_t rr_dep
             if (urr < q) break;
             beta = beta * (1.0f / (1.0f - q));
         }
+        // The loop would trace the next segment only to stop at max_depth, and
+        // with Lambertian surfaces that intersection adds no radiance (emission
+        // is added on the camera segment only), so it is not traced.
+        if (bounces + 1 >= max_depth) break;
     }
     return L;
 }

@@ -71,6 +71,22 @@ class ilm_sphere_desc(ctypes.Structure):
                 ("phi_max_deg", ctypes.c_float), ("reverse_orientation", ctypes.c_int32)]
 
 
+class ilm_pt_scene_desc(ctypes.Structure):
+    _fields_ = [("prim_material", ctypes.c_void_p), ("albedo", ctypes.c_void_p), ("emission", ctypes.c_void_p),
+                ("n_materials", ctypes.c_uint32), ("eye", ctypes.c_float * 3), ("fov_deg", ctypes.c_float),
+                ("width", ctypes.c_uint32), ("height", ctypes.c_uint32)]
+
+
+class ilm_pt_opts(ctypes.Structure):
+    _fields_ = [("spp", ctypes.c_uint32), ("max_depth", ctypes.c_uint32), ("rr_depth", ctypes.c_uint32),
+                ("seed", ctypes.c_uint64), ("wave_paths", ctypes.c_uint32), ("use_graphs", ctypes.c_int32)]
+
+
+class ilm_pt_stats(ctypes.Structure):
+    _fields_ = [("closest_rays", ctypes.c_uint64), ("shadow_rays", ctypes.c_uint64), ("seconds", ctypes.c_double),
+                ("waves", ctypes.c_uint32)]
+
+
 _P = ctypes.c_void_p
 _U32 = ctypes.c_uint32
 _U64 = ctypes.c_uint64
@@ -97,6 +113,8 @@ SIGNATURES = {
     "ilm_intersect_closest": (_I32, [_P, _U32, _P, _U64, _P, _P]),
     "ilm_intersect_any": (_I32, [_P, _U32, _P, _U64, _P, _P]),
     "ilm_intersect_closest_noalloc": (_I32, [_P, _U32, _P, _U64, _P, _P]),
+    "ilm_pt_scene_create": (_I32, [_P, _U32, ctypes.POINTER(ilm_pt_scene_desc), ctypes.POINTER(_U32)]),
+    "ilm_render_pt": (_I32, [_P, _U32, ctypes.POINTER(ilm_pt_opts), _P, ctypes.POINTER(ilm_pt_stats)]),
     "ilm_device_errors": (_I32, [_P, ctypes.POINTER(_U32), _I32]),
     "ilm_synchronize": (_I32, [_P, _P, ctypes.c_double]),
     # workloads

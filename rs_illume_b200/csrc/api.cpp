@@ -118,6 +118,7 @@ int32_t ilm_context_destroy(ilm_context* ctx) {
     if (!ctx) return ILM_ERR_INVALID_ARGUMENT;
     cudaSetDevice(ctx->device);
     cudaDeviceSynchronize();
+    ctx->pt_scenes.clear();
     ctx->accels.clear();
     for (auto& st : ctx->stage) { st.rays.release(); st.out.release(); }
     ctx->err_word.release();

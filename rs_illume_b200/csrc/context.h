@@ -67,6 +67,8 @@ enum class PtrKind { kHost, kDevice };
 
 }  // namespace ilm
 
+#include "pt.h"
+
 struct ilm_context {
     int device = 0;
     int stack_depth = 64;
@@ -84,6 +86,8 @@ struct ilm_context {
     std::map<ilm_accel_id, std::unique_ptr<ilm::Accel>> accels;
     ilm_mesh_id next_mesh = 1;
     ilm_accel_id next_accel = 1;
+    std::map<ilm_pt_scene_id, std::unique_ptr<ilm::PtScene>> pt_scenes;
+    ilm_pt_scene_id next_pt = 1;
     // Work counters of the persistent schedule, one per stream: launches on one
     // stream run in order, so a counter is never shared by two live launches.
     std::map<cudaStream_t, std::unique_ptr<ilm::DeviceBuffer>> counters;

@@ -1,0 +1,34 @@
+// Host-side state of the wavefront path tracer (pt.cu).  Included by
+// context.h after DeviceBuffer is defined.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "illume_gpu.h"
+
+namespace ilm {
+
+// Queues and film, reused across renders of one scene (grown on demand).
+struct PtBuffers {
+    DeviceBuffer rays[2], beta[2], rng[2], pid[2];   // path queues (double-buffered)
+    DeviceBuffer hits;
+    DeviceBuffer srays, scontrib, socc;              // shadow queue
+    DeviceBuffer counts;
+    DeviceBuffer film, out;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    ~PtBuffers() {
+        if (ev0) cudaEventDestroy(ev0);
+        if (ev1) cudaEventDestroy(ev1);
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
+struct PtScene {
+    ilm_accel_id accel = 0;
+    ilm_pt_scene_desc desc{};
+    DeviceBuffer d_tri, d_mat, d_lights, d_light_geo;
+    uint32_t n_lights = 0;
+    PtBuffers buf;
+};
+
+}  // namespace ilm

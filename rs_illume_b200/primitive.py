@@ -239,6 +239,47 @@ class GpuBVHAccel:
         return nodes, order
 
 
+class PathTracer:
+    """Wavefront path tracer over a triangle GpuBVHAccel (ilm_pt_scene_create /
+    ilm_render_pt): Lambertian materials, one-sided diffuse emitters, a pinhole
+    camera looking +z."""
+
+    def __init__(self, accel: GpuBVHAccel, prim_material, albedo, emission, eye, fov_deg: float, width: int,
+                 height: int):
+        self.accel = accel
+        ctx = accel.ctx
+        self._mat = np.ascontiguousarray(prim_material, np.uint32)
+        self._alb = np.ascontiguousarray(albedo, np.float32).reshape(-1, 3)
+        self._emi = np.ascontiguousarray(emission, np.float32).reshape(-1, 3)
+        d = _lib.ilm_pt_scene_desc()
+        d.prim_material = ptr(self._mat)
+        d.albedo = ptr(self._alb)
+        d.emission = ptr(self._emi)
+        d.n_materials = len(self._alb)
+        for k in range(3):
+            d.eye[k] = eye[k]
+        d.fov_deg = fov_deg
+        d.width, d.height = width, height
+        sid = ctypes.c_uint32()
+        ctx.check(ctx._lib.ilm_pt_scene_create(ctx.handle, accel.id, ctypes.byref(d), ctypes.byref(sid)),
+                  "ilm_pt_scene_create")
+        self.id = sid.value
+        self.width, self.height = width, height
+
+    def render(self, spp: int, max_depth: int = 8, rr_depth: int = 3, seed: int = 3, wave_paths: int = 0,
+               use_graphs: bool = True, out=None):
+        """Returns (rgb[h, w, 3] float32 (host) or `out`, stats dict)."""
+        ctx = self.accel.ctx
+        o = _lib.ilm_pt_opts(spp, max_depth, rr_depth, seed, wave_paths, int(use_graphs))
+        st = _lib.ilm_pt_stats()
+        if out is None:
+            out = np.empty((self.height, self.width, 3), np.float32)
+        ctx.check(ctx._lib.ilm_render_pt(ctx.handle, self.id, ctypes.byref(o), ptr(out), ctypes.byref(st)),
+                  "ilm_render_pt")
+        return out, {"closest_rays": st.closest_rays, "shadow_rays": st.shadow_rays, "seconds": st.seconds,
+                     "waves": st.waves}
+
+
 class Scene:
     """Scene (core/scene.rs:10-53): an aggregate plus lights."""
 
