@@ -180,6 +180,56 @@ int32_t ilm_intersect_any(ilm_context* ctx, ilm_accel_id accel, const ilm_ray* r
 int32_t ilm_intersect_closest_noalloc(ilm_context* ctx, ilm_accel_id accel, const ilm_ray* rays,
                                       uint64_t n, ilm_hit* hits, void* stream);
 
+/* ------------------------------------------------------- batched queries */
+/* Many scenes with ray batches of any size, traced by one persistent launch
+ * per BVH width (4 or 8): BVHAccel::intersect / intersect_p of each batch's
+ * accel over its rays.  All buffers are device memory. */
+typedef struct {
+    ilm_accel_id accel;
+    const ilm_ray* rays;
+    uint64_t n;
+    ilm_hit* hits;         /* closest hit output (NULL for any-hit) */
+    uint32_t* occluded;    /* any-hit output (NULL for closest hit) */
+} ilm_batch_desc;
+typedef struct ilm_batch_plan ilm_batch_plan;
+/* Uploads the scene table and captures the launch sequence as a CUDA graph
+ * (runs it once while doing so).  The plan keeps the buffer pointers: launch
+ * it again after refilling the rays. */
+int32_t ilm_batch_plan_create(ilm_context* ctx, const ilm_batch_desc* batches, uint32_t n,
+                              int32_t any_hit, ilm_batch_plan** out);
+/* Replays the plan on `stream`.  Launches of one plan must not overlap. */
+int32_t ilm_batch_plan_launch(ilm_context* ctx, ilm_batch_plan* plan, void* stream);
+int32_t ilm_batch_plan_destroy(ilm_context* ctx, ilm_batch_plan* plan);
+/* One-shot form (builds, launches and waits). */
+int32_t ilm_intersect_batched(ilm_context* ctx, const ilm_batch_desc* batches, uint32_t n,
+                              int32_t any_hit, void* stream);
+
+/* -------------------------------------------------------------- autotune */
+/* Launch choices of one accel. */
+typedef struct {
+    int32_t stack_depth;     /* 32 or 64 */
+    int32_t schedule;        /* 0 persistent, 1 one thread per ray */
+    int32_t high_occupancy;  /* 1: 8 resident blocks per SM (64 registers) */
+} ilm_launch_opts;
+/* Overrides the context's launch choices for queries on `accel`. */
+int32_t ilm_accel_set_launch(ilm_context* ctx, ilm_accel_id accel, const ilm_launch_opts* opts);
+
+typedef struct {
+    int32_t width;           /* best BVH width (2, 4 or 8) */
+    ilm_launch_opts launch;  /* best launch choices at that width */
+    double ms;               /* its median time on the sample */
+    double baseline_ms;      /* width 8, context defaults, same sample */
+    uint32_t n_tried;
+    int32_t from_cache;      /* 1 when answered from the context's cache */
+} ilm_tune_result;
+/* Builds the shapes' accel at widths 2, 4 and 8, times every launch choice on
+ * `sample` (device or host rays; any_hit selects the query) with CUDA events
+ * (median of 3 after a warm-up) and returns the fastest.  Results are cached
+ * in the context per (query kind, log2 of the primitive count, log2 of the
+ * sample size); force = 1 re-measures. */
+int32_t ilm_autotune(ilm_context* ctx, const ilm_mesh_id* meshes, uint32_t n_meshes, const ilm_ray* sample,
+                     uint64_t n, int32_t any_hit, int32_t force, ilm_tune_result* out);
+
 /* ----------------------------------------------------------- path tracing */
 /* Wavefront path tracer over a triangle accel: the PBR-book path loop with
  * the reference's one-light direct lighting with MIS

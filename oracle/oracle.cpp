@@ -74,7 +74,17 @@ static inline V3 offset(const B3& b, const V3& p) {
 
 struct Ray { V3 o, d; float t_max; };
 
-// Bounding3::intersect_p with precomputed inv_dir (bounds3.rs:284-318)
+// D26: a slab distance (bound - o) * inv_dir is NaN exactly when the ray lies
+// in that bounding plane with a zero direction component (0 * inf).  The
+// reference's comparisons then reject the box, although the ray touches it,
+// and its watertight triangle test accepts hits on an edge lying in that
+// plane, so such hits are lost.  The repair treats the slab as unconstrained.
+static inline void unconstrain_nan(float* lo, float* hi) {
+    if (std::isnan(*lo)) *lo = -std::numeric_limits<float>::infinity();
+    if (std::isnan(*hi)) *hi = std::numeric_limits<float>::infinity();
+}
+
+// Bounding3::intersect_p with precomputed inv_dir (bounds3.rs:284-318), D26
 static inline bool box_intersect_p(const orc_bvh_node& n, const Ray& ray, const V3& inv_dir,
                                    const int dir_is_neg[3]) {
     const float* mm[2] = {n.bmin, n.bmax};
@@ -83,6 +93,8 @@ static inline bool box_intersect_p(const orc_bvh_node& n, const Ray& ray, const 
     float t_max = (mm[1 - dir_is_neg[0]][0] - ray.o.x) * inv_dir.x;
     float ty_min = (mm[dir_is_neg[1]][1] - ray.o.y) * inv_dir.y;
     float ty_max = (mm[1 - dir_is_neg[1]][1] - ray.o.y) * inv_dir.y;
+    unconstrain_nan(&t_min, &t_max);
+    unconstrain_nan(&ty_min, &ty_max);
     t_max *= robust;
     ty_max *= robust;
     if (t_min > ty_max || ty_min > t_max) return false;
@@ -90,6 +102,7 @@ static inline bool box_intersect_p(const orc_bvh_node& n, const Ray& ray, const 
     if (ty_max < t_max) t_max = ty_max;
     float tz_min = (mm[dir_is_neg[2]][2] - ray.o.z) * inv_dir.z;
     float tz_max = (mm[1 - dir_is_neg[2]][2] - ray.o.z) * inv_dir.z;
+    unconstrain_nan(&tz_min, &tz_max);
     tz_max *= robust;
     if (t_min > tz_max || tz_min > t_max) return false;
     if (tz_min > t_min) t_min = tz_min;

@@ -87,6 +87,20 @@ class ilm_pt_stats(ctypes.Structure):
                 ("waves", ctypes.c_uint32)]
 
 
+class ilm_batch_desc(ctypes.Structure):
+    _fields_ = [("accel", ctypes.c_uint32), ("rays", ctypes.c_void_p), ("n", ctypes.c_uint64),
+                ("hits", ctypes.c_void_p), ("occluded", ctypes.c_void_p)]
+
+
+class ilm_launch_opts(ctypes.Structure):
+    _fields_ = [("stack_depth", ctypes.c_int32), ("schedule", ctypes.c_int32), ("high_occupancy", ctypes.c_int32)]
+
+
+class ilm_tune_result(ctypes.Structure):
+    _fields_ = [("width", ctypes.c_int32), ("launch", ilm_launch_opts), ("ms", ctypes.c_double),
+                ("baseline_ms", ctypes.c_double), ("n_tried", ctypes.c_uint32), ("from_cache", ctypes.c_int32)]
+
+
 _P = ctypes.c_void_p
 _U32 = ctypes.c_uint32
 _U64 = ctypes.c_uint64
@@ -113,6 +127,12 @@ SIGNATURES = {
     "ilm_intersect_closest": (_I32, [_P, _U32, _P, _U64, _P, _P]),
     "ilm_intersect_any": (_I32, [_P, _U32, _P, _U64, _P, _P]),
     "ilm_intersect_closest_noalloc": (_I32, [_P, _U32, _P, _U64, _P, _P]),
+    "ilm_batch_plan_create": (_I32, [_P, _P, _U32, _I32, ctypes.POINTER(_P)]),
+    "ilm_batch_plan_launch": (_I32, [_P, _P, _P]),
+    "ilm_batch_plan_destroy": (_I32, [_P, _P]),
+    "ilm_intersect_batched": (_I32, [_P, _P, _U32, _I32, _P]),
+    "ilm_accel_set_launch": (_I32, [_P, _U32, ctypes.POINTER(ilm_launch_opts)]),
+    "ilm_autotune": (_I32, [_P, _P, _U32, _P, _U64, _I32, _I32, ctypes.POINTER(ilm_tune_result)]),
     "ilm_pt_scene_create": (_I32, [_P, _U32, ctypes.POINTER(ilm_pt_scene_desc), ctypes.POINTER(_U32)]),
     "ilm_render_pt": (_I32, [_P, _U32, ctypes.POINTER(ilm_pt_opts), _P, ctypes.POINTER(ilm_pt_stats)]),
     "ilm_device_errors": (_I32, [_P, ctypes.POINTER(_U32), _I32]),

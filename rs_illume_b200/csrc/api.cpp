@@ -290,9 +290,10 @@ static int32_t intersect_impl(ilm_context* ctx, ilm_accel_id accel, const ilm_ra
         return ILM_ERR_NOT_FOUND;
     }
     DeviceAccel da = a->view();
-    const int persistent = (ctx->flags & ILM_FLAG_GRID_SCHEDULE) ? 0 : 1;
-    LaunchParams lp{ctx->stack_depth, ctx->block_size, ctx->max_iter, persistent, nullptr,
-                    (ctx->flags & ILM_FLAG_HIGH_OCCUPANCY) ? 8 : 0};
+    const int persistent = a->schedule >= 0 ? (a->schedule == 0) : !(ctx->flags & ILM_FLAG_GRID_SCHEDULE);
+    const int high_occ = a->high_occupancy >= 0 ? a->high_occupancy : (ctx->flags & ILM_FLAG_HIGH_OCCUPANCY) != 0;
+    LaunchParams lp{a->stack_depth > 0 ? a->stack_depth : ctx->stack_depth, ctx->block_size, ctx->max_iter,
+                    persistent, nullptr, high_occ ? 8 : 0};
     uint32_t* err = static_cast<uint32_t*>(ctx->err_word.ptr);
     cudaStream_t user = stream ? static_cast<cudaStream_t>(stream) : ctx->stream;
     PtrKind kr = classify(rays), ko = classify(out);

@@ -6,6 +6,7 @@
 #include <map>
 #include <memory>
 #include <string>
+#include <tuple>
 #include <vector>
 
 #include "builder.h"
@@ -43,6 +44,8 @@ struct Accel {
     DeviceBuffer d_nodes, d_prims, d_spheres;
     uint64_t device_bytes = 0;
     double build_seconds = 0.0;
+    // per-accel launch choices (ilm_accel_set_launch); -1 = context default
+    int stack_depth = -1, schedule = -1, high_occupancy = -1;
 
     DeviceAccel view() const {
         DeviceAccel a;
@@ -88,6 +91,8 @@ struct ilm_context {
     ilm_accel_id next_accel = 1;
     std::map<ilm_pt_scene_id, std::unique_ptr<ilm::PtScene>> pt_scenes;
     ilm_pt_scene_id next_pt = 1;
+    // autotune results per (any-hit, log2 primitives, log2 sample size)
+    std::map<std::tuple<int, int, int>, ilm_tune_result> tune_cache;
     // Work counters of the persistent schedule, one per stream: launches on one
     // stream run in order, so a counter is never shared by two live launches.
     std::map<cudaStream_t, std::unique_ptr<ilm::DeviceBuffer>> counters;

@@ -60,8 +60,18 @@ __device__ __forceinline__ bool prim_test(const PrimRec* __restrict__ prims, con
                          make_float3(c.x, c.y, c.z), tmax, t, u, v);
 }
 
+// A slab distance is NaN exactly when the ray lies in that bounding plane with
+// a zero direction component (0 * inf); the slab then does not constrain the
+// ray (the reference's comparisons would reject the box and lose hits on
+// edges lying in the plane).
+__device__ __forceinline__ void unconstrain_nan(float& lo, float& hi) {
+    if (isnan(lo)) lo = -INFINITY;
+    if (isnan(hi)) hi = INFINITY;
+}
+
 // Bounds3::intersect_p with precomputed inv_dir / dir_is_neg
-// (geometry/bounds3.rs:284-318), on an explicit box.
+// (geometry/bounds3.rs:284-318), on an explicit box, with NaN slabs
+// unconstrained.
 __device__ __forceinline__ bool box_intersect_p(float minx, float miny, float minz, float maxx, float maxy,
                                                 float maxz, const RayIn& r, float ix, float iy, float iz, bool nx,
                                                 bool ny, bool nz, float tmax) {
@@ -69,6 +79,8 @@ __device__ __forceinline__ bool box_intersect_p(float minx, float miny, float mi
     float t_max = __fmul_rn(__fsub_rn(nx ? minx : maxx, r.ox), ix);
     float ty_min = __fmul_rn(__fsub_rn(ny ? maxy : miny, r.oy), iy);
     float ty_max = __fmul_rn(__fsub_rn(ny ? miny : maxy, r.oy), iy);
+    unconstrain_nan(t_min, t_max);
+    unconstrain_nan(ty_min, ty_max);
     t_max = __fmul_rn(t_max, kBoxRobust);
     ty_max = __fmul_rn(ty_max, kBoxRobust);
     if (t_min > ty_max || ty_min > t_max) return false;
@@ -76,6 +88,7 @@ __device__ __forceinline__ bool box_intersect_p(float minx, float miny, float mi
     if (ty_max < t_max) t_max = ty_max;
     float tz_min = __fmul_rn(__fsub_rn(nz ? maxz : minz, r.oz), iz);
     float tz_max = __fmul_rn(__fsub_rn(nz ? minz : maxz, r.oz), iz);
+    unconstrain_nan(tz_min, tz_max);
     tz_max = __fmul_rn(tz_max, kBoxRobust);
     if (t_min > tz_max || tz_min > t_max) return false;
     if (tz_min > t_min) t_min = tz_min;

@@ -1,0 +1,243 @@
+// Wide-BVH traversal state shared by the single-scene and batched kernels.
+//
+// Nodes are the compressed layout of layout.h: 8-bit child planes on a
+// per-node power-of-two grid, dequantised with one fma each and rounded
+// outward at build time, so every test below is at least as permissive as
+// Bounds3::intersect_p on the exact child box (geometry/bounds3.rs:284-318).
+// Hit children are sorted by entry distance (sorting network on keys that
+// pack the distance's bits with the slot) and pushed far-to-near.
+#pragma once
+#include "trace_common.cuh"
+
+namespace ilm {
+
+template <int W> struct WideWords;
+template <> struct WideWords<8> { static constexpr int kWords = 5; };
+template <> struct WideWords<4> { static constexpr int kWords = 4; };
+
+// Byte i of a W-byte array split over 32-bit words lo (bytes 0-3) and hi (4-7).
+__device__ __forceinline__ uint32_t byte_of(uint32_t lo, uint32_t hi, int i) {
+    return ((i < 4 ? lo : hi) >> (8 * (i & 3))) & 0xFFu;
+}
+
+// Decoded node, with near/far planes already swapped for the ray octant.
+template <int W>
+struct WideView {
+    float ox, oy, oz, sx, sy, sz;
+    uint32_t imask, child_base, prim_base;
+    uint32_t meta[2];
+    uint32_t nq[3][2], fq[3][2];   // near / far quantised planes per axis
+};
+
+template <int W>
+__device__ __forceinline__ WideView<W> load_wide(const uint4* __restrict__ nodes, uint32_t idx, bool negx,
+                                                 bool negy, bool negz) {
+    WideView<W> v;
+    const uint4* p = nodes + (size_t)idx * WideWords<W>::kWords;
+    uint4 w0 = __ldg(p), w1 = __ldg(p + 1), w2 = __ldg(p + 2), w3 = __ldg(p + 3);
+    v.ox = __uint_as_float(w0.x); v.oy = __uint_as_float(w0.y); v.oz = __uint_as_float(w0.z);
+    v.sx = __uint_as_float((w0.w & 0xFFu) << 23);
+    v.sy = __uint_as_float(((w0.w >> 8) & 0xFFu) << 23);
+    v.sz = __uint_as_float(((w0.w >> 16) & 0xFFu) << 23);
+    v.imask = w0.w >> 24;
+    v.child_base = w1.x;
+    v.prim_base = w1.y;
+    uint32_t lo[3][2], hi[3][2];
+    if (W == 8) {
+        uint4 w4 = __ldg(p + 4);
+        v.meta[0] = w1.z; v.meta[1] = w1.w;
+        lo[0][0] = w2.x; lo[0][1] = w2.y; lo[1][0] = w2.z; lo[1][1] = w2.w;
+        lo[2][0] = w3.x; lo[2][1] = w3.y; hi[0][0] = w3.z; hi[0][1] = w3.w;
+        hi[1][0] = w4.x; hi[1][1] = w4.y; hi[2][0] = w4.z; hi[2][1] = w4.w;
+    } else {
+        v.meta[0] = w1.z; v.meta[1] = 0;
+        lo[0][0] = w1.w; lo[1][0] = w2.x; lo[2][0] = w2.y; hi[0][0] = w2.z; hi[1][0] = w2.w;
+        hi[2][0] = w3.x;
+        lo[0][1] = lo[1][1] = lo[2][1] = hi[0][1] = hi[1][1] = hi[2][1] = 0;
+    }
+    bool neg[3] = {negx, negy, negz};
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            v.nq[a][h] = neg[a] ? hi[a][h] : lo[a][h];
+            v.fq[a][h] = neg[a] ? lo[a][h] : hi[a][h];
+        }
+    return v;
+}
+
+// Slab test of child i (Bounds3::intersect_p semantics on the dequantised
+// box; fmaxf/fminf skip a NaN slab, which can only widen the accepted set).
+template <int W>
+__device__ __forceinline__ bool child_hit(const WideView<W>& v, int i, const RayIn& r, float ix, float iy,
+                                          float iz, float tmax, float& tn_out) {
+    uint32_t m = byte_of(v.meta[0], v.meta[1], i);
+    float nx = fmaf((float)byte_of(v.nq[0][0], v.nq[0][1], i), v.sx, v.ox);
+    float fx = fmaf((float)byte_of(v.fq[0][0], v.fq[0][1], i), v.sx, v.ox);
+    float ny = fmaf((float)byte_of(v.nq[1][0], v.nq[1][1], i), v.sy, v.oy);
+    float fy = fmaf((float)byte_of(v.fq[1][0], v.fq[1][1], i), v.sy, v.oy);
+    float nz = fmaf((float)byte_of(v.nq[2][0], v.nq[2][1], i), v.sz, v.oz);
+    float fz = fmaf((float)byte_of(v.fq[2][0], v.fq[2][1], i), v.sz, v.oz);
+    float tnx = __fmul_rn(__fsub_rn(nx, r.ox), ix), tfx = __fmul_rn(__fsub_rn(fx, r.ox), ix);
+    float tny = __fmul_rn(__fsub_rn(ny, r.oy), iy), tfy = __fmul_rn(__fsub_rn(fy, r.oy), iy);
+    float tnz = __fmul_rn(__fsub_rn(nz, r.oz), iz), tfz = __fmul_rn(__fsub_rn(fz, r.oz), iz);
+    float tn = fmaxf(fmaxf(tnx, tny), tnz);
+    float tf = __fmul_rn(fminf(fminf(tfx, tfy), tfz), kBoxRobust);
+    tn_out = tn;
+    return m != 0u && tn <= tf && tn < tmax && tf > 0.0f;
+}
+
+template <int W>
+__device__ __forceinline__ uint32_t child_entry(const WideView<W>& v, uint32_t slot) {
+    uint32_t m = byte_of(v.meta[0], v.meta[1], (int)slot);
+    if ((v.imask >> slot) & 1u) return v.child_base + (m & 31u);
+    return kLeafFlag | ((v.prim_base + (m & 31u)) << 3) | ((m >> 5) - 1u);
+}
+
+__device__ __forceinline__ void cswap(uint32_t& a, uint32_t& b) {
+    uint32_t lo = min(a, b), hi = max(a, b);
+    a = lo; b = hi;
+}
+
+template <int W>
+__device__ __forceinline__ void sort_keys(uint32_t* k) {
+    if (W == 8) {
+        // Batcher odd-even merge sort, 19 comparators
+        cswap(k[0], k[1]); cswap(k[2], k[3]); cswap(k[4], k[5]); cswap(k[6], k[7]);
+        cswap(k[0], k[2]); cswap(k[1], k[3]); cswap(k[4], k[6]); cswap(k[5], k[7]);
+        cswap(k[1], k[2]); cswap(k[5], k[6]);
+        cswap(k[0], k[4]); cswap(k[1], k[5]); cswap(k[2], k[6]); cswap(k[3], k[7]);
+        cswap(k[2], k[4]); cswap(k[3], k[5]);
+        cswap(k[1], k[2]); cswap(k[3], k[4]); cswap(k[5], k[6]);
+    } else {
+        cswap(k[0], k[1]); cswap(k[2], k[3]);
+        cswap(k[0], k[2]); cswap(k[1], k[3]);
+        cswap(k[1], k[2]);
+    }
+}
+
+// Per-lane traversal state of one ray.
+template <int W, int kStack, bool kAny>
+struct WideTracer {
+    RayIn ray;
+    float ix, iy, iz;
+    bool negx, negy, negz, tr_ready, occluded;
+    TriRay tr;
+    float best_t, bu, bv;
+    uint32_t best, status, cur, iter;
+    int sp;
+    uint2 stack[kStack];
+
+    __device__ __forceinline__ void init(const RayIn& r) {
+        ray = r;
+        best_t = r.tmax; bu = 0.0f; bv = 0.0f;
+        best = ILM_MISS;
+        occluded = false;
+        status = 0;
+        ix = __frcp_rn(r.dx); iy = __frcp_rn(r.dy); iz = __frcp_rn(r.dz);   // == 1/d exactly
+        negx = ix < 0.0f; negy = iy < 0.0f; negz = iz < 0.0f;
+        tr_ready = false;
+        cur = 0; iter = 0; sp = 0;
+    }
+
+    // The root box test BVHAccel performs first (the root node's bounds are
+    // the world bound).
+    __device__ __forceinline__ bool enters(const float* b) const {
+        return box_intersect_p(b[0], b[1], b[2], b[3], b[4], b[5], ray, ix, iy, iz, negx, negy, negz, ray.tmax);
+    }
+
+    // Next stacked entry still nearer than the current hit; false when none.
+    __device__ __forceinline__ bool pop() {
+        while (sp > 0) {
+            uint2 e = stack[--sp];
+            if (kAny || __uint_as_float(e.y) < best_t) { cur = e.x; return true; }
+        }
+        return false;
+    }
+
+    // Interior node `cur`: true when the traversal continues into a child.
+    __device__ __forceinline__ bool node(const uint4* __restrict__ nodes) {
+        WideView<W> nv = load_wide<W>(nodes, cur, negx, negy, negz);
+        float lim = kAny ? ray.tmax : best_t;
+        if (kAny) {
+            uint32_t first = 0xFFFFFFFFu;
+#pragma unroll
+            for (int c = 0; c < W; ++c) {
+                float tn;
+                if (child_hit<W>(nv, c, ray, ix, iy, iz, lim, tn)) {
+                    uint32_t e = child_entry<W>(nv, (uint32_t)c);
+                    if (first == 0xFFFFFFFFu) first = e;
+                    else if (sp < kStack) stack[sp++] = make_uint2(e, 0u);
+                    else status = kErrStackOverflow;
+                }
+            }
+            if (first != 0xFFFFFFFFu && !status) { cur = first; return true; }
+            return false;
+        }
+        uint32_t keys[W];
+        int nhit = 0;
+#pragma unroll
+        for (int c = 0; c < W; ++c) {
+            float tn;
+            bool h = child_hit<W>(nv, c, ray, ix, iy, iz, lim, tn);
+            keys[c] = h ? ((__float_as_uint(fmaxf(tn, 0.0f)) & ~7u) | (uint32_t)c) : 0xFFFFFFFFu;
+            nhit += h ? 1 : 0;
+        }
+        if (nhit == 0) return false;
+        sort_keys<W>(keys);
+        if (sp + nhit - 1 > kStack) { status = kErrStackOverflow; return false; }
+#pragma unroll
+        for (int j = W - 1; j >= 1; --j)
+            if (j < nhit) stack[sp++] = make_uint2(child_entry<W>(nv, keys[j] & 7u), keys[j] & ~7u);
+        cur = child_entry<W>(nv, keys[0] & 7u);
+        return true;
+    }
+
+    __device__ __forceinline__ void leaf(const PrimRec* __restrict__ prims, const SphereRec* __restrict__ spheres) {
+        uint32_t start = (cur & ~kLeafFlag) >> 3, cnt = (cur & 7u) + 1u;
+        for (uint32_t k = 0; k < cnt; ++k) {
+            float t, u, v;
+            uint32_t pid;
+            if (kAny) {
+                if (prim_test<false>(prims, spheres, start + k, tr, tr_ready, ray, ray.tmax, t, u, v, pid)) {
+                    occluded = true;
+                    return;
+                }
+            } else if (prim_test<true>(prims, spheres, start + k, tr, tr_ready, ray, best_t, t, u, v, pid) &&
+                       (t < best_t || (t == best_t && pid < best))) {
+                best_t = t; best = pid; bu = u; bv = v;
+            }
+        }
+    }
+
+    // Advances by one node or one leaf; true when the ray is finished.
+    __device__ __forceinline__ bool step(const TraceArgs& a) {
+        if (++iter > a.max_iter) { status = kErrIterationCap; return true; }
+        if (cur & kLeafFlag) {
+            leaf(a.prims, a.spheres);
+            if (kAny && occluded) return true;
+        } else if (node(static_cast<const uint4*>(a.nodes))) {
+            return false;
+        } else if (status) {
+            return true;
+        }
+        return !pop();
+    }
+
+    __device__ __forceinline__ void write(uint64_t i, const TraceArgs& a) const {
+        if (status) atomicOr(a.err, status);
+        if (kAny) {
+            a.occ[i] = status ? kHitTraversalError : (occluded ? 1u : 0u);
+        } else {
+            if (status) store_hit(a.hits, i, kHitTraversalError, ray.tmax, 0.0f, 0.0f);
+            else store_hit(a.hits, i, best, best == ILM_MISS ? ray.tmax : best_t, bu, bv);
+        }
+    }
+};
+
+
+// Warp-level ray claiming of the persistent schedules: kChunk rays per
+// atomicAdd on a device counter.
+constexpr uint32_t kChunk = 64;
+
+}  // namespace ilm

@@ -15,6 +15,7 @@ in csrc/workloads.cpp (declared in include/illume_workloads.h).
 from __future__ import annotations
 
 import ctypes
+import math
 
 import numpy as np
 
@@ -88,6 +89,41 @@ def cornell(ico_level: int = 6, seed: int = 3):
     emission = np.empty((4, 3), np.float32)
     lib.ilm_wl_cornell(ico_level, seed, ptr(xyz), ptr(idx), ptr(mat), ptr(albedo), ptr(emission))
     return xyz, idx, mat, albedo, emission
+
+
+def batched_workload(seed: int = 5, n_scenes: int = 32, tris=(1e3, 2e6), rays=(1e4, 4e6)):
+    """Uneven multi-scene workload: per scene (draws of Rng::new(seed), 4 per
+    scene) a kind (icosphere or triangle soup), a triangle count and a ray
+    count, both log-uniform in the given ranges, and a ray mix of one third
+    primary pinhole rays, one third incoherent ball rays (tmax = inf) and one
+    third shadow rays (tmax ~ U[0.1, 4]).  Icospheres take the subdivision
+    level nearest the target count (at most 8); soups keep their triangle
+    size proportional to count^(-1/3).  Returns a list of dicts."""
+    u = rng_floats(seed, 4 * n_scenes).astype(np.float64)
+    out = []
+    for k in range(n_scenes):
+        uk, ut, ur, us = u[4 * k: 4 * k + 4]
+        t = math.exp(math.log(tris[0]) + ut * (math.log(tris[1]) - math.log(tris[0])))
+        r = int(math.exp(math.log(rays[0]) + ur * (math.log(rays[1]) - math.log(rays[0]))))
+        sub_seed = 1000 + 16 * seed + k
+        if uk < 0.5:
+            level = int(min(8, max(1, round(math.log(t / 20.0, 4)))))
+            xyz, idx = icosphere(level, sub_seed, 0.05, 1.0)
+            eye, radius = (0.0, 0.0, -3.5), 3.0
+        else:
+            n = int(t)
+            xyz, idx = soup(sub_seed, n, 0.02 * (32768.0 / n) ** (1.0 / 3.0))
+            eye, radius = (0.5, 0.5, -1.5), 1.5
+        n1 = r // 3
+        side = max(1, int(math.ceil(math.sqrt(n1))))
+        prim = camera_rays(side, side, eye, 45.0)[:n1]
+        inc = ball_rays(sub_seed, 0, r - n1, (r - n1) // 2, radius, 0.1, 4.0)
+        if uk >= 0.5:   # soups live in the unit cube: centre the ball rays on it
+            inc["o"] += np.float32(0.5)
+        rays_k = np.ascontiguousarray(np.concatenate([prim, inc]))
+        out.append({"kind": "icosphere" if uk < 0.5 else "soup", "xyz": xyz, "idx": idx, "rays": rays_k,
+                    "seed": sub_seed})
+    return out
 
 
 def coherent_workload():

@@ -125,6 +125,25 @@ def test_triangle_parallel_ray_misses():
     assert tri((-1, 0.25, 5), (1, 0, 0)) is None
 
 
+def test_ray_in_bounding_plane_finds_edge_hit():
+    # D26: the triangle's edge (0,0,5)-(0,1,6) lies in the plane x = 0, which is
+    # also its bounding box's min-x plane.  A ray with d.x = 0 travelling in that
+    # plane makes the slab distance (0 - 0) * inf = NaN; the reference's box
+    # test would reject the box, although the watertight test accepts the edge hit.
+    xyz = np.array([[0, 0, 5], [1, 0, 5], [0, 1, 6]], np.float32)
+    idx = np.array([[0, 1, 2]], np.uint32)
+    sc = oracle.Scene(xyz, idx)
+    r = np.zeros(1, oracle.RAY_DTYPE)
+    r["o"][0] = (0.0, 0.25, 0.0)
+    r["d"][0] = (0.0, 0.0, 1.0)
+    r["tmax"][0] = np.inf
+    direct = oracle.triangle_intersect(*xyz, (0.0, 0.25, 0.0), (0.0, 0.0, 1.0))
+    assert direct is not None and direct[0] == 5.25 and direct[2] == 0.0
+    h = sc.intersect(r)[0]
+    assert h["prim"] == 0 and h["t"] == 5.25
+    assert sc.intersect_p(r)[0] == 1
+
+
 # numpy restatement of the watertight test (triangle.rs:156-262)
 def watertight_np(p0, p1, p2, o, d, tmax):
     f = np.float32
