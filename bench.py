@@ -43,6 +43,10 @@ N_NODE_CLOSEST, N_TRI_CLOSEST = 9.957535, 0.294104
 N_NODE_ANY, N_TRI_ANY = 6.984437, 0.182989
 BYTES_PER_RAY_CLOSEST = 32 + 16 + 32 * N_NODE_CLOSEST + 36 * N_TRI_CLOSEST
 BYTES_PER_RAY_ANY = 32 + 4 + 32 * N_NODE_ANY + 36 * N_TRI_ANY
+# DRAM bytes (read + write) of one closest-hit launch on this workload, from the
+# ncu capture summarised in profiles/closest_incoherent_w8.md, per
+# (width, schedule, occupancy, stack depth).
+DRAM_TRAFFIC = {(8, "persistent", "high", 64): 256464896}
 WORKLOAD = ("incoherent closest-hit: displaced icosphere level 8 (1,310,720 tris, seed 2), "
             "2,097,152 closest rays of 4,194,304 ball rays (radius 3, uniform directions)")
 METRIC = "closest-hit Mrays/s"
@@ -169,7 +173,7 @@ def run_ours(args):
     dev = torch.device("cuda", local)
 
     xyz, idx, rays = wl.incoherent_workload(N_RAYS)
-    ctx = rb.Context(local, grid_schedule=(args.schedule == "grid"), high_occupancy=args.high_occupancy,
+    ctx = rb.Context(local, grid_schedule=(args.schedule == "grid"), high_occupancy=(args.occupancy == "high"),
                      stack_depth=args.stack_depth)
     t0 = time.perf_counter()
     acc = rb.GpuBVHAccel(ctx, [rb.TriangleMesh(ctx, xyz, idx)], width=args.width)
@@ -271,18 +275,14 @@ def run_ours(args):
         peak, peak_kind = measured_peaks()
         avg_launch = tot / args.steps
         achieved = BYTES_PER_RAY_CLOSEST * N_CLOSEST / avg_launch / 1e9
-        traffic = None
-        tp = os.path.join(ROOT, "profiles", "traffic.json")
-        if os.path.exists(tp):
-            with open(tp) as f:
-                traffic = json.load(f).get(f"closest_w{args.width}")
+        traffic = DRAM_TRAFFIC.get((args.width, args.schedule, args.occupancy, args.stack_depth))
         line = {
             "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(1e3 * tot / args.steps, 4), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded procedural scene and rays)",
             "config": {"workload": WORKLOAD, "bvh_width": args.width, "max_prims_in_node": 4,
-                       "schedule": args.schedule, "high_occupancy": args.high_occupancy,
+                       "schedule": args.schedule, "occupancy": args.occupancy,
                        "stack_depth": args.stack_depth,
                        "l2": "flushed between steps (256 MiB write outside the timed launches)",
                        "parallelism": "replicas" if world > 1 else "single GPU"},
@@ -324,7 +324,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--width", type=int, default=8, choices=[2, 4, 8])
     ap.add_argument("--schedule", default="persistent", choices=["persistent", "grid"])
-    ap.add_argument("--high-occupancy", action="store_true", help="64-register persistent kernel variant")
+    ap.add_argument("--occupancy", default="high", choices=["high", "default"],
+                    help="high: persistent kernel compiled for 8 resident blocks per SM (64 registers)")
     ap.add_argument("--stack-depth", type=int, default=64, choices=[32, 64])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-clocks", action="store_true", help="skip nvidia-smi clock sampling (profiler runs)")
