@@ -274,6 +274,40 @@ int32_t ilm_pt_scene_create(ilm_context* ctx, ilm_accel_id accel, const ilm_pt_s
 int32_t ilm_render_pt(ilm_context* ctx, ilm_pt_scene_id scene, const ilm_pt_opts* opts, float* rgb_out,
                       ilm_pt_stats* stats);
 
+/* ------------------------------------------------- neural radiance cache */
+/* A small MLP that predicts the radiance leaving a surface point (no
+ * counterpart in the reference; a learned stand-in for the tail of a path).
+ * Inputs per sample: 12 floats = position xyz, outgoing direction xyz (unit),
+ * normal xyz (unit), albedo rgb.  Encoding: 12-frequency sin/cos of the
+ * position normalised to `bound`, one-blob (32 bins) of the direction's and
+ * normal's (theta/pi, phi/2pi), albedo: 203 inputs.  Network: 5 hidden layers
+ * of 64 with ReLU, 3 outputs, no biases, BF16 weights with FP32 accumulation
+ * on tensor cores; FP32 master weights; Adam; loss = mean of
+ * (p - y)^2 / (p^2 + 0.01) with p held constant in the denominator. */
+typedef struct {
+    float lr, beta1, beta2, eps;   /* Adam (1e-2, 0.9, 0.99, 1e-10 in the benchmark) */
+    uint64_t seed;                 /* weight initialisation (He-uniform from PCG32) */
+    float bound[6];                /* scene bound for the position encoding */
+} ilm_nrc_config;
+typedef struct ilm_nrc ilm_nrc;
+#define ILM_NRC_PARAMS 30720       /* FP32 master weights: 64x208, 4 x 64x64, 16x64 (rows 3..15 zero) */
+int32_t ilm_nrc_create(ilm_context* ctx, const ilm_nrc_config* cfg, ilm_nrc** out);
+int32_t ilm_nrc_destroy(ilm_context* ctx, ilm_nrc* nrc);
+/* Reads (get) and/or replaces (set) the FP32 master weights, row-major
+ * [out][in] per layer, layers in order. */
+int32_t ilm_nrc_params(ilm_context* ctx, ilm_nrc* nrc, float* get, const float* set);
+/* out[n][3] = network(inputs[n][12]); host or device buffers. */
+int32_t ilm_nrc_infer(ilm_context* ctx, ilm_nrc* nrc, const float* inputs, uint64_t n, float* out, void* stream);
+/* One Adam step on the batch; *loss (optional) receives the batch loss. */
+int32_t ilm_nrc_train_step(ilm_context* ctx, ilm_nrc* nrc, const float* inputs, const float* targets,
+                           uint64_t n, float* loss, void* stream);
+/* Loss gradient with respect to the master weights (ILM_NRC_PARAMS floats),
+ * without a step (for checking). */
+int32_t ilm_nrc_gradients(ilm_context* ctx, ilm_nrc* nrc, const float* inputs, const float* targets,
+                          uint64_t n, float* grad_out, float* loss);
+/* The 208 bf16 inputs the network sees for each sample (n x 416 bytes). */
+int32_t ilm_nrc_encode(ilm_context* ctx, ilm_nrc* nrc, const float* inputs, uint64_t n, void* enc_out);
+
 /* Device error word accumulated by the kernels since the last reset
  * (bit 0: traversal stack overflow, bit 1: iteration cap).  Synchronises. */
 int32_t ilm_device_errors(ilm_context* ctx, uint32_t* out_flags, int32_t reset);

@@ -135,6 +135,13 @@ SIGNATURES = {
     "ilm_autotune": (_I32, [_P, _P, _U32, _P, _U64, _I32, _I32, ctypes.POINTER(ilm_tune_result)]),
     "ilm_pt_scene_create": (_I32, [_P, _U32, ctypes.POINTER(ilm_pt_scene_desc), ctypes.POINTER(_U32)]),
     "ilm_render_pt": (_I32, [_P, _U32, ctypes.POINTER(ilm_pt_opts), _P, ctypes.POINTER(ilm_pt_stats)]),
+    "ilm_nrc_create": (_I32, [_P, _P, ctypes.POINTER(_P)]),
+    "ilm_nrc_destroy": (_I32, [_P, _P]),
+    "ilm_nrc_params": (_I32, [_P, _P, _P, _P]),
+    "ilm_nrc_infer": (_I32, [_P, _P, _P, _U64, _P, _P]),
+    "ilm_nrc_train_step": (_I32, [_P, _P, _P, _P, _U64, ctypes.POINTER(ctypes.c_float), _P]),
+    "ilm_nrc_gradients": (_I32, [_P, _P, _P, _P, _U64, _P, ctypes.POINTER(ctypes.c_float)]),
+    "ilm_nrc_encode": (_I32, [_P, _P, _P, _U64, _P]),
     "ilm_device_errors": (_I32, [_P, ctypes.POINTER(_U32), _I32]),
     "ilm_synchronize": (_I32, [_P, _P, ctypes.c_double]),
     # workloads

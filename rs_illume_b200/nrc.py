@@ -1,0 +1,105 @@
+"""Neural radiance cache (include/illume_gpu.h, ilm_nrc_*).
+
+Inputs are (n, 12) float32 rows: position, outgoing direction, normal,
+albedo.  Outputs are (n, 3) RGB radiance.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from ._lib import ptr
+from .primitive import Context
+
+N_PARAMS = 30720
+LAYERS = [(64, 208), (64, 64), (64, 64), (64, 64), (64, 64), (16, 64)]   # (out, in)
+
+
+class ilm_nrc_config(ctypes.Structure):
+    _fields_ = [("lr", ctypes.c_float), ("beta1", ctypes.c_float), ("beta2", ctypes.c_float),
+                ("eps", ctypes.c_float), ("seed", ctypes.c_uint64), ("bound", ctypes.c_float * 6)]
+
+
+def split_params(p: np.ndarray):
+    """Flat master weights -> list of (out, in) matrices."""
+    out, off = [], 0
+    for o, i in LAYERS:
+        out.append(p[off: off + o * i].reshape(o, i))
+        off += o * i
+    return out
+
+
+class RadianceCache:
+    def __init__(self, ctx: Context, bound, lr=1e-2, beta1=0.9, beta2=0.99, eps=1e-10, seed=4):
+        self.ctx = ctx
+        c = ilm_nrc_config(lr, beta1, beta2, eps, seed)
+        for k in range(6):
+            c.bound[k] = bound[k]
+        h = ctypes.c_void_p()
+        ctx.check(ctx._lib.ilm_nrc_create(ctx.handle, ctypes.addressof(c), ctypes.byref(h)), "ilm_nrc_create")
+        self.handle = h
+
+    def params(self) -> np.ndarray:
+        p = np.empty(N_PARAMS, np.float32)
+        self.ctx.check(self.ctx._lib.ilm_nrc_params(self.ctx.handle, self.handle, ptr(p), None), "ilm_nrc_params")
+        return p
+
+    def set_params(self, p: np.ndarray) -> None:
+        p = np.ascontiguousarray(p, np.float32)
+        self.ctx.check(self.ctx._lib.ilm_nrc_params(self.ctx.handle, self.handle, None, ptr(p)), "ilm_nrc_params")
+
+    def infer(self, inputs, out=None, stream=None):
+        n = _rows(inputs)
+        if out is None:
+            out = np.empty((n, 3), np.float32)
+        self.ctx.check(self.ctx._lib.ilm_nrc_infer(self.ctx.handle, self.handle, ptr(inputs), n, ptr(out),
+                                                   _stream(stream)), "ilm_nrc_infer")
+        return out
+
+    def train_step(self, inputs, targets, stream=None) -> float:
+        loss = ctypes.c_float()
+        self.ctx.check(self.ctx._lib.ilm_nrc_train_step(self.ctx.handle, self.handle, ptr(inputs), ptr(targets),
+                                                        _rows(inputs), ctypes.byref(loss), _stream(stream)),
+                       "ilm_nrc_train_step")
+        return loss.value
+
+    def gradients(self, inputs, targets):
+        g = np.empty(N_PARAMS, np.float32)
+        loss = ctypes.c_float()
+        self.ctx.check(self.ctx._lib.ilm_nrc_gradients(self.ctx.handle, self.handle, ptr(inputs), ptr(targets),
+                                                       _rows(inputs), ptr(g), ctypes.byref(loss)),
+                       "ilm_nrc_gradients")
+        return g, loss.value
+
+    def encode(self, inputs) -> np.ndarray:
+        """bf16 encodings as float32 (n, 208)."""
+        n = _rows(inputs)
+        raw = np.empty((n, 208), np.uint16)
+        self.ctx.check(self.ctx._lib.ilm_nrc_encode(self.ctx.handle, self.handle, ptr(inputs), n, ptr(raw)),
+                       "ilm_nrc_encode")
+        return (raw.astype(np.uint32) << 16).view(np.float32)
+
+    def close(self) -> None:
+        if getattr(self, "handle", None):
+            self.ctx._lib.ilm_nrc_destroy(self.ctx.handle, self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _rows(a) -> int:
+    if isinstance(a, np.ndarray):
+        return a.size // 12 if a.shape[-1] == 12 else a.shape[0]
+    return a.shape[0]
+
+
+def _stream(stream):
+    if stream is None:
+        return None
+    return stream if isinstance(stream, int) else stream.cuda_stream
