@@ -288,6 +288,8 @@ typedef struct {
     float lr, beta1, beta2, eps;   /* Adam (1e-2, 0.9, 0.99, 1e-10 in the benchmark) */
     uint64_t seed;                 /* weight initialisation (He-uniform from PCG32) */
     float bound[6];                /* scene bound for the position encoding */
+    float ema;                     /* inference uses a moving average of the weights over
+                                      Adam steps with this decay (0.99); 0 = latest weights */
 } ilm_nrc_config;
 typedef struct ilm_nrc ilm_nrc;
 #define ILM_NRC_PARAMS 30720       /* FP32 master weights: 64x208, 4 x 64x64, 16x64 (rows 3..15 zero) */
@@ -307,6 +309,40 @@ int32_t ilm_nrc_gradients(ilm_context* ctx, ilm_nrc* nrc, const float* inputs, c
                           uint64_t n, float* grad_out, float* loss);
 /* The 208 bf16 inputs the network sees for each sample (n x 416 bytes). */
 int32_t ilm_nrc_encode(ilm_context* ctx, ilm_nrc* nrc, const float* inputs, uint64_t n, void* enc_out);
+
+/* Path tracing with the radiance cache (no counterpart in the reference; the
+ * estimator around it is ilm_render_pt's).  Frames of spp_per_frame samples
+ * per pixel are averaged.  A rendering path ends at its first vertex n >= 1
+ * whose path spread satisfies s_n^2 > spread_c * a0 (a0 = d1^2 / (4 pi |cos1|),
+ * s_n = sum_{i=2..n} sqrt(d_i^2 / (pdf_{i-1} |cos_i|))), adding throughput x
+ * the cache's prediction there.  One path in max(16, P / train_paths) (P =
+ * paths per frame) runs to the end and its vertices become training samples
+ * (at most train_samples per frame); after each frame (if `train`) the network
+ * takes train_steps Adam steps on interleaved subsets of them. */
+typedef struct {
+    uint32_t frames;          /* frames to render (0 = until time_budget_s) */
+    uint32_t spp_per_frame;   /* a perfect square (0 = 1) */
+    uint32_t max_depth, rr_depth;
+    uint64_t seed;
+    float spread_c;           /* 0 = 0.01 */
+    uint32_t train_paths;     /* training paths per frame (0 = 16384) */
+    uint32_t train_samples;   /* training samples per frame at most (0 = 65536) */
+    double time_budget_s;     /* stop after the frame that reaches this device time (0 = no budget) */
+    int32_t train;            /* 1: train after every frame; 0: inference only */
+    uint32_t train_steps;     /* Adam steps per frame, each on every train_steps-th sample (0 = 4) */
+} ilm_nrc_render_opts;
+
+typedef struct {
+    uint32_t frames;
+    double seconds;           /* device time of all frames (CUDA events) */
+    uint64_t closest_rays, shadow_rays;
+    uint64_t queries;         /* cache queries answered */
+    uint64_t train_samples;   /* training samples used */
+    float last_loss;          /* network loss on the last frame's training batch */
+} ilm_nrc_render_stats;
+
+int32_t ilm_render_nrc(ilm_context* ctx, ilm_pt_scene_id scene, ilm_nrc* nrc, const ilm_nrc_render_opts* opts,
+                       float* rgb_out, ilm_nrc_render_stats* stats);
 
 /* Device error word accumulated by the kernels since the last reset
  * (bit 0: traversal stack overflow, bit 1: iteration cap).  Synchronises. */

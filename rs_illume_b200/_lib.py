@@ -87,6 +87,19 @@ class ilm_pt_stats(ctypes.Structure):
                 ("waves", ctypes.c_uint32)]
 
 
+class ilm_nrc_render_opts(ctypes.Structure):
+    _fields_ = [("frames", ctypes.c_uint32), ("spp_per_frame", ctypes.c_uint32), ("max_depth", ctypes.c_uint32),
+                ("rr_depth", ctypes.c_uint32), ("seed", ctypes.c_uint64), ("spread_c", ctypes.c_float),
+                ("train_paths", ctypes.c_uint32), ("train_samples", ctypes.c_uint32),
+                ("time_budget_s", ctypes.c_double), ("train", ctypes.c_int32), ("train_steps", ctypes.c_uint32)]
+
+
+class ilm_nrc_render_stats(ctypes.Structure):
+    _fields_ = [("frames", ctypes.c_uint32), ("seconds", ctypes.c_double), ("closest_rays", ctypes.c_uint64),
+                ("shadow_rays", ctypes.c_uint64), ("queries", ctypes.c_uint64), ("train_samples", ctypes.c_uint64),
+                ("last_loss", ctypes.c_float)]
+
+
 class ilm_batch_desc(ctypes.Structure):
     _fields_ = [("accel", ctypes.c_uint32), ("rays", ctypes.c_void_p), ("n", ctypes.c_uint64),
                 ("hits", ctypes.c_void_p), ("occluded", ctypes.c_void_p)]
@@ -142,6 +155,8 @@ SIGNATURES = {
     "ilm_nrc_train_step": (_I32, [_P, _P, _P, _P, _U64, ctypes.POINTER(ctypes.c_float), _P]),
     "ilm_nrc_gradients": (_I32, [_P, _P, _P, _P, _U64, _P, ctypes.POINTER(ctypes.c_float)]),
     "ilm_nrc_encode": (_I32, [_P, _P, _P, _U64, _P]),
+    "ilm_render_nrc": (_I32, [_P, _U32, _P, ctypes.POINTER(ilm_nrc_render_opts), _P,
+                              ctypes.POINTER(ilm_nrc_render_stats)]),
     "ilm_device_errors": (_I32, [_P, ctypes.POINTER(_U32), _I32]),
     "ilm_synchronize": (_I32, [_P, _P, ctypes.c_double]),
     # workloads

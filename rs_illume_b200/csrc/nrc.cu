@@ -360,10 +360,14 @@ __global__ void __launch_bounds__(256) k_mlp_wgrad(const __nv_bfloat16* __restri
 }
 
 // Adam on the FP32 master weights (rows 3..15 of the output layer stay zero),
-// then the bf16 forward and transposed packs.
+// then the bf16 forward and transposed packs.  With ema_a > 0 a step also
+// updates ema = ema_a * ema + (1 - ema_a) * w (ema starts at 0) and the
+// inference pack holds ema / ce (ce = 1 - ema_a^steps, the zero-start
+// correction); without a step the inference pack holds w and ema restarts.
 __global__ void k_adam(float* __restrict__ w, const float* __restrict__ grad, float* __restrict__ m,
                        float* __restrict__ v, float lr, float b1, float b2, float eps, float c1, float c2,
-                       int do_step, __nv_bfloat16* __restrict__ wfwd, __nv_bfloat16* __restrict__ wbwd) {
+                       int do_step, __nv_bfloat16* __restrict__ wfwd, __nv_bfloat16* __restrict__ wbwd,
+                       float* __restrict__ ema, float ema_a, float ce, __nv_bfloat16* __restrict__ winf) {
     int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= kParams) return;
     int l = 0;
@@ -383,6 +387,17 @@ __global__ void k_adam(float* __restrict__ w, const float* __restrict__ grad, fl
     __nv_bfloat16 h = __float2bfloat16_rn(x);
     wfwd[fwd_off(l) + o * fwd_stride(l) + i] = h;
     if (l >= 1) wbwd[bwd_off(l) + i * bwd_stride(l) + o] = h;
+    float xi = x;
+    if (ema_a > 0.0f) {
+        if (do_step) {
+            float e = ema_a * ema[p] + (1.0f - ema_a) * x;
+            ema[p] = e;
+            xi = e / ce;
+        } else {
+            ema[p] = 0.0f;
+        }
+    }
+    winf[fwd_off(l) + o * fwd_stride(l) + i] = __float2bfloat16_rn(xi);
 }
 
 }  // namespace nrc
@@ -394,7 +409,9 @@ using namespace ilm::nrc;
 struct ilm_nrc {
     ilm_nrc_config cfg;
     int step = 0;
+    int ema_steps = 0;                           // Adam steps since the inference weights restarted
     DeviceBuffer w, m, v, grad, wfwd, wbwd;      // params and packs
+    DeviceBuffer ema, winf;                      // moving average and its inference pack
     DeviceBuffer raw, enc, out, target, acts, douts, loss;
     uint32_t cap = 0;
     cudaStream_t stream = nullptr;
@@ -423,12 +440,16 @@ cudaError_t ensure_capacity(ilm_nrc* h, uint32_t n) {
 // Re-packs the bf16 weights (and optionally takes an Adam step).
 cudaError_t adam(ilm_nrc* h, int do_step, cudaStream_t s) {
     if (do_step) h->step += 1;
+    h->ema_steps = do_step ? h->ema_steps + 1 : 0;
     float c1 = 1.0f - std::pow(h->cfg.beta1, (float)(h->step > 0 ? h->step : 1));
     float c2 = 1.0f - std::pow(h->cfg.beta2, (float)(h->step > 0 ? h->step : 1));
+    float ea = h->cfg.ema > 0.0f && h->cfg.ema < 1.0f ? h->cfg.ema : 0.0f;
+    float ce = ea > 0.0f ? 1.0f - (float)std::pow((double)ea, (double)(h->ema_steps > 0 ? h->ema_steps : 1)) : 1.0f;
     k_adam<<<(kParams + 255) / 256, 256, 0, s>>>(
         static_cast<float*>(h->w.ptr), static_cast<const float*>(h->grad.ptr), static_cast<float*>(h->m.ptr),
         static_cast<float*>(h->v.ptr), h->cfg.lr, h->cfg.beta1, h->cfg.beta2, h->cfg.eps, c1, c2, do_step,
-        static_cast<__nv_bfloat16*>(h->wfwd.ptr), static_cast<__nv_bfloat16*>(h->wbwd.ptr));
+        static_cast<__nv_bfloat16*>(h->wfwd.ptr), static_cast<__nv_bfloat16*>(h->wbwd.ptr),
+        static_cast<float*>(h->ema.ptr), ea, ce, static_cast<__nv_bfloat16*>(h->winf.ptr));
     return cudaGetLastError();
 }
 
@@ -452,9 +473,9 @@ cudaError_t forward(ilm_nrc* h, uint32_t n, bool train, float* out_dev, cudaStre
         k_mlp_fwd<true><<<blocks_for(n, 64), 128, smem, s>>>(static_cast<const __nv_bfloat16*>(h->enc.ptr), n,
                                                              static_cast<const __nv_bfloat16*>(h->wfwd.ptr), out_dev,
                                                              static_cast<__nv_bfloat16*>(h->acts.ptr));
-    else
+    else   // inference reads the moving-average pack
         k_mlp_fwd<false><<<blocks_for(n, 64), 128, smem, s>>>(static_cast<const __nv_bfloat16*>(h->enc.ptr), n,
-                                                              static_cast<const __nv_bfloat16*>(h->wfwd.ptr), out_dev,
+                                                              static_cast<const __nv_bfloat16*>(h->winf.ptr), out_dev,
                                                               nullptr);
     return cudaGetLastError();
 }
@@ -501,9 +522,10 @@ int32_t ilm_nrc_create(ilm_context* ctx, const ilm_nrc_config* cfg, ilm_nrc** ou
     h->cfg = *cfg;
     cudaError_t e;
     if ((e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking)) != cudaSuccess) return cuda_fail(ctx, e, "nrc");
-    for (DeviceBuffer* b : {&h->w, &h->m, &h->v, &h->grad})
+    for (DeviceBuffer* b : {&h->w, &h->m, &h->v, &h->grad, &h->ema})
         if ((e = b->reserve(kParams * 4)) != cudaSuccess) return cuda_fail(ctx, e, "nrc");
     if ((e = h->wfwd.reserve(kFwdElems * 2)) != cudaSuccess) return cuda_fail(ctx, e, "nrc");
+    if ((e = h->winf.reserve(kFwdElems * 2)) != cudaSuccess) return cuda_fail(ctx, e, "nrc");
     if ((e = h->wbwd.reserve(kBwdElems * 2)) != cudaSuccess) return cuda_fail(ctx, e, "nrc");
     if ((e = h->loss.reserve(4)) != cudaSuccess) return cuda_fail(ctx, e, "nrc");
     // He-uniform initialisation from PCG32; padded inputs and output rows 3..15 zero
@@ -523,7 +545,9 @@ int32_t ilm_nrc_create(ilm_context* ctx, const ilm_nrc_config* cfg, ilm_nrc** ou
     cudaMemset(h->m.ptr, 0, kParams * 4);
     cudaMemset(h->v.ptr, 0, kParams * 4);
     cudaMemset(h->wfwd.ptr, 0, kFwdElems * 2);
+    cudaMemset(h->winf.ptr, 0, kFwdElems * 2);
     cudaMemset(h->wbwd.ptr, 0, kBwdElems * 2);
+    cudaMemset(h->ema.ptr, 0, kParams * 4);
     cudaFuncSetAttribute(k_mlp_fwd<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kFwdElems * 2);
     cudaFuncSetAttribute(k_mlp_fwd<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kFwdElems * 2);
     if ((e = adam(h.get(), 0, h->stream)) != cudaSuccess) return cuda_fail(ctx, e, "nrc pack");

@@ -1,4 +1,5 @@
-// Wavefront path tracer on the ray-query kernels.
+// Wavefront path tracer on the ray-query kernels, with an optional neural
+// radiance cache.
 //
 // The estimator is the PBR-book path loop with the reference's one-light
 // direct lighting (core/integrator.rs:321-494, with the BSDF-sampled MIS term
@@ -21,9 +22,19 @@
 // Queues are compacted with a warp ballot, a prefix popcount and one atomicAdd
 // per warp.  Queue sizes live in device memory, so a bounce is a fixed launch
 // sequence, captured once per queue parity as a CUDA graph and replayed.
+//
+// Radiance-cache mode (kNrc): each path tracks its spread
+//   a0 = d1^2 / (4 pi |cos1|),  s_n = sum_{i=2..n} sqrt(d_i^2 / (pdf_{i-1} |cos_i|)),
+// and a rendering path ends at vertex n >= 1 once s_n^2 > c * a0: the cache's
+// prediction at that vertex, times the path throughput, replaces the rest of
+// the path.  Training paths (one in `train_stride`) never end early; every
+// vertex they reach records its cache inputs and 1/throughput, and each
+// unoccluded contribution c of the path adds c / beta_k to the target of
+// every earlier vertex k: the target is the reflected radiance the rest of the
+// path estimated there.  After the wave the queries are answered in one
+// batch and the network takes one training step on the recorded vertices.
 #include <cuda_runtime.h>
 
-#include <chrono>
 #include <cmath>
 #include <cstring>
 #include <memory>
@@ -41,7 +52,10 @@ namespace {
 
 // counts[] layout
 enum : int { kQ0 = 0, kQ1 = 1, kShadow = 2, kDepth = 3, kTotClosest = 4, kTotShadow = 5, kDropped = 6,
-             kNumCounts = 8 };
+             kQueries = 7, kTrainSlots = 8, kSamples = 9, kTotQueries = 10, kNumCounts = 12 };
+constexpr uint32_t kNone = 0xFFFFFFFFu;
+constexpr int kRec = 18;   // training vertex: inputs (12), 1/beta (3), target (3)
+constexpr uint32_t kMinTrainStride = 16;   // at most one path in 16 trains (the rest use the cache)
 
 struct PtArgs {
     const float4* tri;        // 3 per primitive: p0 (w = material), p1, p2
@@ -63,6 +77,20 @@ struct PtArgs {
     float4* scontrib;         // contribution rgb, pixel (bits)
     const uint32_t* socc;
     unsigned long long* counts;
+    // radiance-cache mode
+    float4* spread[2];        // s, a0, pdf of the last direction, training slot (bits)
+    float* q_in;              // queries: 12 floats each
+    float4* q_beta;           // throughput rgb, pixel (bits)
+    const float* q_out;       // predictions: 3 floats each
+    uint32_t q_cap;
+    float* t_rec;             // [slot][depth][kRec]
+    uint32_t* t_count;        // vertices recorded per slot
+    uint32_t t_cap, train_stride, train_phase;
+    float spread_c;
+    uint2* s_train;           // per shadow entry: training slot, depth
+    float* t_in;              // gathered training inputs (12 each)
+    float* t_tg;              // gathered training targets (3 each)
+    uint32_t sample_cap;
 };
 
 __device__ __forceinline__ float3 f3(float4 v) { return make_float3(v.x, v.y, v.z); }
@@ -148,6 +176,13 @@ __device__ __forceinline__ uint32_t warp_append(unsigned long long* counter, boo
     return (uint32_t)base + __popc(m & ((1u << lane) - 1u));
 }
 
+__device__ __forceinline__ void put_ray(ilm_ray* q, uint32_t slot, float3 o, float3 d, float tmax) {
+    float4* rr = reinterpret_cast<float4*>(q + slot);
+    rr[0] = make_float4(o.x, o.y, o.z, 0.0f);
+    rr[1] = make_float4(d.x, d.y, d.z, tmax);
+}
+
+template <bool kNrc>
 __global__ void k_pt_camera(PtArgs a, unsigned long long p0, uint32_t count) {
     uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k == 0) {
@@ -156,9 +191,17 @@ __global__ void k_pt_camera(PtArgs a, unsigned long long p0, uint32_t count) {
         a.counts[kShadow] = 0;
         a.counts[kDepth] = 0;
     }
-    if (k >= count) return;
-    uint32_t id = (uint32_t)(p0 + k);
-    uint32_t pixel = id % a.npix, sample = id / a.npix;
+    const bool valid = k < count;
+    const uint32_t id = (uint32_t)(p0 + k);
+    uint32_t slot = kNone;
+    if (kNrc) {
+        // kQueries, kTrainSlots and kSamples are zeroed by the host before this launch
+        bool train = valid && (id % a.train_stride) == a.train_phase;
+        uint32_t s = warp_append(&a.counts[kTrainSlots], train);
+        if (train && s < a.t_cap) { slot = s; a.t_count[s] = 0; }
+    }
+    if (!valid) return;
+    uint32_t pixel = id % a.npix, sample = (id / a.npix) % a.spp;
     uint32_t px = pixel % a.width, py = pixel / a.width;
     Pcg32 rng(path_seq(a.seed, id));
     float jx = rng.uniform_float(), jy = rng.uniform_float();
@@ -167,13 +210,14 @@ __global__ void k_pt_camera(PtArgs a, unsigned long long p0, uint32_t count) {
     float sx = (fx / (float)a.width * 2.0f - 1.0f) * a.tan_half * a.aspect;
     float sy = (1.0f - fy / (float)a.height * 2.0f) * a.tan_half;
     float3 d = normalize3(make_float3(sx, sy, 1.0f));
-    reinterpret_cast<float4*>(a.rays[0])[2 * k] = make_float4(a.eye_x, a.eye_y, a.eye_z, 0.0f);
-    reinterpret_cast<float4*>(a.rays[0])[2 * k + 1] = make_float4(d.x, d.y, d.z, INFINITY);
+    put_ray(a.rays[0], k, make_float3(a.eye_x, a.eye_y, a.eye_z), d, INFINITY);
     a.beta[0][k] = make_float4(1.0f, 1.0f, 1.0f, __uint_as_float(pixel));
     a.rng[0][k] = make_uint2((uint32_t)rng.state, (uint32_t)(rng.state >> 32));
     a.pid[0][k] = id;
+    if (kNrc) a.spread[0][k] = make_float4(0.0f, 0.0f, 0.0f, __uint_as_float(slot));
 }
 
+template <bool kNrc>
 __global__ void __launch_bounds__(256) k_pt_shade(PtArgs a, int cur) {
     const uint32_t n = (uint32_t)a.counts[cur];
     const uint32_t depth = (uint32_t)a.counts[kDepth];
@@ -183,12 +227,14 @@ __global__ void __launch_bounds__(256) k_pt_shade(PtArgs a, int cur) {
     for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += stride) {
         uint32_t i = base + threadIdx.x;
         bool valid = i < n;
-        bool cont = false, push_l = false, push_b = false;
-        ilm_ray ray_l, ray_b, ray_c;
+        bool cont = false, push_l = false, push_b = false, query = false;
+        float3 o_l, d_l, o_b, d_b, o_c, d_c;
+        float tm_l = 0.0f, tm_b = 0.0f;
         float3 c_l = make_float3(0, 0, 0), c_b = make_float3(0, 0, 0);
-        float4 beta_out = make_float4(0, 0, 0, 0);
+        float4 beta_out = make_float4(0, 0, 0, 0), spread_out = make_float4(0, 0, 0, 0);
         uint2 rng_out = make_uint2(0, 0);
-        uint32_t id = 0, pixel = 0;
+        uint32_t id = 0, pixel = 0, slot = kNone;
+        float3 q_p, q_wo, q_n, q_alb, q_beta;
         if (valid) {
             float4 b4 = a.beta[cur][i];
             float3 beta = f3(b4);
@@ -198,6 +244,8 @@ __global__ void __launch_bounds__(256) k_pt_shade(PtArgs a, int cur) {
             Pcg32 rng;
             rng.inc = (path_seq(a.seed, id) << 1u) | 1u;
             rng.state = (uint64_t)rs.x | ((uint64_t)rs.y << 32);
+            float4 sp = kNrc ? a.spread[cur][i] : make_float4(0, 0, 0, 0);
+            if (kNrc) slot = __float_as_uint(sp.w);
             ilm_hit h = a.hits[i];
             const float4* rp = reinterpret_cast<const float4*>(a.rays[cur] + i);
             float4 r1 = rp[1];
@@ -217,128 +265,179 @@ __global__ void __launch_bounds__(256) k_pt_shade(PtArgs a, int cur) {
                     float3 le = f3(a.mat[2 * m + 1]);
                     if (dot3(nrm, wo) > 0.0f) film_add(a, pixel, beta * le);
                 }
-                float3 ss, ts;
-                frame(nrm, ss, ts);
                 float wo_z = dot3(wo, nrm);
-                float u_sel = rng.uniform_float();
-                float ul0 = rng.uniform_float(), ul1 = rng.uniform_float();
-                float us0 = rng.uniform_float(), us1 = rng.uniform_float();
-                // a black BSDF (f = 0) casts no visibility rays and ends the path
-                const bool black = albedo.x == 0.0f && albedo.y == 0.0f && albedo.z == 0.0f;
-                if (a.n_lights > 0 && wo_z != 0.0f && !black) {
-                    uint32_t k = min((uint32_t)(u_sel * (float)a.n_lights), a.n_lights - 1u);
-                    uint32_t lp_id = a.lights[k];
-                    float4 lg = a.light_geo[k];
-                    float3 nl = f3(lg);
-                    float area = lg.w;
-                    float3 q0 = f3(a.tri[3 * lp_id]), q1 = f3(a.tri[3 * lp_id + 1]), q2 = f3(a.tri[3 * lp_id + 2]);
-                    float3 le = f3(a.mat[2 * __float_as_uint(a.tri[3 * lp_id].w) + 1]);
-                    float nlf = (float)a.n_lights;
-                    // light sample (uniform_sample_triangle, sampling.rs:264-267)
-                    float su = sqrtf(ul0);
-                    float c0 = 1.0f - su, c1 = ul1 * su, c2 = 1.0f - c0 - c1;
-                    float3 pl = q0 * c0 + q1 * c1 + q2 * c2;
-                    float3 pl_err = (abs3(q0 * c0) + abs3(q1 * c1) + abs3(q2 * c2)) * 0x1.80000ap-22f;   // gamma(6)
-                    float3 wi = pl - p;
-                    float d2 = dot3(wi, wi);
-                    if (d2 > 0.0f) {
-                        wi = wi * rsqrtf(d2);
-                        float cl = dot3(nl, wi * -1.0f);
-                        float light_pdf = d2 / (fabsf(cl) * area);
-                        float wi_z = dot3(wi, nrm);
-                        bool reflect = wi_z * wo_z > 0.0f;
-                        if (cl > 0.0f && isfinite(light_pdf) && light_pdf > 0.0f && reflect) {
-                            float scat_pdf = fabsf(wi_z) * (1.0f / kPiF);
-                            float w = power_heuristic(light_pdf, scat_pdf);
-                            c_l = beta * albedo * le * ((1.0f / kPiF) * fabsf(wi_z) * w / light_pdf * nlf);
-                            float3 o = offset_origin(p, perr, nrm, pl - p);
-                            float3 tgt = offset_origin(pl, pl_err, nl, o - pl);
-                            float3 dd = tgt - o;
-                            ray_l = {{o.x, o.y, o.z}, 0.0f, {dd.x, dd.y, dd.z}, 1.0f - 0.0001f};
-                            push_l = true;
-                        }
+                bool cache_here = false;
+                if (kNrc) {
+                    float cosv = fmaxf(fabsf(wo_z), 1e-6f);
+                    float t2 = h.t * h.t;
+                    if (depth == 0) { sp.x = 0.0f; sp.y = t2 / (4.0f * kPiF * cosv); }
+                    else sp.x += sqrtf(t2 / (fmaxf(sp.z, 1e-12f) * cosv));
+                    cache_here = slot == kNone && depth >= 1 && sp.x * sp.x > a.spread_c * sp.y;
+                    bool record = slot != kNone && depth < a.max_depth;
+                    if (cache_here || record) {
+                        q_p = p; q_wo = wo; q_n = nrm; q_alb = albedo; q_beta = beta;
                     }
-                    // BSDF sample with MIS
-                    float3 wl = cosine_hemisphere(us0, us1);
-                    if (wo_z < 0.0f) wl.z = -wl.z;
-                    float3 wb = ss * wl.x + ts * wl.y + nrm * wl.z;
-                    float scat_pdf = fabsf(wl.z) * (1.0f / kPiF);
-                    float wb_z = dot3(wb, nrm);
-                    if (scat_pdf > 0.0f && wb_z * wo_z > 0.0f) {
-                        float3 o = offset_origin(p, perr, nrm, wb);
-                        TriRay tr = make_tri_ray(o.x, o.y, o.z, wb.x, wb.y, wb.z);
-                        float tl, lb1, lb2;
-                        if (triangle_test(tr, q0, q1, q2, INFINITY, tl, lb1, lb2)) {
-                            float3 pli = q0 * (1.0f - lb1 - lb2) + q1 * lb1 + q2 * lb2;
-                            float3 dv = pli - p;
-                            float lpdf = dot3(dv, dv) / (fabsf(dot3(nl, wb)) * area);
-                            if (isfinite(lpdf) && lpdf > 0.0f && dot3(nl, wb) < 0.0f) {
-                                float w = power_heuristic(scat_pdf, lpdf);
-                                c_b = beta * albedo * le * ((1.0f / kPiF) * fabsf(wb_z) * w / scat_pdf * nlf);
-                                ray_b = {{o.x, o.y, o.z}, 0.0f, {wb.x, wb.y, wb.z}, tl * (1.0f - 0.0001f)};
-                                push_b = true;
+                    if (record) {
+                        float* rec = a.t_rec + ((size_t)slot * a.max_depth + depth) * kRec;
+                        float in[12] = {p.x, p.y, p.z, wo.x, wo.y, wo.z, nrm.x, nrm.y, nrm.z,
+                                        albedo.x, albedo.y, albedo.z};
+#pragma unroll
+                        for (int q = 0; q < 12; ++q) rec[q] = in[q];
+                        rec[12] = beta.x > 0.0f ? 1.0f / beta.x : 0.0f;
+                        rec[13] = beta.y > 0.0f ? 1.0f / beta.y : 0.0f;
+                        rec[14] = beta.z > 0.0f ? 1.0f / beta.z : 0.0f;
+                        rec[15] = rec[16] = rec[17] = 0.0f;
+                        a.t_count[slot] = depth + 1;
+                    }
+                    query = cache_here;
+                }
+                if (!cache_here) {
+                    float3 ss, ts;
+                    frame(nrm, ss, ts);
+                    float u_sel = rng.uniform_float();
+                    float ul0 = rng.uniform_float(), ul1 = rng.uniform_float();
+                    float us0 = rng.uniform_float(), us1 = rng.uniform_float();
+                    // a black BSDF (f = 0) casts no visibility rays and ends the path
+                    const bool black = albedo.x == 0.0f && albedo.y == 0.0f && albedo.z == 0.0f;
+                    if (a.n_lights > 0 && wo_z != 0.0f && !black) {
+                        uint32_t k = min((uint32_t)(u_sel * (float)a.n_lights), a.n_lights - 1u);
+                        uint32_t lp_id = a.lights[k];
+                        float4 lg = a.light_geo[k];
+                        float3 nl = f3(lg);
+                        float area = lg.w;
+                        float3 q0 = f3(a.tri[3 * lp_id]), q1 = f3(a.tri[3 * lp_id + 1]), q2 = f3(a.tri[3 * lp_id + 2]);
+                        float3 le = f3(a.mat[2 * __float_as_uint(a.tri[3 * lp_id].w) + 1]);
+                        float nlf = (float)a.n_lights;
+                        // light sample (uniform_sample_triangle, sampling.rs:264-267)
+                        float su = sqrtf(ul0);
+                        float c0 = 1.0f - su, c1 = ul1 * su, c2 = 1.0f - c0 - c1;
+                        float3 pl = q0 * c0 + q1 * c1 + q2 * c2;
+                        float3 pl_err = (abs3(q0 * c0) + abs3(q1 * c1) + abs3(q2 * c2)) * 0x1.80000ap-22f;   // gamma(6)
+                        float3 wi = pl - p;
+                        float d2 = dot3(wi, wi);
+                        if (d2 > 0.0f) {
+                            wi = wi * rsqrtf(d2);
+                            float cl = dot3(nl, wi * -1.0f);
+                            float light_pdf = d2 / (fabsf(cl) * area);
+                            float wi_z = dot3(wi, nrm);
+                            bool reflect = wi_z * wo_z > 0.0f;
+                            if (cl > 0.0f && isfinite(light_pdf) && light_pdf > 0.0f && reflect) {
+                                float scat_pdf = fabsf(wi_z) * (1.0f / kPiF);
+                                float w = power_heuristic(light_pdf, scat_pdf);
+                                c_l = beta * albedo * le * ((1.0f / kPiF) * fabsf(wi_z) * w / light_pdf * nlf);
+                                o_l = offset_origin(p, perr, nrm, pl - p);
+                                float3 tgt = offset_origin(pl, pl_err, nl, o_l - pl);
+                                d_l = tgt - o_l;
+                                tm_l = 1.0f - 0.0001f;
+                                push_l = true;
+                            }
+                        }
+                        // BSDF sample with MIS
+                        float3 wl = cosine_hemisphere(us0, us1);
+                        if (wo_z < 0.0f) wl.z = -wl.z;
+                        float3 wb = ss * wl.x + ts * wl.y + nrm * wl.z;
+                        float scat_pdf = fabsf(wl.z) * (1.0f / kPiF);
+                        float wb_z = dot3(wb, nrm);
+                        if (scat_pdf > 0.0f && wb_z * wo_z > 0.0f) {
+                            float3 o = offset_origin(p, perr, nrm, wb);
+                            TriRay tr = make_tri_ray(o.x, o.y, o.z, wb.x, wb.y, wb.z);
+                            float tl, lb1, lb2;
+                            if (triangle_test(tr, q0, q1, q2, INFINITY, tl, lb1, lb2)) {
+                                float3 pli = q0 * (1.0f - lb1 - lb2) + q1 * lb1 + q2 * lb2;
+                                float3 dv = pli - p;
+                                float lpdf = dot3(dv, dv) / (fabsf(dot3(nl, wb)) * area);
+                                if (isfinite(lpdf) && lpdf > 0.0f && dot3(nl, wb) < 0.0f) {
+                                    float w = power_heuristic(scat_pdf, lpdf);
+                                    c_b = beta * albedo * le * ((1.0f / kPiF) * fabsf(wb_z) * w / scat_pdf * nlf);
+                                    o_b = o;
+                                    d_b = wb;
+                                    tm_b = tl * (1.0f - 0.0001f);
+                                    push_b = true;
+                                }
                             }
                         }
                     }
-                }
-                // continuation
-                float u0 = rng.uniform_float(), u1 = rng.uniform_float();
-                float urr = rng.uniform_float();
-                float3 wl = cosine_hemisphere(u0, u1);
-                if (wo_z < 0.0f) wl.z = -wl.z;
-                float3 wi = ss * wl.x + ts * wl.y + nrm * wl.z;
-                float pdf = fabsf(wl.z) * (1.0f / kPiF);
-                float wi_z = dot3(wi, nrm);
-                if (!black && wo_z != 0.0f && pdf > 0.0f && wi_z * wo_z > 0.0f) {
-                    float3 nb = beta * albedo * ((1.0f / kPiF) * fabsf(wi_z) / pdf);
-                    bool alive = true;
-                    if (depth >= a.rr_depth) {
-                        float q = fmaxf(0.05f, 1.0f - max3c(nb));
-                        if (urr < q) alive = false;
-                        else nb = nb * (1.0f / (1.0f - q));
-                    }
-                    if (alive && depth + 1 < a.max_depth) {
-                        float3 o = offset_origin(p, perr, nrm, wi);
-                        ray_c = {{o.x, o.y, o.z}, 0.0f, {wi.x, wi.y, wi.z}, INFINITY};
-                        beta_out = make_float4(nb.x, nb.y, nb.z, __uint_as_float(pixel));
-                        rng_out = make_uint2((uint32_t)rng.state, (uint32_t)(rng.state >> 32));
-                        cont = true;
+                    // continuation
+                    float u0 = rng.uniform_float(), u1 = rng.uniform_float();
+                    float urr = rng.uniform_float();
+                    float3 wl = cosine_hemisphere(u0, u1);
+                    if (wo_z < 0.0f) wl.z = -wl.z;
+                    float3 wi = ss * wl.x + ts * wl.y + nrm * wl.z;
+                    float pdf = fabsf(wl.z) * (1.0f / kPiF);
+                    float wi_z = dot3(wi, nrm);
+                    if (!black && wo_z != 0.0f && pdf > 0.0f && wi_z * wo_z > 0.0f) {
+                        float3 nb = beta * albedo * ((1.0f / kPiF) * fabsf(wi_z) / pdf);
+                        bool alive = true;
+                        if (depth >= a.rr_depth) {
+                            float q = fmaxf(0.05f, 1.0f - max3c(nb));
+                            if (urr < q) alive = false;
+                            else nb = nb * (1.0f / (1.0f - q));
+                        }
+                        if (alive && depth + 1 < a.max_depth) {
+                            o_c = offset_origin(p, perr, nrm, wi);
+                            d_c = wi;
+                            beta_out = make_float4(nb.x, nb.y, nb.z, __uint_as_float(pixel));
+                            rng_out = make_uint2((uint32_t)rng.state, (uint32_t)(rng.state >> 32));
+                            spread_out = make_float4(sp.x, sp.y, pdf, __uint_as_float(slot));
+                            cont = true;
+                        }
                     }
                 }
             }
         }
-        uint32_t slot = warp_append(&a.counts[nxt], cont);
+        uint32_t s = warp_append(&a.counts[nxt], cont);
         if (cont) {
-            float4* rr = reinterpret_cast<float4*>(a.rays[nxt] + slot);
-            rr[0] = make_float4(ray_c.o[0], ray_c.o[1], ray_c.o[2], 0.0f);
-            rr[1] = make_float4(ray_c.d[0], ray_c.d[1], ray_c.d[2], ray_c.tmax);
-            a.beta[nxt][slot] = beta_out;
-            a.rng[nxt][slot] = rng_out;
-            a.pid[nxt][slot] = id;
+            put_ray(a.rays[nxt], s, o_c, d_c, INFINITY);
+            a.beta[nxt][s] = beta_out;
+            a.rng[nxt][s] = rng_out;
+            a.pid[nxt][s] = id;
+            if (kNrc) a.spread[nxt][s] = spread_out;
         }
         uint32_t sl = warp_append(&a.counts[kShadow], push_l);
         if (push_l) {
-            float4* rr = reinterpret_cast<float4*>(a.srays + sl);
-            rr[0] = make_float4(ray_l.o[0], ray_l.o[1], ray_l.o[2], 0.0f);
-            rr[1] = make_float4(ray_l.d[0], ray_l.d[1], ray_l.d[2], ray_l.tmax);
+            put_ray(a.srays, sl, o_l, d_l, tm_l);
             a.scontrib[sl] = make_float4(c_l.x, c_l.y, c_l.z, __uint_as_float(pixel));
+            if (kNrc) a.s_train[sl] = make_uint2(slot, depth);
         }
         uint32_t sb = warp_append(&a.counts[kShadow], push_b);
         if (push_b) {
-            float4* rr = reinterpret_cast<float4*>(a.srays + sb);
-            rr[0] = make_float4(ray_b.o[0], ray_b.o[1], ray_b.o[2], 0.0f);
-            rr[1] = make_float4(ray_b.d[0], ray_b.d[1], ray_b.d[2], ray_b.tmax);
+            put_ray(a.srays, sb, o_b, d_b, tm_b);
             a.scontrib[sb] = make_float4(c_b.x, c_b.y, c_b.z, __uint_as_float(pixel));
+            if (kNrc) a.s_train[sb] = make_uint2(slot, depth);
+        }
+        if (kNrc) {
+            uint32_t sq = warp_append(&a.counts[kQueries], query);
+            if (query && sq < a.q_cap) {
+                float* qi = a.q_in + 12 * (size_t)sq;
+                float in[12] = {q_p.x, q_p.y, q_p.z, q_wo.x, q_wo.y, q_wo.z, q_n.x, q_n.y, q_n.z,
+                                q_alb.x, q_alb.y, q_alb.z};
+#pragma unroll
+                for (int q = 0; q < 12; ++q) qi[q] = in[q];
+                a.q_beta[sq] = make_float4(q_beta.x, q_beta.y, q_beta.z, __uint_as_float(pixel));
+            }
         }
     }
 }
 
+template <bool kNrc>
 __global__ void k_pt_accum(PtArgs a) {
     const uint32_t n = (uint32_t)a.counts[kShadow];
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        if (a.socc[i] == 0u) {
-            float4 c = a.scontrib[i];
-            film_add(a, __float_as_uint(c.w), make_float3(c.x, c.y, c.z));
+        if (a.socc[i] != 0u) continue;
+        float4 c4 = a.scontrib[i];
+        float3 c = make_float3(c4.x, c4.y, c4.z);
+        film_add(a, __float_as_uint(c4.w), c);
+        if (kNrc) {
+            uint2 st = a.s_train[i];
+            if (st.x != kNone && good(c)) {
+                // every vertex up to the one that cast this ray gets c / beta_k
+                for (uint32_t k = 0; k <= st.y && k < a.max_depth; ++k) {
+                    float* rec = a.t_rec + ((size_t)st.x * a.max_depth + k) * kRec;
+                    atomicAdd(&rec[15], c.x * rec[12]);
+                    atomicAdd(&rec[16], c.y * rec[13]);
+                    atomicAdd(&rec[17], c.z * rec[14]);
+                }
+            }
         }
     }
 }
@@ -351,36 +450,175 @@ __global__ void k_pt_advance(PtArgs a, int cur) {
     a.counts[kDepth] += 1;
 }
 
+// Flattens the recorded training vertices (at most sample_cap = n_batches *
+// batch_rows).  Sample r goes to row (r % n_batches) * batch_rows + r / n_batches,
+// so batch j (rows j * batch_rows ...) takes every n_batches-th sample and
+// spans the whole image rather than one band of it.
+__global__ void k_nrc_gather(PtArgs a, uint32_t n_batches, uint32_t batch_rows) {
+    uint32_t slots = (uint32_t)min(a.counts[kTrainSlots], (unsigned long long)a.t_cap);
+    for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < slots; s += gridDim.x * blockDim.x) {
+        uint32_t c = a.t_count[s];
+        if (c == 0) continue;
+        unsigned long long pos = atomicAdd(&a.counts[kSamples], (unsigned long long)c);
+        for (uint32_t k = 0; k < c && pos + k < a.sample_cap; ++k) {
+            const float* rec = a.t_rec + ((size_t)s * a.max_depth + k) * kRec;
+            uint32_t r = (uint32_t)(pos + k);
+            size_t row = (size_t)(r % n_batches) * batch_rows + r / n_batches;
+            float* in = a.t_in + 12 * row;
+            for (int q = 0; q < 12; ++q) in[q] = rec[q];
+            float* tg = a.t_tg + 3 * row;
+            tg[0] = rec[15]; tg[1] = rec[16]; tg[2] = rec[17];
+        }
+    }
+}
+
+// film += throughput * max(prediction, 0) for every query of the wave.
+__global__ void k_nrc_apply(PtArgs a) {
+    uint32_t n = (uint32_t)min(a.counts[kQueries], (unsigned long long)a.q_cap);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        float4 b = a.q_beta[i];
+        const float* p = a.q_out + 3 * (size_t)i;
+        float3 c = make_float3(b.x * fmaxf(p[0], 0.0f), b.y * fmaxf(p[1], 0.0f), b.z * fmaxf(p[2], 0.0f));
+        film_add(a, __float_as_uint(b.w), c);
+    }
+}
+
 __global__ void k_pt_resolve(const float* film, float* out, uint32_t n3, float inv_spp) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n3) out[i] = film[i] * inv_spp;
+}
+
+// One bounce: extend, shade, shadow, accumulate, advance (queue parity cur).
+template <bool kNrc>
+cudaError_t bounce(const PtArgs& a, const DeviceAccel& da, const LaunchParams& lp, uint32_t cap, uint32_t* err,
+                   int cur, int blocks, cudaStream_t s) {
+    cudaError_t e = launch_trace(da, a.rays[cur], cap, const_cast<ilm_hit*>(a.hits), nullptr, err, lp, s,
+                                 a.counts + cur);
+    if (e != cudaSuccess) return e;
+    k_pt_shade<kNrc><<<blocks, 256, 0, s>>>(a, cur);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    e = launch_trace(da, a.srays, 2ull * cap, nullptr, const_cast<uint32_t*>(a.socc), err, lp, s,
+                     a.counts + kShadow);
+    if (e != cudaSuccess) return e;
+    k_pt_accum<kNrc><<<blocks, 256, 0, s>>>(a);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    k_pt_advance<<<1, 1, 0, s>>>(a, cur);
+    return cudaGetLastError();
+}
+
+// Everything a render needs; shared by ilm_render_pt and ilm_render_nrc.
+struct RenderSetup {
+    PtArgs a;
+    DeviceAccel da;
+    LaunchParams lp;
+    uint32_t* err;
+    int blocks;
+    uint32_t P;
+    uint64_t npix, total;
+    cudaStream_t s;
+};
+
+int32_t setup_render(ilm_context* ctx, PtScene& sc, uint32_t spp, uint32_t max_depth, uint32_t rr_depth,
+                     uint64_t seed, uint32_t wave_paths, uint64_t total_paths, bool nrc, RenderSetup& r) {
+    Accel* acc = find_accel(ctx, sc.accel);
+    if (!acc) { set_error(ctx, "render: the scene's accel was destroyed"); return ILM_ERR_NOT_FOUND; }
+    const ilm_pt_scene_desc& d = sc.desc;
+    uint32_t ns = (uint32_t)std::lround(std::sqrt((double)spp));
+    if (spp == 0 || ns * ns != spp || max_depth == 0) {
+        set_error(ctx, "render: spp must be a non-zero perfect square and max_depth >= 1");
+        return ILM_ERR_INVALID_ARGUMENT;
+    }
+    r.npix = (uint64_t)d.width * d.height;
+    r.total = total_paths;
+    if (r.total >= (1ull << 32)) { set_error(ctx, "render: more than 2^32 paths"); return ILM_ERR_INVALID_ARGUMENT; }
+    uint32_t P = wave_paths ? wave_paths : (1u << 21);
+    if ((uint64_t)P > r.total) P = (uint32_t)r.total;
+    r.P = P;
+    PtBuffers& b = sc.buf;
+    cudaError_t e = cudaSuccess;
+    for (int q = 0; q < 2 && e == cudaSuccess; ++q) {
+        if ((e = b.rays[q].reserve((size_t)P * sizeof(ilm_ray))) != cudaSuccess) break;
+        if ((e = b.beta[q].reserve((size_t)P * 16)) != cudaSuccess) break;
+        if ((e = b.rng[q].reserve((size_t)P * 8)) != cudaSuccess) break;
+        if ((e = b.pid[q].reserve((size_t)P * 4)) != cudaSuccess) break;
+        if (nrc) e = b.spread[q].reserve((size_t)P * 16);
+    }
+    if (e == cudaSuccess) e = b.hits.reserve((size_t)P * sizeof(ilm_hit));
+    if (e == cudaSuccess) e = b.srays.reserve((size_t)2 * P * sizeof(ilm_ray));
+    if (e == cudaSuccess) e = b.scontrib.reserve((size_t)2 * P * 16);
+    if (e == cudaSuccess) e = b.socc.reserve((size_t)2 * P * 4);
+    if (e == cudaSuccess) e = b.counts.reserve(kNumCounts * 8);
+    if (e == cudaSuccess) e = b.film.reserve(r.npix * 12);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "render buffers");
+    if (!b.stream) {
+        if ((e = cudaStreamCreateWithFlags(&b.stream, cudaStreamNonBlocking)) != cudaSuccess)
+            return cuda_fail(ctx, e, "cudaStreamCreate");
+        cudaEventCreate(&b.ev0);
+        cudaEventCreate(&b.ev1);
+    }
+    r.s = b.stream;
+    PtArgs& a = r.a;
+    std::memset(&a, 0, sizeof a);
+    a.tri = static_cast<const float4*>(sc.d_tri.ptr);
+    a.mat = static_cast<const float4*>(sc.d_mat.ptr);
+    a.lights = static_cast<const uint32_t*>(sc.d_lights.ptr);
+    a.light_geo = static_cast<const float4*>(sc.d_light_geo.ptr);
+    a.n_lights = sc.n_lights;
+    a.film = static_cast<float*>(b.film.ptr);
+    a.width = d.width; a.height = d.height; a.npix = (uint32_t)r.npix; a.spp = spp; a.ns = ns;
+    a.eye_x = d.eye[0]; a.eye_y = d.eye[1]; a.eye_z = d.eye[2];
+    a.tan_half = std::tan(0.5f * d.fov_deg * 3.14159265358979323846f / 180.0f);
+    a.aspect = (float)d.width / (float)d.height;
+    a.max_depth = max_depth; a.rr_depth = rr_depth; a.seed = seed;
+    for (int q = 0; q < 2; ++q) {
+        a.rays[q] = static_cast<ilm_ray*>(b.rays[q].ptr);
+        a.beta[q] = static_cast<float4*>(b.beta[q].ptr);
+        a.rng[q] = static_cast<uint2*>(b.rng[q].ptr);
+        a.pid[q] = static_cast<uint32_t*>(b.pid[q].ptr);
+        a.spread[q] = static_cast<float4*>(b.spread[q].ptr);
+    }
+    a.hits = static_cast<const ilm_hit*>(b.hits.ptr);
+    a.srays = static_cast<ilm_ray*>(b.srays.ptr);
+    a.scontrib = static_cast<float4*>(b.scontrib.ptr);
+    a.socc = static_cast<const uint32_t*>(b.socc.ptr);
+    a.counts = static_cast<unsigned long long*>(b.counts.ptr);
+    r.da = acc->view();
+    unsigned long long* counter = ctx->counter_for(r.s);
+    if (!counter) return ILM_ERR_OUT_OF_MEMORY;
+    r.lp = LaunchParams{ctx->stack_depth, ctx->block_size, ctx->max_iter, 1, counter,
+                        (ctx->flags & ILM_FLAG_HIGH_OCCUPANCY) ? 8 : 0};
+    r.err = static_cast<uint32_t*>(ctx->err_word.ptr);
+    int dev_sms = 148;
+    cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, ctx->device);
+    r.blocks = dev_sms * 8;
+    cudaMemsetAsync(a.counts, 0, kNumCounts * 8, r.s);
+    cudaMemsetAsync(a.film, 0, r.npix * 12, r.s);
+    return ILM_OK;
+}
+
+// Resolves the film into rgb_out (host or device) and reads the counters.
+int32_t finish_render(ilm_context* ctx, PtScene& sc, RenderSetup& r, float* rgb_out, float inv_spp,
+                      unsigned long long* cnts) {
+    PtBuffers& b = sc.buf;
+    cudaError_t e;
+    PtrKind k = classify(rgb_out);
+    float* dst = rgb_out;
+    if (k == PtrKind::kHost) {
+        if ((e = b.out.reserve(r.npix * 12)) != cudaSuccess) return cuda_fail(ctx, e, "cudaMalloc(out)");
+        dst = static_cast<float*>(b.out.ptr);
+    }
+    uint32_t n3 = (uint32_t)(r.npix * 3);
+    k_pt_resolve<<<(n3 + 255) / 256, 256, 0, r.s>>>(r.a.film, dst, n3, inv_spp);
+    if (k == PtrKind::kHost) cudaMemcpyAsync(rgb_out, dst, r.npix * 12, cudaMemcpyDeviceToHost, r.s);
+    cudaMemcpyAsync(cnts, r.a.counts, kNumCounts * 8, cudaMemcpyDeviceToHost, r.s);
+    if ((e = cudaStreamSynchronize(r.s)) != cudaSuccess) return cuda_fail(ctx, e, "render");
+    return ILM_OK;
 }
 
 }  // namespace
 }  // namespace ilm
 
 using namespace ilm;
-
-namespace {
-
-// One bounce: extend, shade, shadow, accumulate, advance (queue parity cur).
-cudaError_t bounce(const PtArgs& a, const DeviceAccel& da, const LaunchParams& lp, uint32_t cap, uint32_t* err,
-                   int cur, int blocks, cudaStream_t s) {
-    cudaError_t e = launch_trace(da, a.rays[cur], cap, const_cast<ilm_hit*>(a.hits), nullptr, err, lp, s,
-                                 a.counts + cur);
-    if (e != cudaSuccess) return e;
-    k_pt_shade<<<blocks, 256, 0, s>>>(a, cur);
-    if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    e = launch_trace(da, a.srays, 2ull * cap, nullptr, const_cast<uint32_t*>(a.socc), err, lp, s,
-                     a.counts + kShadow);
-    if (e != cudaSuccess) return e;
-    k_pt_accum<<<blocks, 256, 0, s>>>(a);
-    if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    k_pt_advance<<<1, 1, 0, s>>>(a, cur);
-    return cudaGetLastError();
-}
-
-}  // namespace
 
 extern "C" {
 
@@ -399,6 +637,7 @@ int32_t ilm_pt_scene_create(ilm_context* ctx, ilm_accel_id accel, const ilm_pt_s
     auto sc = std::make_unique<PtScene>();
     sc->accel = accel;
     sc->desc = *desc;
+    for (int k = 0; k < 6; ++k) sc->bound[k] = h.bound[k];
     uint32_t np = h.n_prims;
     std::vector<float> tri(12ull * np, 0.0f);
     for (const PrimRec& r : h.records) {
@@ -439,17 +678,18 @@ int32_t ilm_pt_scene_create(ilm_context* ctx, ilm_accel_id accel, const ilm_pt_s
         lgeo.insert(lgeo.end(), {(float)(c[0] / l), (float)(c[1] / l), (float)(c[2] / l), (float)(0.5 * l)});
     }
     sc->n_lights = (uint32_t)lights.size();
-    if (cudaError_t e = sc->d_tri.reserve(tri.size() * 4); e != cudaSuccess) return cuda_fail(ctx, e, "cudaMalloc");
-    if (cudaError_t e = sc->d_mat.reserve(mat.size() * 4); e != cudaSuccess) return cuda_fail(ctx, e, "cudaMalloc");
+    cudaError_t e;
+    if ((e = sc->d_tri.reserve(tri.size() * 4 + 16)) != cudaSuccess) return cuda_fail(ctx, e, "cudaMalloc");
+    if ((e = sc->d_mat.reserve(mat.size() * 4)) != cudaSuccess) return cuda_fail(ctx, e, "cudaMalloc");
     if (np) cudaMemcpy(sc->d_tri.ptr, tri.data(), tri.size() * 4, cudaMemcpyHostToDevice);
     cudaMemcpy(sc->d_mat.ptr, mat.data(), mat.size() * 4, cudaMemcpyHostToDevice);
     if (!lights.empty()) {
-        if (cudaError_t e = sc->d_lights.reserve(lights.size() * 4); e != cudaSuccess) return cuda_fail(ctx, e, "cudaMalloc");
-        if (cudaError_t e = sc->d_light_geo.reserve(lgeo.size() * 4); e != cudaSuccess) return cuda_fail(ctx, e, "cudaMalloc");
+        if ((e = sc->d_lights.reserve(lights.size() * 4)) != cudaSuccess) return cuda_fail(ctx, e, "cudaMalloc");
+        if ((e = sc->d_light_geo.reserve(lgeo.size() * 4)) != cudaSuccess) return cuda_fail(ctx, e, "cudaMalloc");
         cudaMemcpy(sc->d_lights.ptr, lights.data(), lights.size() * 4, cudaMemcpyHostToDevice);
         cudaMemcpy(sc->d_light_geo.ptr, lgeo.data(), lgeo.size() * 4, cudaMemcpyHostToDevice);
     }
-    if (cudaError_t e = cudaGetLastError(); e != cudaSuccess) return cuda_fail(ctx, e, "ilm_pt_scene_create");
+    if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(ctx, e, "ilm_pt_scene_create");
     ilm_pt_scene_id id = ctx->next_pt++;
     ctx->pt_scenes[id] = std::move(sc);
     *out = id;
@@ -463,89 +703,25 @@ int32_t ilm_render_pt(ilm_context* ctx, ilm_pt_scene_id scene, const ilm_pt_opts
     auto it = ctx->pt_scenes.find(scene);
     if (it == ctx->pt_scenes.end()) { set_error(ctx, "ilm_render_pt: unknown scene id"); return ILM_ERR_NOT_FOUND; }
     PtScene& sc = *it->second;
-    Accel* acc = find_accel(ctx, sc.accel);
-    if (!acc) { set_error(ctx, "ilm_render_pt: the scene's accel was destroyed"); return ILM_ERR_NOT_FOUND; }
-    const ilm_pt_scene_desc& d = sc.desc;
-    uint32_t ns = (uint32_t)std::lround(std::sqrt((double)opts->spp));
-    if (opts->spp == 0 || ns * ns != opts->spp || opts->max_depth == 0) {
-        set_error(ctx, "ilm_render_pt: spp must be a non-zero perfect square and max_depth >= 1");
-        return ILM_ERR_INVALID_ARGUMENT;
-    }
-    const uint64_t npix = (uint64_t)d.width * d.height;
-    const uint64_t total = npix * opts->spp;
-    if (total >= (1ull << 32)) { set_error(ctx, "ilm_render_pt: more than 2^32 paths"); return ILM_ERR_INVALID_ARGUMENT; }
-    uint32_t P = opts->wave_paths ? opts->wave_paths : (1u << 21);
-    if ((uint64_t)P > total) P = (uint32_t)total;
-    // buffers
-    PtBuffers& b = sc.buf;
-    auto rsv = [&](DeviceBuffer& db, size_t bytes) { return db.reserve(bytes); };
+    RenderSetup r;
+    uint64_t total = (uint64_t)sc.desc.width * sc.desc.height * opts->spp;
+    int32_t st = setup_render(ctx, sc, opts->spp, opts->max_depth, opts->rr_depth, opts->seed, opts->wave_paths,
+                              total, false, r);
+    if (st != ILM_OK) return st;
+    PtArgs& a = r.a;
+    cudaStream_t s = r.s;
     cudaError_t e = cudaSuccess;
-    for (int q = 0; q < 2 && e == cudaSuccess; ++q) {
-        if ((e = rsv(b.rays[q], (size_t)P * sizeof(ilm_ray))) != cudaSuccess) break;
-        if ((e = rsv(b.beta[q], (size_t)P * 16)) != cudaSuccess) break;
-        if ((e = rsv(b.rng[q], (size_t)P * 8)) != cudaSuccess) break;
-        e = rsv(b.pid[q], (size_t)P * 4);
-    }
-    if (e == cudaSuccess) e = rsv(b.hits, (size_t)P * sizeof(ilm_hit));
-    if (e == cudaSuccess) e = rsv(b.srays, (size_t)2 * P * sizeof(ilm_ray));
-    if (e == cudaSuccess) e = rsv(b.scontrib, (size_t)2 * P * 16);
-    if (e == cudaSuccess) e = rsv(b.socc, (size_t)2 * P * 4);
-    if (e == cudaSuccess) e = rsv(b.counts, kNumCounts * 8);
-    if (e == cudaSuccess) e = rsv(b.film, npix * 12);
-    if (e != cudaSuccess) return cuda_fail(ctx, e, "ilm_render_pt buffers");
-    if (!b.stream) {
-        if ((e = cudaStreamCreateWithFlags(&b.stream, cudaStreamNonBlocking)) != cudaSuccess)
-            return cuda_fail(ctx, e, "cudaStreamCreate");
-        cudaEventCreate(&b.ev0);
-        cudaEventCreate(&b.ev1);
-    }
-    cudaStream_t s = b.stream;
-    PtArgs a;
-    a.tri = static_cast<const float4*>(sc.d_tri.ptr);
-    a.mat = static_cast<const float4*>(sc.d_mat.ptr);
-    a.lights = static_cast<const uint32_t*>(sc.d_lights.ptr);
-    a.light_geo = static_cast<const float4*>(sc.d_light_geo.ptr);
-    a.n_lights = sc.n_lights;
-    a.film = static_cast<float*>(b.film.ptr);
-    a.width = d.width; a.height = d.height; a.npix = (uint32_t)npix; a.spp = opts->spp; a.ns = ns;
-    a.eye_x = d.eye[0]; a.eye_y = d.eye[1]; a.eye_z = d.eye[2];
-    a.tan_half = std::tan(0.5f * d.fov_deg * 3.14159265358979323846f / 180.0f);
-    a.aspect = (float)d.width / (float)d.height;
-    a.max_depth = opts->max_depth; a.rr_depth = opts->rr_depth; a.seed = opts->seed;
-    for (int q = 0; q < 2; ++q) {
-        a.rays[q] = static_cast<ilm_ray*>(b.rays[q].ptr);
-        a.beta[q] = static_cast<float4*>(b.beta[q].ptr);
-        a.rng[q] = static_cast<uint2*>(b.rng[q].ptr);
-        a.pid[q] = static_cast<uint32_t*>(b.pid[q].ptr);
-    }
-    a.hits = static_cast<const ilm_hit*>(b.hits.ptr);
-    a.srays = static_cast<ilm_ray*>(b.srays.ptr);
-    a.scontrib = static_cast<float4*>(b.scontrib.ptr);
-    a.socc = static_cast<const uint32_t*>(b.socc.ptr);
-    a.counts = static_cast<unsigned long long*>(b.counts.ptr);
-    DeviceAccel da = acc->view();
-    unsigned long long* counter = ctx->counter_for(s);
-    if (!counter) return ILM_ERR_OUT_OF_MEMORY;
-    LaunchParams lp{ctx->stack_depth, ctx->block_size, ctx->max_iter, 1, counter,
-                    (ctx->flags & ILM_FLAG_HIGH_OCCUPANCY) ? 8 : 0};
-    uint32_t* err = static_cast<uint32_t*>(ctx->err_word.ptr);
-    int dev_sms = 148;
-    cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, ctx->device);
-    const int blocks = dev_sms * 8;
-
-    cudaMemsetAsync(a.counts, 0, kNumCounts * 8, s);
-    cudaMemsetAsync(a.film, 0, npix * 12, s);
-    // graphs: one per queue parity, captured on first use for this buffer set
     cudaGraphExec_t graphs[2] = {nullptr, nullptr};
     if (opts->use_graphs) {
         // One eager bounce over empty queues (every kernel returns at once)
         // does the launchers' one-time setup outside the capture.
-        if ((e = bounce(a, da, lp, P, err, 0, blocks, s)) != cudaSuccess) return cuda_fail(ctx, e, "bounce");
+        if ((e = bounce<false>(a, r.da, r.lp, r.P, r.err, 0, r.blocks, s)) != cudaSuccess)
+            return cuda_fail(ctx, e, "bounce");
         for (int q = 0; q < 2; ++q) {
             cudaGraph_t g;
             if ((e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal)) != cudaSuccess)
                 return cuda_fail(ctx, e, "cudaStreamBeginCapture");
-            cudaError_t eb = bounce(a, da, lp, P, err, q, blocks, s);
+            cudaError_t eb = bounce<false>(a, r.da, r.lp, r.P, r.err, q, r.blocks, s);
             e = cudaStreamEndCapture(s, &g);
             if (eb != cudaSuccess) return cuda_fail(ctx, eb, "bounce capture");
             if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaStreamEndCapture");
@@ -554,47 +730,182 @@ int32_t ilm_render_pt(ilm_context* ctx, ilm_pt_scene_id scene, const ilm_pt_opts
             if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaGraphInstantiate");
         }
     }
-    cudaEventRecord(b.ev0, s);
+    cudaEventRecord(sc.buf.ev0, s);
     uint32_t waves = 0;
-    for (uint64_t p0 = 0; p0 < total; p0 += P, ++waves) {
-        uint32_t cnt = (uint32_t)(total - p0 < P ? total - p0 : P);
-        k_pt_camera<<<(cnt + 255) / 256, 256, 0, s>>>(a, p0, cnt);
+    for (uint64_t p0 = 0; p0 < r.total; p0 += r.P, ++waves) {
+        uint32_t cnt = (uint32_t)(r.total - p0 < r.P ? r.total - p0 : r.P);
+        k_pt_camera<false><<<(cnt + 255) / 256, 256, 0, s>>>(a, p0, cnt);
         for (uint32_t depth = 0; depth < opts->max_depth; ++depth) {
             int cur = depth & 1;
             if (opts->use_graphs) e = cudaGraphLaunch(graphs[cur], s);
-            else e = bounce(a, da, lp, P, err, cur, blocks, s);
+            else e = bounce<false>(a, r.da, r.lp, r.P, r.err, cur, r.blocks, s);
             if (e != cudaSuccess) break;
         }
         if (e != cudaSuccess) break;
     }
-    cudaEventRecord(b.ev1, s);
+    cudaEventRecord(sc.buf.ev1, s);
     for (auto& g : graphs) if (g) cudaGraphExecDestroy(g);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "ilm_render_pt launch");
-    // resolve into the output (device) or a device temp then copy (host)
-    PtrKind k = classify(rgb_out);
-    float* dst = rgb_out;
-    if (k == PtrKind::kHost) {
-        if ((e = b.out.reserve(npix * 12)) != cudaSuccess) return cuda_fail(ctx, e, "cudaMalloc(out)");
-        dst = static_cast<float*>(b.out.ptr);
-    }
-    uint32_t n3 = (uint32_t)(npix * 3);
-    k_pt_resolve<<<(n3 + 255) / 256, 256, 0, s>>>(a.film, dst, n3, 1.0f / (float)opts->spp);
-    if (k == PtrKind::kHost) cudaMemcpyAsync(rgb_out, dst, npix * 12, cudaMemcpyDeviceToHost, s);
     unsigned long long cnts[kNumCounts];
-    cudaMemcpyAsync(cnts, a.counts, sizeof cnts, cudaMemcpyDeviceToHost, s);
-    if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_fail(ctx, e, "ilm_render_pt");
+    if ((st = finish_render(ctx, sc, r, rgb_out, 1.0f / (float)opts->spp, cnts)) != ILM_OK) return st;
     if (stats) {
         float ms = 0.0f;
-        cudaEventElapsedTime(&ms, b.ev0, b.ev1);
+        cudaEventElapsedTime(&ms, sc.buf.ev0, sc.buf.ev1);
         stats->closest_rays = cnts[kTotClosest];
         stats->shadow_rays = cnts[kTotShadow];
         stats->seconds = ms * 1e-3;
         stats->waves = waves;
     }
-    // cnts[kTotClosest/kTotShadow] accumulate over the waves of this call only:
-    // the counters are cleared at the start of every render.
     if (cnts[kDropped]) {
         set_error(ctx, "ilm_render_pt: some paths reached the traversal limits and were dropped");
+        return ILM_ERR_TRAVERSAL_LIMIT;
+    }
+    return ILM_OK;
+}
+
+int32_t ilm_render_nrc(ilm_context* ctx, ilm_pt_scene_id scene, ilm_nrc* nrc, const ilm_nrc_render_opts* o,
+                       float* rgb_out, ilm_nrc_render_stats* stats) {
+    if (!ctx || !nrc || !o || !rgb_out) return ILM_ERR_INVALID_ARGUMENT;
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return ILM_ERR_CUDA;
+    auto it = ctx->pt_scenes.find(scene);
+    if (it == ctx->pt_scenes.end()) { set_error(ctx, "ilm_render_nrc: unknown scene id"); return ILM_ERR_NOT_FOUND; }
+    if (o->frames == 0 && !(o->time_budget_s > 0.0)) {
+        set_error(ctx, "ilm_render_nrc: give frames or a time budget");
+        return ILM_ERR_INVALID_ARGUMENT;
+    }
+    PtScene& sc = *it->second;
+    const uint64_t npix = (uint64_t)sc.desc.width * sc.desc.height;
+    const uint32_t spf = o->spp_per_frame ? o->spp_per_frame : 1;
+    if (npix * spf > (1ull << 27)) {
+        set_error(ctx, "ilm_render_nrc: width * height * spp_per_frame above 2^27");
+        return ILM_ERR_INVALID_ARGUMENT;
+    }
+    // path ids are 32-bit: frame * paths-per-frame stays below 2^32
+    const uint32_t id_frames = (uint32_t)(((1ull << 32) - 1) / (npix * spf));
+    const uint32_t max_frames = std::min(o->frames ? o->frames : 1000000u, id_frames);
+    RenderSetup r;
+    int32_t st = setup_render(ctx, sc, spf, o->max_depth, o->rr_depth, o->seed, (uint32_t)(npix * spf),
+                              npix * spf * (uint64_t)max_frames, true, r);
+    if (st != ILM_OK) return st;
+    const uint32_t P = (uint32_t)(npix * spf);
+    r.P = P;
+    PtBuffers& b = sc.buf;
+    const uint32_t train_paths = o->train_paths ? o->train_paths : 16384u;
+    const uint32_t n_batches = o->train_steps ? o->train_steps : 4u;
+    const uint32_t batch_rows = ((o->train_samples ? o->train_samples : 65536u) + n_batches - 1) / n_batches;
+    const uint32_t sample_cap = batch_rows * n_batches;
+    const uint32_t stride = (uint32_t)std::max<uint64_t>(kMinTrainStride, P / train_paths);
+    const uint32_t t_cap = P / stride + 1;
+    cudaError_t e = cudaSuccess;
+    if ((e = b.q_in.reserve((size_t)P * 48)) == cudaSuccess && (e = b.q_beta.reserve((size_t)P * 16)) == cudaSuccess &&
+        (e = b.q_out.reserve((size_t)P * 12)) == cudaSuccess &&
+        (e = b.t_rec.reserve((size_t)t_cap * o->max_depth * kRec * 4)) == cudaSuccess &&
+        (e = b.t_count.reserve((size_t)t_cap * 4)) == cudaSuccess &&
+        (e = b.s_train.reserve((size_t)2 * P * 8)) == cudaSuccess &&
+        (e = b.t_in.reserve((size_t)sample_cap * 48)) == cudaSuccess)
+        e = b.t_tg.reserve((size_t)sample_cap * 12);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "nrc render buffers");
+    PtArgs& a = r.a;
+    a.q_in = static_cast<float*>(b.q_in.ptr);
+    a.q_beta = static_cast<float4*>(b.q_beta.ptr);
+    a.q_out = static_cast<const float*>(b.q_out.ptr);
+    a.q_cap = P;
+    a.t_rec = static_cast<float*>(b.t_rec.ptr);
+    a.t_count = static_cast<uint32_t*>(b.t_count.ptr);
+    a.t_cap = t_cap;
+    a.train_stride = stride;
+    a.spread_c = o->spread_c > 0.0f ? o->spread_c : 0.01f;
+    a.s_train = static_cast<uint2*>(b.s_train.ptr);
+    a.t_in = static_cast<float*>(b.t_in.ptr);
+    a.t_tg = static_cast<float*>(b.t_tg.ptr);
+    a.sample_cap = sample_cap;
+    cudaStream_t s = r.s;
+    // the bounces as CUDA graphs, one per queue parity (train_phase, the only
+    // per-frame field, is read by the camera kernel alone)
+    cudaGraphExec_t graphs[2] = {nullptr, nullptr};
+    auto drop_graphs = [&]() { for (auto& g : graphs) if (g) { cudaGraphExecDestroy(g); g = nullptr; } };
+    if ((e = bounce<true>(a, r.da, r.lp, P, r.err, 0, r.blocks, s)) != cudaSuccess) return cuda_fail(ctx, e, "bounce");
+    for (int q = 0; q < 2; ++q) {
+        cudaGraph_t g;
+        if ((e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal)) != cudaSuccess) break;
+        cudaError_t eb = bounce<true>(a, r.da, r.lp, P, r.err, q, r.blocks, s);
+        e = cudaStreamEndCapture(s, &g);
+        if (e == cudaSuccess) e = eb;
+        if (e == cudaSuccess) e = cudaGraphInstantiate(&graphs[q], g, 0);
+        if (g) cudaGraphDestroy(g);
+        if (e != cudaSuccess) break;
+    }
+    if (e != cudaSuccess) { drop_graphs(); return cuda_fail(ctx, e, "nrc bounce graphs"); }
+    uint64_t queries = 0, samples = 0;
+    uint32_t last_nt = 0;
+    float loss = 0.0f;
+    uint32_t frame = 0;
+    double elapsed = 0.0;
+    cudaEvent_t f0, f1;
+    cudaEventCreate(&f0);
+    cudaEventCreate(&f1);
+    unsigned long long cnts[kNumCounts];
+    for (; frame < max_frames; ++frame) {
+        cudaEventRecord(f0, s);
+        a.train_phase = frame % stride;
+        uint64_t p0 = (uint64_t)frame * P;
+        cudaMemsetAsync(a.counts + kQueries, 0, 3 * sizeof(unsigned long long), s);
+        k_pt_camera<true><<<(P + 255) / 256, 256, 0, s>>>(a, p0, P);
+        for (uint32_t depth = 0; depth < o->max_depth && e == cudaSuccess; ++depth)
+            e = cudaGraphLaunch(graphs[depth & 1], s);
+        if (e != cudaSuccess) break;
+        k_nrc_gather<<<r.blocks, 256, 0, s>>>(a, n_batches, batch_rows);
+        cudaMemcpyAsync(cnts, a.counts, sizeof cnts, cudaMemcpyDeviceToHost, s);
+        if ((e = cudaStreamSynchronize(s)) != cudaSuccess) break;
+        uint32_t nq = (uint32_t)std::min<unsigned long long>(cnts[kQueries], P);
+        uint32_t nt = (uint32_t)std::min<unsigned long long>(cnts[kSamples], sample_cap);
+        queries += nq;
+        samples += nt;
+        last_nt = nt;
+        // answer this frame's queries with the current network, then train
+        if (nq) {
+            if ((st = ilm_nrc_infer(ctx, nrc, a.q_in, nq, static_cast<float*>(b.q_out.ptr), s)) != ILM_OK) break;
+            k_nrc_apply<<<r.blocks, 256, 0, s>>>(a);
+        }
+        if (o->train) {
+            for (uint32_t j = 0; j < n_batches && j < nt; ++j) {
+                uint32_t nj = (nt - j + n_batches - 1) / n_batches;
+                size_t row = (size_t)j * batch_rows;
+                if ((st = ilm_nrc_train_step(ctx, nrc, a.t_in + 12 * row, a.t_tg + 3 * row, nj, nullptr, s)) != ILM_OK)
+                    break;
+            }
+            if (st != ILM_OK) break;
+        }
+        cudaEventRecord(f1, s);
+        cudaEventSynchronize(f1);
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, f0, f1);
+        elapsed += ms * 1e-3;
+        if (o->time_budget_s > 0.0 && elapsed >= o->time_budget_s) { ++frame; break; }
+    }
+    cudaEventDestroy(f0);
+    cudaEventDestroy(f1);
+    drop_graphs();
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "ilm_render_nrc");
+    if (st != ILM_OK) return st;
+    if ((st = finish_render(ctx, sc, r, rgb_out, 1.0f / (float)(spf * std::max(frame, 1u)), cnts)) != ILM_OK)
+        return st;
+    if (last_nt) {
+        // loss of the network on the first batch of the last frame, for reporting
+        uint32_t n0 = (last_nt + n_batches - 1) / n_batches;
+        if ((st = ilm_nrc_gradients(ctx, nrc, a.t_in, a.t_tg, n0, nullptr, &loss)) != ILM_OK) return st;
+    }
+    if (stats) {
+        stats->frames = frame;
+        stats->seconds = elapsed;
+        stats->closest_rays = cnts[kTotClosest];
+        stats->shadow_rays = cnts[kTotShadow];
+        stats->queries = queries;
+        stats->train_samples = samples;
+        stats->last_loss = loss;
+    }
+    if (cnts[kDropped]) {
+        set_error(ctx, "ilm_render_nrc: some paths reached the traversal limits and were dropped");
         return ILM_ERR_TRAVERSAL_LIMIT;
     }
     return ILM_OK;

@@ -14,6 +14,8 @@ struct PtBuffers {
     DeviceBuffer srays, scontrib, socc;              // shadow queue
     DeviceBuffer counts;
     DeviceBuffer film, out;
+    // radiance-cache mode: spread per path, cache queries, training records
+    DeviceBuffer spread[2], q_in, q_beta, q_out, t_rec, t_count, s_train, t_in, t_tg;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     ~PtBuffers() {
@@ -26,6 +28,7 @@ struct PtBuffers {
 struct PtScene {
     ilm_accel_id accel = 0;
     ilm_pt_scene_desc desc{};
+    float bound[6] = {0, 0, 0, 0, 0, 0};   // world bound of the accel (min xyz, max xyz)
     DeviceBuffer d_tri, d_mat, d_lights, d_light_geo;
     uint32_t n_lights = 0;
     PtBuffers buf;

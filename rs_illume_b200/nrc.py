@@ -19,7 +19,8 @@ LAYERS = [(64, 208), (64, 64), (64, 64), (64, 64), (64, 64), (16, 64)]   # (out,
 
 class ilm_nrc_config(ctypes.Structure):
     _fields_ = [("lr", ctypes.c_float), ("beta1", ctypes.c_float), ("beta2", ctypes.c_float),
-                ("eps", ctypes.c_float), ("seed", ctypes.c_uint64), ("bound", ctypes.c_float * 6)]
+                ("eps", ctypes.c_float), ("seed", ctypes.c_uint64), ("bound", ctypes.c_float * 6),
+                ("ema", ctypes.c_float)]
 
 
 def split_params(p: np.ndarray):
@@ -32,11 +33,16 @@ def split_params(p: np.ndarray):
 
 
 class RadianceCache:
-    def __init__(self, ctx: Context, bound, lr=1e-2, beta1=0.9, beta2=0.99, eps=1e-10, seed=4):
+    def __init__(self, ctx: Context, bound, lr=1e-2, beta1=0.9, beta2=0.99, eps=1e-10, seed=4, ema=0.99):
+        """`ema`: inference uses a moving average of the weights over Adam
+        steps with this decay (0 = the latest weights)."""
         self.ctx = ctx
+        if hasattr(bound, "min") and hasattr(bound, "max"):      # Bounds3f
+            bound = tuple(bound.min) + tuple(bound.max)
         c = ilm_nrc_config(lr, beta1, beta2, eps, seed)
         for k in range(6):
             c.bound[k] = bound[k]
+        c.ema = ema
         h = ctypes.c_void_p()
         ctx.check(ctx._lib.ilm_nrc_create(ctx.handle, ctypes.addressof(c), ctypes.byref(h)), "ilm_nrc_create")
         self.handle = h

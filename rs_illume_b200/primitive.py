@@ -279,6 +279,24 @@ class PathTracer:
         return out, {"closest_rays": st.closest_rays, "shadow_rays": st.shadow_rays, "seconds": st.seconds,
                      "waves": st.waves}
 
+    def render_nrc(self, cache, frames: int = 0, spp_per_frame: int = 1, max_depth: int = 8, rr_depth: int = 3,
+                   seed: int = 3, spread_c: float = 0.01, train_paths: int = 16384, train_samples: int = 65536,
+                   time_budget_s: float = 0.0, train: bool = True, train_steps: int = 4, out=None):
+        """Path tracing with a RadianceCache (ilm_render_nrc): frames of
+        spp_per_frame samples, the cache answering paths whose spread has
+        grown, train_steps Adam steps per frame.  Returns (rgb or `out`, stats)."""
+        ctx = self.accel.ctx
+        o = _lib.ilm_nrc_render_opts(frames, spp_per_frame, max_depth, rr_depth, seed, spread_c, train_paths,
+                                     train_samples, time_budget_s, int(train), train_steps)
+        st = _lib.ilm_nrc_render_stats()
+        if out is None:
+            out = np.empty((self.height, self.width, 3), np.float32)
+        ctx.check(ctx._lib.ilm_render_nrc(ctx.handle, self.id, cache.handle, ctypes.byref(o), ptr(out),
+                                          ctypes.byref(st)), "ilm_render_nrc")
+        return out, {"frames": st.frames, "seconds": st.seconds, "closest_rays": st.closest_rays,
+                     "shadow_rays": st.shadow_rays, "queries": st.queries, "train_samples": st.train_samples,
+                     "last_loss": st.last_loss}
+
 
 class Scene:
     """Scene (core/scene.rs:10-53): an aggregate plus lights."""

@@ -31,8 +31,28 @@ def random_inputs(n, seed):
 
 @pytest.fixture
 def cache(ctx):
-    c = RadianceCache(ctx, BOUND, seed=7)
+    c = RadianceCache(ctx, BOUND, seed=7, ema=0.0)     # inference with the latest weights
     yield c
+    c.close()
+
+
+def test_inference_uses_the_weight_average(ctx):
+    ema = 0.9
+    c = RadianceCache(ctx, BOUND, seed=7, ema=ema)
+    x, y = random_inputs(4096, 8)
+    avg = np.zeros(30720, np.float64)
+    for k in range(1, 6):
+        c.train_step(x, y)
+        avg = ema * avg + (1 - ema) * c.params()
+    want_w = (avg / (1 - ema ** 5)).astype(np.float32)
+    xt, yt = random_inputs(512, 9)
+    out = c.infer(xt)
+    pred, _, _ = ref.forward_backward(c.encode(xt), want_w, yt)
+    close = np.abs(out - pred) <= 1e-4 + 1e-4 * np.abs(pred)
+    assert close.mean() > 0.99
+    # and it differs from inference with the latest weights
+    latest, _, _ = ref.forward_backward(c.encode(xt), c.params(), yt)
+    assert np.abs(out - latest).max() > 1e-3
     c.close()
 
 
