@@ -318,7 +318,10 @@ int32_t ilm_nrc_encode(ilm_context* ctx, ilm_nrc* nrc, const float* inputs, uint
  * the cache's prediction there.  One path in max(16, P / train_paths) (P =
  * paths per frame) runs to the end and its vertices become training samples
  * (at most train_samples per frame); after each frame (if `train`) the network
- * takes train_steps Adam steps on interleaved subsets of them. */
+ * takes train_steps Adam steps on interleaved subsets of them.  A frame runs on
+ * the device as one CUDA graph; with a time budget, frames are launched until
+ * the finished ones reach it (the frame queued by then is completed and
+ * counted). */
 typedef struct {
     uint32_t frames;          /* frames to render (0 = until time_budget_s) */
     uint32_t spp_per_frame;   /* a perfect square (0 = 1) */
@@ -328,8 +331,11 @@ typedef struct {
     uint32_t train_paths;     /* training paths per frame (0 = 16384) */
     uint32_t train_samples;   /* training samples per frame at most (0 = 65536) */
     double time_budget_s;     /* stop after the frame that reaches this device time (0 = no budget) */
-    int32_t train;            /* 1: train after every frame; 0: inference only */
+    int32_t train;            /* 1: train after every frame; 0: inference only (no training paths) */
     uint32_t train_steps;     /* Adam steps per frame, each on every train_steps-th sample (0 = 4) */
+    uint32_t train_suffix;    /* a training path goes on for this many vertices past the point where a
+                                 rendering path ends, then ends in the cache too, whose prediction
+                                 joins its targets (0 = 1; >= max_depth: full-length paths) */
 } ilm_nrc_render_opts;
 
 typedef struct {

@@ -91,7 +91,8 @@ class ilm_nrc_render_opts(ctypes.Structure):
     _fields_ = [("frames", ctypes.c_uint32), ("spp_per_frame", ctypes.c_uint32), ("max_depth", ctypes.c_uint32),
                 ("rr_depth", ctypes.c_uint32), ("seed", ctypes.c_uint64), ("spread_c", ctypes.c_float),
                 ("train_paths", ctypes.c_uint32), ("train_samples", ctypes.c_uint32),
-                ("time_budget_s", ctypes.c_double), ("train", ctypes.c_int32), ("train_steps", ctypes.c_uint32)]
+                ("time_budget_s", ctypes.c_double), ("train", ctypes.c_int32), ("train_steps", ctypes.c_uint32),
+                ("train_suffix", ctypes.c_uint32)]
 
 
 class ilm_nrc_render_stats(ctypes.Structure):

@@ -10,17 +10,24 @@
 //   loss = mean over samples and channels of (p - y)^2 / (sg(p)^2 + 0.01).
 //
 // Kernels
-//   k_nrc_encode   raw (p, wo, n, albedo) -> 208 bf16
-//   k_mlp_fwd      one warp per 16 rows: every layer's output fragments are
-//                  turned into the next layer's A fragments in registers;
-//                  weights in shared memory (rows padded to avoid bank
-//                  conflicts); training stores the bf16 activations
+//   k_mlp_fwd      one warp per 16 rows: the encoding is computed straight
+//                  into layer 0's A fragments (each lane evaluates the 8
+//                  features its fragment holds), every layer's output
+//                  fragments become the next layer's A fragments in
+//                  registers; weights in shared memory (rows padded against
+//                  bank conflicts); training stores the encoding and the
+//                  bf16 activations
 //   k_mlp_bwd      loss gradient, then back through the layers the same way
 //                  (transposed weights in shared memory), storing dOut
-//   k_mlp_wgrad    dW = dOut^T * in, reduced over the batch: each CTA stages a
-//                  64-row chunk transposed in shared memory, warps own output
-//                  tiles, partial sums are added to the FP32 gradient
-//   k_adam         Adam on FP32 master weights; writes the bf16 weight packs
+//   k_wgrad_all    dW_l = dOut_l^T * in_l for all six layers: each CTA takes
+//                  64-row chunks (16-byte cp.async into padded shared tiles),
+//                  ldmatrix.trans gives both operands' fragments, warps own
+//                  output tiles; one FP32 partial sum per CTA, no atomics
+//   k_reduce_adam  sums the CTA partials, Adam on the FP32 master weights,
+//                  bf16 weight packs and the inference moving average
+//   k_nrc_encode   the encoding alone (for inspection)
+// Row counts may live in device memory (NrcCount), so the path tracer enqueues
+// inference and training without reading its queue sizes on the host.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -31,6 +38,7 @@
 
 #include "context.h"
 #include "illume_gpu.h"
+#include "nrc.h"
 #include "pcg32.h"
 
 namespace ilm {
@@ -55,6 +63,34 @@ __host__ __device__ constexpr int bwd_stride(int l) { return out_dim(l) + 8; }
 __host__ __device__ constexpr int bwd_off(int l) { return (l - 1) * kHid * (kHid + 8); }   // l = 1..5
 constexpr int kBwdElems = 4 * kHid * (kHid + 8) + kHid * (kOut + 8);                        // 19968
 constexpr float kLossEps = 0.01f;
+constexpr int kMaxPartials = 148;   // CTAs of k_wgrad_all (one FP32 partial gradient each)
+constexpr int kChunk = 64;          // rows per k_wgrad_all staging step
+
+struct Enc {   // position normalisation: q = (p - origin) * scale
+    float x0, y0, z0, sx, sy, sz;
+};
+
+struct AdamArgs {
+    float lr, b1, b2, eps;
+    float ema_a;   // moving-average decay (0 = off)
+};
+
+// Optimiser counters in device memory, so that a captured training step
+// replays with the right bias corrections.
+struct StepState {
+    int step;        // Adam steps taken
+    int ema_steps;   // Adam steps since the inference weights restarted
+};
+
+__device__ __forceinline__ uint32_t rows_of(const NrcCount& c) {
+    uint32_t n = c.cap;
+    if (c.dev) {
+        unsigned long long d = *c.dev;
+        n = d < (unsigned long long)c.cap ? (uint32_t)d : c.cap;
+    }
+    if (c.batches > 1) n = n > c.batch ? (n - c.batch + c.batches - 1) / c.batches : 0u;
+    return n;
+}
 
 __device__ __forceinline__ void mma(float (&d)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
     asm volatile(
@@ -62,6 +98,24 @@ __device__ __forceinline__ void mma(float (&d)[4], const uint32_t (&a)[4], uint3
         "{%0,%1,%2,%3};\n"
         : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
         : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+// Four transposed 8x8 bf16 tiles; lane l addresses row (l & 7) of tile l >> 3.
+__device__ __forceinline__ void ldsm_x4_t(uint32_t (&r)[4], const __nv_bfloat16* p) {
+    uint32_t a = (uint32_t)__cvta_generic_to_shared(p);
+    asm volatile("ldmatrix.sync.aligned.m8n8.x4.trans.shared.b16 {%0,%1,%2,%3}, [%4];\n"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+                 : "r"(a));
+}
+
+// 16-byte global -> shared copy; zero-filled when !ok.
+__device__ __forceinline__ void cp_async16(void* dst, const void* src, bool ok) {
+    uint32_t d = (uint32_t)__cvta_generic_to_shared(dst);
+    int sz = ok ? 16 : 0;
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(d), "l"(src), "r"(sz));
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+    asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
 }
 
 __device__ __forceinline__ uint32_t pack(float lo, float hi) {
@@ -78,6 +132,76 @@ __device__ __forceinline__ void stage(__nv_bfloat16* dst, const __nv_bfloat16* s
     for (int i = threadIdx.x; i < n / 8; i += blockDim.x) d[i] = s[i];
 }
 
+// ---------------------------------------------------------------- encoding
+// What the encoder needs of one input row.
+struct RowIn {
+    float q[3];     // normalised position
+    float u[4];     // theta/pi, phi/2pi of the direction, then of the normal
+    float alb[3];
+};
+
+__device__ __forceinline__ RowIn load_row(const float* __restrict__ raw, uint32_t r, const Enc& e) {
+    const float* p = raw + 12 * (size_t)r;
+    RowIn v;
+    v.q[0] = (p[0] - e.x0) * e.sx;
+    v.q[1] = (p[1] - e.y0) * e.sy;
+    v.q[2] = (p[2] - e.z0) * e.sz;
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+        float x = p[3 + 3 * k], y = p[4 + 3 * k], z = p[5 + 3 * k];
+        v.u[2 * k] = acosf(fminf(fmaxf(z, -1.0f), 1.0f)) * (1.0f / 3.14159265358979f);
+        v.u[2 * k + 1] = atan2f(y, x) * (0.5f / 3.14159265358979f) + 0.5f;
+    }
+    v.alb[0] = p[9];
+    v.alb[1] = p[10];
+    v.alb[2] = p[11];
+    return v;
+}
+
+// Features F + 2t and F + 2t + 1 as a bf16 pair; F is a multiple of 8, so the
+// eight features F..F+7 lie in one block of the layout:
+//   [0, 72)    axis F/24, octave k = (f % 24) / 2: (sin, cos)(2^k pi q)
+//   [72, 200)  one-blob of u[(f - 72) / 32], bin j = (f - 72) % 32:
+//              exp(-((u - (j + 1/2)/32) * 32)^2 / 2)
+//   200..202   albedo, then zeros
+template <int F>
+__device__ __forceinline__ uint32_t feat2(const RowIn& v, int t) {
+    if constexpr (F < 72) {
+        constexpr int a = F / 24;
+        const int oct = ((F % 24) >> 1) + t;
+        float s, c;
+        sincospif(v.q[a] * (float)(1 << oct), &s, &c);
+        return pack(s, c);
+    } else if constexpr (F < 200) {
+        constexpr int ui = (F - 72) >> 5;
+        const int j = ((F - 72) & 31) + 2 * t;
+        const float u = v.u[ui];
+        float d0 = (u - (j + 0.5f) * (1.0f / 32.0f)) * 32.0f;
+        float d1 = (u - (j + 1.5f) * (1.0f / 32.0f)) * 32.0f;
+        return pack(__expf(-0.5f * d0 * d0), __expf(-0.5f * d1 * d1));
+    } else {
+        if (t == 0) return pack(v.alb[0], v.alb[1]);
+        if (t == 1) return pack(v.alb[2], 0.0f);
+        return 0u;
+    }
+}
+
+// Whole-row encoder (104 words) for k_nrc_encode.
+template <int B>
+__device__ __forceinline__ void encode_row(const RowIn& v, uint32_t* out) {
+#pragma unroll
+    for (int t = 0; t < 4; ++t) out[4 * B + t] = feat2<8 * B>(v, t);
+    if constexpr (B + 1 < kIn / 8) encode_row<B + 1>(v, out);
+}
+
+__global__ void k_nrc_encode(const float* __restrict__ raw, uint32_t n, Enc ec, __nv_bfloat16* __restrict__ enc) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    RowIn v = load_row(raw, i, ec);
+    encode_row<0>(v, reinterpret_cast<uint32_t*>(enc + (size_t)i * kIn));
+}
+
+// ---------------------------------------------------------------- forward
 // C fragments of 8 n-tiles (64 columns) -> ReLU'd bf16 A fragments of 4 k-steps.
 __device__ __forceinline__ void to_a_frags(const float (&c)[8][4], uint32_t (&a)[4][4], bool relu) {
 #pragma unroll
@@ -98,8 +222,7 @@ __device__ __forceinline__ void to_a_frags(const float (&c)[8][4], uint32_t (&a)
     }
 }
 
-// Stores / loads 4 k-steps of A fragments as a [rows][64] bf16 tile (row
-// stride 32 words).
+// Stores 4 k-steps of A fragments as a [rows][64] bf16 tile (row stride 32 words).
 __device__ __forceinline__ void store_frags(uint32_t* base, uint32_t row0, uint32_t nrows, const uint32_t (&a)[4][4]) {
     const unsigned lane = threadIdx.x & 31u, g = lane >> 2, t = lane & 3u;
     uint32_t r0 = row0 + g, r1 = row0 + g + 8;
@@ -131,80 +254,52 @@ __device__ __forceinline__ void gemm64(float (&acc)[NT][4], const uint32_t (&a)[
         }
 }
 
-__global__ void k_nrc_encode(const float* __restrict__ raw, uint32_t n, float bx0, float by0, float bz0, float sx,
-                             float sy, float sz, __nv_bfloat16* __restrict__ enc) {
-    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const float* r = raw + 12 * (size_t)i;
-    uint32_t* out = reinterpret_cast<uint32_t*>(enc + (size_t)i * kIn);
-    float q[3] = {(r[0] - bx0) * sx, (r[1] - by0) * sy, (r[2] - bz0) * sz};
-    int w = 0;
-    // 72: for each axis, 12 octaves of (sin, cos)(2^k pi q)
-#pragma unroll
-    for (int a = 0; a < 3; ++a) {
-        float f = q[a];
-#pragma unroll
-        for (int k = 0; k < 12; ++k) {
-            float s, c;
-            sincospif(f, &s, &c);
-            out[w++] = pack(s, c);
-            f *= 2.0f;
-        }
+// Layer 0, k-steps KS..12: A fragments evaluated from the rows' inputs;
+// optionally stored as the encoding ([rows][208] bf16, 104 words per row).
+template <int KS, bool kStore>
+__device__ __forceinline__ void layer0(float (&acc)[8][4], const RowIn& v0, const RowIn& v1, bool ok0, bool ok1,
+                                       const __nv_bfloat16* sw, uint32_t* enc, uint32_t r0, uint32_t r1) {
+    const unsigned lane = threadIdx.x & 31u, g = lane >> 2, t = lane & 3u;
+    uint32_t a[4];
+    a[0] = ok0 ? feat2<KS * 16>(v0, t) : 0u;
+    a[1] = ok1 ? feat2<KS * 16>(v1, t) : 0u;
+    a[2] = ok0 ? feat2<KS * 16 + 8>(v0, t) : 0u;
+    a[3] = ok1 ? feat2<KS * 16 + 8>(v1, t) : 0u;
+    if (kStore) {
+        if (ok0) { enc[(size_t)r0 * 104 + 8 * KS + t] = a[0]; enc[(size_t)r0 * 104 + 8 * KS + 4 + t] = a[2]; }
+        if (ok1) { enc[(size_t)r1 * 104 + 8 * KS + t] = a[1]; enc[(size_t)r1 * 104 + 8 * KS + 4 + t] = a[3]; }
     }
-    // 128: one-blob of (theta/pi, phi/2pi) for wo then n, 32 bins, sigma 1/32
 #pragma unroll
-    for (int v = 0; v < 2; ++v) {
-        float x = r[3 + 3 * v], y = r[4 + 3 * v], z = r[5 + 3 * v];
-        float th = acosf(fminf(fmaxf(z, -1.0f), 1.0f)) * (1.0f / 3.14159265358979f);
-        float ph = atan2f(y, x) * (0.5f / 3.14159265358979f) + 0.5f;
-        float u[2] = {th, ph};
-#pragma unroll
-        for (int h = 0; h < 2; ++h)
-#pragma unroll
-            for (int j = 0; j < 32; j += 2) {
-                float d0 = (u[h] - (j + 0.5f) * (1.0f / 32.0f)) * 32.0f;
-                float d1 = (u[h] - (j + 1.5f) * (1.0f / 32.0f)) * 32.0f;
-                out[w++] = pack(__expf(-0.5f * d0 * d0), __expf(-0.5f * d1 * d1));
-            }
+    for (int nt = 0; nt < 8; ++nt) {
+        const __nv_bfloat16* p = sw + fwd_off(0) + (nt * 8 + g) * fwd_stride(0) + KS * 16 + 2 * t;
+        mma(acc[nt], a, *reinterpret_cast<const uint32_t*>(p), *reinterpret_cast<const uint32_t*>(p + 8));
     }
-    // albedo (3) and 5 zeros of padding
-    out[w++] = pack(r[9], r[10]);
-    out[w++] = pack(r[11], 0.0f);
-    out[w++] = 0u;
-    out[w++] = 0u;
+    if constexpr (KS + 1 < kIn / 16) layer0<KS + 1, kStore>(acc, v0, v1, ok0, ok1, sw, enc, r0, r1);
 }
 
-// Forward pass; kTrain stores the five hidden activations (bf16 [n][64]).
+// Forward pass from raw inputs.  kTrain stores the encoding ([n][208]) and the
+// five hidden activations (layer l at acts + l * ld * 64, [n][64] bf16).
 template <bool kTrain>
-__global__ void __launch_bounds__(128) k_mlp_fwd(const __nv_bfloat16* __restrict__ enc, uint32_t n,
+__global__ void __launch_bounds__(128) k_mlp_fwd(const float* __restrict__ raw, NrcCount cnt, Enc ec, uint32_t ld,
                                                  const __nv_bfloat16* __restrict__ wfwd, float* __restrict__ out,
-                                                 __nv_bfloat16* __restrict__ acts) {
+                                                 __nv_bfloat16* __restrict__ acts, __nv_bfloat16* __restrict__ enc) {
     extern __shared__ __align__(16) __nv_bfloat16 sw[];
     stage(sw, wfwd, kFwdElems);
     __syncthreads();
+    const uint32_t n = rows_of(cnt);
     const unsigned lane = threadIdx.x & 31u, g = lane >> 2, t = lane & 3u, warp = threadIdx.x >> 5;
-    const uint32_t* enc32 = reinterpret_cast<const uint32_t*>(enc);
     for (uint32_t tile = blockIdx.x * 4 + warp; tile * 16 < n; tile += gridDim.x * 4) {
         const uint32_t row0 = tile * 16, r0 = row0 + g, r1 = row0 + g + 8;
+        const bool ok0 = r0 < n, ok1 = r1 < n;
+        RowIn v0 = {}, v1 = {};
+        if (ok0) v0 = load_row(raw, r0, ec);
+        if (ok1) v1 = load_row(raw, r1, ec);
         float acc[8][4];
 #pragma unroll
         for (int nt = 0; nt < 8; ++nt)
 #pragma unroll
             for (int q = 0; q < 4; ++q) acc[nt][q] = 0.0f;
-        // layer 0: K = 208 (13 k-steps), A straight from the encoded inputs
-#pragma unroll 1
-        for (int ks = 0; ks < 13; ++ks) {
-            uint32_t a[4];
-            a[0] = r0 < n ? enc32[(size_t)r0 * 104 + 8 * ks + t] : 0u;
-            a[1] = r1 < n ? enc32[(size_t)r1 * 104 + 8 * ks + t] : 0u;
-            a[2] = r0 < n ? enc32[(size_t)r0 * 104 + 8 * ks + 4 + t] : 0u;
-            a[3] = r1 < n ? enc32[(size_t)r1 * 104 + 8 * ks + 4 + t] : 0u;
-#pragma unroll
-            for (int nt = 0; nt < 8; ++nt) {
-                const __nv_bfloat16* p = sw + fwd_off(0) + (nt * 8 + g) * fwd_stride(0) + ks * 16 + 2 * t;
-                mma(acc[nt], a, *reinterpret_cast<const uint32_t*>(p), *reinterpret_cast<const uint32_t*>(p + 8));
-            }
-        }
+        layer0<0, kTrain>(acc, v0, v1, ok0, ok1, sw, reinterpret_cast<uint32_t*>(enc), r0, r1);
         uint32_t af[4][4];
         to_a_frags(acc, af, true);
         if (kTrain) store_frags(reinterpret_cast<uint32_t*>(acts), row0, n, af);
@@ -212,30 +307,35 @@ __global__ void __launch_bounds__(128) k_mlp_fwd(const __nv_bfloat16* __restrict
         for (int l = 1; l <= 4; ++l) {
             gemm64<8>(acc, af, sw + fwd_off(l), fwd_stride(l));
             to_a_frags(acc, af, true);
-            if (kTrain) store_frags(reinterpret_cast<uint32_t*>(acts + (size_t)l * n * kHid), row0, n, af);
+            if (kTrain) store_frags(reinterpret_cast<uint32_t*>(acts + (size_t)l * ld * kHid), row0, n, af);
         }
         float o[2][4];
         gemm64<2>(o, af, sw + fwd_off(5), fwd_stride(5));
         // columns 0..2 of n-tile 0: lanes t = 0 (cols 0, 1) and t = 1 (col 2)
         if (t == 0) {
-            if (r0 < n) { out[3 * (size_t)r0] = o[0][0]; out[3 * (size_t)r0 + 1] = o[0][1]; }
-            if (r1 < n) { out[3 * (size_t)r1] = o[0][2]; out[3 * (size_t)r1 + 1] = o[0][3]; }
+            if (ok0) { out[3 * (size_t)r0] = o[0][0]; out[3 * (size_t)r0 + 1] = o[0][1]; }
+            if (ok1) { out[3 * (size_t)r1] = o[0][2]; out[3 * (size_t)r1 + 1] = o[0][3]; }
         } else if (t == 1) {
-            if (r0 < n) out[3 * (size_t)r0 + 2] = o[0][0];
-            if (r1 < n) out[3 * (size_t)r1 + 2] = o[0][2];
+            if (ok0) out[3 * (size_t)r0 + 2] = o[0][0];
+            if (ok1) out[3 * (size_t)r1 + 2] = o[0][2];
         }
     }
 }
 
-// Backward pass: loss gradient and dOut of every layer (bf16: layers 0-4
-// [n][64], layer 5 [n][16]); accumulates the loss sum.
+// ---------------------------------------------------------------- backward
+// Loss gradient (mean over the n rows and 3 channels) and dOut of every layer
+// (layer l at douts + l * ld * 64: layers 0-4 [n][64], layer 5 [n][16]);
+// accumulates the loss sum.
 __global__ void __launch_bounds__(128) k_mlp_bwd(const float* __restrict__ pred, const float* __restrict__ target,
-                                                 uint32_t n, float scale, const __nv_bfloat16* __restrict__ acts,
+                                                 NrcCount cnt, uint32_t ld, const __nv_bfloat16* __restrict__ acts,
                                                  const __nv_bfloat16* __restrict__ wbwd,
                                                  __nv_bfloat16* __restrict__ douts, float* __restrict__ loss_sum) {
     extern __shared__ __align__(16) __nv_bfloat16 sw[];
     stage(sw, wbwd, kBwdElems);
     __syncthreads();
+    const uint32_t n = rows_of(cnt);
+    if (n == 0) return;
+    const float scale = 1.0f / (3.0f * (float)n);
     const unsigned lane = threadIdx.x & 31u, g = lane >> 2, t = lane & 3u, warp = threadIdx.x >> 5;
     float loss = 0.0f;
     for (uint32_t tile = blockIdx.x * 4 + warp; tile * 16 < n; tile += gridDim.x * 4) {
@@ -259,7 +359,7 @@ __global__ void __launch_bounds__(128) k_mlp_bwd(const float* __restrict__ pred,
         }
         uint32_t a5[4] = {pack(d[0][0], d[0][1]), pack(d[1][0], d[1][1]), 0u, 0u};
         // store dOut5 ([n][16], 8 words per row)
-        uint32_t* d5 = reinterpret_cast<uint32_t*>(douts + (size_t)5 * n * kHid);
+        uint32_t* d5 = reinterpret_cast<uint32_t*>(douts + (size_t)5 * ld * kHid);
         if (r0 < n) { d5[r0 * 8 + t] = a5[0]; d5[r0 * 8 + 4 + t] = 0u; }
         if (r1 < n) { d5[r1 * 8 + t] = a5[1]; d5[r1 * 8 + 4 + t] = 0u; }
         // dAct4 = dOut5 * W5 (K = 16): B[k][n] = W5[k][n] = W5^T[n][k]
@@ -274,7 +374,7 @@ __global__ void __launch_bounds__(128) k_mlp_bwd(const float* __restrict__ pred,
 #pragma unroll 1
         for (int l = 4; l >= 0; --l) {
             // ReLU mask from the stored activation of layer l
-            const uint32_t* act = reinterpret_cast<const uint32_t*>(acts + (size_t)l * n * kHid);
+            const uint32_t* act = reinterpret_cast<const uint32_t*>(acts + (size_t)l * ld * kHid);
 #pragma unroll
             for (int nt = 0; nt < 8; ++nt) {
                 uint32_t m0 = r0 < n ? act[r0 * 32 + 4 * nt + t] : 0u;
@@ -286,7 +386,7 @@ __global__ void __launch_bounds__(128) k_mlp_bwd(const float* __restrict__ pred,
             }
             uint32_t af[4][4];
             to_a_frags(acc, af, false);
-            store_frags(reinterpret_cast<uint32_t*>(douts + (size_t)l * n * kHid), row0, n, af);
+            store_frags(reinterpret_cast<uint32_t*>(douts + (size_t)l * ld * kHid), row0, n, af);
             if (l == 0) break;
             // dAct_{l-1} = dOut_l * W_l: B[k][n] = W_l[k][n] = W_l^T[n][k]
             gemm64<8>(acc, af, sw + bwd_off(l), bwd_stride(l));
@@ -298,106 +398,160 @@ __global__ void __launch_bounds__(128) k_mlp_bwd(const float* __restrict__ pred,
     if (lane == 0) atomicAdd(loss_sum, loss);
 }
 
-// dW_l[o][i] = sum_r dOut_l[r][o] * in_l[r][i], reduced over the batch.
-// OUT in {16, 64}, IN in {64, 208}; 8 warps; 64-row chunks.
+// ---------------------------------------------------------------- weight gradient
+// Partial dW[o][i] = sum over this CTA's chunks of dOut[r][o] * in[r][i].
+// A (16 x 16: o x r) and B (16 x 8: r x i) fragments come from the row-major
+// [r][o] / [r][i] shared tiles through ldmatrix.trans; each warp owns
+// (16-row o tile, 16-column i pair) items.
 template <int OUT, int IN>
-__global__ void __launch_bounds__(256) k_mlp_wgrad(const __nv_bfloat16* __restrict__ dout, int dout_cols,
-                                                   const __nv_bfloat16* __restrict__ in, uint32_t n,
-                                                   float* __restrict__ grad) {
-    constexpr int kRows = 64, kStride = kRows + 8;
-    constexpr int kMT = OUT / 16, kNT = IN / 8, kTiles = kMT * kNT, kPerWarp = (kTiles + 7) / 8;
-    __shared__ __align__(16) __nv_bfloat16 sd[OUT * kStride];   // dOut^T chunk
-    __shared__ __align__(16) __nv_bfloat16 sa[IN * kStride];    // in^T chunk
-    const unsigned lane = threadIdx.x & 31u, g = lane >> 2, t = lane & 3u, warp = threadIdx.x >> 5;
-    float acc[kPerWarp][4];
+__device__ __forceinline__ void wgrad_layer(const __nv_bfloat16* __restrict__ dout,
+                                            const __nv_bfloat16* __restrict__ in, uint32_t n, __nv_bfloat16* sD,
+                                            __nv_bfloat16* sI, float* __restrict__ part) {
+    constexpr int SD = OUT + 8, SI = IN + 8;
+    constexpr int kIP = IN / 16, kItems = (OUT / 16) * kIP, kPer = (kItems + 7) / 8;
+    constexpr int kVecD = OUT / 8, kVecI = IN / 8;   // 16-byte vectors per row
+    const unsigned lane = threadIdx.x & 31u, warp = threadIdx.x >> 5, g = lane >> 2, t = lane & 3u;
+    const unsigned li = lane >> 3, lj = lane & 7u;
+    float acc[kPer][2][4];
 #pragma unroll
-    for (int k = 0; k < kPerWarp; ++k)
+    for (int k = 0; k < kPer; ++k)
 #pragma unroll
-        for (int q = 0; q < 4; ++q) acc[k][q] = 0.0f;
-    const uint32_t chunks = (n + kRows - 1) / kRows;
+        for (int h = 0; h < 2; ++h)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) acc[k][h][q] = 0.0f;
+    const uint32_t chunks = (n + kChunk - 1) / kChunk;
     for (uint32_t ch = blockIdx.x; ch < chunks; ch += gridDim.x) {
-        const uint32_t base = ch * kRows;
-        __syncthreads();
-        // stage transposed: element (r, c) -> s[c * kStride + r]
-        for (int e = threadIdx.x; e < kRows * OUT; e += blockDim.x) {
-            int r = e / OUT, c = e % OUT;
-            sd[c * kStride + r] = base + r < n ? dout[(size_t)(base + r) * dout_cols + c] : __float2bfloat16(0.0f);
+        const uint32_t base = ch * kChunk;
+        __syncthreads();   // the previous chunk's fragments have been read
+        for (int e = threadIdx.x; e < kChunk * kVecD; e += blockDim.x) {
+            int r = e / kVecD, c = e - r * kVecD;
+            bool ok = base + r < n;
+            cp_async16(sD + r * SD + c * 8, dout + (size_t)(ok ? base + r : 0) * OUT + c * 8, ok);
         }
-        for (int e = threadIdx.x; e < kRows * IN; e += blockDim.x) {
-            int r = e / IN, c = e % IN;
-            sa[c * kStride + r] = base + r < n ? in[(size_t)(base + r) * IN + c] : __float2bfloat16(0.0f);
+        for (int e = threadIdx.x; e < kChunk * kVecI; e += blockDim.x) {
+            int r = e / kVecI, c = e - r * kVecI;
+            bool ok = base + r < n;
+            cp_async16(sI + r * SI + c * 8, in + (size_t)(ok ? base + r : 0) * IN + c * 8, ok);
         }
+        cp_async_wait_all();
         __syncthreads();
 #pragma unroll
-        for (int ks = 0; ks < kRows / 16; ++ks)
+        for (int ks = 0; ks < kChunk / 16; ++ks)
 #pragma unroll
-            for (int k = 0; k < kPerWarp; ++k) {
-                int tile = warp + 8 * k;
-                if (tile < kTiles) {
-                    int mt = tile / kNT, nt = tile % kNT;
-                    const __nv_bfloat16* pa = sd + (mt * 16 + g) * kStride + ks * 16 + 2 * t;
-                    uint32_t a[4] = {*reinterpret_cast<const uint32_t*>(pa),
-                                     *reinterpret_cast<const uint32_t*>(pa + 8 * kStride),
-                                     *reinterpret_cast<const uint32_t*>(pa + 8),
-                                     *reinterpret_cast<const uint32_t*>(pa + 8 * kStride + 8)};
-                    const __nv_bfloat16* pb = sa + (nt * 8 + g) * kStride + ks * 16 + 2 * t;
-                    mma(acc[k], a, *reinterpret_cast<const uint32_t*>(pb), *reinterpret_cast<const uint32_t*>(pb + 8));
+            for (int k = 0; k < kPer; ++k) {
+                const int item = warp + 8 * k;
+                if (item < kItems) {
+                    const int mt = item / kIP, np = item % kIP;
+                    uint32_t a[4], b[4];
+                    ldsm_x4_t(a, sD + (ks * 16 + lj + ((li & 2) ? 8 : 0)) * SD + mt * 16 + ((li & 1) ? 8 : 0));
+                    ldsm_x4_t(b, sI + (ks * 16 + lj + ((li & 1) ? 8 : 0)) * SI + np * 16 + ((li & 2) ? 8 : 0));
+                    mma(acc[k][0], a, b[0], b[1]);
+                    mma(acc[k][1], a, b[2], b[3]);
                 }
             }
     }
 #pragma unroll
-    for (int k = 0; k < kPerWarp; ++k) {
-        int tile = warp + 8 * k;
-        if (tile < kTiles) {
-            int mt = tile / kNT, nt = tile % kNT;
-            int o0 = mt * 16 + g, i0 = nt * 8 + 2 * t;
-            atomicAdd(&grad[o0 * IN + i0], acc[k][0]);
-            atomicAdd(&grad[o0 * IN + i0 + 1], acc[k][1]);
-            atomicAdd(&grad[(o0 + 8) * IN + i0], acc[k][2]);
-            atomicAdd(&grad[(o0 + 8) * IN + i0 + 1], acc[k][3]);
+    for (int k = 0; k < kPer; ++k) {
+        const int item = warp + 8 * k;
+        if (item < kItems) {
+            const int mt = item / kIP, np = item % kIP;
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int o0 = mt * 16 + g, i0 = (2 * np + h) * 8 + 2 * t;
+                *reinterpret_cast<float2*>(part + o0 * IN + i0) = make_float2(acc[k][h][0], acc[k][h][1]);
+                *reinterpret_cast<float2*>(part + (o0 + 8) * IN + i0) = make_float2(acc[k][h][2], acc[k][h][3]);
+            }
         }
     }
 }
 
-// Adam on the FP32 master weights (rows 3..15 of the output layer stay zero),
-// then the bf16 forward and transposed packs.  With ema_a > 0 a step also
-// updates ema = ema_a * ema + (1 - ema_a) * w (ema starts at 0) and the
-// inference pack holds ema / ce (ce = 1 - ema_a^steps, the zero-start
-// correction); without a step the inference pack holds w and ema restarts.
-__global__ void k_adam(float* __restrict__ w, const float* __restrict__ grad, float* __restrict__ m,
-                       float* __restrict__ v, float lr, float b1, float b2, float eps, float c1, float c2,
-                       int do_step, __nv_bfloat16* __restrict__ wfwd, __nv_bfloat16* __restrict__ wbwd,
-                       float* __restrict__ ema, float ema_a, float ce, __nv_bfloat16* __restrict__ winf) {
+// Also advances the step counters (read by k_reduce_adam, which follows).
+__global__ void __launch_bounds__(256) k_wgrad_all(NrcCount cnt, uint32_t ld, const __nv_bfloat16* __restrict__ enc,
+                                                   const __nv_bfloat16* __restrict__ acts,
+                                                   const __nv_bfloat16* __restrict__ douts,
+                                                   float* __restrict__ partial, StepState* st, int do_step) {
+    __shared__ __align__(16) __nv_bfloat16 sD[kChunk * (kHid + 8)];
+    __shared__ __align__(16) __nv_bfloat16 sI[kChunk * (kIn + 8)];
+    const uint32_t n = rows_of(cnt);
+    if (do_step && n > 0 && blockIdx.x == 0 && threadIdx.x == 0) {   // an empty batch takes no step
+        st->step += 1;
+        st->ema_steps += 1;
+    }
+    float* part = partial + (size_t)blockIdx.x * kParams;
+    const size_t layer = (size_t)ld * kHid;
+    wgrad_layer<kHid, kIn>(douts, enc, n, sD, sI, part + param_off(0));
+#pragma unroll 1
+    for (int l = 1; l <= 4; ++l)
+        wgrad_layer<kHid, kHid>(douts + l * layer, acts + (l - 1) * layer, n, sD, sI, part + param_off(l));
+    wgrad_layer<kOut, kHid>(douts + 5 * layer, acts + 4 * layer, n, sD, sI, part + param_off(5));
+}
+
+// ---------------------------------------------------------------- optimiser
+__device__ __forceinline__ void param_coords(int p, int& l, int& o, int& i) {
+    l = 0;
+    while (l < 5 && p >= param_off(l + 1)) ++l;
+    int local = p - param_off(l), in = in_dim(l);
+    o = local / in;
+    i = local - o * in;
+}
+
+// grad = sum of the CTA partials; with do_step, Adam on the FP32 master
+// weights (bias corrections 1 - beta^step; rows 3..15 of the output layer and
+// the padded inputs stay zero), the bf16 forward / transposed packs, and the
+// inference pack: with ema_a > 0, ema = ema_a * ema + (1 - ema_a) * w (ema
+// starts at 0) and the pack holds ema / (1 - ema_a^ema_steps), else w.
+__global__ void k_reduce_adam(const float* __restrict__ partial, int n_part, NrcCount cnt, float* __restrict__ grad,
+                              float* __restrict__ w, float* __restrict__ m, float* __restrict__ v, AdamArgs ar,
+                              const StepState* __restrict__ st, int do_step, __nv_bfloat16* __restrict__ wfwd,
+                              __nv_bfloat16* __restrict__ wbwd, float* __restrict__ ema,
+                              __nv_bfloat16* __restrict__ winf) {
     int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= kParams) return;
-    int l = 0;
-    while (l < 5 && p >= param_off(l + 1)) ++l;
-    int local = p - param_off(l), in = in_dim(l), o = local / in, i = local % in;
+    float gsum = 0.0f;
+    for (int k = 0; k < n_part; ++k) gsum += partial[(size_t)k * kParams + p];
+    grad[p] = gsum;
+    if (!do_step || rows_of(cnt) == 0) return;
+    const float step = (float)st->step;
+    const float c1 = 1.0f - powf(ar.b1, step), c2 = 1.0f - powf(ar.b2, step);
+    int l, o, i;
+    param_coords(p, l, o, i);
     float x = w[p];
     bool frozen = (l == 5 && o >= 3) || (l == 0 && i >= kInReal);
-    if (do_step && !frozen) {
-        float gr = grad[p];
-        float mm = b1 * m[p] + (1.0f - b1) * gr;
-        float vv = b2 * v[p] + (1.0f - b2) * gr * gr;
+    if (!frozen) {
+        float mm = ar.b1 * m[p] + (1.0f - ar.b1) * gsum;
+        float vv = ar.b2 * v[p] + (1.0f - ar.b2) * gsum * gsum;
         m[p] = mm;
         v[p] = vv;
-        x -= lr * (mm / c1) / (sqrtf(vv / c2) + eps);
+        x -= ar.lr * (mm / c1) / (sqrtf(vv / c2) + ar.eps);
         w[p] = x;
     }
     __nv_bfloat16 h = __float2bfloat16_rn(x);
     wfwd[fwd_off(l) + o * fwd_stride(l) + i] = h;
     if (l >= 1) wbwd[bwd_off(l) + i * bwd_stride(l) + o] = h;
     float xi = x;
-    if (ema_a > 0.0f) {
-        if (do_step) {
-            float e = ema_a * ema[p] + (1.0f - ema_a) * x;
-            ema[p] = e;
-            xi = e / ce;
-        } else {
-            ema[p] = 0.0f;
-        }
+    if (ar.ema_a > 0.0f) {
+        float e = ar.ema_a * ema[p] + (1.0f - ar.ema_a) * x;
+        ema[p] = e;
+        xi = e / (1.0f - powf(ar.ema_a, (float)st->ema_steps));
     }
     winf[fwd_off(l) + o * fwd_stride(l) + i] = __float2bfloat16_rn(xi);
+}
+
+// Packs the master weights (after creation or replacement) and restarts the
+// moving average: the inference pack holds w.
+__global__ void k_pack(const float* __restrict__ w, __nv_bfloat16* __restrict__ wfwd,
+                       __nv_bfloat16* __restrict__ wbwd, float* __restrict__ ema, __nv_bfloat16* __restrict__ winf,
+                       StepState* st) {
+    int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p == 0) st->ema_steps = 0;
+    if (p >= kParams) return;
+    int l, o, i;
+    param_coords(p, l, o, i);
+    __nv_bfloat16 h = __float2bfloat16_rn(w[p]);
+    wfwd[fwd_off(l) + o * fwd_stride(l) + i] = h;
+    winf[fwd_off(l) + o * fwd_stride(l) + i] = h;
+    if (l >= 1) wbwd[bwd_off(l) + i * bwd_stride(l) + o] = h;
+    ema[p] = 0.0f;
 }
 
 }  // namespace nrc
@@ -408,12 +562,11 @@ using namespace ilm::nrc;
 
 struct ilm_nrc {
     ilm_nrc_config cfg;
-    int step = 0;
-    int ema_steps = 0;                           // Adam steps since the inference weights restarted
+    DeviceBuffer state;                          // StepState
     DeviceBuffer w, m, v, grad, wfwd, wbwd;      // params and packs
     DeviceBuffer ema, winf;                      // moving average and its inference pack
+    DeviceBuffer partial;                        // k_wgrad_all partial sums
     DeviceBuffer raw, enc, out, target, acts, douts, loss;
-    uint32_t cap = 0;
     cudaStream_t stream = nullptr;
     ~ilm_nrc() {
         if (stream) cudaStreamDestroy(stream);
@@ -422,95 +575,105 @@ struct ilm_nrc {
 
 namespace {
 
-cudaError_t ensure_capacity(ilm_nrc* h, uint32_t n) {
-    if (n <= h->cap) return cudaSuccess;
-    uint32_t c = 1024;
-    while (c < n) c <<= 1;
-    cudaError_t e;
-    if ((e = h->raw.reserve((size_t)c * 12 * 4)) != cudaSuccess) return e;
-    if ((e = h->enc.reserve((size_t)c * kIn * 2)) != cudaSuccess) return e;
-    if ((e = h->out.reserve((size_t)c * 3 * 4)) != cudaSuccess) return e;
-    if ((e = h->target.reserve((size_t)c * 3 * 4)) != cudaSuccess) return e;
-    if ((e = h->acts.reserve((size_t)c * 5 * kHid * 2)) != cudaSuccess) return e;
-    if ((e = h->douts.reserve((size_t)c * 6 * kHid * 2)) != cudaSuccess) return e;
-    h->cap = c;
-    return cudaSuccess;
-}
-
-// Re-packs the bf16 weights (and optionally takes an Adam step).
-cudaError_t adam(ilm_nrc* h, int do_step, cudaStream_t s) {
-    if (do_step) h->step += 1;
-    h->ema_steps = do_step ? h->ema_steps + 1 : 0;
-    float c1 = 1.0f - std::pow(h->cfg.beta1, (float)(h->step > 0 ? h->step : 1));
-    float c2 = 1.0f - std::pow(h->cfg.beta2, (float)(h->step > 0 ? h->step : 1));
-    float ea = h->cfg.ema > 0.0f && h->cfg.ema < 1.0f ? h->cfg.ema : 0.0f;
-    float ce = ea > 0.0f ? 1.0f - (float)std::pow((double)ea, (double)(h->ema_steps > 0 ? h->ema_steps : 1)) : 1.0f;
-    k_adam<<<(kParams + 255) / 256, 256, 0, s>>>(
-        static_cast<float*>(h->w.ptr), static_cast<const float*>(h->grad.ptr), static_cast<float*>(h->m.ptr),
-        static_cast<float*>(h->v.ptr), h->cfg.lr, h->cfg.beta1, h->cfg.beta2, h->cfg.eps, c1, c2, do_step,
-        static_cast<__nv_bfloat16*>(h->wfwd.ptr), static_cast<__nv_bfloat16*>(h->wbwd.ptr),
-        static_cast<float*>(h->ema.ptr), ea, ce, static_cast<__nv_bfloat16*>(h->winf.ptr));
-    return cudaGetLastError();
-}
-
 int blocks_for(uint32_t n, int rows_per_block) {
     int b = (int)((n + rows_per_block - 1) / rows_per_block);
     return b < 1 ? 1 : (b > 148 * 8 ? 148 * 8 : b);
 }
 
-cudaError_t encode(ilm_nrc* h, const float* raw_dev, uint32_t n, cudaStream_t s) {
+Enc enc_params(const ilm_nrc* h) {
     const float* b = h->cfg.bound;
-    float sx = 1.0f / fmaxf(b[3] - b[0], 1e-12f), sy = 1.0f / fmaxf(b[4] - b[1], 1e-12f),
-          sz = 1.0f / fmaxf(b[5] - b[2], 1e-12f);
-    k_nrc_encode<<<(n + 127) / 128, 128, 0, s>>>(raw_dev, n, b[0], b[1], b[2], sx, sy, sz,
-                                                 static_cast<__nv_bfloat16*>(h->enc.ptr));
+    return Enc{b[0], b[1], b[2], 1.0f / fmaxf(b[3] - b[0], 1e-12f), 1.0f / fmaxf(b[4] - b[1], 1e-12f),
+               1.0f / fmaxf(b[5] - b[2], 1e-12f)};
+}
+
+cudaError_t pack(ilm_nrc* h, cudaStream_t s) {
+    k_pack<<<(kParams + 255) / 256, 256, 0, s>>>(
+        static_cast<const float*>(h->w.ptr), static_cast<__nv_bfloat16*>(h->wfwd.ptr),
+        static_cast<__nv_bfloat16*>(h->wbwd.ptr), static_cast<float*>(h->ema.ptr),
+        static_cast<__nv_bfloat16*>(h->winf.ptr), static_cast<StepState*>(h->state.ptr));
     return cudaGetLastError();
 }
 
-cudaError_t forward(ilm_nrc* h, uint32_t n, bool train, float* out_dev, cudaStream_t s) {
-    size_t smem = (size_t)kFwdElems * 2;
-    if (train)
-        k_mlp_fwd<true><<<blocks_for(n, 64), 128, smem, s>>>(static_cast<const __nv_bfloat16*>(h->enc.ptr), n,
-                                                             static_cast<const __nv_bfloat16*>(h->wfwd.ptr), out_dev,
-                                                             static_cast<__nv_bfloat16*>(h->acts.ptr));
-    else   // inference reads the moving-average pack
-        k_mlp_fwd<false><<<blocks_for(n, 64), 128, smem, s>>>(static_cast<const __nv_bfloat16*>(h->enc.ptr), n,
-                                                              static_cast<const __nv_bfloat16*>(h->winf.ptr), out_dev,
-                                                              nullptr);
-    return cudaGetLastError();
-}
+// Rows per batch that a count can give (the batch's share of the cap).
+uint32_t batch_cap(const NrcCount& c) { return c.batches > 1 ? (c.cap + c.batches - 1) / c.batches : c.cap; }
 
-// Loss gradient into h->grad (zeroed first) and the loss sum into h->loss.
-cudaError_t gradients(ilm_nrc* h, uint32_t n, cudaStream_t s) {
+cudaError_t reserve_train(ilm_nrc* h, uint32_t rows) {
     cudaError_t e;
-    if ((e = cudaMemsetAsync(h->grad.ptr, 0, kParams * 4, s)) != cudaSuccess) return e;
+    if ((e = h->enc.reserve((size_t)rows * kIn * 2)) != cudaSuccess) return e;
+    if ((e = h->out.reserve((size_t)rows * 3 * 4)) != cudaSuccess) return e;
+    if ((e = h->acts.reserve((size_t)rows * 5 * kHid * 2)) != cudaSuccess) return e;
+    return h->douts.reserve((size_t)rows * 6 * kHid * 2);
+}
+
+cudaError_t forward(ilm_nrc* h, const float* raw, NrcCount cnt, bool train, float* out, cudaStream_t s) {
+    size_t smem = (size_t)kFwdElems * 2;
+    const uint32_t rows = batch_cap(cnt);
+    int blocks = blocks_for(rows, 64);
+    if (train)
+        k_mlp_fwd<true><<<blocks, 128, smem, s>>>(raw, cnt, enc_params(h), rows,
+                                                  static_cast<const __nv_bfloat16*>(h->wfwd.ptr), out,
+                                                  static_cast<__nv_bfloat16*>(h->acts.ptr),
+                                                  static_cast<__nv_bfloat16*>(h->enc.ptr));
+    else   // inference reads the moving-average pack
+        k_mlp_fwd<false><<<blocks, 128, smem, s>>>(raw, cnt, enc_params(h), rows,
+                                                   static_cast<const __nv_bfloat16*>(h->winf.ptr), out, nullptr,
+                                                   nullptr);
+    return cudaGetLastError();
+}
+
+// Loss gradient into h->grad (and the loss sum into h->loss, zeroed first);
+// with do_step, one Adam step.
+cudaError_t train_rows(ilm_nrc* h, const float* raw, const float* target, NrcCount cnt, int do_step,
+                       cudaStream_t s) {
+    cudaError_t e;
+    const uint32_t cap = batch_cap(cnt);   // layer stride of acts / douts
+    if ((e = reserve_train(h, cap)) != cudaSuccess) return e;
     if ((e = cudaMemsetAsync(h->loss.ptr, 0, 4, s)) != cudaSuccess) return e;
-    if ((e = forward(h, n, true, static_cast<float*>(h->out.ptr), s)) != cudaSuccess) return e;
+    float* pred = static_cast<float*>(h->out.ptr);
+    if ((e = forward(h, raw, cnt, true, pred, s)) != cudaSuccess) return e;
     const __nv_bfloat16* acts = static_cast<const __nv_bfloat16*>(h->acts.ptr);
     __nv_bfloat16* douts = static_cast<__nv_bfloat16*>(h->douts.ptr);
-    k_mlp_bwd<<<blocks_for(n, 64), 128, (size_t)kBwdElems * 2, s>>>(
-        static_cast<const float*>(h->out.ptr), static_cast<const float*>(h->target.ptr), n, 1.0f / (3.0f * n),
-        acts, static_cast<const __nv_bfloat16*>(h->wbwd.ptr), douts, static_cast<float*>(h->loss.ptr));
+    k_mlp_bwd<<<blocks_for(cap, 64), 128, (size_t)kBwdElems * 2, s>>>(
+        pred, target, cnt, cap, acts, static_cast<const __nv_bfloat16*>(h->wbwd.ptr), douts,
+        static_cast<float*>(h->loss.ptr));
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    float* gr = static_cast<float*>(h->grad.ptr);
-    const __nv_bfloat16* enc = static_cast<const __nv_bfloat16*>(h->enc.ptr);
-    int wb = blocks_for(n, 64 * 4);
-    k_mlp_wgrad<64, 208><<<wb, 256, 0, s>>>(douts, kHid, enc, n, gr + param_off(0));
-    for (int l = 1; l <= 4; ++l)
-        k_mlp_wgrad<64, 64><<<wb, 256, 0, s>>>(douts + (size_t)l * n * kHid, kHid, acts + (size_t)(l - 1) * n * kHid,
-                                               n, gr + param_off(l));
-    k_mlp_wgrad<16, 64><<<wb, 256, 0, s>>>(douts + (size_t)5 * n * kHid, kOut, acts + (size_t)4 * n * kHid, n,
-                                           gr + param_off(5));
+    int n_part = (int)std::min<uint32_t>(kMaxPartials, std::max<uint32_t>(1, (cap + kChunk - 1) / kChunk));
+    StepState* st = static_cast<StepState*>(h->state.ptr);
+    k_wgrad_all<<<n_part, 256, 0, s>>>(cnt, cap, static_cast<const __nv_bfloat16*>(h->enc.ptr), acts, douts,
+                                       static_cast<float*>(h->partial.ptr), st, do_step);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    AdamArgs ar{h->cfg.lr, h->cfg.beta1, h->cfg.beta2, h->cfg.eps,
+                h->cfg.ema > 0.0f && h->cfg.ema < 1.0f ? h->cfg.ema : 0.0f};
+    k_reduce_adam<<<(kParams + 255) / 256, 256, 0, s>>>(
+        static_cast<const float*>(h->partial.ptr), n_part, cnt, static_cast<float*>(h->grad.ptr),
+        static_cast<float*>(h->w.ptr), static_cast<float*>(h->m.ptr), static_cast<float*>(h->v.ptr), ar, st, do_step,
+        static_cast<__nv_bfloat16*>(h->wfwd.ptr), static_cast<__nv_bfloat16*>(h->wbwd.ptr),
+        static_cast<float*>(h->ema.ptr), static_cast<__nv_bfloat16*>(h->winf.ptr));
     return cudaGetLastError();
 }
 
-// Device copy of host-or-device input into h's buffer.
+// Device copy of host-or-device input into dst (grown as needed).
 cudaError_t take(DeviceBuffer& dst, const float* src, size_t bytes, cudaStream_t s) {
-    if (!src) return cudaSuccess;
+    cudaError_t e = dst.reserve(bytes);
+    if (e != cudaSuccess) return e;
     return cudaMemcpyAsync(dst.ptr, src, bytes, cudaMemcpyDefault, s);
 }
 
 }  // namespace
+
+namespace ilm {
+
+cudaError_t nrc_infer_async(ilm_nrc* h, const float* raw, NrcCount n, float* out, cudaStream_t s) {
+    return forward(h, raw, n, false, out, s);
+}
+
+cudaError_t nrc_train_async(ilm_nrc* h, const float* raw, const float* target, NrcCount n, cudaStream_t s) {
+    return train_rows(h, raw, target, n, 1, s);
+}
+
+cudaError_t nrc_reserve(ilm_nrc* h, uint32_t rows) { return reserve_train(h, rows); }
+
+}  // namespace ilm
 
 extern "C" {
 
@@ -524,10 +687,13 @@ int32_t ilm_nrc_create(ilm_context* ctx, const ilm_nrc_config* cfg, ilm_nrc** ou
     if ((e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking)) != cudaSuccess) return cuda_fail(ctx, e, "nrc");
     for (DeviceBuffer* b : {&h->w, &h->m, &h->v, &h->grad, &h->ema})
         if ((e = b->reserve(kParams * 4)) != cudaSuccess) return cuda_fail(ctx, e, "nrc");
+    if ((e = h->partial.reserve((size_t)kMaxPartials * kParams * 4)) != cudaSuccess) return cuda_fail(ctx, e, "nrc");
     if ((e = h->wfwd.reserve(kFwdElems * 2)) != cudaSuccess) return cuda_fail(ctx, e, "nrc");
     if ((e = h->winf.reserve(kFwdElems * 2)) != cudaSuccess) return cuda_fail(ctx, e, "nrc");
     if ((e = h->wbwd.reserve(kBwdElems * 2)) != cudaSuccess) return cuda_fail(ctx, e, "nrc");
     if ((e = h->loss.reserve(4)) != cudaSuccess) return cuda_fail(ctx, e, "nrc");
+    if ((e = h->state.reserve(sizeof(StepState))) != cudaSuccess) return cuda_fail(ctx, e, "nrc");
+    cudaMemset(h->state.ptr, 0, sizeof(StepState));
     // He-uniform initialisation from PCG32; padded inputs and output rows 3..15 zero
     std::vector<float> w(kParams, 0.0f);
     Pcg32 rng(cfg->seed);
@@ -547,10 +713,9 @@ int32_t ilm_nrc_create(ilm_context* ctx, const ilm_nrc_config* cfg, ilm_nrc** ou
     cudaMemset(h->wfwd.ptr, 0, kFwdElems * 2);
     cudaMemset(h->winf.ptr, 0, kFwdElems * 2);
     cudaMemset(h->wbwd.ptr, 0, kBwdElems * 2);
-    cudaMemset(h->ema.ptr, 0, kParams * 4);
     cudaFuncSetAttribute(k_mlp_fwd<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kFwdElems * 2);
     cudaFuncSetAttribute(k_mlp_fwd<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kFwdElems * 2);
-    if ((e = adam(h.get(), 0, h->stream)) != cudaSuccess) return cuda_fail(ctx, e, "nrc pack");
+    if ((e = pack(h.get(), h->stream)) != cudaSuccess) return cuda_fail(ctx, e, "nrc pack");
     if ((e = cudaStreamSynchronize(h->stream)) != cudaSuccess) return cuda_fail(ctx, e, "nrc");
     *out = h.release();
     return ILM_OK;
@@ -571,7 +736,7 @@ int32_t ilm_nrc_params(ilm_context* ctx, ilm_nrc* h, float* get, const float* se
     cudaError_t e;
     if (set) {
         if ((e = cudaMemcpy(h->w.ptr, set, kParams * 4, cudaMemcpyDefault)) != cudaSuccess) return cuda_fail(ctx, e, "nrc");
-        if ((e = adam(h, 0, h->stream)) != cudaSuccess) return cuda_fail(ctx, e, "nrc");
+        if ((e = pack(h, h->stream)) != cudaSuccess) return cuda_fail(ctx, e, "nrc");
         cudaStreamSynchronize(h->stream);
     }
     if (get && (e = cudaMemcpy(get, h->w.ptr, kParams * 4, cudaMemcpyDefault)) != cudaSuccess)
@@ -586,16 +751,19 @@ int32_t ilm_nrc_infer(ilm_context* ctx, ilm_nrc* h, const float* inputs, uint64_
     if (cudaSetDevice(ctx->device) != cudaSuccess) return ILM_ERR_CUDA;
     cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : h->stream;
     cudaError_t e;
-    if ((e = ensure_capacity(h, (uint32_t)n)) != cudaSuccess) return cuda_fail(ctx, e, "nrc buffers");
     bool dev_in = classify(inputs) == PtrKind::kDevice, dev_out = classify(out) == PtrKind::kDevice;
     const float* raw = inputs;
     if (!dev_in) {
         if ((e = take(h->raw, inputs, n * 12 * 4, s)) != cudaSuccess) return cuda_fail(ctx, e, "nrc");
         raw = static_cast<const float*>(h->raw.ptr);
     }
-    if ((e = encode(h, raw, (uint32_t)n, s)) != cudaSuccess) return cuda_fail(ctx, e, "nrc encode");
-    float* dst = dev_out ? out : static_cast<float*>(h->out.ptr);
-    if ((e = forward(h, (uint32_t)n, false, dst, s)) != cudaSuccess) return cuda_fail(ctx, e, "nrc forward");
+    float* dst = out;
+    if (!dev_out) {
+        if ((e = h->out.reserve(n * 12)) != cudaSuccess) return cuda_fail(ctx, e, "nrc buffers");
+        dst = static_cast<float*>(h->out.ptr);
+    }
+    if ((e = forward(h, raw, NrcCount{nullptr, (uint32_t)n, 1, 0}, false, dst, s)) != cudaSuccess)
+        return cuda_fail(ctx, e, "nrc forward");
     if (!dev_out) {
         cudaMemcpyAsync(out, dst, n * 12, cudaMemcpyDeviceToHost, s);
         if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_fail(ctx, e, "nrc");
@@ -609,16 +777,18 @@ static int32_t train_impl(ilm_context* ctx, ilm_nrc* h, const float* inputs, con
     if (cudaSetDevice(ctx->device) != cudaSuccess) return ILM_ERR_CUDA;
     cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : h->stream;
     cudaError_t e;
-    if ((e = ensure_capacity(h, (uint32_t)n)) != cudaSuccess) return cuda_fail(ctx, e, "nrc buffers");
     const float* raw = inputs;
     if (classify(inputs) != PtrKind::kDevice) {
         if ((e = take(h->raw, inputs, n * 12 * 4, s)) != cudaSuccess) return cuda_fail(ctx, e, "nrc");
         raw = static_cast<const float*>(h->raw.ptr);
     }
-    if ((e = take(h->target, targets, n * 3 * 4, s)) != cudaSuccess) return cuda_fail(ctx, e, "nrc");
-    if ((e = encode(h, raw, (uint32_t)n, s)) != cudaSuccess) return cuda_fail(ctx, e, "nrc encode");
-    if ((e = gradients(h, (uint32_t)n, s)) != cudaSuccess) return cuda_fail(ctx, e, "nrc gradients");
-    if (step && (e = adam(h, 1, s)) != cudaSuccess) return cuda_fail(ctx, e, "nrc adam");
+    const float* tg = targets;
+    if (classify(targets) != PtrKind::kDevice) {
+        if ((e = take(h->target, targets, n * 3 * 4, s)) != cudaSuccess) return cuda_fail(ctx, e, "nrc");
+        tg = static_cast<const float*>(h->target.ptr);
+    }
+    if ((e = train_rows(h, raw, tg, NrcCount{nullptr, (uint32_t)n, 1, 0}, step, s)) != cudaSuccess)
+        return cuda_fail(ctx, e, "nrc training");
     if (grad_out) cudaMemcpyAsync(grad_out, h->grad.ptr, kParams * 4, cudaMemcpyDefault, s);
     if (loss) {
         float ls = 0.0f;
@@ -642,13 +812,15 @@ int32_t ilm_nrc_gradients(ilm_context* ctx, ilm_nrc* h, const float* inputs, con
 }
 
 int32_t ilm_nrc_encode(ilm_context* ctx, ilm_nrc* h, const float* inputs, uint64_t n, void* enc_out) {
-    if (!ctx || !h || !inputs || !enc_out || n == 0) return ILM_ERR_INVALID_ARGUMENT;
+    if (!ctx || !h || !inputs || !enc_out || n == 0 || n > (1ull << 28)) return ILM_ERR_INVALID_ARGUMENT;
     if (cudaSetDevice(ctx->device) != cudaSuccess) return ILM_ERR_CUDA;
     cudaError_t e;
-    if ((e = ensure_capacity(h, (uint32_t)n)) != cudaSuccess) return cuda_fail(ctx, e, "nrc buffers");
     if ((e = take(h->raw, inputs, n * 12 * 4, h->stream)) != cudaSuccess) return cuda_fail(ctx, e, "nrc");
-    if ((e = encode(h, static_cast<const float*>(h->raw.ptr), (uint32_t)n, h->stream)) != cudaSuccess)
-        return cuda_fail(ctx, e, "nrc encode");
+    if ((e = h->enc.reserve(n * kIn * 2)) != cudaSuccess) return cuda_fail(ctx, e, "nrc buffers");
+    k_nrc_encode<<<(unsigned)((n + 127) / 128), 128, 0, h->stream>>>(static_cast<const float*>(h->raw.ptr),
+                                                                     (uint32_t)n, enc_params(h),
+                                                                     static_cast<__nv_bfloat16*>(h->enc.ptr));
+    if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(ctx, e, "nrc encode");
     cudaMemcpyAsync(enc_out, h->enc.ptr, n * kIn * 2, cudaMemcpyDefault, h->stream);
     if ((e = cudaStreamSynchronize(h->stream)) != cudaSuccess) return cuda_fail(ctx, e, "nrc");
     return ILM_OK;

@@ -43,6 +43,7 @@
 #include "context.h"
 #include "illume_gpu.h"
 #include "kernels.h"
+#include "nrc.h"
 #include "pcg32.h"
 #include "pt.h"
 #include "shapes.cuh"
@@ -52,8 +53,14 @@ namespace {
 
 // counts[] layout
 enum : int { kQ0 = 0, kQ1 = 1, kShadow = 2, kDepth = 3, kTotClosest = 4, kTotShadow = 5, kDropped = 6,
-             kQueries = 7, kTrainSlots = 8, kSamples = 9, kTotQueries = 10, kNumCounts = 12 };
+             kQueries = 7, kTrainSlots = 8, kSamples = 9, kTotQueries = 10, kTotSamples = 11, kFrame = 12,
+             kTrainRows = 13,   // samples gathered by the last frame (kept across renders; trained next frame)
+             kNumCounts = 16 };
 constexpr uint32_t kNone = 0xFFFFFFFFu;
+// A training path's word: slot (bits 0-23) and the vertices it still goes on
+// for past the point where a rendering path would end (bits 24-30;
+// kNotReached before that point).  Rendering paths hold kNone.
+constexpr uint32_t kSlotMask = 0xFFFFFFu, kNotReached = 0x7Fu;
 constexpr int kRec = 18;   // training vertex: inputs (12), 1/beta (3), target (3)
 constexpr uint32_t kMinTrainStride = 16;   // at most one path in 16 trains (the rest use the cache)
 
@@ -78,14 +85,16 @@ struct PtArgs {
     const uint32_t* socc;
     unsigned long long* counts;
     // radiance-cache mode
-    float4* spread[2];        // s, a0, pdf of the last direction, training slot (bits)
+    float4* spread[2];        // s, a0, pdf of the last direction, training word (bits)
     float* q_in;              // queries: 12 floats each
     float4* q_beta;           // throughput rgb, pixel (bits)
+    uint2* q_train;           // training slot (or kNone) and depth of the query vertex
     const float* q_out;       // predictions: 3 floats each
     uint32_t q_cap;
     float* t_rec;             // [slot][depth][kRec]
     uint32_t* t_count;        // vertices recorded per slot
-    uint32_t t_cap, train_stride, train_phase;
+    uint32_t t_cap, train_stride;   // one path in train_stride trains (0: none)
+    uint32_t train_suffix;          // vertices a training path goes on for past the rendering end
     float spread_c;
     uint2* s_train;           // per shadow entry: training slot, depth
     float* t_in;              // gathered training inputs (12 each)
@@ -192,13 +201,18 @@ __global__ void k_pt_camera(PtArgs a, unsigned long long p0, uint32_t count) {
         a.counts[kDepth] = 0;
     }
     const bool valid = k < count;
+    uint32_t frame = 0;
+    if (kNrc) {   // frame f renders path ids f * count ... (the frame counter lives in counts[])
+        frame = (uint32_t)a.counts[kFrame];
+        p0 = (unsigned long long)frame * count;
+    }
     const uint32_t id = (uint32_t)(p0 + k);
-    uint32_t slot = kNone;
+    uint32_t tw = kNone;
     if (kNrc) {
-        // kQueries, kTrainSlots and kSamples are zeroed by the host before this launch
-        bool train = valid && (id % a.train_stride) == a.train_phase;
+        // kQueries, kTrainSlots and kSamples were zeroed before this launch
+        bool train = valid && a.train_stride && (id % a.train_stride) == frame % a.train_stride;
         uint32_t s = warp_append(&a.counts[kTrainSlots], train);
-        if (train && s < a.t_cap) { slot = s; a.t_count[s] = 0; }
+        if (train && s < a.t_cap) { tw = s | (kNotReached << 24); a.t_count[s] = 0; }
     }
     if (!valid) return;
     uint32_t pixel = id % a.npix, sample = (id / a.npix) % a.spp;
@@ -214,7 +228,7 @@ __global__ void k_pt_camera(PtArgs a, unsigned long long p0, uint32_t count) {
     a.beta[0][k] = make_float4(1.0f, 1.0f, 1.0f, __uint_as_float(pixel));
     a.rng[0][k] = make_uint2((uint32_t)rng.state, (uint32_t)(rng.state >> 32));
     a.pid[0][k] = id;
-    if (kNrc) a.spread[0][k] = make_float4(0.0f, 0.0f, 0.0f, __uint_as_float(slot));
+    if (kNrc) a.spread[0][k] = make_float4(0.0f, 0.0f, 0.0f, __uint_as_float(tw));
 }
 
 template <bool kNrc>
@@ -231,9 +245,9 @@ __global__ void __launch_bounds__(256) k_pt_shade(PtArgs a, int cur) {
         float3 o_l, d_l, o_b, d_b, o_c, d_c;
         float tm_l = 0.0f, tm_b = 0.0f;
         float3 c_l = make_float3(0, 0, 0), c_b = make_float3(0, 0, 0);
-        float4 beta_out = make_float4(0, 0, 0, 0), spread_out = make_float4(0, 0, 0, 0);
+        float4 beta_out = make_float4(0, 0, 0, 0), spread_next = make_float4(0, 0, 0, 0);
         uint2 rng_out = make_uint2(0, 0);
-        uint32_t id = 0, pixel = 0, slot = kNone;
+        uint32_t id = 0, pixel = 0, tw = kNone;
         float3 q_p, q_wo, q_n, q_alb, q_beta;
         if (valid) {
             float4 b4 = a.beta[cur][i];
@@ -245,7 +259,7 @@ __global__ void __launch_bounds__(256) k_pt_shade(PtArgs a, int cur) {
             rng.inc = (path_seq(a.seed, id) << 1u) | 1u;
             rng.state = (uint64_t)rs.x | ((uint64_t)rs.y << 32);
             float4 sp = kNrc ? a.spread[cur][i] : make_float4(0, 0, 0, 0);
-            if (kNrc) slot = __float_as_uint(sp.w);
+            if (kNrc) tw = __float_as_uint(sp.w);
             ilm_hit h = a.hits[i];
             const float4* rp = reinterpret_cast<const float4*>(a.rays[cur] + i);
             float4 r1 = rp[1];
@@ -272,8 +286,26 @@ __global__ void __launch_bounds__(256) k_pt_shade(PtArgs a, int cur) {
                     float t2 = h.t * h.t;
                     if (depth == 0) { sp.x = 0.0f; sp.y = t2 / (4.0f * kPiF * cosv); }
                     else sp.x += sqrtf(t2 / (fmaxf(sp.z, 1e-12f) * cosv));
-                    cache_here = slot == kNone && depth >= 1 && sp.x * sp.x > a.spread_c * sp.y;
-                    bool record = slot != kNone && depth < a.max_depth;
+                    const bool spread_out = depth >= 1 && sp.x * sp.x > a.spread_c * sp.y;
+                    if (tw == kNone) {
+                        cache_here = spread_out;
+                    } else {
+                        // a training path goes on for train_suffix vertices past
+                        // the rendering end, then it too ends in the cache
+                        uint32_t left = tw >> 24;
+                        if (left == kNotReached) {
+                            if (spread_out) {
+                                left = min(a.train_suffix, kNotReached - 1u);
+                                cache_here = left == 0;
+                            }
+                        } else {
+                            left -= 1;
+                            cache_here = left == 0;
+                        }
+                        tw = (tw & kSlotMask) | (left << 24);
+                    }
+                    const uint32_t slot = tw == kNone ? kNone : tw & kSlotMask;
+                    const bool record = slot != kNone && !cache_here;
                     if (cache_here || record) {
                         q_p = p; q_wo = wo; q_n = nrm; q_alb = albedo; q_beta = beta;
                     }
@@ -378,7 +410,7 @@ __global__ void __launch_bounds__(256) k_pt_shade(PtArgs a, int cur) {
                             d_c = wi;
                             beta_out = make_float4(nb.x, nb.y, nb.z, __uint_as_float(pixel));
                             rng_out = make_uint2((uint32_t)rng.state, (uint32_t)(rng.state >> 32));
-                            spread_out = make_float4(sp.x, sp.y, pdf, __uint_as_float(slot));
+                            spread_next = make_float4(sp.x, sp.y, pdf, __uint_as_float(tw));
                             cont = true;
                         }
                     }
@@ -391,19 +423,19 @@ __global__ void __launch_bounds__(256) k_pt_shade(PtArgs a, int cur) {
             a.beta[nxt][s] = beta_out;
             a.rng[nxt][s] = rng_out;
             a.pid[nxt][s] = id;
-            if (kNrc) a.spread[nxt][s] = spread_out;
+            if (kNrc) a.spread[nxt][s] = spread_next;
         }
         uint32_t sl = warp_append(&a.counts[kShadow], push_l);
         if (push_l) {
             put_ray(a.srays, sl, o_l, d_l, tm_l);
             a.scontrib[sl] = make_float4(c_l.x, c_l.y, c_l.z, __uint_as_float(pixel));
-            if (kNrc) a.s_train[sl] = make_uint2(slot, depth);
+            if (kNrc) a.s_train[sl] = make_uint2(tw == kNone ? kNone : tw & kSlotMask, depth);
         }
         uint32_t sb = warp_append(&a.counts[kShadow], push_b);
         if (push_b) {
             put_ray(a.srays, sb, o_b, d_b, tm_b);
             a.scontrib[sb] = make_float4(c_b.x, c_b.y, c_b.z, __uint_as_float(pixel));
-            if (kNrc) a.s_train[sb] = make_uint2(slot, depth);
+            if (kNrc) a.s_train[sb] = make_uint2(tw == kNone ? kNone : tw & kSlotMask, depth);
         }
         if (kNrc) {
             uint32_t sq = warp_append(&a.counts[kQueries], query);
@@ -414,6 +446,7 @@ __global__ void __launch_bounds__(256) k_pt_shade(PtArgs a, int cur) {
 #pragma unroll
                 for (int q = 0; q < 12; ++q) qi[q] = in[q];
                 a.q_beta[sq] = make_float4(q_beta.x, q_beta.y, q_beta.z, __uint_as_float(pixel));
+                a.q_train[sq] = make_uint2(tw == kNone ? kNone : tw & kSlotMask, depth);
             }
         }
     }
@@ -472,7 +505,9 @@ __global__ void k_nrc_gather(PtArgs a, uint32_t n_batches, uint32_t batch_rows) 
     }
 }
 
-// film += throughput * max(prediction, 0) for every query of the wave.
+// film += throughput * max(prediction, 0) for every query of the frame; a
+// training path's final query also adds that radiance / beta_k to the target
+// of each vertex k it recorded (self-training).
 __global__ void k_nrc_apply(PtArgs a) {
     uint32_t n = (uint32_t)min(a.counts[kQueries], (unsigned long long)a.q_cap);
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -480,7 +515,24 @@ __global__ void k_nrc_apply(PtArgs a) {
         const float* p = a.q_out + 3 * (size_t)i;
         float3 c = make_float3(b.x * fmaxf(p[0], 0.0f), b.y * fmaxf(p[1], 0.0f), b.z * fmaxf(p[2], 0.0f));
         film_add(a, __float_as_uint(b.w), c);
+        uint2 qt = a.q_train[i];
+        if (qt.x != kNone && good(c)) {
+            for (uint32_t k = 0; k < qt.y && k < a.max_depth; ++k) {
+                float* rec = a.t_rec + ((size_t)qt.x * a.max_depth + k) * kRec;
+                atomicAdd(&rec[15], c.x * rec[12]);
+                atomicAdd(&rec[16], c.y * rec[13]);
+                atomicAdd(&rec[17], c.z * rec[14]);
+            }
+        }
     }
+}
+
+// End of a frame: running totals and the frame counter.
+__global__ void k_nrc_tally(PtArgs a, uint32_t sample_cap) {
+    a.counts[kTotQueries] += min(a.counts[kQueries], (unsigned long long)a.q_cap);
+    a.counts[kTotSamples] += min(a.counts[kSamples], (unsigned long long)sample_cap);
+    a.counts[kFrame] += 1;
+    a.counts[kTrainRows] = a.counts[kSamples];
 }
 
 __global__ void k_pt_resolve(const float* film, float* out, uint32_t n3, float inv_spp) {
@@ -547,6 +599,7 @@ int32_t setup_render(ilm_context* ctx, PtScene& sc, uint32_t spp, uint32_t max_d
     if (e == cudaSuccess) e = b.srays.reserve((size_t)2 * P * sizeof(ilm_ray));
     if (e == cudaSuccess) e = b.scontrib.reserve((size_t)2 * P * 16);
     if (e == cudaSuccess) e = b.socc.reserve((size_t)2 * P * 4);
+    const bool fresh_counts = b.counts.bytes < kNumCounts * 8;
     if (e == cudaSuccess) e = b.counts.reserve(kNumCounts * 8);
     if (e == cudaSuccess) e = b.film.reserve(r.npix * 12);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "render buffers");
@@ -591,7 +644,8 @@ int32_t setup_render(ilm_context* ctx, PtScene& sc, uint32_t spp, uint32_t max_d
     int dev_sms = 148;
     cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, ctx->device);
     r.blocks = dev_sms * 8;
-    cudaMemsetAsync(a.counts, 0, kNumCounts * 8, r.s);
+    // everything but kTrainRows restarts; that one is kept for the next render's first frame
+    cudaMemsetAsync(a.counts, 0, (fresh_counts ? kNumCounts : kTrainRows) * 8, r.s);
     cudaMemsetAsync(a.film, 0, r.npix * 12, r.s);
     return ILM_OK;
 }
@@ -794,114 +848,147 @@ int32_t ilm_render_nrc(ilm_context* ctx, ilm_pt_scene_id scene, ilm_nrc* nrc, co
     const uint32_t n_batches = o->train_steps ? o->train_steps : 4u;
     const uint32_t batch_rows = ((o->train_samples ? o->train_samples : 65536u) + n_batches - 1) / n_batches;
     const uint32_t sample_cap = batch_rows * n_batches;
-    const uint32_t stride = (uint32_t)std::max<uint64_t>(kMinTrainStride, P / train_paths);
-    const uint32_t t_cap = P / stride + 1;
+    // with training off there are no training paths
+    const uint32_t stride = o->train ? (uint32_t)std::max<uint64_t>(kMinTrainStride, P / train_paths) : 0u;
+    const uint32_t t_cap = stride ? P / stride + 1 : 1;
+    const uint32_t q_cap = P + t_cap;
     cudaError_t e = cudaSuccess;
-    if ((e = b.q_in.reserve((size_t)P * 48)) == cudaSuccess && (e = b.q_beta.reserve((size_t)P * 16)) == cudaSuccess &&
-        (e = b.q_out.reserve((size_t)P * 12)) == cudaSuccess &&
+    if ((e = b.q_in.reserve((size_t)q_cap * 48)) == cudaSuccess &&
+        (e = b.q_beta.reserve((size_t)q_cap * 16)) == cudaSuccess &&
+        (e = b.q_train.reserve((size_t)q_cap * 8)) == cudaSuccess &&
+        (e = b.q_out.reserve((size_t)q_cap * 12)) == cudaSuccess &&
         (e = b.t_rec.reserve((size_t)t_cap * o->max_depth * kRec * 4)) == cudaSuccess &&
         (e = b.t_count.reserve((size_t)t_cap * 4)) == cudaSuccess &&
         (e = b.s_train.reserve((size_t)2 * P * 8)) == cudaSuccess &&
-        (e = b.t_in.reserve((size_t)sample_cap * 48)) == cudaSuccess)
-        e = b.t_tg.reserve((size_t)sample_cap * 12);
+        (e = b.t_in.reserve((size_t)sample_cap * 48)) == cudaSuccess &&
+        (e = b.t_tg.reserve((size_t)sample_cap * 12)) == cudaSuccess)
+        e = nrc_reserve(nrc, batch_rows);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "nrc render buffers");
     PtArgs& a = r.a;
     a.q_in = static_cast<float*>(b.q_in.ptr);
     a.q_beta = static_cast<float4*>(b.q_beta.ptr);
+    a.q_train = static_cast<uint2*>(b.q_train.ptr);
     a.q_out = static_cast<const float*>(b.q_out.ptr);
-    a.q_cap = P;
+    a.q_cap = q_cap;
     a.t_rec = static_cast<float*>(b.t_rec.ptr);
     a.t_count = static_cast<uint32_t*>(b.t_count.ptr);
     a.t_cap = t_cap;
     a.train_stride = stride;
+    a.train_suffix = o->train_suffix ? o->train_suffix : 1u;
     a.spread_c = o->spread_c > 0.0f ? o->spread_c : 0.01f;
     a.s_train = static_cast<uint2*>(b.s_train.ptr);
     a.t_in = static_cast<float*>(b.t_in.ptr);
     a.t_tg = static_cast<float*>(b.t_tg.ptr);
     a.sample_cap = sample_cap;
     cudaStream_t s = r.s;
-    // the bounces as CUDA graphs, one per queue parity (train_phase, the only
-    // per-frame field, is read by the camera kernel alone)
-    cudaGraphExec_t graphs[2] = {nullptr, nullptr};
-    auto drop_graphs = [&]() { for (auto& g : graphs) if (g) { cudaGraphExecDestroy(g); g = nullptr; } };
-    if ((e = bounce<true>(a, r.da, r.lp, P, r.err, 0, r.blocks, s)) != cudaSuccess) return cuda_fail(ctx, e, "bounce");
-    for (int q = 0; q < 2; ++q) {
-        cudaGraph_t g;
-        if ((e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal)) != cudaSuccess) break;
-        cudaError_t eb = bounce<true>(a, r.da, r.lp, P, r.err, q, r.blocks, s);
-        e = cudaStreamEndCapture(s, &g);
-        if (e == cudaSuccess) e = eb;
-        if (e == cudaSuccess) e = cudaGraphInstantiate(&graphs[q], g, 0);
-        if (g) cudaGraphDestroy(g);
-        if (e != cudaSuccess) break;
+    if (!b.train_stream) {
+        if ((e = cudaStreamCreateWithFlags(&b.train_stream, cudaStreamNonBlocking)) != cudaSuccess)
+            return cuda_fail(ctx, e, "cudaStreamCreate");
+        cudaEventCreateWithFlags(&b.fork, cudaEventDisableTiming);
+        cudaEventCreateWithFlags(&b.join, cudaEventDisableTiming);
     }
-    if (e != cudaSuccess) { drop_graphs(); return cuda_fail(ctx, e, "nrc bounce graphs"); }
-    uint64_t queries = 0, samples = 0;
-    uint32_t last_nt = 0;
-    float loss = 0.0f;
-    uint32_t frame = 0;
-    double elapsed = 0.0;
-    cudaEvent_t f0, f1;
-    cudaEventCreate(&f0);
-    cudaEventCreate(&f1);
-    unsigned long long cnts[kNumCounts];
-    for (; frame < max_frames; ++frame) {
-        cudaEventRecord(f0, s);
-        a.train_phase = frame % stride;
-        uint64_t p0 = (uint64_t)frame * P;
-        cudaMemsetAsync(a.counts + kQueries, 0, 3 * sizeof(unsigned long long), s);
-        k_pt_camera<true><<<(P + 255) / 256, 256, 0, s>>>(a, p0, P);
-        for (uint32_t depth = 0; depth < o->max_depth && e == cudaSuccess; ++depth)
-            e = cudaGraphLaunch(graphs[depth & 1], s);
-        if (e != cudaSuccess) break;
-        k_nrc_gather<<<r.blocks, 256, 0, s>>>(a, n_batches, batch_rows);
-        cudaMemcpyAsync(cnts, a.counts, sizeof cnts, cudaMemcpyDeviceToHost, s);
-        if ((e = cudaStreamSynchronize(s)) != cudaSuccess) break;
-        uint32_t nq = (uint32_t)std::min<unsigned long long>(cnts[kQueries], P);
-        uint32_t nt = (uint32_t)std::min<unsigned long long>(cnts[kSamples], sample_cap);
-        queries += nq;
-        samples += nt;
-        last_nt = nt;
-        // answer this frame's queries with the current network, then train
-        if (nq) {
-            if ((st = ilm_nrc_infer(ctx, nrc, a.q_in, nq, static_cast<float*>(b.q_out.ptr), s)) != ILM_OK) break;
-            k_nrc_apply<<<r.blocks, 256, 0, s>>>(a);
-        }
+    // samples kept from an earlier render are trained on only if they were
+    // gathered with this batch layout
+    if (!o->train || b.train_layout[0] != n_batches || b.train_layout[1] != batch_rows)
+        cudaMemsetAsync(a.counts + kTrainRows, 0, sizeof(unsigned long long), s);
+    b.train_layout[0] = n_batches;
+    b.train_layout[1] = batch_rows;
+    // One frame, all on the device.  The training branch (train_steps Adam
+    // steps on the samples the previous frame gathered) runs beside the camera
+    // and the bounces, whose later, shorter queues leave most SMs idle; the
+    // cache queries are answered after both, then applied, this frame's
+    // samples gathered and the counters tallied.  Queue sizes and the frame
+    // index stay in device memory, so the frame is one CUDA graph replayed
+    // every frame.
+    cudaStream_t ts = b.train_stream;
+    auto enqueue_frame = [&]() -> cudaError_t {
+        cudaError_t e2;
         if (o->train) {
-            for (uint32_t j = 0; j < n_batches && j < nt; ++j) {
-                uint32_t nj = (nt - j + n_batches - 1) / n_batches;
+            cudaEventRecord(b.fork, s);
+            cudaStreamWaitEvent(ts, b.fork, 0);
+            for (uint32_t j = 0; j < n_batches; ++j) {
                 size_t row = (size_t)j * batch_rows;
-                if ((st = ilm_nrc_train_step(ctx, nrc, a.t_in + 12 * row, a.t_tg + 3 * row, nj, nullptr, s)) != ILM_OK)
-                    break;
+                if ((e2 = nrc_train_async(nrc, a.t_in + 12 * row, a.t_tg + 3 * row,
+                                          NrcCount{a.counts + kTrainRows, sample_cap, n_batches, j}, ts)) !=
+                    cudaSuccess)
+                    return e2;
             }
-            if (st != ILM_OK) break;
+            cudaEventRecord(b.join, ts);
         }
-        cudaEventRecord(f1, s);
-        cudaEventSynchronize(f1);
-        float ms = 0.0f;
-        cudaEventElapsedTime(&ms, f0, f1);
-        elapsed += ms * 1e-3;
-        if (o->time_budget_s > 0.0 && elapsed >= o->time_budget_s) { ++frame; break; }
+        if ((e2 = cudaMemsetAsync(a.counts + kQueries, 0, 3 * sizeof(unsigned long long), s)) != cudaSuccess)
+            return e2;
+        k_pt_camera<true><<<(P + 255) / 256, 256, 0, s>>>(a, 0, P);
+        for (uint32_t depth = 0; depth < o->max_depth; ++depth)
+            if ((e2 = bounce<true>(a, r.da, r.lp, P, r.err, depth & 1, r.blocks, s)) != cudaSuccess) return e2;
+        if (o->train) cudaStreamWaitEvent(s, b.join, 0);
+        if ((e2 = nrc_infer_async(nrc, a.q_in, NrcCount{a.counts + kQueries, q_cap, 1, 0},
+                                  static_cast<float*>(b.q_out.ptr), s)) != cudaSuccess)
+            return e2;
+        k_nrc_apply<<<r.blocks, 256, 0, s>>>(a);
+        k_nrc_gather<<<r.blocks, 256, 0, s>>>(a, n_batches, batch_rows);
+        k_nrc_tally<<<1, 1, 0, s>>>(a, sample_cap);
+        return cudaGetLastError();
+    };
+    // one eager bounce over the empty queues does the launchers' one-time
+    // setup outside the capture
+    if ((e = bounce<true>(a, r.da, r.lp, P, r.err, 0, r.blocks, s)) != cudaSuccess) return cuda_fail(ctx, e, "bounce");
+    cudaGraphExec_t frame_graph = nullptr;
+    {
+        cudaGraph_t g = nullptr;
+        if ((e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal)) != cudaSuccess)
+            return cuda_fail(ctx, e, "cudaStreamBeginCapture");
+        cudaError_t ef = enqueue_frame();
+        e = cudaStreamEndCapture(s, &g);
+        if (e == cudaSuccess) e = ef;
+        if (e == cudaSuccess) e = cudaGraphInstantiate(&frame_graph, g, 0);
+        if (g) cudaGraphDestroy(g);
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "nrc frame graph");
     }
-    cudaEventDestroy(f0);
-    cudaEventDestroy(f1);
-    drop_graphs();
-    if (e != cudaSuccess) return cuda_fail(ctx, e, "ilm_render_nrc");
+    // frames; with a time budget the host keeps one frame queued ahead and
+    // stops launching once the finished frames reach the budget
+    cudaEvent_t done[2];
+    cudaEventCreate(&done[0]);
+    cudaEventCreate(&done[1]);
+    cudaEventRecord(b.ev0, s);
+    uint32_t frame = 0;
+    for (; frame < max_frames; ++frame) {
+        if ((e = cudaGraphLaunch(frame_graph, s)) != cudaSuccess) break;
+        cudaEventRecord(done[frame & 1], s);
+        if (o->time_budget_s > 0.0 && frame >= 1) {
+            if ((e = cudaEventSynchronize(done[(frame - 1) & 1])) != cudaSuccess) break;
+            float ms = 0.0f;
+            cudaEventElapsedTime(&ms, b.ev0, done[(frame - 1) & 1]);
+            if (ms * 1e-3 >= o->time_budget_s) { ++frame; break; }
+        }
+    }
+    cudaEventRecord(b.ev1, s);
+    cudaGraphExecDestroy(frame_graph);
+    if (e != cudaSuccess) {
+        cudaEventDestroy(done[0]);
+        cudaEventDestroy(done[1]);
+        return cuda_fail(ctx, e, "ilm_render_nrc");
+    }
+    unsigned long long cnts[kNumCounts];
+    st = finish_render(ctx, sc, r, rgb_out, 1.0f / (float)(spf * std::max(frame, 1u)), cnts);
+    cudaEventDestroy(done[0]);
+    cudaEventDestroy(done[1]);
     if (st != ILM_OK) return st;
-    if ((st = finish_render(ctx, sc, r, rgb_out, 1.0f / (float)(spf * std::max(frame, 1u)), cnts)) != ILM_OK)
-        return st;
-    if (last_nt) {
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, b.ev0, b.ev1);
+    float loss = 0.0f;
+    uint32_t last_nt = (uint32_t)std::min<unsigned long long>(cnts[kSamples], sample_cap);
+    if (o->train && last_nt) {
         // loss of the network on the first batch of the last frame, for reporting
         uint32_t n0 = (last_nt + n_batches - 1) / n_batches;
         if ((st = ilm_nrc_gradients(ctx, nrc, a.t_in, a.t_tg, n0, nullptr, &loss)) != ILM_OK) return st;
     }
     if (stats) {
         stats->frames = frame;
-        stats->seconds = elapsed;
+        stats->seconds = ms * 1e-3;
         stats->closest_rays = cnts[kTotClosest];
         stats->shadow_rays = cnts[kTotShadow];
-        stats->queries = queries;
-        stats->train_samples = samples;
+        stats->queries = cnts[kTotQueries];
+        stats->train_samples = cnts[kTotSamples];
         stats->last_loss = loss;
     }
     if (cnts[kDropped]) {

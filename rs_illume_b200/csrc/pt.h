@@ -15,13 +15,21 @@ struct PtBuffers {
     DeviceBuffer counts;
     DeviceBuffer film, out;
     // radiance-cache mode: spread per path, cache queries, training records
-    DeviceBuffer spread[2], q_in, q_beta, q_out, t_rec, t_count, s_train, t_in, t_tg;
+    DeviceBuffer spread[2], q_in, q_beta, q_train, q_out, t_rec, t_count, s_train, t_in, t_tg;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    // radiance-cache mode: the training branch's stream, fork/join events, and
+    // the batch layout (batches, rows per batch) of the kept training samples
+    cudaStream_t train_stream = nullptr;
+    cudaEvent_t fork = nullptr, join = nullptr;
+    uint32_t train_layout[2] = {0, 0};
     ~PtBuffers() {
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
+        if (fork) cudaEventDestroy(fork);
+        if (join) cudaEventDestroy(join);
         if (stream) cudaStreamDestroy(stream);
+        if (train_stream) cudaStreamDestroy(train_stream);
     }
 };
 

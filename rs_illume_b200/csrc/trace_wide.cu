@@ -4,7 +4,7 @@
 // Schedules:
 //  * grid: one thread per ray.
 //  * persistent (default): a grid sized to fill the GPU once; each warp claims
-//    rays 64 at a time from a device counter and hands them to lanes that are
+//    rays 64 at a time (32 for short queues) from a device counter and hands them to lanes that are
 //    free.  A claimed ray is first tested against the scene's root box; rays
 //    that miss it (most incoherent rays) are answered at once, at full warp
 //    width, and never occupy a lane.  Each loop iteration advances every busy
@@ -33,6 +33,9 @@ __global__ void __launch_bounds__(128) k_trace_wide(TraceArgs a) {
 template <int W, int kStack, bool kAny, int kMinBlocks>
 __global__ void __launch_bounds__(128, kMinBlocks) k_trace_wide_persistent(TraceArgs a) {
     const uint64_t n = ray_count(a);
+    // A short queue (fewer than two rays per resident lane) is claimed one ray
+    // per lane, so that its rays run side by side rather than two per lane.
+    const unsigned chunk = n < 2ull * gridDim.x * blockDim.x ? 32u : kChunk;
     const unsigned lane = threadIdx.x & 31u;
     const unsigned below = (1u << lane) - 1u;
     WideTracer<W, kStack, kAny> T;
@@ -47,11 +50,11 @@ __global__ void __launch_bounds__(128, kMinBlocks) k_trace_wide_persistent(Trace
         while (need != 0u && !exhausted) {
             if (chunk_next == chunk_end) {
                 unsigned long long b = 0;
-                if (lane == 0) b = atomicAdd(a.counter, (unsigned long long)kChunk);
+                if (lane == 0) b = atomicAdd(a.counter, (unsigned long long)chunk);
                 b = __shfl_sync(0xFFFFFFFFu, b, 0);
                 if (b >= n) { exhausted = true; break; }
                 chunk_next = b;
-                chunk_end = b + kChunk < n ? b + kChunk : n;
+                chunk_end = b + chunk < n ? b + chunk : n;
             }
             unsigned avail = (unsigned)(chunk_end - chunk_next);
             unsigned rank = __popc(need & below);

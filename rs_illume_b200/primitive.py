@@ -281,13 +281,14 @@ class PathTracer:
 
     def render_nrc(self, cache, frames: int = 0, spp_per_frame: int = 1, max_depth: int = 8, rr_depth: int = 3,
                    seed: int = 3, spread_c: float = 0.01, train_paths: int = 16384, train_samples: int = 65536,
-                   time_budget_s: float = 0.0, train: bool = True, train_steps: int = 4, out=None):
+                   time_budget_s: float = 0.0, train: bool = True, train_steps: int = 4, train_suffix: int = 1,
+                   out=None):
         """Path tracing with a RadianceCache (ilm_render_nrc): frames of
         spp_per_frame samples, the cache answering paths whose spread has
         grown, train_steps Adam steps per frame.  Returns (rgb or `out`, stats)."""
         ctx = self.accel.ctx
         o = _lib.ilm_nrc_render_opts(frames, spp_per_frame, max_depth, rr_depth, seed, spread_c, train_paths,
-                                     train_samples, time_budget_s, int(train), train_steps)
+                                     train_samples, time_budget_s, int(train), train_steps, train_suffix)
         st = _lib.ilm_nrc_render_stats()
         if out is None:
             out = np.empty((self.height, self.width, 3), np.float32)

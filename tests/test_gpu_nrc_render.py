@@ -114,6 +114,8 @@ def test_equal_time_relmse_beats_plain_tracer():
     gain = r_plain / r_nrc
     print(f"\nframe {t_frame * 1e3:.2f} ms (plain {t_spp * 1e3:.2f} ms/spp): relMSE cache {r_nrc:.4f}, "
           f"plain at equal time {r_plain:.4f}: gain {gain:.2f}x")
-    assert gain > 1.0, gain
+    # measured about 2x on B200 (1-spp frames at 1024^2); the bar keeps a
+    # margin for frame-time and noise variation between runs
+    assert gain > 1.5, gain
     cache.close()
     ctx.close()
