@@ -19,7 +19,22 @@ Lines printed (rank 0, one JSON line):
             triangle tests per ray on its binary SAH BVH for the same rays.
   cpu_baseline  the CPU oracle (scalar C++ restatement of BVHAccel::intersect)
             on all host threads, same rays.
-`--impl reference` times that CPU restatement alone (the reference itself is
+Further keys, one per workload of the path (each skippable):
+  path_tracer   wavefront path tracer, Cornell box with the level-6 icosphere
+                (81,920 + 34 triangles), 1024x1024, 64 spp stratified, max depth
+                8, Russian roulette from depth 3: rays/s and paths/s, with the
+                CPU path-tracing oracle timed on a 256x256 tile beside it.
+  neural_cache  the same scene with the radiance cache: 1-spp frames at
+                1024x1024 after 200 frames of online training; relMSE per frame
+                against a 2048-spp plain reference (its own noise removed), and
+                the plain tracer's relMSE at the same device time (relMSE(1 spp)
+                * t_spp / t_frame); gain = their ratio.  Also the network's
+                inference throughput and training-step time.
+  batched       32 scenes (icospheres and soups, 1k-2M triangles log-uniform)
+                with 10k-4M rays each (log-uniform; primary, incoherent, shadow
+                thirds), all in one persistent launch per BVH width replayed as
+                a CUDA graph: aggregate Mrays/s.
+`--impl reference` times the CPU restatement alone (the reference itself is
 Rust and cannot be built in this image).
 """
 import argparse
@@ -128,6 +143,146 @@ def cpu_leg(xyz, idx, rays, threads, steps, warmup):
     _, nv, nt = sc.intersect(sub, threads=threads, counters=True)
     value = len(c) * len(times) / sum(times) / 1e6
     return value, times, float(nv.mean()), float(nt.mean()), sc.build_seconds
+
+
+def relmse_fn(ref, var_ref, eps=0.01):
+    def f(x):   # the reference's own noise removed: E[(x - ref)^2] = MSE(x) + Var(ref)
+        return float(np.mean(((x - ref) ** 2 - var_ref) / (ref ** 2 + eps)))
+    return f
+
+
+def path_tracer_leg(rb, wl, ctx, device, steps, cpu):
+    """Cornell box, 1024^2, 64 spp, depth 8, RR from 3."""
+    xyz, idx, mat, alb, emi = wl.cornell(6, 3)
+    cam = wl.CORNELL_CAMERA
+    acc = rb.GpuBVHAccel(ctx, [rb.TriangleMesh(ctx, xyz, idx)], width=8)
+    pt = rb.PathTracer(acc, mat, alb, emi, cam["eye"], cam["fov_deg"], 1024, 1024)
+    pt.render(4, seed=1)
+    secs, rays = [], []
+    for k in range(max(3, min(steps, 5))):
+        _, st = pt.render(64, seed=10 + k)
+        secs.append(st["seconds"])
+        rays.append(st["closest_rays"] + st["shadow_rays"])
+    t = sum(secs)
+    out = {"value": round(sum(rays) / t / 1e6, 2), "unit": "Mrays/s",
+           "paths_per_s": round(len(secs) * 1024 * 1024 * 64 / t / 1e6, 2),
+           "ms_per_frame": round(1e3 * t / len(secs), 3), "rays_per_path": round(rays[0] / (1024 * 1024 * 64), 3),
+           "config": "Cornell box + level-6 icosphere, 1024x1024, 64 spp, depth 8, RR from 3, wave 2^21 paths"}
+    if cpu:
+        import oracle
+        sc = oracle.Scene(xyz, idx)
+        threads = os.cpu_count() or 1
+        t0 = time.perf_counter()
+        _, (nc, ns) = oracle.render_pt(sc, xyz, idx, mat, alb, emi, cam["eye"], cam["fov_deg"], 1024, 1024, 64,
+                                       8, 3, 3, window=(384, 384, 640, 640), threads=threads)
+        tc = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": round((nc + ns) / tc / 1e6, 3), "unit": "Mrays/s", "cores": threads,
+                               "kind": "port", "sample": "256x256 centre tile of the same frame, 64 spp "
+                                                         "(CPU oracle of PathIntegrator)",
+                               "paths_per_s": round(256 * 256 * 64 / tc / 1e6, 4)}
+    return out
+
+
+def neural_cache_leg(rb, wl, ctx, torch, dev):
+    from rs_illume_b200.nrc import RadianceCache
+    res = 1024
+    xyz, idx, mat, alb, emi = wl.cornell(6, 3)
+    cam = wl.CORNELL_CAMERA
+    acc = rb.GpuBVHAccel(ctx, [rb.TriangleMesh(ctx, xyz, idx)], width=8)
+    pt = rb.PathTracer(acc, mat, alb, emi, cam["eye"], cam["fov_deg"], res, res)
+    ra, _ = pt.render(1024, seed=1)
+    rb_, _ = pt.render(1024, seed=2)
+    ref = 0.5 * (ra + rb_)
+    rel = relmse_fn(ref, ((ra - rb_) / 2) ** 2)
+    pt.render(16, seed=3)
+    _, sp = pt.render(16, seed=4)
+    t_spp = sp["seconds"] / 16
+    r1 = float(np.mean([rel(pt.render(1, seed=20 + k)[0]) for k in range(4)]))
+    cache = RadianceCache(ctx, acc.world_bound(), seed=4)
+    _, sw = pt.render_nrc(cache, frames=200, seed=9)
+    rs, ts, qs = [], [], []
+    for k in range(8):
+        img, st = pt.render_nrc(cache, frames=1, seed=100 + k)
+        rs.append(rel(img))
+        ts.append(st["seconds"])
+        qs.append(st["queries"])
+    r_nrc, t_frame = float(np.mean(rs)), float(np.median(ts))
+    r_plain = r1 * t_spp / t_frame
+    # the network alone: inference on 1M rows, a training step on 16384 rows (device buffers)
+    rows = 1 << 20
+    g = torch.Generator(device="cpu").manual_seed(0)
+    x = torch.rand(rows, 12, generator=g)
+    x[:, 3:9] = torch.nn.functional.normalize(x[:, 3:9].reshape(-1, 2, 3) - 0.5, dim=2).reshape(-1, 6)
+    dx = x.to(dev)
+    dy = torch.rand(rows, 3, generator=g).to(dev)
+    dout = torch.empty(rows, 3, device=dev)
+    # a stream of our own: a null stream handle would select the network's stream
+    st_ = torch.cuda.Stream(dev)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    torch.cuda.synchronize()
+    for _ in range(3):
+        cache.infer(dx, dout, stream=st_)
+        cache.train_step(dx[:16384], dy[:16384], stream=st_, with_loss=False)
+    ev[0].record(st_)
+    for _ in range(10):
+        cache.infer(dx, dout, stream=st_)
+    ev[1].record(st_)
+    for _ in range(10):
+        cache.train_step(dx[:16384], dy[:16384], stream=st_, with_loss=False)
+    ev[2].record(st_)
+    torch.cuda.synchronize()
+    t_inf = ev[0].elapsed_time(ev[1]) / 10 / 1e3
+    t_train = ev[1].elapsed_time(ev[2]) / 10 / 1e3
+    flops_row = 2 * (64 * 208 + 4 * 64 * 64 + 16 * 64)
+    cache.close()
+    return {"gain": round(r_plain / r_nrc, 3), "relmse_cache_frame": round(r_nrc, 5),
+            "relmse_plain_equal_time": round(r_plain, 5), "relmse_plain_1spp": round(r1, 5),
+            "ms_per_frame": round(1e3 * t_frame, 3), "plain_ms_per_spp": round(1e3 * t_spp, 3),
+            "queries_per_path": round(float(np.mean(qs)) / res / res, 3),
+            "warm_frames": sw["frames"], "warm_ms_per_frame": round(1e3 * sw["seconds"] / sw["frames"], 3),
+            "mlp": {"infer_rows_per_s": round(rows / t_inf / 1e6, 1), "infer_tflops": round(
+                        rows * flops_row / t_inf / 1e12, 2),
+                    "train_step_ms_16384": round(1e3 * t_train, 4),
+                    "train_tflops": round(3 * 16384 * flops_row / t_train / 1e12, 2),
+                    "kernels": "mma.sync m16n8k16 bf16, FP32 accumulate"},
+            "config": "Cornell box, 1024x1024, 1-spp frames, spread c 0.01, 16384 training paths and "
+                      "4 x 16384 samples per frame, one-vertex self-training suffix, reference 2048 spp"}
+
+
+def batched_leg(rb, wl, ctx, torch, dev, steps):
+    from rs_illume_b200 import batch as bt
+    scenes = wl.batched_workload(5, 32)
+    t0 = time.perf_counter()
+    entries, keep = [], []
+    n_rays = 0
+    for s in scenes:
+        acc = rb.GpuBVHAccel(ctx, [rb.TriangleMesh(ctx, s["xyz"], s["idx"])], width=8)
+        d_rays = torch.from_numpy(s["rays"].view(np.uint8)).to(dev)
+        out = torch.empty(len(s["rays"]) * 16, dtype=torch.uint8, device=dev)
+        entries.append((acc, d_rays, out))
+        keep.append((acc, d_rays, out))
+        n_rays += len(s["rays"])
+    build_s = time.perf_counter() - t0
+    plan = bt.BatchPlan(ctx, entries)
+    stream = torch.cuda.Stream(dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    for _ in range(3):
+        plan.launch(stream)
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    with torch.cuda.stream(stream):
+        for a, b in evs:
+            flush.zero_()
+            a.record(stream)
+            plan.launch(stream)
+            b.record(stream)
+    torch.cuda.synchronize()
+    t = sum(a.elapsed_time(b) for a, b in evs) / 1e3
+    plan.close()
+    return {"value": round(n_rays * steps / t / 1e6, 2), "unit": "Mrays/s", "rays_per_step": n_rays,
+            "ms_per_step": round(1e3 * t / steps, 3), "scenes": len(scenes),
+            "triangles": int(sum(len(s["idx"]) for s in scenes)), "build_seconds": round(build_s, 2),
+            "config": "32 scenes, 1k-2M triangles and 10k-4M rays per scene (log-uniform), closest-hit, "
+                      "width 8, one persistent launch replayed as a CUDA graph, L2 flushed between steps"}
 
 
 def run_reference(args):
@@ -309,6 +464,18 @@ def run_ours(args):
             line["cpu_baseline"] = {"value": round(cv, 3), "unit": UNIT, "cores": threads, "kind": "port",
                                     "sample": "all 2,097,152 closest rays x 3 passes (CPU oracle, binary SAH BVH)",
                                     "n_node_sample": round(nn, 4), "n_tri_sample": round(nt, 4)}
+        for key, enabled, fn in (
+                ("path_tracer", not args.no_pt,
+                 lambda: path_tracer_leg(rb, wl, ctx, dev, args.steps, world == 1 and not args.no_cpu)),
+                ("neural_cache", not args.no_nrc, lambda: neural_cache_leg(rb, wl, ctx, torch, dev)),
+                ("batched", not args.no_batched, lambda: batched_leg(rb, wl, ctx, torch, dev, args.steps))):
+            if not enabled:
+                continue
+            try:
+                line[key] = fn()
+            except Exception as ex:     # a failed leg is reported, not hidden
+                line[key] = {"error": f"{type(ex).__name__}: {ex}"}
+        line["gpu_launches"] = args.steps
         print(json.dumps(line), flush=True)
     ctx.close()
     if dist is not None:
@@ -329,6 +496,9 @@ def main():
     ap.add_argument("--stack-depth", type=int, default=64, choices=[32, 64])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-clocks", action="store_true", help="skip nvidia-smi clock sampling (profiler runs)")
+    ap.add_argument("--no-pt", action="store_true", help="skip the path-tracer workload")
+    ap.add_argument("--no-nrc", action="store_true", help="skip the radiance-cache workload")
+    ap.add_argument("--no-batched", action="store_true", help="skip the batched multi-scene workload")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -64,12 +64,15 @@ class RadianceCache:
                                                    _stream(stream)), "ilm_nrc_infer")
         return out
 
-    def train_step(self, inputs, targets, stream=None) -> float:
+    def train_step(self, inputs, targets, stream=None, with_loss: bool = True):
+        """One Adam step; returns the batch loss, or None without waiting for
+        the step when with_loss is False."""
         loss = ctypes.c_float()
         self.ctx.check(self.ctx._lib.ilm_nrc_train_step(self.ctx.handle, self.handle, ptr(inputs), ptr(targets),
-                                                        _rows(inputs), ctypes.byref(loss), _stream(stream)),
+                                                        _rows(inputs), ctypes.byref(loss) if with_loss else None,
+                                                        _stream(stream)),
                        "ilm_nrc_train_step")
-        return loss.value
+        return loss.value if with_loss else None
 
     def gradients(self, inputs, targets):
         g = np.empty(N_PARAMS, np.float32)
