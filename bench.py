@@ -145,6 +145,22 @@ def cpu_leg(xyz, idx, rays, threads, steps, warmup):
     return value, times, float(nv.mean()), float(nt.mean()), sc.build_seconds
 
 
+def max_over_ranks(values, dist, device):
+    """Per-rank timings -> the maximum over ranks (identity on one rank)."""
+    if dist is None:
+        return list(values)
+    import torch
+    t = torch.tensor(list(values), dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return t.tolist()
+
+
+def replica_throughput(units_per_rank, world, steps, seconds):
+    """Whole-job throughput of `world` replicas, each doing units_per_rank per
+    step for `steps` steps, timed as the max over ranks (weak scaling)."""
+    return world * units_per_rank * steps / seconds
+
+
 def relmse_fn(ref, var_ref, eps=0.01):
     def f(x):   # the reference's own noise removed: E[(x - ref)^2] = MSE(x) + Var(ref)
         return float(np.mean(((x - ref) ** 2 - var_ref) / (ref ** 2 + eps)))
@@ -415,18 +431,12 @@ def run_ours(args):
     h2d_ms = min(x[0] for x in link)
     d2h_ms = min(x[1] for x in link)
 
-    tot = sum(ms) / 1e3
-    tot_any = sum(ms_any) / 1e3
-    tot_e2e = sum(e2e_s)
-    if dist is not None:
-        t = torch.tensor([tot, tot_any, tot_e2e], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        tot, tot_any, tot_e2e = t.tolist()
+    tot, tot_any, tot_e2e = max_over_ranks([sum(ms) / 1e3, sum(ms_any) / 1e3, sum(e2e_s)], dist, dev)
 
     if rank == 0:
-        value = world * N_CLOSEST * args.steps / tot / 1e6
-        any_value = world * N_CLOSEST * args.steps / tot_any / 1e6
-        e2e_value = world * N_CLOSEST * args.steps / tot_e2e / 1e6
+        value = replica_throughput(N_CLOSEST, world, args.steps, tot) / 1e6
+        any_value = replica_throughput(N_CLOSEST, world, args.steps, tot_any) / 1e6
+        e2e_value = replica_throughput(N_CLOSEST, world, args.steps, tot_e2e) / 1e6
         peak, peak_kind = measured_peaks()
         avg_launch = tot / args.steps
         achieved = BYTES_PER_RAY_CLOSEST * N_CLOSEST / avg_launch / 1e9
