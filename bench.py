@@ -65,7 +65,16 @@ DRAM_TRAFFIC = {(8, "persistent", "high", 64): 256464896}
 WORKLOAD = ("incoherent closest-hit: displaced icosphere level 8 (1,310,720 tris, seed 2), "
             "2,097,152 closest rays of 4,194,304 ball rays (radius 3, uniform directions)")
 METRIC = "closest-hit Mrays/s"
+REF_SPP = 16384   # plain-tracer reference of the radiance-cache comparison
 UNIT = "Mrays/s"
+
+
+def measured_bf16():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return float(json.load(f)["bf16_tflops"])
+    return 1590.0
 
 
 def measured_peaks():
@@ -206,10 +215,11 @@ def neural_cache_leg(rb, wl, ctx, torch, dev):
     cam = wl.CORNELL_CAMERA
     acc = rb.GpuBVHAccel(ctx, [rb.TriangleMesh(ctx, xyz, idx)], width=8)
     pt = rb.PathTracer(acc, mat, alb, emi, cam["eye"], cam["fov_deg"], res, res)
-    ra, _ = pt.render(1024, seed=1)
-    rb_, _ = pt.render(1024, seed=2)
-    ref = 0.5 * (ra + rb_)
-    rel = relmse_fn(ref, ((ra - rb_) / 2) ** 2)
+    # reference: the mean of 4 renders of REF_SPP / 4 (a perfect square) spp;
+    # the spread between them estimates its own variance
+    parts = np.stack([pt.render(REF_SPP // 4, seed=1 + k)[0] for k in range(4)])
+    ref = parts.mean(axis=0)
+    rel = relmse_fn(ref, parts.var(axis=0, ddof=1) / 4)
     pt.render(16, seed=3)
     _, sp = pt.render(16, seed=4)
     t_spp = sp["seconds"] / 16
@@ -224,7 +234,43 @@ def neural_cache_leg(rb, wl, ctx, torch, dev):
         qs.append(st["queries"])
     r_nrc, t_frame = float(np.mean(rs)), float(np.median(ts))
     r_plain = r1 * t_spp / t_frame
-    # the network alone: inference on 1M rows, a training step on 16384 rows (device buffers)
+    mlp = mlp_leg(rb, ctx, torch, dev, cache)
+    cache.close()
+    return {"gain": round(r_plain / r_nrc, 3), "relmse_cache_frame": round(r_nrc, 5),
+            "relmse_plain_equal_time": round(r_plain, 5), "relmse_plain_1spp": round(r1, 5),
+            "ms_per_frame": round(1e3 * t_frame, 3), "plain_ms_per_spp": round(1e3 * t_spp, 3),
+            "queries_per_path": round(float(np.mean(qs)) / res / res, 3),
+            "warm_frames": sw["frames"], "warm_ms_per_frame": round(1e3 * sw["seconds"] / sw["frames"], 3),
+            "mlp": mlp,
+            "config": f"Cornell box, 1024x1024, 1-spp frames, spread c 0.01, 16384 training paths and "
+                      f"4 x 16384 samples per frame, one-vertex self-training suffix, reference {REF_SPP} spp"}
+
+
+def nrc_frame_leg(rb, wl, ctx):
+    """Radiance-cache frames alone (profiling): 1024^2, 3 frames of warm-up
+    and one timed 1-spp frame."""
+    from rs_illume_b200.nrc import RadianceCache
+    xyz, idx, mat, alb, emi = wl.cornell(6, 3)
+    cam = wl.CORNELL_CAMERA
+    acc = rb.GpuBVHAccel(ctx, [rb.TriangleMesh(ctx, xyz, idx)], width=8)
+    pt = rb.PathTracer(acc, mat, alb, emi, cam["eye"], cam["fov_deg"], 1024, 1024)
+    cache = RadianceCache(ctx, acc.world_bound(), seed=4)
+    pt.render_nrc(cache, frames=3, seed=9)
+    _, st = pt.render_nrc(cache, frames=1, seed=10)
+    cache.close()
+    return {"ms_per_frame": round(1e3 * st["seconds"], 3), "queries": st["queries"],
+            "rays": st["closest_rays"] + st["shadow_rays"]}
+
+
+def mlp_leg(rb, ctx, torch, dev, cache=None):
+    """The network alone on device buffers: inference on 1M rows and a
+    training step on 16384 rows, CUDA events on a stream of our own.
+    FLOP counts are the algorithmic ones (203 inputs, 3 outputs):
+    forward 59,136 per row, training 3x forward."""
+    from rs_illume_b200.nrc import RadianceCache
+    own = cache is None
+    if own:
+        cache = RadianceCache(ctx, (0.0, 0.0, 0.0, 1.0, 1.0, 1.0), seed=4)
     rows = 1 << 20
     g = torch.Generator(device="cpu").manual_seed(0)
     x = torch.rand(rows, 12, generator=g)
@@ -249,20 +295,16 @@ def neural_cache_leg(rb, wl, ctx, torch, dev):
     torch.cuda.synchronize()
     t_inf = ev[0].elapsed_time(ev[1]) / 10 / 1e3
     t_train = ev[1].elapsed_time(ev[2]) / 10 / 1e3
-    flops_row = 2 * (64 * 208 + 4 * 64 * 64 + 16 * 64)
-    cache.close()
-    return {"gain": round(r_plain / r_nrc, 3), "relmse_cache_frame": round(r_nrc, 5),
-            "relmse_plain_equal_time": round(r_plain, 5), "relmse_plain_1spp": round(r1, 5),
-            "ms_per_frame": round(1e3 * t_frame, 3), "plain_ms_per_spp": round(1e3 * t_spp, 3),
-            "queries_per_path": round(float(np.mean(qs)) / res / res, 3),
-            "warm_frames": sw["frames"], "warm_ms_per_frame": round(1e3 * sw["seconds"] / sw["frames"], 3),
-            "mlp": {"infer_rows_per_s": round(rows / t_inf / 1e6, 1), "infer_tflops": round(
-                        rows * flops_row / t_inf / 1e12, 2),
-                    "train_step_ms_16384": round(1e3 * t_train, 4),
-                    "train_tflops": round(3 * 16384 * flops_row / t_train / 1e12, 2),
-                    "kernels": "mma.sync m16n8k16 bf16, FP32 accumulate"},
-            "config": "Cornell box, 1024x1024, 1-spp frames, spread c 0.01, 16384 training paths and "
-                      "4 x 16384 samples per frame, one-vertex self-training suffix, reference 2048 spp"}
+    if own:
+        cache.close()
+    flops_row = 2 * (203 * 64 + 4 * 64 * 64 + 64 * 3)
+    peak = measured_bf16()
+    inf_tf = rows * flops_row / t_inf / 1e12
+    return {"infer_mrows_per_s": round(rows / t_inf / 1e6, 1), "infer_tflops": round(inf_tf, 2),
+            "infer_frac": round(inf_tf / peak, 4), "train_step_ms_16384": round(1e3 * t_train, 4),
+            "train_tflops": round(3 * 16384 * flops_row / t_train / 1e12, 2),
+            "peak_tflops": peak, "flop_per_row_forward": flops_row,
+            "kernels": "mma.sync m16n8k16 bf16, FP32 accumulate"}
 
 
 def batched_leg(rb, wl, ctx, torch, dev, steps):
@@ -343,6 +385,20 @@ def run_ours(args):
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
 
+    if args.only and args.only != "closest":
+        # one workload alone (profiling runs): its key and nothing else
+        ctx = rb.Context(local)
+        legs = {"pt": ("path_tracer", lambda: path_tracer_leg(rb, wl, ctx, dev, args.steps, False)),
+                "nrc": ("neural_cache", lambda: neural_cache_leg(rb, wl, ctx, torch, dev)),
+                "mlp": ("neural_cache", lambda: mlp_leg(rb, ctx, torch, dev)),
+                "nrcframe": ("neural_cache", lambda: nrc_frame_leg(rb, wl, ctx)),
+                "batched": ("batched", lambda: batched_leg(rb, wl, ctx, torch, dev, args.steps))}
+        key, fn = legs[args.only]
+        res = fn()
+        if rank == 0:
+            print(json.dumps({"only": args.only, key: res}), flush=True)
+        ctx.close()
+        return
     xyz, idx, rays = wl.incoherent_workload(N_RAYS)
     ctx = rb.Context(local, grid_schedule=(args.schedule == "grid"), high_occupancy=(args.occupancy == "high"),
                      stack_depth=args.stack_depth)
@@ -475,10 +531,10 @@ def run_ours(args):
                                     "sample": "all 2,097,152 closest rays x 3 passes (CPU oracle, binary SAH BVH)",
                                     "n_node_sample": round(nn, 4), "n_tri_sample": round(nt, 4)}
         for key, enabled, fn in (
-                ("path_tracer", not args.no_pt,
+                ("path_tracer", not args.no_pt and not args.only,
                  lambda: path_tracer_leg(rb, wl, ctx, dev, args.steps, world == 1 and not args.no_cpu)),
-                ("neural_cache", not args.no_nrc, lambda: neural_cache_leg(rb, wl, ctx, torch, dev)),
-                ("batched", not args.no_batched, lambda: batched_leg(rb, wl, ctx, torch, dev, args.steps))):
+                ("neural_cache", not args.no_nrc and not args.only, lambda: neural_cache_leg(rb, wl, ctx, torch, dev)),
+                ("batched", not args.no_batched and not args.only, lambda: batched_leg(rb, wl, ctx, torch, dev, args.steps))):
             if not enabled:
                 continue
             try:
@@ -509,6 +565,8 @@ def main():
     ap.add_argument("--no-pt", action="store_true", help="skip the path-tracer workload")
     ap.add_argument("--no-nrc", action="store_true", help="skip the radiance-cache workload")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched multi-scene workload")
+    ap.add_argument("--only", choices=["closest", "pt", "nrc", "nrcframe", "mlp", "batched"],
+                    help="run one workload alone (profiling)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

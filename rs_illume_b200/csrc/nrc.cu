@@ -65,6 +65,10 @@ constexpr int kBwdElems = 4 * kHid * (kHid + 8) + kHid * (kOut + 8);            
 constexpr float kLossEps = 0.01f;
 constexpr int kMaxPartials = 148;   // CTAs of k_wgrad_all (one FP32 partial gradient each)
 constexpr int kChunk = 64;          // rows per k_wgrad_all staging step
+// Warps per CTA of the forward / backward kernels: the CTA's weights in shared
+// memory (67 / 40 KB) are shared by all its warps, so more warps per CTA means
+// more warps per SM (3 CTAs fit either way).
+constexpr int kMlpWarps = 8;
 
 struct Enc {   // position normalisation: q = (p - origin) * scale
     float x0, y0, z0, sx, sy, sz;
@@ -280,7 +284,8 @@ __device__ __forceinline__ void layer0(float (&acc)[8][4], const RowIn& v0, cons
 // Forward pass from raw inputs.  kTrain stores the encoding ([n][208]) and the
 // five hidden activations (layer l at acts + l * ld * 64, [n][64] bf16).
 template <bool kTrain>
-__global__ void __launch_bounds__(128) k_mlp_fwd(const float* __restrict__ raw, NrcCount cnt, Enc ec, uint32_t ld,
+__global__ void __launch_bounds__(32 * kMlpWarps) k_mlp_fwd(const float* __restrict__ raw, NrcCount cnt, Enc ec,
+                                                            uint32_t ld,
                                                  const __nv_bfloat16* __restrict__ wfwd, float* __restrict__ out,
                                                  __nv_bfloat16* __restrict__ acts, __nv_bfloat16* __restrict__ enc) {
     extern __shared__ __align__(16) __nv_bfloat16 sw[];
@@ -288,7 +293,7 @@ __global__ void __launch_bounds__(128) k_mlp_fwd(const float* __restrict__ raw, 
     __syncthreads();
     const uint32_t n = rows_of(cnt);
     const unsigned lane = threadIdx.x & 31u, g = lane >> 2, t = lane & 3u, warp = threadIdx.x >> 5;
-    for (uint32_t tile = blockIdx.x * 4 + warp; tile * 16 < n; tile += gridDim.x * 4) {
+    for (uint32_t tile = blockIdx.x * kMlpWarps + warp; tile * 16 < n; tile += gridDim.x * kMlpWarps) {
         const uint32_t row0 = tile * 16, r0 = row0 + g, r1 = row0 + g + 8;
         const bool ok0 = r0 < n, ok1 = r1 < n;
         RowIn v0 = {}, v1 = {};
@@ -326,7 +331,8 @@ __global__ void __launch_bounds__(128) k_mlp_fwd(const float* __restrict__ raw, 
 // Loss gradient (mean over the n rows and 3 channels) and dOut of every layer
 // (layer l at douts + l * ld * 64: layers 0-4 [n][64], layer 5 [n][16]);
 // accumulates the loss sum.
-__global__ void __launch_bounds__(128) k_mlp_bwd(const float* __restrict__ pred, const float* __restrict__ target,
+__global__ void __launch_bounds__(32 * kMlpWarps) k_mlp_bwd(const float* __restrict__ pred,
+                                                            const float* __restrict__ target,
                                                  NrcCount cnt, uint32_t ld, const __nv_bfloat16* __restrict__ acts,
                                                  const __nv_bfloat16* __restrict__ wbwd,
                                                  __nv_bfloat16* __restrict__ douts, float* __restrict__ loss_sum) {
@@ -338,7 +344,7 @@ __global__ void __launch_bounds__(128) k_mlp_bwd(const float* __restrict__ pred,
     const float scale = 1.0f / (3.0f * (float)n);
     const unsigned lane = threadIdx.x & 31u, g = lane >> 2, t = lane & 3u, warp = threadIdx.x >> 5;
     float loss = 0.0f;
-    for (uint32_t tile = blockIdx.x * 4 + warp; tile * 16 < n; tile += gridDim.x * 4) {
+    for (uint32_t tile = blockIdx.x * kMlpWarps + warp; tile * 16 < n; tile += gridDim.x * kMlpWarps) {
         const uint32_t row0 = tile * 16, r0 = row0 + g, r1 = row0 + g + 8;
         // dL/dpred for this lane's output columns 2t, 2t+1 (only 0..2 exist)
         float d[2][2] = {{0.0f, 0.0f}, {0.0f, 0.0f}};
@@ -575,9 +581,12 @@ struct ilm_nrc {
 
 namespace {
 
+// Grid for n rows at rows_per_block, at most the CTAs that are resident at
+// once (3 per SM for the forward / backward kernels' shared memory): each CTA
+// stages its weights once and strides over row tiles.
 int blocks_for(uint32_t n, int rows_per_block) {
     int b = (int)((n + rows_per_block - 1) / rows_per_block);
-    return b < 1 ? 1 : (b > 148 * 8 ? 148 * 8 : b);
+    return b < 1 ? 1 : (b > 148 * 3 ? 148 * 3 : b);
 }
 
 Enc enc_params(const ilm_nrc* h) {
@@ -608,14 +617,14 @@ cudaError_t reserve_train(ilm_nrc* h, uint32_t rows) {
 cudaError_t forward(ilm_nrc* h, const float* raw, NrcCount cnt, bool train, float* out, cudaStream_t s) {
     size_t smem = (size_t)kFwdElems * 2;
     const uint32_t rows = batch_cap(cnt);
-    int blocks = blocks_for(rows, 64);
+    int blocks = blocks_for(rows, 16 * kMlpWarps);
     if (train)
-        k_mlp_fwd<true><<<blocks, 128, smem, s>>>(raw, cnt, enc_params(h), rows,
+        k_mlp_fwd<true><<<blocks, 32 * kMlpWarps, smem, s>>>(raw, cnt, enc_params(h), rows,
                                                   static_cast<const __nv_bfloat16*>(h->wfwd.ptr), out,
                                                   static_cast<__nv_bfloat16*>(h->acts.ptr),
                                                   static_cast<__nv_bfloat16*>(h->enc.ptr));
     else   // inference reads the moving-average pack
-        k_mlp_fwd<false><<<blocks, 128, smem, s>>>(raw, cnt, enc_params(h), rows,
+        k_mlp_fwd<false><<<blocks, 32 * kMlpWarps, smem, s>>>(raw, cnt, enc_params(h), rows,
                                                    static_cast<const __nv_bfloat16*>(h->winf.ptr), out, nullptr,
                                                    nullptr);
     return cudaGetLastError();
@@ -633,7 +642,7 @@ cudaError_t train_rows(ilm_nrc* h, const float* raw, const float* target, NrcCou
     if ((e = forward(h, raw, cnt, true, pred, s)) != cudaSuccess) return e;
     const __nv_bfloat16* acts = static_cast<const __nv_bfloat16*>(h->acts.ptr);
     __nv_bfloat16* douts = static_cast<__nv_bfloat16*>(h->douts.ptr);
-    k_mlp_bwd<<<blocks_for(cap, 64), 128, (size_t)kBwdElems * 2, s>>>(
+    k_mlp_bwd<<<blocks_for(cap, 16 * kMlpWarps), 32 * kMlpWarps, (size_t)kBwdElems * 2, s>>>(
         pred, target, cnt, cap, acts, static_cast<const __nv_bfloat16*>(h->wbwd.ptr), douts,
         static_cast<float*>(h->loss.ptr));
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
