@@ -215,11 +215,12 @@ def neural_cache_leg(rb, wl, ctx, torch, dev):
     cam = wl.CORNELL_CAMERA
     acc = rb.GpuBVHAccel(ctx, [rb.TriangleMesh(ctx, xyz, idx)], width=8)
     pt = rb.PathTracer(acc, mat, alb, emi, cam["eye"], cam["fov_deg"], res, res)
-    # reference: the mean of 4 renders of REF_SPP / 4 (a perfect square) spp;
-    # the spread between them estimates its own variance
-    parts = np.stack([pt.render(REF_SPP // 4, seed=1 + k)[0] for k in range(4)])
+    # reference: the mean of 16 renders of REF_SPP / 16 spp (a perfect square,
+    # and 2^30 paths per render, within the 32-bit path ids); the spread
+    # between them estimates its own variance
+    parts = np.stack([pt.render(REF_SPP // 16, seed=1 + k)[0] for k in range(16)])
     ref = parts.mean(axis=0)
-    rel = relmse_fn(ref, parts.var(axis=0, ddof=1) / 4)
+    rel = relmse_fn(ref, parts.var(axis=0, ddof=1) / 16)
     pt.render(16, seed=3)
     _, sp = pt.render(16, seed=4)
     t_spp = sp["seconds"] / 16
