@@ -17,7 +17,16 @@ template <> struct WideWords<4> { static constexpr int kWords = 4; };
 
 // Byte i of a W-byte array split over 32-bit words lo (bytes 0-3) and hi (4-7).
 __device__ __forceinline__ uint32_t byte_of(uint32_t lo, uint32_t hi, int i) {
-    return ((i < 4 ? lo : hi) >> (8 * (i & 3))) & 0xFFu;
+    return __byte_perm(i < 4 ? lo : hi, 0u, (uint32_t)(i & 3) | 0x4440u);
+}
+
+// The same byte as an exact float, without an integer-to-float conversion
+// (those issue on the narrow XU pipe, which the 48 conversions per node
+// saturate): the byte becomes the low mantissa bits of 2^23, and 2^23 is
+// subtracted again.  Both steps are exact, so the value equals (float)byte.
+__device__ __forceinline__ float byte_float(uint32_t lo, uint32_t hi, int i) {
+    uint32_t bits = __byte_perm(i < 4 ? lo : hi, 0x4B000000u, (uint32_t)(i & 3) | 0x7650u);
+    return __fsub_rn(__uint_as_float(bits), 8388608.0f);
 }
 
 // Decoded node, with near/far planes already swapped for the ray octant.
@@ -72,12 +81,12 @@ template <int W>
 __device__ __forceinline__ bool child_hit(const WideView<W>& v, int i, const RayIn& r, float ix, float iy,
                                           float iz, float tmax, float& tn_out) {
     uint32_t m = byte_of(v.meta[0], v.meta[1], i);
-    float nx = fmaf((float)byte_of(v.nq[0][0], v.nq[0][1], i), v.sx, v.ox);
-    float fx = fmaf((float)byte_of(v.fq[0][0], v.fq[0][1], i), v.sx, v.ox);
-    float ny = fmaf((float)byte_of(v.nq[1][0], v.nq[1][1], i), v.sy, v.oy);
-    float fy = fmaf((float)byte_of(v.fq[1][0], v.fq[1][1], i), v.sy, v.oy);
-    float nz = fmaf((float)byte_of(v.nq[2][0], v.nq[2][1], i), v.sz, v.oz);
-    float fz = fmaf((float)byte_of(v.fq[2][0], v.fq[2][1], i), v.sz, v.oz);
+    float nx = fmaf(byte_float(v.nq[0][0], v.nq[0][1], i), v.sx, v.ox);
+    float fx = fmaf(byte_float(v.fq[0][0], v.fq[0][1], i), v.sx, v.ox);
+    float ny = fmaf(byte_float(v.nq[1][0], v.nq[1][1], i), v.sy, v.oy);
+    float fy = fmaf(byte_float(v.fq[1][0], v.fq[1][1], i), v.sy, v.oy);
+    float nz = fmaf(byte_float(v.nq[2][0], v.nq[2][1], i), v.sz, v.oz);
+    float fz = fmaf(byte_float(v.fq[2][0], v.fq[2][1], i), v.sz, v.oz);
     float tnx = __fmul_rn(__fsub_rn(nx, r.ox), ix), tfx = __fmul_rn(__fsub_rn(fx, r.ox), ix);
     float tny = __fmul_rn(__fsub_rn(ny, r.oy), iy), tfy = __fmul_rn(__fsub_rn(fy, r.oy), iy);
     float tnz = __fmul_rn(__fsub_rn(nz, r.oz), iz), tfz = __fmul_rn(__fsub_rn(fz, r.oz), iz);
