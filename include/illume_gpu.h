@@ -350,6 +350,36 @@ typedef struct {
 int32_t ilm_render_nrc(ilm_context* ctx, ilm_pt_scene_id scene, ilm_nrc* nrc, const ilm_nrc_render_opts* opts,
                        float* rgb_out, ilm_nrc_render_stats* stats);
 
+/* ------------------------------------------------------- film output (host) */
+/* write_image_pfm (core/imageio.rs:264-310): "PF\n<w> <h>\n-1\n", then the
+ * rows bottom to top, 3 little-endian floats per pixel.  rgb holds
+ * width*height*3 floats, row 0 at the top (as ilm_render_pt writes them).
+ * No context or GPU is needed. */
+int32_t ilm_write_pfm(const char* path, const float* rgb, uint32_t width, uint32_t height);
+/* Reads a 3-channel PFM of either byte order back into top-to-bottom rows.
+ * With rgb == NULL only *width and *height are filled; otherwise rgb must
+ * hold (*width)*(*height)*3 floats for the size given on input. */
+int32_t ilm_read_pfm(const char* path, float* rgb, uint32_t* width, uint32_t* height);
+
+/* Film filters (the filters/ directory) and the film's weight table (core/film.rs:70-82):
+ * table[y*16 + x] = evaluate((x + 0.5) * radius.x / 16, (y + 0.5) * radius.y / 16). */
+enum {
+    ILM_FILTER_BOX = 0,        /* filters/box_filter.rs */
+    ILM_FILTER_TRIANGLE = 1,   /* filters/triangle.rs */
+    ILM_FILTER_GAUSSIAN = 2,   /* filters/gaussian.rs: a = alpha */
+    ILM_FILTER_MITCHELL = 3,   /* filters/mitchell.rs: a = B, b = C */
+    ILM_FILTER_LANCZOS = 4     /* filters/sinc.rs: a = tau */
+};
+typedef struct {
+    int32_t kind;
+    float radius[2];
+    float a, b;
+} ilm_filter_desc;
+#define ILM_FILTER_TABLE_WIDTH 16
+/* One filter value at film offset (x, y) from the sample. */
+int32_t ilm_filter_evaluate(const ilm_filter_desc* filter, float x, float y, float* out);
+int32_t ilm_filter_table(const ilm_filter_desc* filter, float* table /* 16 x 16 */);
+
 /* Device error word accumulated by the kernels since the last reset
  * (bit 0: traversal stack overflow, bit 1: iteration cap).  Synchronises. */
 int32_t ilm_device_errors(ilm_context* ctx, uint32_t* out_flags, int32_t reset);

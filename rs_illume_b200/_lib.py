@@ -101,6 +101,11 @@ class ilm_nrc_render_stats(ctypes.Structure):
                 ("last_loss", ctypes.c_float)]
 
 
+class ilm_filter_desc(ctypes.Structure):
+    _fields_ = [("kind", ctypes.c_int32), ("radius", ctypes.c_float * 2), ("a", ctypes.c_float),
+                ("b", ctypes.c_float)]
+
+
 class ilm_batch_desc(ctypes.Structure):
     _fields_ = [("accel", ctypes.c_uint32), ("rays", ctypes.c_void_p), ("n", ctypes.c_uint64),
                 ("hits", ctypes.c_void_p), ("occluded", ctypes.c_void_p)]
@@ -158,6 +163,10 @@ SIGNATURES = {
     "ilm_nrc_encode": (_I32, [_P, _P, _P, _U64, _P]),
     "ilm_render_nrc": (_I32, [_P, _U32, _P, ctypes.POINTER(ilm_nrc_render_opts), _P,
                               ctypes.POINTER(ilm_nrc_render_stats)]),
+    "ilm_write_pfm": (_I32, [ctypes.c_char_p, _P, _U32, _U32]),
+    "ilm_read_pfm": (_I32, [ctypes.c_char_p, _P, ctypes.POINTER(_U32), ctypes.POINTER(_U32)]),
+    "ilm_filter_evaluate": (_I32, [ctypes.POINTER(ilm_filter_desc), _F, _F, ctypes.POINTER(_F)]),
+    "ilm_filter_table": (_I32, [ctypes.POINTER(ilm_filter_desc), _P]),
     "ilm_device_errors": (_I32, [_P, ctypes.POINTER(_U32), _I32]),
     "ilm_synchronize": (_I32, [_P, _P, ctypes.c_double]),
     # workloads

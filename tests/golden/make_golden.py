@@ -17,6 +17,7 @@ Fixtures (golden.npz):
   spheres_*     four spheres (full, z-clipped, phi-clipped, reversed) and a
                 triangle soup, 4,096 ball rays
   pt_*          Cornell box (level-3 icosphere), 24x24, 16 spp, depth 8
+pt_tile.pfm holds the same image as a PFM file (ilm_write_pfm).
 """
 import hashlib
 import os
@@ -93,6 +94,8 @@ def main():
     out.update(pt_image=img, pt_rays=np.array([nc, ns], np.uint64),
                pt_scene=np.frombuffer(digest(xyz, idx, mat, alb, emi).encode(), np.uint8))
     np.savez_compressed(os.path.join(HERE, "golden.npz"), **out)
+    from rs_illume_b200 import image
+    image.write_pfm(os.path.join(HERE, "pt_tile.pfm"), img)
     print("wrote", os.path.join(HERE, "golden.npz"), {k: v.shape for k, v in out.items()})
 
 

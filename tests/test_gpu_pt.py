@@ -98,3 +98,12 @@ def test_render_rejects_bad_options(cornell_small):
         pt.render(10)          # not a perfect square
     with pytest.raises(rb.IllumeError):
         pt.render(16, max_depth=0)
+
+
+def test_render_written_as_pfm(cornell_small, tmp_path):
+    from rs_illume_b200 import image
+    pt, _, _ = cornell_small
+    img, _ = pt.render(4, seed=2)
+    p = str(tmp_path / "frame.pfm")
+    image.write_pfm(p, img)
+    assert image.read_pfm(p).tobytes() == img.tobytes()
