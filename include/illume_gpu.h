@@ -136,6 +136,46 @@ int32_t ilm_accel_get_info(ilm_context* ctx, ilm_accel_id accel, ilm_accel_info*
 int32_t ilm_accel_binary_nodes(ilm_context* ctx, ilm_accel_id accel, void* out_nodes,
                                uint32_t* out_prim_order);
 
+/* ------------------------------------------------- surface interactions */
+/* Optional per-vertex data of a triangle mesh (TriangleMesh::new,
+ * shapes/triangle.rs:36-73): shading normals n and tangents s (3 floats per
+ * vertex), parametric uv (2 floats per vertex), each NULL when absent, and
+ * reverse_orientation.  Set before the mesh is used by ilm_accel_build. */
+typedef struct {
+    const float* n;
+    const float* s;
+    const float* uv;
+    int32_t reverse_orientation;
+} ilm_mesh_attrs;
+int32_t ilm_mesh_set_attrs(ilm_context* ctx, ilm_mesh_id mesh, const ilm_mesh_attrs* attrs);
+
+/* The SurfaceInteraction that Triangle::intersect builds for a hit
+ * (shapes/triangle.rs:264-415 with SurfaceInteraction::new and
+ * set_shading_geometry, core/interaction.rs:262-339): the barycentrics are
+ * recomputed with the same watertight arithmetic as the traversal, then
+ * uv, dpdu/dpdv (uv determinant as in pbrt, D14 repaired; coordinate frame of
+ * the geometric normal when degenerate), p and its error bound gamma(7),
+ * the geometric normal of (p0-p2)x(p1-p2) (flipped for reverse_orientation),
+ * and, when the mesh has normals or tangents, the shading frame and dndu/dndv.
+ * Without them the shading frame is the geometric one (n, dpdu, dpdv, 0, 0). */
+typedef struct {
+    float p[3], p_error[3];
+    float n[3];
+    float uv[2];
+    float dpdu[3], dpdv[3], dndu[3], dndv[3];
+    float shading_n[3], shading_dpdu[3], shading_dpdv[3], shading_dndu[3], shading_dndv[3];
+    float wo[3];
+    float t;
+    uint32_t prim;
+    uint32_t kind;   /* ILM_SI_MISS, ILM_SI_TRIANGLE, or ILM_SI_SPHERE (p, wo, t, prim only) */
+} ilm_surface_interaction;
+enum { ILM_SI_MISS = 0, ILM_SI_TRIANGLE = 1, ILM_SI_SPHERE = 2 };
+/* For each (ray, hit) pair from ilm_intersect_closest on the same accel, its
+ * SurfaceInteraction (176 bytes).  Buffers all on the host (the call returns
+ * with the results) or all on the device (stream-ordered). */
+int32_t ilm_surface_interactions(ilm_context* ctx, ilm_accel_id accel, const ilm_ray* rays, const ilm_hit* hits,
+                                 uint64_t n, ilm_surface_interaction* out, void* stream);
+
 /* Host-only build of the same structure, for inspection and tests (no GPU
  * needed): one triangle mesh followed by one sphere set.  ilm_host_layout_copy
  * fills any non-NULL output: binary nodes (32 B each), ordered primitive ids,

@@ -51,6 +51,7 @@ _SIG = {
     "orc_intersect": (ctypes.c_int64, [_P, _P, ctypes.c_uint64, _P, _P, _P, ctypes.c_int]),
     "orc_intersect_p": (ctypes.c_int64, [_P, _P, ctypes.c_uint64, _P, _P, _P, ctypes.c_int]),
     "orc_triangle_intersect": (ctypes.c_int, [_P, _P, _P, _P, ctypes.c_int, _P]),
+    "orc_surface_interaction": (ctypes.c_int, [_P, _P, _P, _P, ctypes.c_int, _P, _P]),
     "orc_sphere_intersect": (ctypes.c_int, [_P, _P, ctypes.c_int, _P]),
     "orc_sphere_world_bound": (None, [_P, _P]),
     "orc_last_trace_seconds": (ctypes.c_double, []),
@@ -209,6 +210,27 @@ def triangle_intersect(p0, p1, p2, o, d, tmax=float("inf"), closest=True):
     out = np.zeros(4, np.float32)
     ok = load().orc_triangle_intersect(_p(pts[0]), _p(pts[1]), _p(pts[2]), _p(r), int(closest), _p(out))
     return tuple(float(x) for x in out) if ok else None
+
+
+SI_DTYPE = np.dtype([
+    ("p", "<f4", (3,)), ("p_error", "<f4", (3,)), ("n", "<f4", (3,)), ("uv", "<f4", (2,)),
+    ("dpdu", "<f4", (3,)), ("dpdv", "<f4", (3,)), ("dndu", "<f4", (3,)), ("dndv", "<f4", (3,)),
+    ("shading_n", "<f4", (3,)), ("shading_dpdu", "<f4", (3,)), ("shading_dpdv", "<f4", (3,)),
+    ("shading_dndu", "<f4", (3,)), ("shading_dndv", "<f4", (3,)), ("wo", "<f4", (3,)), ("t", "<f4"),
+    ("prim", "<u4"), ("kind", "<u4")])
+
+
+def surface_interaction(p, o, d, tmax=float("inf"), n=None, s=None, uv=None, reverse=False):
+    """The SurfaceInteraction of the hit on triangle p (3 x 3 vertices)
+    (oracle/interaction.cpp); None on a miss."""
+    p = np.ascontiguousarray(p, np.float32).reshape(9)
+    arrs = [None if a is None else np.ascontiguousarray(a, np.float32).ravel() for a in (n, s, uv)]
+    r = np.zeros(1, RAY_DTYPE)
+    r["o"], r["d"], r["tmax"] = o, d, tmax
+    out = np.zeros(1, SI_DTYPE)
+    hit = load().orc_surface_interaction(_p(p), *(_p(a) if a is not None else None for a in arrs), int(reverse),
+                                         _p(r), _p(out))
+    return out[0] if hit else None
 
 
 def sphere_intersect(desc: orc_sphere_desc, o, d, tmax=float("inf")):

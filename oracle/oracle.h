@@ -83,6 +83,22 @@ int64_t orc_intersect_p(void* scene, const orc_ray* rays, uint64_t n, uint8_t* o
 /* Single-shape tests for known-answer checks.  out = {t, b0, b1, b2}. */
 int orc_triangle_intersect(const float* p0, const float* p1, const float* p2,
                            const orc_ray* r, int closest, float* out);
+/* The SurfaceInteraction of a hit on triangle p (9 floats), with optional
+ * per-vertex normals / tangents (9 floats) and uvs (6 floats); 1 on a hit.
+ * Same layout as ilm_surface_interaction (kind 1 = triangle). */
+typedef struct {
+    float p[3], p_error[3];
+    float n[3];
+    float uv[2];
+    float dpdu[3], dpdv[3], dndu[3], dndv[3];
+    float shading_n[3], shading_dpdu[3], shading_dpdv[3], shading_dndu[3], shading_dndv[3];
+    float wo[3];
+    float t;
+    uint32_t prim;
+    uint32_t kind;
+} orc_si;
+int orc_surface_interaction(const float* p, const float* n, const float* s, const float* uv, int reverse,
+                            const orc_ray* r, orc_si* out);
 /* out = {t, u, v}. */
 int orc_sphere_intersect(const orc_sphere_desc* s, const orc_ray* r, int closest, float* out);
 void orc_sphere_world_bound(const orc_sphere_desc* s, float out[6]);

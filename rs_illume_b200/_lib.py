@@ -46,7 +46,14 @@ BIN_NODE_DTYPE = np.dtype([("bmin", "<f4", (3,)), ("bmax", "<f4", (3,)), ("offse
                            ("n_prims", "<u2"), ("axis", "u1"), ("pad", "u1")])
 PRIM_REC_DTYPE = np.dtype([("p0", "<f4", (3,)), ("prim", "<u4"), ("p1", "<f4", (3,)), ("flags", "<u4"),
                            ("p2", "<f4", (3,)), ("aux", "<u4")])
-assert RAY_DTYPE.itemsize == 32 and HIT_DTYPE.itemsize == 16
+SURFACE_INTERACTION_DTYPE = np.dtype([
+    ("p", "<f4", (3,)), ("p_error", "<f4", (3,)), ("n", "<f4", (3,)), ("uv", "<f4", (2,)),
+    ("dpdu", "<f4", (3,)), ("dpdv", "<f4", (3,)), ("dndu", "<f4", (3,)), ("dndv", "<f4", (3,)),
+    ("shading_n", "<f4", (3,)), ("shading_dpdu", "<f4", (3,)), ("shading_dpdv", "<f4", (3,)),
+    ("shading_dndu", "<f4", (3,)), ("shading_dndv", "<f4", (3,)), ("wo", "<f4", (3,)), ("t", "<f4"),
+    ("prim", "<u4"), ("kind", "<u4")])
+SI_MISS, SI_TRIANGLE, SI_SPHERE = 0, 1, 2
+assert RAY_DTYPE.itemsize == 32 and HIT_DTYPE.itemsize == 16 and SURFACE_INTERACTION_DTYPE.itemsize == 176
 assert BIN_NODE_DTYPE.itemsize == 32 and PRIM_REC_DTYPE.itemsize == 48
 
 
@@ -101,6 +108,11 @@ class ilm_nrc_render_stats(ctypes.Structure):
                 ("last_loss", ctypes.c_float)]
 
 
+class ilm_mesh_attrs(ctypes.Structure):
+    _fields_ = [("n", ctypes.c_void_p), ("s", ctypes.c_void_p), ("uv", ctypes.c_void_p),
+                ("reverse_orientation", ctypes.c_int32)]
+
+
 class ilm_filter_desc(ctypes.Structure):
     _fields_ = [("kind", ctypes.c_int32), ("radius", ctypes.c_float * 2), ("a", ctypes.c_float),
                 ("b", ctypes.c_float)]
@@ -133,6 +145,8 @@ SIGNATURES = {
     "ilm_last_error_string": (ctypes.c_char_p, [_P]),
     "ilm_mesh_upload": (_I32, [_P, _P, _U32, _P, _U32, ctypes.POINTER(_U32)]),
     "ilm_spheres_upload": (_I32, [_P, _P, _U32, ctypes.POINTER(_U32)]),
+    "ilm_mesh_set_attrs": (_I32, [_P, _U32, ctypes.POINTER(ilm_mesh_attrs)]),
+    "ilm_surface_interactions": (_I32, [_P, _U32, _P, _P, _U64, _P, _P]),
     "ilm_accel_build": (_I32, [_P, _P, _U32, ctypes.POINTER(ilm_build_opts), ctypes.POINTER(_U32)]),
     "ilm_accel_destroy": (_I32, [_P, _U32]),
     "ilm_accel_world_bound": (_I32, [_P, _U32, _P]),

@@ -158,6 +158,36 @@ int32_t ilm_mesh_upload(ilm_context* ctx, const float* xyz, uint32_t nv, const u
     return ILM_OK;
 }
 
+int32_t ilm_mesh_set_attrs(ilm_context* ctx, ilm_mesh_id mesh, const ilm_mesh_attrs* attrs) {
+    if (!ctx || !attrs) return ILM_ERR_INVALID_ARGUMENT;
+    auto it = ctx->meshes.find(mesh);
+    if (it == ctx->meshes.end()) {
+        set_error(ctx, "ilm_mesh_set_attrs: unknown mesh id");
+        return ILM_ERR_NOT_FOUND;
+    }
+    Mesh& m = *it->second;
+    if (m.is_spheres || m.built) {
+        set_error(ctx, "ilm_mesh_set_attrs: not a triangle mesh, or already used by an accel build");
+        return ILM_ERR_INVALID_ARGUMENT;
+    }
+    const size_t nv = m.xyz.size() / 3;
+    auto take = [&](const float* src, size_t per, std::vector<float>& dst) -> bool {
+        dst.clear();
+        if (!src) return true;
+        dst.assign(src, src + per * nv);
+        for (float v : dst)
+            if (!std::isfinite(v)) return false;
+        return true;
+    };
+    if (!take(attrs->n, 3, m.n) || !take(attrs->s, 3, m.s) || !take(attrs->uv, 2, m.uv)) {
+        set_error(ctx, "ilm_mesh_set_attrs: non-finite attribute value");
+        m.n.clear(); m.s.clear(); m.uv.clear();
+        return ILM_ERR_INVALID_ARGUMENT;
+    }
+    m.reverse = attrs->reverse_orientation != 0;
+    return ILM_OK;
+}
+
 int32_t ilm_spheres_upload(ilm_context* ctx, const ilm_sphere_desc* spheres, uint32_t n, ilm_mesh_id* out) {
     if (!ctx || !out || (n > 0 && !spheres)) return ILM_ERR_INVALID_ARGUMENT;
     auto m = std::make_unique<Mesh>();
@@ -200,6 +230,8 @@ int32_t ilm_accel_build(ilm_context* ctx, const ilm_mesh_id* meshes, uint32_t n_
         views.push_back({m.is_spheres, m.xyz.data(), m.idx.data(), m.spheres.data(), m.n_prims});
     }
     auto acc = std::make_unique<Accel>();
+    acc->mesh_ids.assign(meshes, meshes + n_meshes);
+    for (uint32_t k = 0; k < n_meshes; ++k) ctx->meshes[meshes[k]]->built = true;
     std::string msg = build_layout(views, width, max_prims, (int)std::thread::hardware_concurrency(), acc->host);
     if (!msg.empty()) {
         set_error(ctx, "ilm_accel_build: " + msg);

@@ -37,6 +37,20 @@ struct Mesh {
     std::vector<uint32_t> idx;
     std::vector<SphereRec> spheres;
     uint32_t n_prims = 0;
+    // optional per-vertex shading data (ilm_mesh_set_attrs)
+    std::vector<float> n, s, uv;
+    bool reverse = false;
+    bool built = false;              // used by an accel build: attributes are fixed
+};
+
+// Per-accel data for rebuilding SurfaceInteractions (built on first use):
+// vertices and attributes of all its triangle meshes, concatenated, and per
+// primitive id its three global vertex indices and its mesh slot.
+struct ShadingData {
+    DeviceBuffer vtx, nrm, tan, uv;  // 3, 3, 3, 2 floats per vertex
+    DeviceBuffer tri;                // uint4 per primitive: i0, i1, i2, mesh slot (kShadeSphere for spheres)
+    DeviceBuffer mesh;               // uint32 flags per mesh slot
+    bool ready = false;
 };
 
 struct Accel {
@@ -46,6 +60,8 @@ struct Accel {
     double build_seconds = 0.0;
     // per-accel launch choices (ilm_accel_set_launch); -1 = context default
     int stack_depth = -1, schedule = -1, high_occupancy = -1;
+    std::vector<ilm_mesh_id> mesh_ids;   // the shapes, in primitive-id order
+    ShadingData shading;
 
     DeviceAccel view() const {
         DeviceAccel a;

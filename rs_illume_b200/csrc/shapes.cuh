@@ -16,6 +16,7 @@ namespace ilm {
 constexpr float kGamma2 = 0x1.000002p-23f;
 constexpr float kGamma3 = 0x1.800004p-23f;
 constexpr float kGamma5 = 0x1.400006p-22f;
+constexpr float kGamma7 = 0x1.c0000cp-22f;
 // 1 + 2*gamma(3): far-plane scale of Bounds3::intersect_p (bounds3.rs:292-307)
 constexpr float kBoxRobust = 0x1.000006p+0f;
 constexpr float kMachineEps = 0x1p-24f;
@@ -55,10 +56,11 @@ __device__ __forceinline__ float max3f(float a, float b, float c) { return fmaxf
 
 // Watertight ray-triangle test: Triangle::intersect / intersect_p
 // (shapes/triangle.rs:156-262 and 435-541).  Returns true with t and
-// barycentrics b1, b2 on a hit with 0 < t and t_scaled within tmax.
+// barycentrics b1, b2 (and b0 when asked) on a hit with 0 < t and t_scaled
+// within tmax.
 __device__ __forceinline__ bool triangle_test(const TriRay& r, float3 p0, float3 p1, float3 p2,
                                               float tmax, float& t_out, float& b1_out,
-                                              float& b2_out) {
+                                              float& b2_out, float* b0_out = nullptr) {
     // translate + permute (157-174)
     float3 a = permute3(p0.x, p0.y, p0.z, r.kz);
     float3 b = permute3(p1.x, p1.y, p1.z, r.kz);
@@ -116,6 +118,7 @@ __device__ __forceinline__ bool triangle_test(const TriRay& r, float3 p0, float3
     t_out = t;
     b1_out = __fmul_rn(e1, inv_det);
     b2_out = __fmul_rn(e2, inv_det);
+    if (b0_out) *b0_out = __fmul_rn(e0, inv_det);
     return true;
 }
 

@@ -107,9 +107,11 @@ class Context:
 
 
 class TriangleMesh:
-    """TriangleMesh (shapes/triangle.rs:17-74) with world-space vertices."""
+    """TriangleMesh (shapes/triangle.rs:17-74) with world-space vertices and
+    optional per-vertex shading normals n, tangents s (nv x 3) and uv (nv x 2)."""
 
-    def __init__(self, ctx: Context, xyz: np.ndarray, idx: np.ndarray):
+    def __init__(self, ctx: Context, xyz: np.ndarray, idx: np.ndarray, n=None, s=None, uv=None,
+                 reverse_orientation: bool = False):
         xyz = np.ascontiguousarray(xyz, np.float32).reshape(-1, 3)
         idx = np.ascontiguousarray(idx, np.uint32).reshape(-1, 3)
         mid = ctypes.c_uint32()
@@ -117,6 +119,10 @@ class TriangleMesh:
                   "ilm_mesh_upload")
         self.id = mid.value
         self.n_prims = len(idx)
+        if n is not None or s is not None or uv is not None or reverse_orientation:
+            arrs = [None if a is None else np.ascontiguousarray(a, np.float32).reshape(len(xyz), -1) for a in (n, s, uv)]
+            at = _lib.ilm_mesh_attrs(*(ptr(a) for a in arrs), int(reverse_orientation))
+            ctx.check(ctx._lib.ilm_mesh_set_attrs(ctx.handle, self.id, ctypes.byref(at)), "ilm_mesh_set_attrs")
 
 
 def sphere_desc(radius: float, translate=(0.0, 0.0, 0.0), scale: float = 1.0, z_min: Optional[float] = None,
@@ -168,6 +174,17 @@ class GpuBVHAccel:
         self.id = aid.value
         self.width = width
         self.n_prims = sum(s.n_prims for s in shapes)
+
+    def surface_interactions(self, rays, hits, out=None, stream=None):
+        """SurfaceInteraction records (SURFACE_INTERACTION_DTYPE) for the hits
+        of intersect_batch: host numpy in/out, or device tensors (stream-ordered)."""
+        n = len(rays) if isinstance(rays, np.ndarray) else _count(rays, RAY_DTYPE.itemsize)
+        if out is None:
+            out = np.empty(n, _lib.SURFACE_INTERACTION_DTYPE)
+        s = None if stream is None else (stream if isinstance(stream, int) else stream.cuda_stream)
+        self.ctx.check(self.ctx._lib.ilm_surface_interactions(self.ctx.handle, self.id, ptr(rays), ptr(hits), n,
+                                                              ptr(out), s), "ilm_surface_interactions")
+        return out
 
     # -- Primitive surface (primitive/mod.rs:9-20) -------------------------
     def world_bound(self) -> Bounds3f:
