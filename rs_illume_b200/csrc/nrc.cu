@@ -52,6 +52,13 @@ __host__ __device__ constexpr int param_off(int l) {
     return l == 0 ? 0 : kHid * kIn + (l - 1) * kHid * kHid;
 }
 constexpr int kParams = kHid * kIn + 4 * kHid * kHid + kOut * kHid;   // 30720
+// bf16 inference pack in the tensor cores' canonical K-major layout without
+// swizzle: layer l's [out][in] matrix as 8x8 core matrices of 128 contiguous
+// bytes, core matrix (o/8, i/8) at (o/8 * in/8 + i/8) * 64 elements from the
+// layer's start (param_off(l)), row o%8 at 8 elements, column i%8.
+__host__ __device__ constexpr int tc_index(int l, int o, int i) {
+    return param_off(l) + ((o >> 3) * (in_dim(l) >> 3) + (i >> 3)) * 64 + (o & 7) * 8 + (i & 7);
+}
 // bf16 packs: forward W_l rows padded to in+8; backward W_l^T (l >= 1) rows
 // padded to out+8
 __host__ __device__ constexpr int fwd_stride(int l) { return in_dim(l) + 8; }
@@ -327,6 +334,219 @@ __global__ void __launch_bounds__(32 * kMlpWarps) k_mlp_fwd(const float* __restr
     }
 }
 
+
+// ---------------------------------------------------------------- inference on tcgen05
+// k_mlp_infer_tc: the forward pass on the 5th-generation tensor cores.
+// A CTA of kTcGroups warpgroups; each warpgroup owns 128-row tiles (thread t
+// = row t), its own A operand buffer in shared memory, 64 TMEM columns of
+// FP32 accumulator (rows = TMEM lanes) and an mbarrier.  Per tile:
+//   layer 0 in two K halves (features 0-111, 112-207): the threads evaluate
+//     their row's encoding into A, one thread issues tcgen05.mma
+//     (M 128, N 64, K 16, bf16 x bf16 -> f32) and commits to the mbarrier;
+//   layers 1-4: tcgen05.ld of the accumulator, ReLU, bf16 into A, MMA;
+//   layer 5: N = 16, the first 3 columns are the output.
+// The weights (61,440 bytes, all layers) are staged once per CTA.  Operands
+// use the canonical K-major layout without swizzle: 8x8 core matrices of 128
+// contiguous bytes; LBO = 128 bytes (next core matrix along K), SBO = the
+// stride between 8-row groups.  Every mbarrier wait is bounded; a timeout
+// sets kErrMlpTimeout in *err and the warpgroup stops.
+constexpr int kTcGroups = 4;
+constexpr int kTcHalfCols = 14;                                // core-matrix columns of an A buffer (112 features)
+constexpr int kTcABytes = 128 / 8 * kTcHalfCols * 128;         // 28,672
+constexpr int kTcWBytes = kParams * 2;                         // 61,440
+constexpr int kTcSmem = kTcWBytes + kTcGroups * kTcABytes;     // 176,128
+constexpr uint32_t kErrMlpTimeout = 4u;
+constexpr uint32_t kTcWaitCap = 1u << 22;   // try_wait polls before a wait gives up
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// Shared-memory matrix descriptor: start, LBO, SBO (bytes), version 1, no swizzle.
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+    return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+           ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+// Instruction descriptor, kind::f16: D f32, A and B bf16, both K-major.
+__host__ __device__ constexpr uint32_t idesc_bf16(int m, int n) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(m >> 4) << 24);
+}
+__device__ __forceinline__ void umma(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
+        :
+        : "r"(tmem_d), "l"(a), "l"(b), "r"(idesc), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+}
+__device__ __forceinline__ void umma_commit(uint32_t mbar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar)
+                 : "memory");
+}
+__device__ __forceinline__ void mbar_init(uint32_t mbar) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mbar) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint32_t mbar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(ok)
+        : "r"(mbar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void group_sync(int g) {
+    asm volatile("bar.sync %0, 128;" ::"r"(g + 1) : "memory");
+}
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int k = 0; k < 16; ++k) v[k] = __uint_as_float(r[k]);
+}
+
+// Row t's 8 features F..F+7 (F = 8 * KC) into core-matrix column c of an A buffer.
+template <int KC>
+__device__ __forceinline__ void put_features(uint8_t* a, int c, int row, const RowIn& v) {
+    uint4 q;
+    q.x = feat2<8 * KC>(v, 0);
+    q.y = feat2<8 * KC>(v, 1);
+    q.z = feat2<8 * KC>(v, 2);
+    q.w = feat2<8 * KC>(v, 3);
+    *reinterpret_cast<uint4*>(a + ((row >> 3) * kTcHalfCols + c) * 128 + (row & 7) * 16) = q;
+}
+template <int KC, int KEND>
+__device__ __forceinline__ void encode_cols(uint8_t* a, int c0, int row, const RowIn& v) {
+    put_features<KC>(a, KC - c0, row, v);
+    if constexpr (KC + 1 < KEND) encode_cols<KC + 1, KEND>(a, c0, row, v);
+}
+
+// One warpgroup's MMA batch: layer with `ksteps` K-steps of 16, A from
+// `a_base` (SBO a_sbo), B = layer weights from `w_base` (SBO w_sbo) starting at
+// K-step k0; then commit and (thread 0) wait.  Returns false on a timeout.
+__device__ __forceinline__ bool mma_batch(int g, int t, uint32_t tmem_d, uint32_t a_base, uint32_t a_sbo,
+                                          uint32_t w_base, uint32_t w_sbo, int k0, int ksteps, int n_out,
+                                          bool accumulate, uint32_t mbar, uint32_t& phase, volatile int* fail) {
+    fence_proxy_async();   // the A tile written by this warpgroup, visible to the tensor core
+    tc_fence_before();     // the accumulator reads above, ordered before the MMAs below
+    group_sync(g);
+    if (t == 0) {
+        tc_fence_after();
+        const uint32_t idesc = idesc_bf16(128, n_out);
+        for (int k = 0; k < ksteps; ++k) {
+            uint64_t da = umma_desc(a_base + (uint32_t)k * 256u, 128u, a_sbo);
+            uint64_t db = umma_desc(w_base + (uint32_t)(k0 + k) * 256u, 128u, w_sbo);
+            umma(tmem_d, da, db, idesc, (accumulate || k > 0) ? 1u : 0u);
+        }
+        umma_commit(mbar);
+        uint32_t it = 0;
+        while (!mbar_try_wait(mbar, phase) && ++it < kTcWaitCap) {}
+        if (it >= kTcWaitCap) *fail = 1;
+    }
+    phase ^= 1u;
+    group_sync(g);
+    tc_fence_after();
+    return *fail == 0;
+}
+
+// Accumulator row t (64 columns) -> ReLU -> bf16 A operand (K = 64, SBO 1024).
+__device__ __forceinline__ void acc_to_a(uint32_t tmem_row, uint8_t* a, int row) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        float v[16];
+        tmem_ld16(tmem_row + 16 * q, v);
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            uint4 w;
+            w.x = pack(fmaxf(v[8 * h], 0.0f), fmaxf(v[8 * h + 1], 0.0f));
+            w.y = pack(fmaxf(v[8 * h + 2], 0.0f), fmaxf(v[8 * h + 3], 0.0f));
+            w.z = pack(fmaxf(v[8 * h + 4], 0.0f), fmaxf(v[8 * h + 5], 0.0f));
+            w.w = pack(fmaxf(v[8 * h + 6], 0.0f), fmaxf(v[8 * h + 7], 0.0f));
+            *reinterpret_cast<uint4*>(a + ((row >> 3) * 8 + 2 * q + h) * 128 + (row & 7) * 16) = w;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(128 * kTcGroups, 1) k_mlp_infer_tc(const float* __restrict__ raw, NrcCount cnt,
+                                                                     Enc ec, const __nv_bfloat16* __restrict__ wtc,
+                                                                     float* __restrict__ out, uint32_t* err) {
+    extern __shared__ __align__(1024) uint8_t tc_smem[];
+    __shared__ __align__(8) uint64_t mbar[kTcGroups];
+    __shared__ int fail[kTcGroups];
+    __shared__ uint32_t tmem_base;
+    const int warp = threadIdx.x >> 5, g = warp >> 2, t = threadIdx.x & 127;
+    // stage the weights; barriers; TMEM (64 columns per warpgroup)
+    {
+        const uint4* src = reinterpret_cast<const uint4*>(wtc);
+        uint4* dst = reinterpret_cast<uint4*>(tc_smem);
+        for (int k = threadIdx.x; k < kTcWBytes / 16; k += blockDim.x) dst[k] = src[k];
+    }
+    if (threadIdx.x < kTcGroups) {
+        mbar_init(smem_u32(&mbar[threadIdx.x]));
+        fail[threadIdx.x] = 0;
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base)),
+                     "r"(64u * kTcGroups));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    fence_proxy_async();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t n = rows_of(cnt);
+    const uint32_t tmem_d = tmem_base + 64u * g;                          // this warpgroup's columns
+    const uint32_t tmem_row = tmem_d + ((uint32_t)(32 * (warp & 3)) << 16);   // this warp's lanes
+    uint8_t* a = tc_smem + kTcWBytes + g * kTcABytes;
+    const uint32_t a_base = smem_u32(a), w_base = smem_u32(tc_smem);
+    const uint32_t mb = smem_u32(&mbar[g]);
+    uint32_t phase = 0;
+    const uint32_t tiles = (n + 127) / 128;
+    for (uint32_t tile = blockIdx.x * kTcGroups + g; tile < tiles; tile += gridDim.x * kTcGroups) {
+        const uint32_t row = tile * 128 + t;
+        RowIn v = {};
+        if (row < n) v = load_row(raw, row, ec);
+        // layer 0, features 0-111 (K-steps 0-6)
+        encode_cols<0, kTcHalfCols>(a, 0, t, v);
+        if (!mma_batch(g, t, tmem_d, a_base, kTcHalfCols * 128, w_base + 2 * param_off(0), 26 * 128, 0, 7, 64,
+                       false, mb, phase, &fail[g]))
+            break;
+        // features 112-207 (K-steps 7-12), accumulated
+        encode_cols<kTcHalfCols, 26>(a, kTcHalfCols, t, v);
+        if (!mma_batch(g, t, tmem_d, a_base, kTcHalfCols * 128, w_base + 2 * param_off(0), 26 * 128, 7, 6, 64,
+                       true, mb, phase, &fail[g]))
+            break;
+        bool ok = true;
+        for (int l = 1; l <= 5 && ok; ++l) {
+            acc_to_a(tmem_row, a, t);
+            ok = mma_batch(g, t, tmem_d, a_base, 8 * 128, w_base + 2 * param_off(l), 8 * 128, 0, 4, l == 5 ? 16 : 64,
+                           false, mb, phase, &fail[g]);
+        }
+        if (!ok) break;
+        float o[16];
+        tmem_ld16(tmem_row, o);
+        if (row < n) {
+            out[3 * (size_t)row] = o[0];
+            out[3 * (size_t)row + 1] = o[1];
+            out[3 * (size_t)row + 2] = o[2];
+        }
+    }
+    if (t == 0 && fail[g]) atomicOr(err, kErrMlpTimeout);
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base), "r"(64u * kTcGroups));
+    }
+}
+
 // ---------------------------------------------------------------- backward
 // Loss gradient (mean over the n rows and 3 channels) and dOut of every layer
 // (layer l at douts + l * ld * 64: layers 0-4 [n][64], layer 5 [n][16]);
@@ -540,7 +760,7 @@ __global__ void k_reduce_adam(const float* __restrict__ partial, int n_part, Nrc
         ema[p] = e;
         xi = e / (1.0f - powf(ar.ema_a, (float)st->ema_steps));
     }
-    winf[fwd_off(l) + o * fwd_stride(l) + i] = __float2bfloat16_rn(xi);
+    winf[tc_index(l, o, i)] = __float2bfloat16_rn(xi);
 }
 
 // Packs the master weights (after creation or replacement) and restarts the
@@ -555,7 +775,7 @@ __global__ void k_pack(const float* __restrict__ w, __nv_bfloat16* __restrict__ 
     param_coords(p, l, o, i);
     __nv_bfloat16 h = __float2bfloat16_rn(w[p]);
     wfwd[fwd_off(l) + o * fwd_stride(l) + i] = h;
-    winf[fwd_off(l) + o * fwd_stride(l) + i] = h;
+    winf[tc_index(l, o, i)] = h;
     if (l >= 1) wbwd[bwd_off(l) + i * bwd_stride(l) + o] = h;
     ema[p] = 0.0f;
 }
@@ -572,6 +792,7 @@ struct ilm_nrc {
     DeviceBuffer w, m, v, grad, wfwd, wbwd;      // params and packs
     DeviceBuffer ema, winf;                      // moving average and its inference pack
     DeviceBuffer partial;                        // k_wgrad_all partial sums
+    DeviceBuffer err;                            // device error word (kErrMlpTimeout)
     DeviceBuffer raw, enc, out, target, acts, douts, loss;
     cudaStream_t stream = nullptr;
     ~ilm_nrc() {
@@ -623,10 +844,14 @@ cudaError_t forward(ilm_nrc* h, const float* raw, NrcCount cnt, bool train, floa
                                                   static_cast<const __nv_bfloat16*>(h->wfwd.ptr), out,
                                                   static_cast<__nv_bfloat16*>(h->acts.ptr),
                                                   static_cast<__nv_bfloat16*>(h->enc.ptr));
-    else   // inference reads the moving-average pack
-        k_mlp_fwd<false><<<blocks, 32 * kMlpWarps, smem, s>>>(raw, cnt, enc_params(h), rows,
-                                                   static_cast<const __nv_bfloat16*>(h->winf.ptr), out, nullptr,
-                                                   nullptr);
+    else {   // inference: tcgen05 kernel on the moving-average pack
+        uint32_t tiles = (rows + 127) / 128;
+        uint32_t grid = (tiles + kTcGroups - 1) / kTcGroups;
+        grid = grid < 1 ? 1 : (grid > 148 ? 148 : grid);
+        k_mlp_infer_tc<<<grid, 128 * kTcGroups, kTcSmem, s>>>(raw, cnt, enc_params(h),
+                                                             static_cast<const __nv_bfloat16*>(h->winf.ptr), out,
+                                                             static_cast<uint32_t*>(h->err.ptr));
+    }
     return cudaGetLastError();
 }
 
@@ -682,6 +907,8 @@ cudaError_t nrc_train_async(ilm_nrc* h, const float* raw, const float* target, N
 
 cudaError_t nrc_reserve(ilm_nrc* h, uint32_t rows) { return reserve_train(h, rows); }
 
+uint32_t* nrc_error_word(ilm_nrc* h) { return static_cast<uint32_t*>(h->err.ptr); }
+
 }  // namespace ilm
 
 extern "C" {
@@ -701,6 +928,8 @@ int32_t ilm_nrc_create(ilm_context* ctx, const ilm_nrc_config* cfg, ilm_nrc** ou
     if ((e = h->winf.reserve(kFwdElems * 2)) != cudaSuccess) return cuda_fail(ctx, e, "nrc");
     if ((e = h->wbwd.reserve(kBwdElems * 2)) != cudaSuccess) return cuda_fail(ctx, e, "nrc");
     if ((e = h->loss.reserve(4)) != cudaSuccess) return cuda_fail(ctx, e, "nrc");
+    if ((e = h->err.reserve(4)) != cudaSuccess) return cuda_fail(ctx, e, "nrc");
+    cudaMemset(h->err.ptr, 0, 4);
     if ((e = h->state.reserve(sizeof(StepState))) != cudaSuccess) return cuda_fail(ctx, e, "nrc");
     cudaMemset(h->state.ptr, 0, sizeof(StepState));
     // He-uniform initialisation from PCG32; padded inputs and output rows 3..15 zero
@@ -723,7 +952,7 @@ int32_t ilm_nrc_create(ilm_context* ctx, const ilm_nrc_config* cfg, ilm_nrc** ou
     cudaMemset(h->winf.ptr, 0, kFwdElems * 2);
     cudaMemset(h->wbwd.ptr, 0, kBwdElems * 2);
     cudaFuncSetAttribute(k_mlp_fwd<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kFwdElems * 2);
-    cudaFuncSetAttribute(k_mlp_fwd<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kFwdElems * 2);
+    cudaFuncSetAttribute(k_mlp_infer_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem);
     if ((e = pack(h.get(), h->stream)) != cudaSuccess) return cuda_fail(ctx, e, "nrc pack");
     if ((e = cudaStreamSynchronize(h->stream)) != cudaSuccess) return cuda_fail(ctx, e, "nrc");
     *out = h.release();
@@ -775,7 +1004,13 @@ int32_t ilm_nrc_infer(ilm_context* ctx, ilm_nrc* h, const float* inputs, uint64_
         return cuda_fail(ctx, e, "nrc forward");
     if (!dev_out) {
         cudaMemcpyAsync(out, dst, n * 12, cudaMemcpyDeviceToHost, s);
+        uint32_t flags = 0;
+        cudaMemcpyAsync(&flags, h->err.ptr, 4, cudaMemcpyDeviceToHost, s);
         if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_fail(ctx, e, "nrc");
+        if (flags) {
+            set_error(ctx, "ilm_nrc_infer: a tensor-core wait ran out of time");
+            return ILM_ERR_TIMEOUT;
+        }
     }
     return ILM_OK;
 }

@@ -28,5 +28,7 @@ cudaError_t nrc_train_async(ilm_nrc* h, const float* raw, const float* target, N
 // Grows the training buffers to `rows` rows per step, so that later steps of
 // at most that many rows allocate nothing (and can be captured in a graph).
 cudaError_t nrc_reserve(ilm_nrc* h, uint32_t rows);
+// The network's device error word (non-zero after a tensor-core wait timed out).
+uint32_t* nrc_error_word(ilm_nrc* h);
 
 }  // namespace ilm

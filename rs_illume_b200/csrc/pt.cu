@@ -975,6 +975,12 @@ int32_t ilm_render_nrc(ilm_context* ctx, ilm_pt_scene_id scene, ilm_nrc* nrc, co
     if (st != ILM_OK) return st;
     float ms = 0.0f;
     cudaEventElapsedTime(&ms, b.ev0, b.ev1);
+    uint32_t net_err = 0;
+    cudaMemcpy(&net_err, nrc_error_word(nrc), 4, cudaMemcpyDeviceToHost);
+    if (net_err) {
+        set_error(ctx, "ilm_render_nrc: a tensor-core wait of the cache network ran out of time");
+        return ILM_ERR_TIMEOUT;
+    }
     float loss = 0.0f;
     uint32_t last_nt = (uint32_t)std::min<unsigned long long>(cnts[kSamples], sample_cap);
     if (o->train && last_nt) {
