@@ -20,6 +20,9 @@ Lines printed (rank 0, one JSON line):
   cpu_baseline  the CPU oracle (scalar C++ restatement of BVHAccel::intersect)
             on all host threads, same rays.
 Further keys, one per workload of the path (each skippable):
+  coherent      32,768-triangle soup with 256x256 primary rays, L2-resident:
+                closest-hit Mrays/s against the L2 copy bandwidth measured in
+                the same run and the HBM peak.
   path_tracer   wavefront path tracer, Cornell box with the level-6 icosphere
                 (81,920 + 34 triangles), 1024x1024, 64 spp stratified, max depth
                 8, Russian roulette from depth 3: rays/s and paths/s, with the
@@ -345,6 +348,56 @@ def batched_leg(rb, wl, ctx, torch, dev, steps):
                       "width 8, one persistent launch replayed as a CUDA graph, L2 flushed between steps"}
 
 
+N_NODE_COHERENT, N_TRI_COHERENT = 57.515228, 2.256424
+BYTES_PER_RAY_COHERENT = 32 + 16 + 32 * N_NODE_COHERENT + 36 * N_TRI_COHERENT
+
+
+def l2_copy_gbs(torch, dev):
+    """Device-to-device copy of 24 MiB (48 MiB of traffic, resident in the
+    126 MB L2) timed with CUDA events: the L2 bandwidth this kernel can see."""
+    a = torch.empty(24 << 20, dtype=torch.uint8, device=dev)
+    b = torch.empty_like(a)
+    for _ in range(5):
+        b.copy_(a)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(50):
+        b.copy_(a)
+    e1.record()
+    torch.cuda.synchronize()
+    return 2 * a.numel() * 50 / (e0.elapsed_time(e1) / 1e3) / 1e9
+
+
+def coherent_leg(rb, wl, ctx, torch, dev, steps):
+    """Config 1: 32,768-triangle soup, 256x256 primary rays (scene and rays
+    fully L2-resident): closest-hit Mrays/s and its roofline against the L2
+    copy bandwidth measured here and the HBM peak."""
+    xyz, idx, rays = wl.coherent_workload()
+    acc = rb.GpuBVHAccel(ctx, [rb.TriangleMesh(ctx, xyz, idx)], width=8)
+    d_rays = torch.from_numpy(rays.view(np.uint8)).to(dev)
+    d_hits = torch.empty(len(rays) * 16, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.Stream(dev)
+    for _ in range(5):
+        acc.intersect_batch(d_rays, d_hits, stream=stream)
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    for a, b in evs:
+        a.record(stream)
+        acc.intersect_batch(d_rays, d_hits, stream=stream)
+        b.record(stream)
+    torch.cuda.synchronize()
+    t = sum(a.elapsed_time(b) for a, b in evs) / 1e3 / steps
+    l2 = l2_copy_gbs(torch, dev)
+    hbm, kind = measured_peaks()
+    ach = BYTES_PER_RAY_COHERENT * len(rays) / t / 1e9
+    return {"value": round(len(rays) / t / 1e6, 2), "unit": "Mrays/s", "us_per_launch": round(t * 1e6, 2),
+            "roofline": {"bound": "l2", "achieved": round(ach, 1), "unit": "GB/s",
+                         "l2_copy_gbs": round(l2, 1), "frac_of_l2": round(ach / l2, 4),
+                         "hbm_peak": hbm, "frac_of_hbm": round(ach / hbm, 4),
+                         "bytes_per_ray": round(BYTES_PER_RAY_COHERENT, 2)},
+            "config": "32,768-triangle soup (seed 1), 65,536 primary rays 256x256 from (0.5,0.5,-1.5), 45 deg, "
+                      "width 8; scene and rays L2-resident (no flush: the workload is the L2 case)"}
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -394,6 +447,7 @@ def run_ours(args):
                 "nrc": ("neural_cache", lambda: neural_cache_leg(rb, wl, ctx, torch, dev)),
                 "mlp": ("neural_cache", lambda: mlp_leg(rb, ctx, torch, dev)),
                 "nrcframe": ("neural_cache", lambda: nrc_frame_leg(rb, wl, ctx)),
+                "coherent": ("coherent", lambda: coherent_leg(rb, wl, ctx, torch, dev, args.steps)),
                 "batched": ("batched", lambda: batched_leg(rb, wl, ctx, torch, dev, args.steps))}
         key, fn = legs[args.only]
         res = fn()
@@ -533,6 +587,7 @@ def run_ours(args):
                                     "sample": "all 2,097,152 closest rays x 3 passes (CPU oracle, binary SAH BVH)",
                                     "n_node_sample": round(nn, 4), "n_tri_sample": round(nt, 4)}
         for key, enabled, fn in (
+                ("coherent", not args.only, lambda: coherent_leg(rb, wl, ctx, torch, dev, args.steps)),
                 ("path_tracer", not args.no_pt and not args.only,
                  lambda: path_tracer_leg(rb, wl, ctx, dev, args.steps, world == 1 and not args.no_cpu)),
                 ("neural_cache", not args.no_nrc and not args.only, lambda: neural_cache_leg(rb, wl, ctx, torch, dev)),
@@ -567,7 +622,7 @@ def main():
     ap.add_argument("--no-pt", action="store_true", help="skip the path-tracer workload")
     ap.add_argument("--no-nrc", action="store_true", help="skip the radiance-cache workload")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched multi-scene workload")
-    ap.add_argument("--only", choices=["closest", "pt", "nrc", "nrcframe", "mlp", "batched"],
+    ap.add_argument("--only", choices=["closest", "coherent", "pt", "nrc", "nrcframe", "mlp", "batched"],
                     help="run one workload alone (profiling)")
     args = ap.parse_args()
     if args.warmup < 3:

@@ -270,6 +270,22 @@ typedef struct {
 int32_t ilm_autotune(ilm_context* ctx, const ilm_mesh_id* meshes, uint32_t n_meshes, const ilm_ray* sample,
                      uint64_t n, int32_t any_hit, int32_t force, ilm_tune_result* out);
 
+/* Film filters (the filters/ directory) and the film's weight table (core/film.rs:70-82):
+ * table[y*16 + x] = evaluate((x + 0.5) * radius.x / 16, (y + 0.5) * radius.y / 16). */
+enum {
+    ILM_FILTER_BOX = 0,        /* filters/box_filter.rs */
+    ILM_FILTER_TRIANGLE = 1,   /* filters/triangle.rs */
+    ILM_FILTER_GAUSSIAN = 2,   /* filters/gaussian.rs: a = alpha */
+    ILM_FILTER_MITCHELL = 3,   /* filters/mitchell.rs: a = B, b = C */
+    ILM_FILTER_LANCZOS = 4     /* filters/sinc.rs: a = tau */
+};
+typedef struct {
+    int32_t kind;
+    float radius[2];
+    float a, b;
+} ilm_filter_desc;
+#define ILM_FILTER_TABLE_WIDTH 16
+
 /* ----------------------------------------------------------- path tracing */
 /* Wavefront path tracer over a triangle accel: the PBR-book path loop with
  * the reference's one-light direct lighting with MIS
@@ -296,6 +312,8 @@ typedef struct {
     uint64_t seed;
     uint32_t wave_paths;   /* paths in flight per wave (0 = 2^21) */
     int32_t use_graphs;    /* replay each bounce as a CUDA graph */
+    ilm_filter_desc filter; /* film filter (FilmTile::add_sample, film.rs:288-333); radius 0 or the box
+                               of radius 0.5: each sample counts in its own pixel */
 } ilm_pt_opts;
 
 typedef struct {
@@ -401,21 +419,6 @@ int32_t ilm_write_pfm(const char* path, const float* rgb, uint32_t width, uint32
  * hold (*width)*(*height)*3 floats for the size given on input. */
 int32_t ilm_read_pfm(const char* path, float* rgb, uint32_t* width, uint32_t* height);
 
-/* Film filters (the filters/ directory) and the film's weight table (core/film.rs:70-82):
- * table[y*16 + x] = evaluate((x + 0.5) * radius.x / 16, (y + 0.5) * radius.y / 16). */
-enum {
-    ILM_FILTER_BOX = 0,        /* filters/box_filter.rs */
-    ILM_FILTER_TRIANGLE = 1,   /* filters/triangle.rs */
-    ILM_FILTER_GAUSSIAN = 2,   /* filters/gaussian.rs: a = alpha */
-    ILM_FILTER_MITCHELL = 3,   /* filters/mitchell.rs: a = B, b = C */
-    ILM_FILTER_LANCZOS = 4     /* filters/sinc.rs: a = tau */
-};
-typedef struct {
-    int32_t kind;
-    float radius[2];
-    float a, b;
-} ilm_filter_desc;
-#define ILM_FILTER_TABLE_WIDTH 16
 /* One filter value at film offset (x, y) from the sample. */
 int32_t ilm_filter_evaluate(const ilm_filter_desc* filter, float x, float y, float* out);
 int32_t ilm_filter_table(const ilm_filter_desc* filter, float* table /* 16 x 16 */);

@@ -52,6 +52,10 @@ _SIG = {
     "orc_intersect_p": (ctypes.c_int64, [_P, _P, ctypes.c_uint64, _P, _P, _P, ctypes.c_int]),
     "orc_triangle_intersect": (ctypes.c_int, [_P, _P, _P, _P, ctypes.c_int, _P]),
     "orc_surface_interaction": (ctypes.c_int, [_P, _P, _P, _P, ctypes.c_int, _P, _P]),
+    "orc_render_pt_filtered": (ctypes.c_int, [_P, _P, _P, ctypes.c_uint32, _P, _P, _P, _P, ctypes.c_float,
+                                              ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32,
+                                              ctypes.c_uint32, ctypes.c_uint64, _P, ctypes.c_float, ctypes.c_float,
+                                              ctypes.c_int, _P, _P]),
     "orc_sphere_intersect": (ctypes.c_int, [_P, _P, ctypes.c_int, _P]),
     "orc_sphere_world_bound": (None, [_P, _P]),
     "orc_last_trace_seconds": (ctypes.c_double, []),
@@ -193,6 +197,26 @@ def render_pt(scene: "Scene", xyz, idx, mat, albedo, emission, eye, fov_deg, wid
                               fov_deg, width, height, spp, max_depth, rr_depth, seed, x0, y0, x1, y1, threads,
                               _p(out), _p(counts))
     assert st == 0, "invalid render arguments"
+    return out, (int(counts[0]), int(counts[1]))
+
+
+def render_pt_filtered(scene: "Scene", xyz, idx, mat, albedo, emission, eye, fov_deg, width, height, spp,
+                       table, radius, max_depth=8, rr_depth=3, seed=3, threads=0):
+    """Full-frame render through a filtered film (16 x 16 weight table,
+    radius (rx, ry)).  Returns (rgb[h, w, 3], (closest rays, shadow rays))."""
+    xyz = np.ascontiguousarray(xyz, np.float32)
+    idx = np.ascontiguousarray(idx, np.uint32)
+    mat = np.ascontiguousarray(mat, np.uint32)
+    albedo = np.ascontiguousarray(albedo, np.float32)
+    emission = np.ascontiguousarray(emission, np.float32)
+    eye = np.asarray(eye, np.float32)
+    table = np.ascontiguousarray(table, np.float32)
+    out = np.zeros((height, width, 3), np.float32)
+    counts = np.zeros(2, np.uint64)
+    st = load().orc_render_pt_filtered(scene.h, _p(xyz), _p(idx), len(idx.reshape(-1, 3)), _p(mat), _p(albedo),
+                                       _p(emission), _p(eye), fov_deg, width, height, spp, max_depth, rr_depth, seed,
+                                       _p(table), radius[0], radius[1], threads, _p(out), _p(counts))
+    assert st == 0
     return out, (int(counts[0]), int(counts[1]))
 
 

@@ -18,6 +18,7 @@
 // film: a pixel is the mean of its samples), D21 (the BSDF-sampled light term
 // is accumulated), D25 (pdf_with_point divides by |cos|*area; shape.rs:77-78
 // multiplies by area).
+#include <algorithm>
 #include <atomic>
 #include <cmath>
 #include <thread>
@@ -320,6 +321,102 @@ RGB li(const PtScene& s, V o, V d, Rng& rng, uint32_t max_depth, uint32_t rr_dep
 }  // namespace orc
 
 using namespace orc;
+
+// FilmTile::add_sample (film.rs:288-333) with D20 repaired (footprint upper
+// corner floor(p + radius) + 1, both loops run): the sample's L times the
+// table weight of each pixel within the filter radius, and the weight.
+static void film_splat(float* sums, float* wsum, uint32_t width, uint32_t height, const float* table, float rx,
+                       float ry, float fx, float fy, const RGB& L) {
+    const float dx = fx - 0.5f, dy = fy - 0.5f;
+    const float irx = 1.0f / rx, iry = 1.0f / ry;
+    int x0 = (int)std::ceil(dx - rx), y0 = (int)std::ceil(dy - ry);
+    int x1 = (int)std::floor(dx + rx) + 1, y1 = (int)std::floor(dy + ry) + 1;
+    x0 = std::max(x0, 0); y0 = std::max(y0, 0);
+    x1 = std::min(x1, (int)width); y1 = std::min(y1, (int)height);
+    for (int y = y0; y < y1; ++y) {
+        int ify = std::min((int)std::floor(std::fabs(((float)y - dy) * iry * 16.0f)), 15);
+        for (int x = x0; x < x1; ++x) {
+            int ifx = std::min((int)std::floor(std::fabs(((float)x - dx) * irx * 16.0f)), 15);
+            float w = table[ify * 16 + ifx];
+            size_t p = (size_t)y * width + x;
+            sums[3 * p] += L.r * w;
+            sums[3 * p + 1] += L.g * w;
+            sums[3 * p + 2] += L.b * w;
+            wsum[p] += w;
+        }
+    }
+}
+
+extern "C" int orc_render_pt_filtered(void* scene, const float* verts, const uint32_t* idx, uint32_t nt,
+                                      const uint32_t* prim_material, const float* albedo, const float* emission,
+                                      const float eye[3], float fov_deg, uint32_t width, uint32_t height,
+                                      uint32_t spp, uint32_t max_depth, uint32_t rr_depth, uint64_t seed,
+                                      const float* table, float rx, float ry, int nthreads, float* rgb_out,
+                                      uint64_t* ray_counts) {
+    uint32_t ns = (uint32_t)std::lround(std::sqrt((double)spp));
+    if (ns * ns != spp || width == 0 || height == 0 || !(rx > 0.0f) || !(ry > 0.0f)) return -1;
+    PtScene s;
+    s.scene = scene;
+    s.mat = prim_material;
+    s.albedo = albedo;
+    s.emission = emission;
+    s.tris.resize(nt);
+    for (uint32_t i = 0; i < nt; ++i) {
+        const float* a = verts + 3 * idx[3 * i];
+        const float* b = verts + 3 * idx[3 * i + 1];
+        const float* c = verts + 3 * idx[3 * i + 2];
+        s.tris[i] = {{a[0], a[1], a[2]}, {b[0], b[1], b[2]}, {c[0], c[1], c[2]}};
+        const float* e = emission + 3 * prim_material[i];
+        if (e[0] > 0.0f || e[1] > 0.0f || e[2] > 0.0f) s.lights.push_back(i);
+    }
+    const float th = std::tan(0.5f * fov_deg * kPi / 180.0f);
+    const float aspect = (float)width / (float)height;
+    if (nthreads <= 0) nthreads = (int)std::thread::hardware_concurrency();
+    const size_t npix = (size_t)width * height;
+    std::vector<std::vector<float>> sums(nthreads, std::vector<float>(3 * npix, 0.0f)),
+        wsums(nthreads, std::vector<float>(npix, 0.0f));
+    std::atomic<uint32_t> next_row{0};
+    std::atomic<uint64_t> ext{0}, sh{0};
+    auto worker = [&](int tid) {
+        Counters cnt;
+        for (;;) {
+            uint32_t py = next_row.fetch_add(1);
+            if (py >= height) break;
+            for (uint32_t px = 0; px < width; ++px) {
+                Rng rng((seed << 32) ^ ((uint64_t)py * width + px));
+                for (uint32_t k = 0; k < spp; ++k) {
+                    float jx = rng.uniform_float(), jy = rng.uniform_float();
+                    float fx = (float)px + ((float)(k % ns) + jx) / (float)ns;
+                    float fy = (float)py + ((float)(k / ns) + jy) / (float)ns;
+                    float sx = (fx / (float)width * 2.0f - 1.0f) * th * aspect;
+                    float sy = (1.0f - fy / (float)height * 2.0f) * th;
+                    V d = normalize(V{sx, sy, 1.0f});
+                    RGB L = li(s, V{eye[0], eye[1], eye[2]}, d, rng, max_depth, rr_depth, cnt);
+                    if (std::isnan(L.r) || std::isnan(L.g) || std::isnan(L.b) || luminance(L) < -1e-5f ||
+                        std::isinf(luminance(L)))
+                        L = {0, 0, 0};
+                    film_splat(sums[tid].data(), wsums[tid].data(), width, height, table, rx, ry, fx, fy, L);
+                }
+            }
+        }
+        ext += cnt.ext;
+        sh += cnt.shadow;
+    };
+    std::vector<std::thread> th_;
+    for (int i = 0; i < nthreads; ++i) th_.emplace_back(worker, i);
+    for (auto& t : th_) t.join();
+    // merge the threads' films, then Film::write_image's division (film.rs:187-226)
+    for (size_t p = 0; p < npix; ++p) {
+        float w = 0.0f, c[3] = {0.0f, 0.0f, 0.0f};
+        for (int t = 0; t < nthreads; ++t) {
+            w += wsums[t][p];
+            for (int k = 0; k < 3; ++k) c[k] += sums[t][3 * p + k];
+        }
+        for (int k = 0; k < 3; ++k) rgb_out[3 * p + k] = w != 0.0f ? c[k] * (1.0f / w) : 0.0f;
+    }
+    if (ray_counts) { ray_counts[0] = ext.load(); ray_counts[1] = sh.load(); }
+    return 0;
+}
 
 extern "C" int orc_render_pt(void* scene, const float* verts, const uint32_t* idx, uint32_t nt,
                              const uint32_t* prim_material, const float* albedo, const float* emission,

@@ -84,9 +84,15 @@ class ilm_pt_scene_desc(ctypes.Structure):
                 ("width", ctypes.c_uint32), ("height", ctypes.c_uint32)]
 
 
+class ilm_filter_desc(ctypes.Structure):
+    _fields_ = [("kind", ctypes.c_int32), ("radius", ctypes.c_float * 2), ("a", ctypes.c_float),
+                ("b", ctypes.c_float)]
+
+
 class ilm_pt_opts(ctypes.Structure):
     _fields_ = [("spp", ctypes.c_uint32), ("max_depth", ctypes.c_uint32), ("rr_depth", ctypes.c_uint32),
-                ("seed", ctypes.c_uint64), ("wave_paths", ctypes.c_uint32), ("use_graphs", ctypes.c_int32)]
+                ("seed", ctypes.c_uint64), ("wave_paths", ctypes.c_uint32), ("use_graphs", ctypes.c_int32),
+                ("filter", ilm_filter_desc)]
 
 
 class ilm_pt_stats(ctypes.Structure):
@@ -111,11 +117,6 @@ class ilm_nrc_render_stats(ctypes.Structure):
 class ilm_mesh_attrs(ctypes.Structure):
     _fields_ = [("n", ctypes.c_void_p), ("s", ctypes.c_void_p), ("uv", ctypes.c_void_p),
                 ("reverse_orientation", ctypes.c_int32)]
-
-
-class ilm_filter_desc(ctypes.Structure):
-    _fields_ = [("kind", ctypes.c_int32), ("radius", ctypes.c_float * 2), ("a", ctypes.c_float),
-                ("b", ctypes.c_float)]
 
 
 class ilm_batch_desc(ctypes.Structure):

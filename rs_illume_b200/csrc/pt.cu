@@ -71,23 +71,27 @@ struct PtArgs {
     const float4* light_geo;  // per light: normal (xyz), area (w)
     uint32_t n_lights;
     float* film;              // RGB sums, 3 per pixel
+    float* wsum;              // filter weight sums per pixel (general filters only)
+    const float* ftable;      // the film's 16 x 16 filter weight table (film.rs:70-82)
+    float frx, fry, firx, firy;   // filter radius and its inverse
+    int fbox;                 // 1: box of radius 0.5, each sample to its own pixel with weight 1
     uint32_t width, height, npix, spp, ns;
     float eye_x, eye_y, eye_z, tan_half, aspect;
     uint32_t max_depth, rr_depth;
     unsigned long long seed;
     ilm_ray* rays[2];
-    float4* beta[2];          // throughput rgb, pixel (bits)
+    float4* beta[2];          // throughput rgb, path id (bits)
     uint2* rng[2];            // PCG state (lo, hi)
     uint32_t* pid[2];         // path id (selects the PCG stream)
     const ilm_hit* hits;
     ilm_ray* srays;
-    float4* scontrib;         // contribution rgb, pixel (bits)
+    float4* scontrib;         // contribution rgb, path id (bits)
     const uint32_t* socc;
     unsigned long long* counts;
     // radiance-cache mode
     float4* spread[2];        // s, a0, pdf of the last direction, training word (bits)
     float* q_in;              // queries: 12 floats each
-    float4* q_beta;           // throughput rgb, pixel (bits)
+    float4* q_beta;           // throughput rgb, path id (bits)
     uint2* q_train;           // training slot (or kNone) and depth of the query vertex
     const float* q_out;       // predictions: 3 floats each
     uint32_t q_cap;
@@ -166,11 +170,58 @@ __device__ __forceinline__ bool good(float3 c) {
     return isfinite(c.x) && isfinite(c.y) && isfinite(c.z) && y >= 0.0f && (c.x > 0.0f || c.y > 0.0f || c.z > 0.0f);
 }
 
-__device__ __forceinline__ void film_add(const PtArgs& a, uint32_t pixel, float3 c) {
+// Raster position of path `id`'s camera sample: pixel, ns x ns stratum and
+// the first two draws of the path's PCG stream (the camera kernel draws the
+// same two numbers first).
+__device__ __forceinline__ void sample_position(const PtArgs& a, uint32_t id, float& fx, float& fy) {
+    uint32_t pixel = id % a.npix, sample = (id / a.npix) % a.spp;
+    uint32_t px = pixel % a.width, py = pixel / a.width;
+    Pcg32 rng(path_seq(a.seed, id));
+    float jx = rng.uniform_float(), jy = rng.uniform_float();
+    fx = (float)px + ((float)(sample % a.ns) + jx) / (float)a.ns;
+    fy = (float)py + ((float)(sample / a.ns) + jy) / (float)a.ns;
+}
+
+// FilmTile::add_sample (film.rs:288-333, D20 repaired: the footprint's upper
+// corner is floor(p + radius) + 1 and both loops run): every pixel within the
+// filter radius of the sample gets weight table[ify][ifx] (the table at the
+// pixel's offset), times c, or only the weight with weight_only.
+__device__ __forceinline__ void splat(const PtArgs& a, float fx, float fy, float3 c, bool weight_only) {
+    const float dx = __fsub_rn(fx, 0.5f), dy = __fsub_rn(fy, 0.5f);
+    int x0 = (int)ceilf(__fsub_rn(dx, a.frx)), y0 = (int)ceilf(__fsub_rn(dy, a.fry));
+    int x1 = (int)floorf(__fadd_rn(dx, a.frx)) + 1, y1 = (int)floorf(__fadd_rn(dy, a.fry)) + 1;
+    x0 = max(x0, 0); y0 = max(y0, 0);
+    x1 = min(x1, (int)a.width); y1 = min(y1, (int)a.height);
+    for (int y = y0; y < y1; ++y) {
+        int ify = min((int)floorf(fabsf(__fmul_rn(__fmul_rn(__fsub_rn((float)y, dy), a.firy), 16.0f))), 15);
+        for (int x = x0; x < x1; ++x) {
+            int ifx = min((int)floorf(fabsf(__fmul_rn(__fmul_rn(__fsub_rn((float)x, dx), a.firx), 16.0f))), 15);
+            float w = a.ftable[ify * 16 + ifx];
+            size_t p = (size_t)y * a.width + x;
+            if (weight_only) {
+                atomicAdd(&a.wsum[p], w);
+            } else {
+                atomicAdd(&a.film[3 * p], __fmul_rn(c.x, w));
+                atomicAdd(&a.film[3 * p + 1], __fmul_rn(c.y, w));
+                atomicAdd(&a.film[3 * p + 2], __fmul_rn(c.z, w));
+            }
+        }
+    }
+}
+
+// A contribution c of path `id` to the film.
+__device__ __forceinline__ void film_add(const PtArgs& a, uint32_t id, float3 c) {
     if (!good(c)) return;
-    atomicAdd(&a.film[3 * pixel], c.x);
-    atomicAdd(&a.film[3 * pixel + 1], c.y);
-    atomicAdd(&a.film[3 * pixel + 2], c.z);
+    if (a.fbox) {
+        uint32_t pixel = id % a.npix;
+        atomicAdd(&a.film[3 * pixel], c.x);
+        atomicAdd(&a.film[3 * pixel + 1], c.y);
+        atomicAdd(&a.film[3 * pixel + 2], c.z);
+        return;
+    }
+    float fx, fy;
+    sample_position(a, id, fx, fy);
+    splat(a, fx, fy, c, false);
 }
 
 // Warp-aggregated append: one atomicAdd per warp, slots in lane order.
@@ -225,7 +276,8 @@ __global__ void k_pt_camera(PtArgs a, unsigned long long p0, uint32_t count) {
     float sy = (1.0f - fy / (float)a.height * 2.0f) * a.tan_half;
     float3 d = normalize3(make_float3(sx, sy, 1.0f));
     put_ray(a.rays[0], k, make_float3(a.eye_x, a.eye_y, a.eye_z), d, INFINITY);
-    a.beta[0][k] = make_float4(1.0f, 1.0f, 1.0f, __uint_as_float(pixel));
+    a.beta[0][k] = make_float4(1.0f, 1.0f, 1.0f, __uint_as_float(id));
+    if (!a.fbox) splat(a, fx, fy, make_float3(0.0f, 0.0f, 0.0f), true);   // the sample's filter weights
     a.rng[0][k] = make_uint2((uint32_t)rng.state, (uint32_t)(rng.state >> 32));
     a.pid[0][k] = id;
     if (kNrc) a.spread[0][k] = make_float4(0.0f, 0.0f, 0.0f, __uint_as_float(tw));
@@ -247,12 +299,12 @@ __global__ void __launch_bounds__(256) k_pt_shade(PtArgs a, int cur) {
         float3 c_l = make_float3(0, 0, 0), c_b = make_float3(0, 0, 0);
         float4 beta_out = make_float4(0, 0, 0, 0), spread_next = make_float4(0, 0, 0, 0);
         uint2 rng_out = make_uint2(0, 0);
-        uint32_t id = 0, pixel = 0, tw = kNone;
+        uint32_t id = 0, fid = 0, tw = kNone;
         float3 q_p, q_wo, q_n, q_alb, q_beta;
         if (valid) {
             float4 b4 = a.beta[cur][i];
             float3 beta = f3(b4);
-            pixel = __float_as_uint(b4.w);
+            fid = __float_as_uint(b4.w);
             id = a.pid[cur][i];
             uint2 rs = a.rng[cur][i];
             Pcg32 rng;
@@ -277,7 +329,7 @@ __global__ void __launch_bounds__(256) k_pt_shade(PtArgs a, int cur) {
                 float3 albedo = f3(a.mat[2 * m]);
                 if (depth == 0) {
                     float3 le = f3(a.mat[2 * m + 1]);
-                    if (dot3(nrm, wo) > 0.0f) film_add(a, pixel, beta * le);
+                    if (dot3(nrm, wo) > 0.0f) film_add(a, fid, beta * le);
                 }
                 float wo_z = dot3(wo, nrm);
                 bool cache_here = false;
@@ -408,7 +460,7 @@ __global__ void __launch_bounds__(256) k_pt_shade(PtArgs a, int cur) {
                         if (alive && depth + 1 < a.max_depth) {
                             o_c = offset_origin(p, perr, nrm, wi);
                             d_c = wi;
-                            beta_out = make_float4(nb.x, nb.y, nb.z, __uint_as_float(pixel));
+                            beta_out = make_float4(nb.x, nb.y, nb.z, __uint_as_float(fid));
                             rng_out = make_uint2((uint32_t)rng.state, (uint32_t)(rng.state >> 32));
                             spread_next = make_float4(sp.x, sp.y, pdf, __uint_as_float(tw));
                             cont = true;
@@ -428,13 +480,13 @@ __global__ void __launch_bounds__(256) k_pt_shade(PtArgs a, int cur) {
         uint32_t sl = warp_append(&a.counts[kShadow], push_l);
         if (push_l) {
             put_ray(a.srays, sl, o_l, d_l, tm_l);
-            a.scontrib[sl] = make_float4(c_l.x, c_l.y, c_l.z, __uint_as_float(pixel));
+            a.scontrib[sl] = make_float4(c_l.x, c_l.y, c_l.z, __uint_as_float(fid));
             if (kNrc) a.s_train[sl] = make_uint2(tw == kNone ? kNone : tw & kSlotMask, depth);
         }
         uint32_t sb = warp_append(&a.counts[kShadow], push_b);
         if (push_b) {
             put_ray(a.srays, sb, o_b, d_b, tm_b);
-            a.scontrib[sb] = make_float4(c_b.x, c_b.y, c_b.z, __uint_as_float(pixel));
+            a.scontrib[sb] = make_float4(c_b.x, c_b.y, c_b.z, __uint_as_float(fid));
             if (kNrc) a.s_train[sb] = make_uint2(tw == kNone ? kNone : tw & kSlotMask, depth);
         }
         if (kNrc) {
@@ -445,7 +497,7 @@ __global__ void __launch_bounds__(256) k_pt_shade(PtArgs a, int cur) {
                                 q_alb.x, q_alb.y, q_alb.z};
 #pragma unroll
                 for (int q = 0; q < 12; ++q) qi[q] = in[q];
-                a.q_beta[sq] = make_float4(q_beta.x, q_beta.y, q_beta.z, __uint_as_float(pixel));
+                a.q_beta[sq] = make_float4(q_beta.x, q_beta.y, q_beta.z, __uint_as_float(fid));
                 a.q_train[sq] = make_uint2(tw == kNone ? kNone : tw & kSlotMask, depth);
             }
         }
@@ -535,9 +587,18 @@ __global__ void k_nrc_tally(PtArgs a, uint32_t sample_cap) {
     a.counts[kTrainRows] = a.counts[kSamples];
 }
 
-__global__ void k_pt_resolve(const float* film, float* out, uint32_t n3, float inv_spp) {
+// Film::write_image's division (film.rs:187-226): contribution sums times
+// 1 / (filter weight sum), zero where no weight landed; for the pixel box
+// film the weight sum of every pixel is its sample count.
+__global__ void k_pt_resolve(const float* film, const float* wsum, float* out, uint32_t n3, float inv_spp) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n3) out[i] = film[i] * inv_spp;
+    if (i >= n3) return;
+    if (!wsum) {
+        out[i] = film[i] * inv_spp;
+    } else {
+        float w = wsum[i / 3];
+        out[i] = w != 0.0f ? film[i] * (1.0f / w) : 0.0f;
+    }
 }
 
 // One bounce: extend, shade, shadow, accumulate, advance (queue parity cur).
@@ -571,7 +632,8 @@ struct RenderSetup {
 };
 
 int32_t setup_render(ilm_context* ctx, PtScene& sc, uint32_t spp, uint32_t max_depth, uint32_t rr_depth,
-                     uint64_t seed, uint32_t wave_paths, uint64_t total_paths, bool nrc, RenderSetup& r) {
+                     uint64_t seed, uint32_t wave_paths, uint64_t total_paths, bool nrc, RenderSetup& r,
+                     const ilm_filter_desc* filter = nullptr) {
     Accel* acc = find_accel(ctx, sc.accel);
     if (!acc) { set_error(ctx, "render: the scene's accel was destroyed"); return ILM_ERR_NOT_FOUND; }
     const ilm_pt_scene_desc& d = sc.desc;
@@ -644,6 +706,29 @@ int32_t setup_render(ilm_context* ctx, PtScene& sc, uint32_t spp, uint32_t max_d
     int dev_sms = 148;
     cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, ctx->device);
     r.blocks = dev_sms * 8;
+    // film filter: the default (no filter, or the box of radius 0.5) puts each
+    // sample in its own pixel; any other filter splats through its table
+    a.fbox = 1;
+    a.wsum = nullptr;
+    if (filter && filter->radius[0] > 0.0f &&
+        !(filter->kind == ILM_FILTER_BOX && filter->radius[0] == 0.5f && filter->radius[1] == 0.5f)) {
+        float table[ILM_FILTER_TABLE_WIDTH * ILM_FILTER_TABLE_WIDTH];
+        if (ilm_filter_table(filter, table) != ILM_OK) {
+            set_error(ctx, "render: invalid film filter");
+            return ILM_ERR_INVALID_ARGUMENT;
+        }
+        if ((e = b.ftable.reserve(sizeof table)) != cudaSuccess || (e = b.wsum.reserve(r.npix * 4)) != cudaSuccess)
+            return cuda_fail(ctx, e, "film filter buffers");
+        cudaMemcpyAsync(b.ftable.ptr, table, sizeof table, cudaMemcpyHostToDevice, r.s);
+        cudaMemsetAsync(b.wsum.ptr, 0, r.npix * 4, r.s);
+        a.fbox = 0;
+        a.ftable = static_cast<const float*>(b.ftable.ptr);
+        a.wsum = static_cast<float*>(b.wsum.ptr);
+        a.frx = filter->radius[0];
+        a.fry = filter->radius[1];
+        a.firx = 1.0f / filter->radius[0];
+        a.firy = 1.0f / filter->radius[1];
+    }
     // everything but kTrainRows restarts; that one is kept for the next render's first frame
     cudaMemsetAsync(a.counts, 0, (fresh_counts ? kNumCounts : kTrainRows) * 8, r.s);
     cudaMemsetAsync(a.film, 0, r.npix * 12, r.s);
@@ -662,7 +747,7 @@ int32_t finish_render(ilm_context* ctx, PtScene& sc, RenderSetup& r, float* rgb_
         dst = static_cast<float*>(b.out.ptr);
     }
     uint32_t n3 = (uint32_t)(r.npix * 3);
-    k_pt_resolve<<<(n3 + 255) / 256, 256, 0, r.s>>>(r.a.film, dst, n3, inv_spp);
+    k_pt_resolve<<<(n3 + 255) / 256, 256, 0, r.s>>>(r.a.film, r.a.wsum, dst, n3, inv_spp);
     if (k == PtrKind::kHost) cudaMemcpyAsync(rgb_out, dst, r.npix * 12, cudaMemcpyDeviceToHost, r.s);
     cudaMemcpyAsync(cnts, r.a.counts, kNumCounts * 8, cudaMemcpyDeviceToHost, r.s);
     if ((e = cudaStreamSynchronize(r.s)) != cudaSuccess) return cuda_fail(ctx, e, "render");
@@ -760,7 +845,7 @@ int32_t ilm_render_pt(ilm_context* ctx, ilm_pt_scene_id scene, const ilm_pt_opts
     RenderSetup r;
     uint64_t total = (uint64_t)sc.desc.width * sc.desc.height * opts->spp;
     int32_t st = setup_render(ctx, sc, opts->spp, opts->max_depth, opts->rr_depth, opts->seed, opts->wave_paths,
-                              total, false, r);
+                              total, false, r, &opts->filter);
     if (st != ILM_OK) return st;
     PtArgs& a = r.a;
     cudaStream_t s = r.s;

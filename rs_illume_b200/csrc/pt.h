@@ -14,6 +14,7 @@ struct PtBuffers {
     DeviceBuffer srays, scontrib, socc;              // shadow queue
     DeviceBuffer counts;
     DeviceBuffer film, out;
+    DeviceBuffer ftable, wsum;                       // film filter table and weight sums
     // radiance-cache mode: spread per path, cache queries, training records
     DeviceBuffer spread[2], q_in, q_beta, q_train, q_out, t_rec, t_count, s_train, t_in, t_tg;
     cudaStream_t stream = nullptr;

@@ -284,10 +284,13 @@ class PathTracer:
         self.width, self.height = width, height
 
     def render(self, spp: int, max_depth: int = 8, rr_depth: int = 3, seed: int = 3, wave_paths: int = 0,
-               use_graphs: bool = True, out=None):
-        """Returns (rgb[h, w, 3] float32 (host) or `out`, stats dict)."""
+               use_graphs: bool = True, out=None, filter=None):
+        """Returns (rgb[h, w, 3] float32 (host) or `out`, stats dict).  `filter`:
+        an image.filter_desc (default: each sample in its own pixel)."""
         ctx = self.accel.ctx
         o = _lib.ilm_pt_opts(spp, max_depth, rr_depth, seed, wave_paths, int(use_graphs))
+        if filter is not None:
+            o.filter = filter
         st = _lib.ilm_pt_stats()
         if out is None:
             out = np.empty((self.height, self.width, 3), np.float32)

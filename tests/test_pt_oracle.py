@@ -9,6 +9,7 @@ import numpy as np
 import pytest
 
 import oracle
+from rs_illume_b200 import workloads as wl
 
 EYE = (0.0, 0.0, -1.0)
 
@@ -79,3 +80,33 @@ def test_cornell_render_properties():
     left, right = img[8:24, 1:4].mean(axis=(0, 1)), img[8:24, 28:31].mean(axis=(0, 1))
     assert left[0] > 2 * left[1] and right[1] > 2 * right[0]
     assert nc > 32 * 32 * 16 and ns > 0
+
+
+def test_filtered_film_box_equals_pixel_mean():
+    """A box of radius 0.5 through the filtered film is the per-pixel mean."""
+    import numpy as np
+    from rs_illume_b200 import image
+    xyz, idx, mat, alb, emi = wl.cornell(2, 3)
+    cam = wl.CORNELL_CAMERA
+    sc = oracle.Scene(xyz, idx)
+    plain, _ = oracle.render_pt(sc, xyz, idx, mat, alb, emi, cam["eye"], cam["fov_deg"], 12, 12, 4, 8, 3, 5)
+    table = image.filter_table(image.filter_desc("box", (0.5, 0.5)))
+    filt, _ = oracle.render_pt_filtered(sc, xyz, idx, mat, alb, emi, cam["eye"], cam["fov_deg"], 12, 12, 4, table,
+                                        (0.5, 0.5), seed=5)
+    np.testing.assert_allclose(filt, plain, rtol=1e-6, atol=1e-7)
+
+
+def test_filtered_film_gaussian_is_smoother():
+    import numpy as np
+    from rs_illume_b200 import image
+    xyz, idx, mat, alb, emi = wl.cornell(2, 3)
+    cam = wl.CORNELL_CAMERA
+    sc = oracle.Scene(xyz, idx)
+    box, _ = oracle.render_pt(sc, xyz, idx, mat, alb, emi, cam["eye"], cam["fov_deg"], 16, 16, 4, 8, 3, 5)
+    f = image.filter_desc("gaussian", (1.5, 1.5), 2.0)
+    g, _ = oracle.render_pt_filtered(sc, xyz, idx, mat, alb, emi, cam["eye"], cam["fov_deg"], 16, 16, 4,
+                                     image.filter_table(f), (1.5, 1.5), seed=5)
+    assert np.all(np.isfinite(g)) and g.min() >= 0
+    # same mean radiance, less pixel-to-pixel variation
+    assert abs(g.mean() / box.mean() - 1) < 0.05
+    assert np.abs(np.diff(g, axis=1)).mean() < np.abs(np.diff(box, axis=1)).mean()
