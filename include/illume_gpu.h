@@ -58,13 +58,22 @@ typedef struct { float o[3]; float tmin; float d[3]; float tmax; } ilm_ray;
 typedef struct { uint32_t prim; float t; float u; float v; } ilm_hit;
 #define ILM_MISS 0xFFFFFFFFu
 
-/* Sphere shape: mirrors Sphere::new (shapes/sphere.rs:50-75).  Transforms are
- * row-major 4x4, m[i][j] at [4*i + j]; world_to_object must be the inverse. */
+/* Sphere or another quadric.  Transforms are row-major 4x4, m[i][j] at
+ * [4*i + j]; world_to_object must be the inverse.  kind selects
+ *   ILM_QUADRIC_SPHERE   Sphere::new (shapes/sphere.rs:50-75): radius, z_min, z_max, phi_max_deg;
+ *   ILM_QUADRIC_DISK     Disk::new (disk.rs:27-47): height, radius, inner_radius, phi_max_deg;
+ *   ILM_QUADRIC_CYLINDER Cylinder::new (cylinder.rs:26-46): radius, z_min, z_max, phi_max_deg
+ *                        (in degrees and ordered, as pbrt; the reference keeps the raw values);
+ *   ILM_QUADRIC_CONE     Cone::new (cone.rs:26-41): height, radius, phi_max_deg.
+ * Zero-initialised extra fields keep the sphere layout of earlier callers. */
+enum { ILM_QUADRIC_SPHERE = 0, ILM_QUADRIC_DISK = 1, ILM_QUADRIC_CYLINDER = 2, ILM_QUADRIC_CONE = 3 };
 typedef struct {
     float object_to_world[16];
     float world_to_object[16];
     float radius, z_min, z_max, phi_max_deg;
     int32_t reverse_orientation;
+    int32_t kind;
+    float height, inner_radius;
 } ilm_sphere_desc;
 
 typedef struct {
@@ -116,7 +125,7 @@ const char* ilm_last_error_string(const ilm_context* ctx);
  * copied; the caller keeps ownership. */
 int32_t ilm_mesh_upload(ilm_context* ctx, const float* xyz, uint32_t nv,
                         const uint32_t* idx, uint32_t nt, ilm_mesh_id* out);
-/* A set of spheres (shapes/sphere.rs). */
+/* A set of spheres and other quadrics (shapes/{sphere,disk,cylinder,cone}.rs). */
 int32_t ilm_spheres_upload(ilm_context* ctx, const ilm_sphere_desc* spheres, uint32_t n,
                            ilm_mesh_id* out);
 

@@ -30,7 +30,8 @@ BIN_NODE_DTYPE = np.dtype([("bmin", "<f4", (3,)), ("bmax", "<f4", (3,)), ("offse
 class orc_sphere_desc(ctypes.Structure):
     _fields_ = [("object_to_world", ctypes.c_float * 16), ("world_to_object", ctypes.c_float * 16),
                 ("radius", ctypes.c_float), ("z_min", ctypes.c_float), ("z_max", ctypes.c_float),
-                ("phi_max_deg", ctypes.c_float), ("reverse_orientation", ctypes.c_int32)]
+                ("phi_max_deg", ctypes.c_float), ("reverse_orientation", ctypes.c_int32),
+                ("kind", ctypes.c_int32), ("height", ctypes.c_float), ("inner_radius", ctypes.c_float)]
 
 
 _P = ctypes.c_void_p
@@ -106,6 +107,22 @@ def rng_u32(seq: int, n: int) -> np.ndarray:
     out = np.empty(n, np.uint32)
     load().orc_rng_u32(seq, n, _p(out))
     return out
+
+
+def quadric_desc(kind: int, radius: float, matrix, z_min: float = 0.0, z_max: float = 0.0,
+                 phi_max_deg: float = 360.0, height: float = 0.0, inner_radius: float = 0.0,
+                 reverse: bool = False) -> orc_sphere_desc:
+    """Any quadric (kind 0 sphere, 1 disk, 2 cylinder, 3 cone) under a 4x4
+    object-to-world matrix (its inverse computed in float64)."""
+    m = np.asarray(matrix, np.float64).reshape(4, 4)
+    inv = np.linalg.inv(m)
+    d = orc_sphere_desc()
+    for i in range(16):
+        d.object_to_world[i] = float(np.float32(m.flat[i]))
+        d.world_to_object[i] = float(np.float32(inv.flat[i]))
+    d.kind, d.radius, d.z_min, d.z_max = kind, radius, z_min, z_max
+    d.phi_max_deg, d.height, d.inner_radius, d.reverse_orientation = phi_max_deg, height, inner_radius, int(reverse)
+    return d
 
 
 def sphere_desc(radius: float, translate=(0.0, 0.0, 0.0), scale: float = 1.0, z_min=None, z_max=None,

@@ -235,26 +235,51 @@ static bool ef_quadratic(EF a, EF b, EF c, EF* t0, EF* t1) {
 }
 
 // ---------------------------------------------------------------- sphere.rs
+// A sphere or another quadric.  z_min / z_max bound the object box in z for
+// every kind (disk: both = height; cone: 0 and height).
 struct Sphere {
     float m[16], mi[16];   // object_to_world, world_to_object (row-major)
     float radius, z_min, z_max, theta_min, theta_max, phi_max;
+    float inner_radius, height;
+    int kind;              // 0 sphere, 1 disk, 2 cylinder, 3 cone
     bool reverse;
 };
-// Sphere::new (sphere.rs:50-75; D22: made public)
+// Sphere::new (sphere.rs:50-75; D22: made public), Disk::new (disk.rs:27-47),
+// Cylinder::new (cylinder.rs:26-46; D29: phi_max in radians of the clamped
+// degrees and z_min <= z_max, as pbrt), Cone::new (cone.rs:26-41).
 static Sphere sphere_new(const orc_sphere_desc& d) {
     Sphere s;
+    std::memset(&s, 0, sizeof s);
     std::memcpy(s.m, d.object_to_world, sizeof s.m);
     std::memcpy(s.mi, d.world_to_object, sizeof s.mi);
-    float mn = std::fmin(d.z_min, d.z_max), mx = std::fmax(d.z_min, d.z_max);
     auto clamp = [](float v, float lo, float hi) { return v < lo ? lo : (v > hi ? hi : v); };
+    float mn = std::fmin(d.z_min, d.z_max), mx = std::fmax(d.z_min, d.z_max);
+    s.kind = d.kind;
     s.radius = d.radius;
-    s.z_min = clamp(mn, -d.radius, d.radius);
-    s.z_max = clamp(mx, -d.radius, d.radius);
-    s.theta_min = std::acos(clamp(mn / d.radius, -1.0f, 1.0f));
-    s.theta_max = std::acos(clamp(mx / d.radius, -1.0f, 1.0f));
     // radians(): FRAC_PI_180 * deg (pbrt.rs:51-53)
     s.phi_max = (kPi / 180.0f) * clamp(d.phi_max_deg, 0.0f, 360.0f);
     s.reverse = d.reverse_orientation != 0;
+    switch (d.kind) {
+        case 1:   // disk
+            s.height = d.height;
+            s.inner_radius = d.inner_radius;
+            s.z_min = s.z_max = d.height;
+            break;
+        case 2:   // cylinder
+            s.z_min = mn;
+            s.z_max = mx;
+            break;
+        case 3:   // cone
+            s.height = d.height;
+            s.z_min = 0.0f;
+            s.z_max = d.height;
+            break;
+        default:   // sphere
+            s.z_min = clamp(mn, -d.radius, d.radius);
+            s.z_max = clamp(mx, -d.radius, d.radius);
+            s.theta_min = std::acos(clamp(mn / d.radius, -1.0f, 1.0f));
+            s.theta_max = std::acos(clamp(mx / d.radius, -1.0f, 1.0f));
+    }
     return s;
 }
 // Transform::transform_bounds -> Bounds3::transform (bounds3.rs:320-356)
@@ -351,6 +376,127 @@ static bool sphere_test(const Sphere& s, const Ray& world_ray, float* t_out, flo
     *t_out = th.v;
     uv_out[0] = u; uv_out[1] = v;
     return true;
+}
+
+// Disk::intersect / intersect_p (disk.rs:110-166, 168-203): the plane z =
+// height in object space, then the radii and phi_max.
+static bool disk_test(const Sphere& s, const Ray& world_ray, float* t_out, float* uv_out) {
+    V3 o, d, oe, de;
+    transform_ray_with_error(s.mi, world_ray, &o, &d, &oe, &de);
+    if (d.z == 0.0f) return false;
+    float t = (s.height - o.z) / d.z;
+    if (t <= 0.0f || t >= world_ray.t_max) return false;
+    V3 p{o.x + d.x * t, o.y + d.y * t, o.z + d.z * t};
+    float dist2 = p.x * p.x + p.y * p.y;
+    if (dist2 > s.radius * s.radius || dist2 < s.inner_radius * s.inner_radius) return false;
+    float phi = std::atan2(p.y, p.x);
+    if (phi < 0.0f) phi += 2.0f * kPi;
+    if (phi > s.phi_max) return false;
+    float r_hit = std::sqrt(dist2);
+    *t_out = t;
+    uv_out[0] = phi / s.phi_max;
+    uv_out[1] = (s.radius - r_hit) / (s.radius - s.inner_radius);
+    return true;
+}
+
+// The nearest root of [t0, t1] within (0, t_max] (sphere.rs:135-144 and the
+// same lines of cylinder.rs / cone.rs); false when neither qualifies.
+static bool nearest_root(const EF& t0, const EF& t1, float t_max, EF* th) {
+    if (t0.high > t_max || t1.low <= 0.0f) return false;
+    *th = t0;
+    if (th->low <= 0.0f) {
+        *th = t1;
+        if (th->high > t_max) return false;
+    }
+    return true;
+}
+
+// Cylinder::intersect / intersect_p (cylinder.rs:77-...): x^2 + y^2 = r^2,
+// the hit refined onto the radius, clipped by z and phi (retry with t1).
+static bool cylinder_test(const Sphere& s, const Ray& world_ray, float* t_out, float* uv_out) {
+    V3 o, d, oe, de;
+    transform_ray_with_error(s.mi, world_ray, &o, &d, &oe, &de);
+    EF ox = ef_new(o.x, oe.x), oy = ef_new(o.y, oe.y);
+    EF dx = ef_new(d.x, de.x), dy = ef_new(d.y, de.y);
+    EF a = ef_add(ef_mul(dx, dx), ef_mul(dy, dy));
+    EF b = ef_mul(ef_add(ef_mul(dx, ox), ef_mul(dy, oy)), ef_new(2.0f, 0.0f));
+    EF rr = ef_new(s.radius, 0.0f);
+    EF c = ef_sub(ef_add(ef_mul(ox, ox), ef_mul(oy, oy)), ef_mul(rr, rr));
+    EF t0, t1, th;
+    if (!ef_quadratic(a, b, c, &t0, &t1)) return false;
+    if (!nearest_root(t0, t1, world_ray.t_max, &th)) return false;
+    V3 p;
+    float phi;
+    auto hit_point = [&](float t) {
+        p = {o.x + d.x * t, o.y + d.y * t, o.z + d.z * t};
+        float hit_rad = std::sqrt(p.x * p.x + p.y * p.y);
+        p.x *= s.radius / hit_rad;
+        p.y *= s.radius / hit_rad;
+        phi = std::atan2(p.y, p.x);
+        if (phi < 0.0f) phi += 2.0f * kPi;
+    };
+    auto clipped = [&]() { return p.z < s.z_min || p.z > s.z_max || phi > s.phi_max; };
+    hit_point(th.v);
+    if (clipped()) {
+        if (th.v == t1.v) return false;
+        if (t1.high > world_ray.t_max) return false;
+        th = t1;
+        hit_point(th.v);
+        if (clipped()) return false;
+    }
+    *t_out = th.v;
+    uv_out[0] = phi / s.phi_max;
+    uv_out[1] = (p.z - s.z_min) / (s.z_max - s.z_min);
+    return true;
+}
+
+// Cone::intersect / intersect_p (cone.rs:91-...): x^2 + y^2 = k (z - h)^2
+// with k = (r / h)^2, clipped by 0 <= z <= h and phi (retry with t1).  D28:
+// the reference's b = dx*ox + dy*oy - k*dz*(oz - h)*2 doubles only the last
+// term; repaired to 2 (dx*ox + dy*oy - k*dz*(oz - h)) as pbrt.
+static bool cone_test(const Sphere& s, const Ray& world_ray, float* t_out, float* uv_out) {
+    V3 o, d, oe, de;
+    transform_ray_with_error(s.mi, world_ray, &o, &d, &oe, &de);
+    EF ox = ef_new(o.x, oe.x), oy = ef_new(o.y, oe.y), oz = ef_new(o.z, oe.z);
+    EF dx = ef_new(d.x, de.x), dy = ef_new(d.y, de.y), dz = ef_new(d.z, de.z);
+    EF k = ef_div(ef_new(s.radius, 0.0f), ef_new(s.height, 0.0f));
+    k = ef_mul(k, k);
+    EF ozh = ef_sub(oz, ef_new(s.height, 0.0f));
+    EF a = ef_sub(ef_add(ef_mul(dx, dx), ef_mul(dy, dy)), ef_mul(ef_mul(k, dz), dz));
+    EF b = ef_mul(ef_sub(ef_add(ef_mul(dx, ox), ef_mul(dy, oy)), ef_mul(ef_mul(k, dz), ozh)), ef_new(2.0f, 0.0f));
+    EF c = ef_sub(ef_add(ef_mul(ox, ox), ef_mul(oy, oy)), ef_mul(ef_mul(k, ozh), ozh));
+    EF t0, t1, th;
+    if (!ef_quadratic(a, b, c, &t0, &t1)) return false;
+    if (!nearest_root(t0, t1, world_ray.t_max, &th)) return false;
+    V3 p;
+    float phi;
+    auto hit_point = [&](float t) {
+        p = {o.x + d.x * t, o.y + d.y * t, o.z + d.z * t};
+        phi = std::atan2(p.y, p.x);
+        if (phi < 0.0f) phi += 2.0f * kPi;
+    };
+    auto clipped = [&]() { return p.z < 0.0f || p.z > s.height || phi > s.phi_max; };
+    hit_point(th.v);
+    if (clipped()) {
+        if (th.v == t1.v) return false;
+        if (t1.high > world_ray.t_max) return false;
+        th = t1;
+        hit_point(th.v);
+        if (clipped()) return false;
+    }
+    *t_out = th.v;
+    uv_out[0] = phi / s.phi_max;
+    uv_out[1] = p.z / s.height;
+    return true;
+}
+
+static bool quadric_test(const Sphere& s, const Ray& ray, float* t_out, float* uv_out) {
+    switch (s.kind) {
+        case 1: return disk_test(s, ray, t_out, uv_out);
+        case 2: return cylinder_test(s, ray, t_out, uv_out);
+        case 3: return cone_test(s, ray, t_out, uv_out);
+        default: return sphere_test(s, ray, t_out, uv_out);
+    }
 }
 
 // ---------------------------------------------------------------- bvh.rs
@@ -503,7 +649,7 @@ static bool prim_test(const Scene& s, uint32_t prim, const Ray& ray, bool closes
         if (h) { uv[0] = b[1]; uv[1] = b[2]; }
         return h;
     }
-    return sphere_test(s.spheres[prim - s.nt], ray, t, uv);
+    return quadric_test(s.spheres[prim - s.nt], ray, t, uv);
 }
 
 // BVHAccel::intersect (bvh.rs:563-612).  D4: the far child is pushed in both
@@ -738,7 +884,7 @@ int orc_sphere_intersect(const orc_sphere_desc* sd, const orc_ray* r, int closes
     Sphere s = sphere_new(*sd);
     Ray ray{{r->o[0], r->o[1], r->o[2]}, {r->d[0], r->d[1], r->d[2]}, r->tmax};
     float t, uv[2];
-    if (!sphere_test(s, ray, &t, uv)) return 0;
+    if (!quadric_test(s, ray, &t, uv)) return 0;
     out[0] = t; out[1] = uv[0]; out[2] = uv[1];
     return 1;
 }

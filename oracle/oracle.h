@@ -29,13 +29,18 @@ typedef struct { float o[3]; float tmin; float d[3]; float tmax; } orc_ray;
 /* 16-byte hit record: primitive id (0xFFFFFFFF = miss), t, u (=b1), v (=b2). */
 typedef struct { uint32_t prim; float t; float u; float v; } orc_hit;
 
-/* Sphere shape (shapes/sphere.rs:15-75): object_to_world / world_to_object
- * are row-major 4x4 (m[i][j] at [4*i+j]). */
+/* Quadric shape: object_to_world / world_to_object are row-major 4x4
+ * (m[i][j] at [4*i+j]).  kind 0: Sphere (shapes/sphere.rs:15-75; radius,
+ * z_min, z_max, phi_max); 1: Disk (disk.rs:27-47; height, radius,
+ * inner_radius, phi_max); 2: Cylinder (cylinder.rs:26-46; radius, z_min,
+ * z_max, phi_max); 3: Cone (cone.rs:26-41; height, radius, phi_max). */
 typedef struct {
     float object_to_world[16];
     float world_to_object[16];
     float radius, z_min, z_max, phi_max_deg;
     int32_t reverse_orientation;
+    int32_t kind;
+    float height, inner_radius;
 } orc_sphere_desc;
 
 /* 32-byte flattened BVH node (accelerators/bvh.rs:665-673, 32 B per D6). */

@@ -198,11 +198,20 @@ int32_t ilm_spheres_upload(ilm_context* ctx, const ilm_sphere_desc* spheres, uin
             set_error(ctx, "ilm_spheres_upload: radius must be positive and finite");
             return ILM_ERR_INVALID_ARGUMENT;
         }
+        if (d.kind < ILM_QUADRIC_SPHERE || d.kind > ILM_QUADRIC_CONE ||
+            (d.kind == ILM_QUADRIC_CONE && !(d.height > 0.0f)) ||
+            (d.kind == ILM_QUADRIC_DISK && !(d.inner_radius >= 0.0f && d.inner_radius < d.radius)) ||
+            (d.kind == ILM_QUADRIC_CYLINDER && !(d.z_min != d.z_max)) || !std::isfinite(d.height) ||
+            !std::isfinite(d.z_min) || !std::isfinite(d.z_max)) {
+            set_error(ctx, "ilm_spheres_upload: invalid quadric parameters");
+            return ILM_ERR_INVALID_ARGUMENT;
+        }
         SphereInput in;
         std::memcpy(in.o2w, d.object_to_world, sizeof in.o2w);
         std::memcpy(in.w2o, d.world_to_object, sizeof in.w2o);
         in.radius = d.radius; in.z_min = d.z_min; in.z_max = d.z_max; in.phi_max_deg = d.phi_max_deg;
         in.reverse = d.reverse_orientation;
+        in.kind = d.kind; in.height = d.height; in.inner_radius = d.inner_radius;
         m->spheres.push_back(make_sphere(in));
     }
     m->n_prims = n;

@@ -237,14 +237,30 @@ SphereRec make_sphere(const SphereInput& in) {
     std::memcpy(s.w2o, in.w2o, sizeof s.w2o);
     auto clamp = [](float v, float lo, float hi) { return v < lo ? lo : (v > hi ? hi : v); };
     float mn = std::fmin(in.z_min, in.z_max), mx = std::fmax(in.z_min, in.z_max);
-    s.radius = in.radius;
-    s.z_min = clamp(mn, -in.radius, in.radius);
-    s.z_max = clamp(mx, -in.radius, in.radius);
-    s.theta_min = std::acos(clamp(mn / in.radius, -1.0f, 1.0f));
-    s.theta_max = std::acos(clamp(mx / in.radius, -1.0f, 1.0f));
     const float kPi = 3.14159265358979323846f;
+    s.radius = in.radius;
     s.phi_max = (kPi / 180.0f) * clamp(in.phi_max_deg, 0.0f, 360.0f);
     s.reverse = in.reverse;
+    s.kind = in.kind;
+    switch (in.kind) {
+        case kQuadricDisk:   // Disk::new (disk.rs:27-47)
+            s.z_min = s.z_max = in.height;
+            s.theta_min = in.inner_radius;
+            break;
+        case kQuadricCylinder:   // Cylinder::new (cylinder.rs:26-46), z range ordered and phi in radians as pbrt
+            s.z_min = mn;
+            s.z_max = mx;
+            break;
+        case kQuadricCone:   // Cone::new (cone.rs:26-41)
+            s.z_min = 0.0f;
+            s.z_max = in.height;
+            break;
+        default:   // Sphere::new (sphere.rs:50-75)
+            s.z_min = clamp(mn, -in.radius, in.radius);
+            s.z_max = clamp(mx, -in.radius, in.radius);
+            s.theta_min = std::acos(clamp(mn / in.radius, -1.0f, 1.0f));
+            s.theta_max = std::acos(clamp(mx / in.radius, -1.0f, 1.0f));
+    }
     return s;
 }
 

@@ -49,6 +49,8 @@ struct SphereInput {
     float o2w[16], w2o[16];
     float radius, z_min, z_max, phi_max_deg;
     int32_t reverse;
+    int32_t kind = 0;              // kQuadric*
+    float height = 0.0f, inner_radius = 0.0f;
 };
 SphereRec make_sphere(const SphereInput& in);
 Box sphere_bound(const SphereRec& s);

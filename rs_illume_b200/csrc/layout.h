@@ -32,12 +32,16 @@ enum : uint32_t {
 };
 
 // Sphere record (shapes/sphere.rs:15-75) with Sphere::new's derived values.
+// A sphere or another quadric (kind).  z_min / z_max bound the object box in
+// z for every kind; a disk keeps its height in z_min (= z_max) and its inner
+// radius in theta_min, a cone its height in z_max (z_min = 0).
+enum : int32_t { kQuadricSphere = 0, kQuadricDisk = 1, kQuadricCylinder = 2, kQuadricCone = 3 };
 struct SphereRec {
     float o2w[16];
     float w2o[16];
     float radius, z_min, z_max, theta_min, theta_max, phi_max;
     int32_t reverse;
-    int32_t pad;
+    int32_t kind;
 };
 static_assert(sizeof(SphereRec) == 160, "SphereRec must be 160 bytes");
 

@@ -166,14 +166,15 @@ __device__ __forceinline__ EF ef_div(EF a, EF b) {
             next_up(fmaxf(fmaxf(fmaxf(d0, d1), d2), d3))};
 }
 
-// Sphere::intersect / intersect_p (shapes/sphere.rs:105-188, 238-323) with
-// Transform::transform_ray_with_error (core/transform.rs:392-435).  The
-// refine step uses the Euclidean distance (point3.rs:62-66 computes sqrt of a
-// dot product instead).  Returns t and the parametric (u, v).
-static __device__ __noinline__ bool sphere_test(const SphereRec& s, float rox, float roy, float roz, float rdx,
-                                         float rdy, float rdz, float tmax, float& t_out, float& u_out,
-                                         float& v_out) {
-    const float* m = s.w2o;
+// A ray in a quadric's object space with its error bounds:
+// Transform::transform_ray_with_error (core/transform.rs:392-435).
+struct ObjRay {
+    float ox, oy, oz, oex, oey, oez;   // origin and its error
+    float dx, dy, dz, dex, dey, dez;   // direction and its error
+};
+
+__device__ __forceinline__ ObjRay xform_ray(const float* m, float rox, float roy, float roz, float rdx, float rdy,
+                                           float rdz) {
     // transform_point_with_error (transform.rs:224-247)
     float xp = __fadd_rn(__fadd_rn(__fmul_rn(m[0], rox), __fmul_rn(m[1], roy)), __fadd_rn(__fmul_rn(m[2], roz), m[3]));
     float yp = __fadd_rn(__fadd_rn(__fmul_rn(m[4], rox), __fmul_rn(m[5], roy)), __fadd_rn(__fmul_rn(m[6], roz), m[7]));
@@ -200,14 +201,11 @@ static __device__ __noinline__ bool sphere_test(const SphereRec& s, float rox, f
         oy = __fadd_rn(oy, __fmul_rn(dy, dt));
         oz = __fadd_rn(oz, __fmul_rn(dz, dt));
     }
-    // quadratic coefficients (sphere.rs:116-126)
-    EF eox = ef_new(ox, oex), eoy = ef_new(oy, oey), eoz = ef_new(oz, oez);
-    EF edx = ef_new(dx, dex), edy = ef_new(dy, dey), edz = ef_new(dz, dez);
-    EF a = ef_add(ef_add(ef_mul(edx, edx), ef_mul(edy, edy)), ef_mul(edz, edz));
-    EF b = ef_mul(ef_add(ef_add(ef_mul(edx, eox), ef_mul(edy, eoy)), ef_mul(edz, eoz)), EF{2.0f, 2.0f, 2.0f});
-    EF rr = EF{s.radius, s.radius, s.radius};
-    EF c = ef_sub(ef_add(ef_add(ef_mul(eox, eox), ef_mul(eoy, eoy)), ef_mul(eoz, eoz)), ef_mul(rr, rr));
-    // quadratic (efloat.rs:232-257)
+    return ObjRay{ox, oy, oz, oex, oey, oez, dx, dy, dz, dex, dey, dez};
+}
+
+// EFloat quadratic (efloat.rs:232-257): false without real roots; t0 <= t1.
+__device__ __forceinline__ bool ef_quadratic(EF a, EF b, EF c, EF& t0, EF& t1) {
     double disc = __dsub_rn(__dmul_rn((double)b.v, (double)b.v), __dmul_rn(__dmul_rn(4.0, (double)a.v), (double)c.v));
     if (disc < 0.0) return false;
     double root = __dsqrt_rn(disc);
@@ -215,15 +213,46 @@ static __device__ __noinline__ bool sphere_test(const SphereRec& s, float rox, f
     EF froot = ef_new(fr, __fmul_rn(kMachineEps, fr));
     EF half = EF{-0.5f, -0.5f, -0.5f};
     EF q = (b.v < 0.0f) ? ef_mul(ef_sub(b, froot), half) : ef_mul(ef_add(b, froot), half);
-    EF t0 = ef_div(q, a), t1 = ef_div(c, q);
+    t0 = ef_div(q, a);
+    t1 = ef_div(c, q);
     if (t0.v > t1.v) { EF sw = t0; t0 = t1; t1 = sw; }
-    // nearest valid root (sphere.rs:135-144)
+    return true;
+}
+
+// Nearest root within (0, tmax] (sphere.rs:135-144; the same lines in
+// cylinder.rs and cone.rs).
+__device__ __forceinline__ bool nearest_root(const EF& t0, const EF& t1, float tmax, EF& th) {
     if (t0.hi > tmax || t1.lo <= 0.0f) return false;
-    EF th = t0;
+    th = t0;
     if (th.lo <= 0.0f) {
         th = t1;
         if (th.hi > tmax) return false;
     }
+    return true;
+}
+
+__device__ __forceinline__ float phi_of(float y, float x) {
+    float phi = atan2f(y, x);
+    if (phi < 0.0f) phi = __fadd_rn(phi, 2.0f * kPiF);
+    return phi;
+}
+
+// Sphere::intersect / intersect_p (shapes/sphere.rs:105-188, 238-323).  The
+// refine step uses the Euclidean distance (point3.rs:62-66 computes sqrt of a
+// dot product instead).  Returns t and the parametric (u, v).
+__device__ __forceinline__ bool sphere_test(const SphereRec& s, const ObjRay& r, float tmax, float& t_out,
+                                            float& u_out, float& v_out) {
+    const float ox = r.ox, oy = r.oy, oz = r.oz, dx = r.dx, dy = r.dy, dz = r.dz;
+    // quadratic coefficients (sphere.rs:116-126)
+    EF eox = ef_new(ox, r.oex), eoy = ef_new(oy, r.oey), eoz = ef_new(oz, r.oez);
+    EF edx = ef_new(dx, r.dex), edy = ef_new(dy, r.dey), edz = ef_new(dz, r.dez);
+    EF a = ef_add(ef_add(ef_mul(edx, edx), ef_mul(edy, edy)), ef_mul(edz, edz));
+    EF b = ef_mul(ef_add(ef_add(ef_mul(edx, eox), ef_mul(edy, eoy)), ef_mul(edz, eoz)), EF{2.0f, 2.0f, 2.0f});
+    EF rr = EF{s.radius, s.radius, s.radius};
+    EF c = ef_sub(ef_add(ef_add(ef_mul(eox, eox), ef_mul(eoy, eoy)), ef_mul(eoz, eoz)), ef_mul(rr, rr));
+    EF t0, t1, th;
+    if (!ef_quadratic(a, b, c, t0, t1)) return false;
+    if (!nearest_root(t0, t1, tmax, th)) return false;
     float px, py, pz, phi;
     auto hit_point = [&](float t) {
         px = __fadd_rn(ox, __fmul_rn(dx, t));
@@ -233,8 +262,7 @@ static __device__ __noinline__ bool sphere_test(const SphereRec& s, float rox, f
         float k = __fdiv_rn(s.radius, dist);
         px = __fmul_rn(px, k); py = __fmul_rn(py, k); pz = __fmul_rn(pz, k);
         if (px == 0.0f && py == 0.0f) px = __fmul_rn(1e-5f, s.radius);
-        phi = atan2f(py, px);
-        if (phi < 0.0f) phi = __fadd_rn(phi, 2.0f * kPiF);
+        phi = phi_of(py, px);
     };
     auto clipped = [&]() {
         return (s.z_min > -s.radius && pz < s.z_min) || (s.z_max < s.radius && pz > s.z_max) || phi > s.phi_max;
@@ -253,6 +281,119 @@ static __device__ __noinline__ bool sphere_test(const SphereRec& s, float rox, f
     u_out = __fdiv_rn(phi, s.phi_max);
     v_out = __fdiv_rn(__fsub_rn(theta, s.theta_min), __fsub_rn(s.theta_max, s.theta_min));
     return true;
+}
+
+// Disk::intersect / intersect_p (disk.rs:110-166, 168-203): the plane
+// z = height, then the radii and phi_max.  Disk records keep the height in
+// z_min (= z_max) and the inner radius in theta_min.
+__device__ __forceinline__ bool disk_test(const SphereRec& s, const ObjRay& r, float tmax, float& t_out,
+                                          float& u_out, float& v_out) {
+    const float height = s.z_min, inner = s.theta_min;
+    if (r.dz == 0.0f) return false;
+    float t = __fdiv_rn(__fsub_rn(height, r.oz), r.dz);
+    if (t <= 0.0f || t >= tmax) return false;
+    float px = __fadd_rn(r.ox, __fmul_rn(r.dx, t)), py = __fadd_rn(r.oy, __fmul_rn(r.dy, t));
+    float dist2 = __fadd_rn(__fmul_rn(px, px), __fmul_rn(py, py));
+    if (dist2 > __fmul_rn(s.radius, s.radius) || dist2 < __fmul_rn(inner, inner)) return false;
+    float phi = phi_of(py, px);
+    if (phi > s.phi_max) return false;
+    float r_hit = __fsqrt_rn(dist2);
+    t_out = t;
+    u_out = __fdiv_rn(phi, s.phi_max);
+    v_out = __fdiv_rn(__fsub_rn(s.radius, r_hit), __fsub_rn(s.radius, inner));
+    return true;
+}
+
+// Cylinder::intersect / intersect_p (cylinder.rs:77-...): x^2 + y^2 = r^2,
+// the hit refined onto the radius, clipped by z and phi (retry with t1).
+__device__ __forceinline__ bool cylinder_test(const SphereRec& s, const ObjRay& r, float tmax, float& t_out,
+                                              float& u_out, float& v_out) {
+    EF eox = ef_new(r.ox, r.oex), eoy = ef_new(r.oy, r.oey);
+    EF edx = ef_new(r.dx, r.dex), edy = ef_new(r.dy, r.dey);
+    EF a = ef_add(ef_mul(edx, edx), ef_mul(edy, edy));
+    EF b = ef_mul(ef_add(ef_mul(edx, eox), ef_mul(edy, eoy)), EF{2.0f, 2.0f, 2.0f});
+    EF rr = EF{s.radius, s.radius, s.radius};
+    EF c = ef_sub(ef_add(ef_mul(eox, eox), ef_mul(eoy, eoy)), ef_mul(rr, rr));
+    EF t0, t1, th;
+    if (!ef_quadratic(a, b, c, t0, t1)) return false;
+    if (!nearest_root(t0, t1, tmax, th)) return false;
+    float px, py, pz, phi;
+    auto hit_point = [&](float t) {
+        px = __fadd_rn(r.ox, __fmul_rn(r.dx, t));
+        py = __fadd_rn(r.oy, __fmul_rn(r.dy, t));
+        pz = __fadd_rn(r.oz, __fmul_rn(r.dz, t));
+        float hit_rad = __fsqrt_rn(__fadd_rn(__fmul_rn(px, px), __fmul_rn(py, py)));
+        px = __fmul_rn(px, __fdiv_rn(s.radius, hit_rad));
+        py = __fmul_rn(py, __fdiv_rn(s.radius, hit_rad));
+        phi = phi_of(py, px);
+    };
+    auto clipped = [&]() { return pz < s.z_min || pz > s.z_max || phi > s.phi_max; };
+    hit_point(th.v);
+    if (clipped()) {
+        if (th.v == t1.v) return false;
+        if (t1.hi > tmax) return false;
+        th = t1;
+        hit_point(th.v);
+        if (clipped()) return false;
+    }
+    t_out = th.v;
+    u_out = __fdiv_rn(phi, s.phi_max);
+    v_out = __fdiv_rn(__fsub_rn(pz, s.z_min), __fsub_rn(s.z_max, s.z_min));
+    return true;
+}
+
+// Cone::intersect / intersect_p (cone.rs:91-...): x^2 + y^2 = k (z - h)^2,
+// k = (r / h)^2, clipped by 0 <= z <= h and phi (retry with t1).  Cone
+// records keep the height in z_max.  b = 2 (dx ox + dy oy - k dz (oz - h))
+// (the reference doubles only the last term; repaired as pbrt).
+__device__ __forceinline__ bool cone_test(const SphereRec& s, const ObjRay& r, float tmax, float& t_out,
+                                          float& u_out, float& v_out) {
+    const float height = s.z_max;
+    EF eox = ef_new(r.ox, r.oex), eoy = ef_new(r.oy, r.oey), eoz = ef_new(r.oz, r.oez);
+    EF edx = ef_new(r.dx, r.dex), edy = ef_new(r.dy, r.dey), edz = ef_new(r.dz, r.dez);
+    EF k = ef_div(EF{s.radius, s.radius, s.radius}, EF{height, height, height});
+    k = ef_mul(k, k);
+    EF ozh = ef_sub(eoz, EF{height, height, height});
+    EF a = ef_sub(ef_add(ef_mul(edx, edx), ef_mul(edy, edy)), ef_mul(ef_mul(k, edz), edz));
+    EF b = ef_mul(ef_sub(ef_add(ef_mul(edx, eox), ef_mul(edy, eoy)), ef_mul(ef_mul(k, edz), ozh)),
+                  EF{2.0f, 2.0f, 2.0f});
+    EF c = ef_sub(ef_add(ef_mul(eox, eox), ef_mul(eoy, eoy)), ef_mul(ef_mul(k, ozh), ozh));
+    EF t0, t1, th;
+    if (!ef_quadratic(a, b, c, t0, t1)) return false;
+    if (!nearest_root(t0, t1, tmax, th)) return false;
+    float px, py, pz, phi;
+    auto hit_point = [&](float t) {
+        px = __fadd_rn(r.ox, __fmul_rn(r.dx, t));
+        py = __fadd_rn(r.oy, __fmul_rn(r.dy, t));
+        pz = __fadd_rn(r.oz, __fmul_rn(r.dz, t));
+        phi = phi_of(py, px);
+    };
+    auto clipped = [&]() { return pz < 0.0f || pz > height || phi > s.phi_max; };
+    hit_point(th.v);
+    if (clipped()) {
+        if (th.v == t1.v) return false;
+        if (t1.hi > tmax) return false;
+        th = t1;
+        hit_point(th.v);
+        if (clipped()) return false;
+    }
+    t_out = th.v;
+    u_out = __fdiv_rn(phi, s.phi_max);
+    v_out = __fdiv_rn(pz, height);
+    return true;
+}
+
+// The quadric record's test (SphereRec::kind), in its object space.
+static __device__ __noinline__ bool quadric_test(const SphereRec& s, float rox, float roy, float roz, float rdx,
+                                                 float rdy, float rdz, float tmax, float& t_out, float& u_out,
+                                                 float& v_out) {
+    const ObjRay r = xform_ray(s.w2o, rox, roy, roz, rdx, rdy, rdz);
+    switch (s.kind) {
+        case kQuadricDisk: return disk_test(s, r, tmax, t_out, u_out, v_out);
+        case kQuadricCylinder: return cylinder_test(s, r, tmax, t_out, u_out, v_out);
+        case kQuadricCone: return cone_test(s, r, tmax, t_out, u_out, v_out);
+        default: return sphere_test(s, r, tmax, t_out, u_out, v_out);
+    }
 }
 
 }  // namespace ilm

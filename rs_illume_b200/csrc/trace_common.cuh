@@ -48,8 +48,8 @@ __device__ __forceinline__ bool prim_test(const PrimRec* __restrict__ prims, con
     uint32_t flags = __float_as_uint(b.w);
     prim_id = __float_as_uint(a.w);
     if (flags & kPrimSphere) {
-        return sphere_test(spheres[__float_as_uint(c.w)], ray.ox, ray.oy, ray.oz, ray.dx, ray.dy, ray.dz,
-                           tmax, t, u, v);
+        return quadric_test(spheres[__float_as_uint(c.w)], ray.ox, ray.oy, ray.oz, ray.dx, ray.dy, ray.dz,
+                            tmax, t, u, v);
     }
     if (kClosest && (flags & kPrimDegenerate)) return false;
     if (!tr_ready) {
