@@ -33,6 +33,8 @@ Further keys, one per workload of the path (each skippable):
                 the plain tracer's relMSE at the same device time (relMSE(1 spp)
                 * t_spp / t_frame); gain = their ratio.  Also the network's
                 inference throughput and training-step time.
+  kdtree        the kd-tree aggregate (KdTreeAccel) over the headline scene
+                and rays: closest-hit and any-hit Mrays/s, build time.
   batched       32 scenes (icospheres and soups, 1k-2M triangles log-uniform)
                 with 10k-4M rays each (log-uniform; primary, incoherent, shadow
                 thirds), all in one persistent launch per BVH width replayed as
@@ -398,6 +400,61 @@ def coherent_leg(rb, wl, ctx, torch, dev, steps):
                       "width 8; scene and rays L2-resident (no flush: the workload is the L2 case)"}
 
 
+# Oracle kd-tree (KdTreeAccel defaults 80 / 1 / 0.5 / 1, depth 34) on the same
+# scene and rays: mean node visits / primitive tests per ray.
+N_NODE_KD_CLOSEST, N_TRI_KD_CLOSEST = 9.904898, 1.864308
+N_NODE_KD_ANY, N_TRI_KD_ANY = 7.529678, 0.806322
+BYTES_PER_RAY_KD_CLOSEST = 32 + 16 + 8 * N_NODE_KD_CLOSEST + 36 * N_TRI_KD_CLOSEST
+BYTES_PER_RAY_KD_ANY = 32 + 4 + 8 * N_NODE_KD_ANY + 36 * N_TRI_KD_ANY
+
+
+def kdtree_leg(rb, wl, ctx, torch, dev, steps, warmup, scene=None):
+    """The kd-tree aggregate on the headline scene and rays: closest-hit and
+    any-hit Mrays/s (device buffers, L2 flushed between launches), host build
+    time, and the roofline of the closest-hit launch."""
+    xyz, idx, rays = scene if scene is not None else wl.incoherent_workload(N_RAYS)
+    t0 = time.perf_counter()
+    acc = rb.GpuKdTreeAccel(ctx, [rb.TriangleMesh(ctx, xyz, idx)])
+    build_s = time.perf_counter() - t0
+    info = acc.info()
+    d_closest = torch.from_numpy(np.ascontiguousarray(rays[:N_CLOSEST]).view(np.uint8)).to(dev)
+    d_shadow = torch.from_numpy(np.ascontiguousarray(rays[N_CLOSEST:]).view(np.uint8)).to(dev)
+    d_hits = torch.empty(N_CLOSEST * 16, dtype=torch.uint8, device=dev)
+    d_occ = torch.empty(N_CLOSEST, dtype=torch.int32, device=dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.Stream(dev)
+
+    def timed(fn):
+        with torch.cuda.stream(stream):
+            for _ in range(warmup):
+                flush.zero_()
+                fn()
+            evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+            for a, b in evs:
+                flush.zero_()
+                a.record(stream)
+                fn()
+                b.record(stream)
+        torch.cuda.synchronize(dev)
+        return sum(a.elapsed_time(b) for a, b in evs) / 1e3 / steps
+
+    t = timed(lambda: acc.intersect_batch(d_closest, d_hits, stream=stream))
+    t_any = timed(lambda: acc.intersect_p_batch(d_shadow, d_occ, stream=stream))
+    hbm, kind = measured_peaks()
+    ach = BYTES_PER_RAY_KD_CLOSEST * N_CLOSEST / t / 1e9
+    return {"value": round(N_CLOSEST / t / 1e6, 2), "unit": "Mrays/s", "ms_per_launch": round(t * 1e3, 4),
+            "anyhit": {"value": round(N_CLOSEST / t_any / 1e6, 2), "unit": "Mrays/s",
+                       "achieved_gbs": round(BYTES_PER_RAY_KD_ANY * N_CLOSEST / t_any / 1e9, 1)},
+            "roofline": {"bound": "hbm", "achieved": round(ach, 1), "peak": hbm, "unit": "GB/s",
+                         "frac": round(ach / hbm, 4), "peak_source": f"{kind} hbm_gbs",
+                         "bytes_per_ray": round(BYTES_PER_RAY_KD_CLOSEST, 3)},
+            "build_seconds": round(build_s, 3), "n_nodes": int(info["n_nodes"]),
+            "n_leaf_refs": int(info["n_leaf_refs"]), "max_depth": int(info["max_depth"]),
+            "device_bytes": int(info["device_bytes"]),
+            "config": "KdTreeAccel 80/1/0.5/1 over the headline scene; the headline's 2,097,152 closest and "
+                      "2,097,152 any-hit rays; one thread per ray; L2 flushed between launches"}
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -441,14 +498,17 @@ def run_ours(args):
     dev = torch.device("cuda", local)
 
     if args.only and args.only != "closest":
-        # one workload alone (profiling runs): its key and nothing else
-        ctx = rb.Context(local)
+        # one workload alone (profiling runs): its key and nothing else, with
+        # the launch choices of the full run
+        ctx = rb.Context(local, grid_schedule=(args.schedule == "grid"), high_occupancy=(args.occupancy == "high"),
+                         stack_depth=args.stack_depth)
         legs = {"pt": ("path_tracer", lambda: path_tracer_leg(rb, wl, ctx, dev, args.steps, False)),
                 "nrc": ("neural_cache", lambda: neural_cache_leg(rb, wl, ctx, torch, dev)),
                 "mlp": ("neural_cache", lambda: mlp_leg(rb, ctx, torch, dev)),
                 "nrcframe": ("neural_cache", lambda: nrc_frame_leg(rb, wl, ctx)),
                 "coherent": ("coherent", lambda: coherent_leg(rb, wl, ctx, torch, dev, args.steps)),
-                "batched": ("batched", lambda: batched_leg(rb, wl, ctx, torch, dev, args.steps))}
+                "batched": ("batched", lambda: batched_leg(rb, wl, ctx, torch, dev, args.steps)),
+                "kd": ("kdtree", lambda: kdtree_leg(rb, wl, ctx, torch, dev, args.steps, args.warmup))}
         key, fn = legs[args.only]
         res = fn()
         if rank == 0:
@@ -588,6 +648,8 @@ def run_ours(args):
                                     "n_node_sample": round(nn, 4), "n_tri_sample": round(nt, 4)}
         for key, enabled, fn in (
                 ("coherent", not args.only, lambda: coherent_leg(rb, wl, ctx, torch, dev, args.steps)),
+                ("kdtree", not args.no_kd and not args.only,
+                 lambda: kdtree_leg(rb, wl, ctx, torch, dev, args.steps, args.warmup, (xyz, idx, rays))),
                 ("path_tracer", not args.no_pt and not args.only,
                  lambda: path_tracer_leg(rb, wl, ctx, dev, args.steps, world == 1 and not args.no_cpu)),
                 ("neural_cache", not args.no_nrc and not args.only, lambda: neural_cache_leg(rb, wl, ctx, torch, dev)),
@@ -622,7 +684,8 @@ def main():
     ap.add_argument("--no-pt", action="store_true", help="skip the path-tracer workload")
     ap.add_argument("--no-nrc", action="store_true", help="skip the radiance-cache workload")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched multi-scene workload")
-    ap.add_argument("--only", choices=["closest", "coherent", "pt", "nrc", "nrcframe", "mlp", "batched"],
+    ap.add_argument("--no-kd", action="store_true", help="skip the kd-tree workload")
+    ap.add_argument("--only", choices=["closest", "coherent", "pt", "nrc", "nrcframe", "mlp", "batched", "kd"],
                     help="run one workload alone (profiling)")
     args = ap.parse_args()
     if args.warmup < 3:

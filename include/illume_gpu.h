@@ -104,10 +104,25 @@ typedef struct {
     uint32_t n_prims;
     uint32_t n_binary_nodes;   /* nodes of the SAH binary tree (bvh.rs layout) */
     uint32_t n_nodes;          /* nodes of the device layout for `width` */
-    uint32_t width;
-    uint64_t device_bytes;     /* nodes + primitive records in HBM */
-    double build_seconds;      /* host SAH build + collapse + upload */
+    uint32_t width;            /* BVH width (2, 4, 8), or ILM_LAYOUT_KDTREE */
+    uint64_t device_bytes;     /* nodes + primitive records (+ kd leaf runs) in HBM */
+    double build_seconds;      /* host build (+ collapse) + upload */
+    uint32_t n_leaf_refs;      /* kd-tree: entries of the leaf index list */
+    uint32_t max_depth;        /* kd-tree: the depth limit used */
 } ilm_accel_info;
+/* ilm_accel_info.width of a kd-tree accel. */
+#define ILM_LAYOUT_KDTREE 1
+
+/* KdTreeAccel::new parameters (accelerators/kdtreeaccel.rs:25-32).  A NULL
+ * opts pointer selects 80, 1, 0.5, 1, -1 (pbrt-v3's kd-tree defaults; the
+ * reference has no factory of its own). */
+typedef struct {
+    int32_t isect_cost;
+    int32_t traversal_cost;
+    float empty_bonus;         /* in [0, 1] */
+    uint32_t max_prims;
+    int32_t max_depth;         /* <= 0: round(8 + 1.3 log2(N)); at most 64 */
+} ilm_kdtree_opts;
 
 typedef uint32_t ilm_mesh_id;
 typedef uint32_t ilm_accel_id;
@@ -136,6 +151,20 @@ int32_t ilm_spheres_upload(ilm_context* ctx, const ilm_sphere_desc* spheres, uin
  * nodes collapsed from the same binary tree). */
 int32_t ilm_accel_build(ilm_context* ctx, const ilm_mesh_id* meshes, uint32_t n_meshes,
                         const ilm_build_opts* opts, ilm_accel_id* out);
+/* KdTreeAccel::new (accelerators/kdtreeaccel.rs:25-244): SAH over sorted
+ * bound edges, one axis at a time, 8-byte nodes (kdtreeaccel.rs:470-545) laid
+ * out depth first.  The accel answers every query below (closest and any
+ * hit, the no-alloc form, surface interactions, path tracing) through
+ * KdTreeAccel::intersect / intersect_p (kdtreeaccel.rs:256-465): front-to-
+ * back traversal with a 64-entry stack of deferred far children.  Not
+ * accepted by the batched queries, which run the wide BVH layouts. */
+int32_t ilm_kdtree_build(ilm_context* ctx, const ilm_mesh_id* meshes, uint32_t n_meshes,
+                         const ilm_kdtree_opts* opts, ilm_accel_id* out);
+/* Copies of a kd-tree accel's nodes (info.n_nodes x 8 bytes: word = split
+ * bits, the primitive of a one-primitive leaf or the first slot of a leaf's
+ * run; flags = axis or 3 for a leaf, and above-child or count << 2) and of its
+ * leaf index list (info.n_leaf_refs primitive ids). */
+int32_t ilm_accel_kd_nodes(ilm_context* ctx, ilm_accel_id accel, void* out_nodes, uint32_t* out_index);
 int32_t ilm_accel_destroy(ilm_context* ctx, ilm_accel_id accel);
 /* Primitive::world_bound for BVHAccel (bvh.rs:555-561): {min xyz, max xyz}. */
 int32_t ilm_accel_world_bound(ilm_context* ctx, ilm_accel_id accel, float out[6]);
@@ -198,6 +227,14 @@ int32_t ilm_host_layout_info(const ilm_host_layout* layout, ilm_accel_info* out)
 int32_t ilm_host_layout_copy(const ilm_host_layout* layout, void* bin_nodes, uint32_t* prim_order, void* nodes,
                              void* records, float* bound);
 int32_t ilm_host_layout_destroy(ilm_host_layout* layout);
+/* Host-only kd-tree build on up to `threads` host threads (<= 0: all); the
+ * nodes do not depend on the thread count.  ilm_host_layout_copy's `nodes`
+ * receives the kd nodes, `records` one record per primitive id. */
+int32_t ilm_host_kdtree_build(const float* xyz, uint32_t nv, const uint32_t* idx, uint32_t nt,
+                              const ilm_sphere_desc* spheres, uint32_t ns, const ilm_kdtree_opts* opts,
+                              int32_t threads, ilm_host_layout** out);
+/* The kd-tree's leaf index list (info.n_leaf_refs entries). */
+int32_t ilm_host_layout_kd_index(const ilm_host_layout* layout, uint32_t* out);
 
 /* ----------------------------------------------------------------- queries */
 /* Primitive::intersect for BVHAccel (bvh.rs:563-612), batched: one closest

@@ -23,6 +23,7 @@ LIB_PATH = os.path.join(_HERE, "liboracle.so")
 
 RAY_DTYPE = np.dtype([("o", "<f4", (3,)), ("tmin", "<f4"), ("d", "<f4", (3,)), ("tmax", "<f4")])
 HIT_DTYPE = np.dtype([("prim", "<u4"), ("t", "<f4"), ("u", "<f4"), ("v", "<f4")])
+KD_NODE_DTYPE = np.dtype([("word", "<u4"), ("flags", "<u4")])
 BIN_NODE_DTYPE = np.dtype([("bmin", "<f4", (3,)), ("bmax", "<f4", (3,)), ("offset", "<i4"),
                            ("n_prims", "<u2"), ("axis", "u1"), ("pad", "u1")])
 
@@ -60,6 +61,15 @@ _SIG = {
     "orc_sphere_intersect": (ctypes.c_int, [_P, _P, ctypes.c_int, _P]),
     "orc_sphere_world_bound": (None, [_P, _P]),
     "orc_last_trace_seconds": (ctypes.c_double, []),
+    "orc_kdtree_create": (_P, [_P, ctypes.c_int, ctypes.c_int, ctypes.c_float, ctypes.c_uint32, ctypes.c_int]),
+    "orc_kdtree_destroy": (None, [_P]),
+    "orc_kdtree_node_count": (ctypes.c_uint32, [_P]),
+    "orc_kdtree_index_count": (ctypes.c_uint32, [_P]),
+    "orc_kdtree_max_depth": (ctypes.c_int, [_P]),
+    "orc_kdtree_nodes": (None, [_P, _P]),
+    "orc_kdtree_indices": (None, [_P, _P]),
+    "orc_kdtree_intersect": (ctypes.c_int64, [_P, _P, ctypes.c_uint64, _P, _P, _P, ctypes.c_int]),
+    "orc_kdtree_intersect_p": (ctypes.c_int64, [_P, _P, ctypes.c_uint64, _P, _P, _P, ctypes.c_int]),
     "orc_render_pt": (ctypes.c_int, [_P, _P, _P, ctypes.c_uint32, _P, _P, _P, _P, ctypes.c_float, ctypes.c_uint32,
                                      ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32,
                                      ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32,
@@ -195,6 +205,53 @@ class Scene:
         nt = np.empty(len(rays), np.uint32) if counters else None
         ovf = load().orc_intersect_p(self.h, _p(rays), len(rays), _p(occ), _p(nv), _p(nt), threads)
         assert ovf == 0, f"{ovf} rays overflowed the 64-entry traversal stack"
+        return (occ, nv, nt) if counters else occ
+
+
+class KdTree:
+    """KdTreeAccel (accelerators/kdtreeaccel.rs:25-465) over a Scene's
+    primitives, with the same primitive ids."""
+
+    def __init__(self, scene: Scene, isect_cost: int = 80, traversal_cost: int = 1, empty_bonus: float = 0.5,
+                 max_prims: int = 1, max_depth: int = -1):
+        self.scene = scene          # the tree's primitive tests read the scene
+        self.h = load().orc_kdtree_create(scene.h, isect_cost, traversal_cost, empty_bonus, max_prims, max_depth)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            load().orc_kdtree_destroy(self.h)
+            self.h = None
+
+    @property
+    def max_depth(self) -> int:
+        return load().orc_kdtree_max_depth(self.h)
+
+    def nodes(self) -> np.ndarray:
+        out = np.zeros(load().orc_kdtree_node_count(self.h), KD_NODE_DTYPE)
+        load().orc_kdtree_nodes(self.h, _p(out))
+        return out
+
+    def indices(self) -> np.ndarray:
+        out = np.zeros(load().orc_kdtree_index_count(self.h), np.uint32)
+        load().orc_kdtree_indices(self.h, _p(out))
+        return out
+
+    def intersect(self, rays: np.ndarray, threads: int = 0, counters: bool = False):
+        rays = np.ascontiguousarray(rays)
+        hits = np.empty(len(rays), HIT_DTYPE)
+        nv = np.empty(len(rays), np.uint32) if counters else None
+        nt = np.empty(len(rays), np.uint32) if counters else None
+        ovf = load().orc_kdtree_intersect(self.h, _p(rays), len(rays), _p(hits), _p(nv), _p(nt), threads)
+        assert ovf == 0, f"{ovf} rays overflowed the 64-entry kd-tree stack"
+        return (hits, nv, nt) if counters else hits
+
+    def intersect_p(self, rays: np.ndarray, threads: int = 0, counters: bool = False):
+        rays = np.ascontiguousarray(rays)
+        occ = np.empty(len(rays), np.uint8)
+        nv = np.empty(len(rays), np.uint32) if counters else None
+        nt = np.empty(len(rays), np.uint32) if counters else None
+        ovf = load().orc_kdtree_intersect_p(self.h, _p(rays), len(rays), _p(occ), _p(nv), _p(nt), threads)
+        assert ovf == 0, f"{ovf} rays overflowed the 64-entry kd-tree stack"
         return (occ, nv, nt) if counters else occ
 
 

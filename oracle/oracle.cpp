@@ -6,6 +6,7 @@
 #include "oracle.h"
 #include "oracle_common.h"
 
+#include <algorithm>
 #include <atomic>
 #include <chrono>
 #include <cmath>
@@ -774,6 +775,222 @@ static int64_t parallel_rays(uint64_t n, int nthreads, F&& fn) {
     return overflow.load();
 }
 
+// ---------------------------------------------------------------- kd-tree
+// KdTreeAccel (accelerators/kdtreeaccel.rs:11-596) over a Scene's primitives.
+// Repairs, shared with the product: the split axis is rebound on each retry
+// (kdtreeaccel.rs:130 binds it immutably, 189 assigns it); equal edges are
+// ordered by primitive id after (position, start before end) so that the
+// tree is fixed; a leaf's run is read entry by entry (kdtreeaccel.rs:351 and
+// 440 read `offset + 1` on every iteration).
+
+enum KdEdgeType { kStart = 0, kEnd = 1 };
+struct KdEdge { float t; uint32_t prim; int type; };
+
+struct KdTree {
+    const Scene* scene = nullptr;
+    int isect_cost = 80, traversal_cost = 1;
+    float empty_bonus = 0.5f;
+    uint32_t max_prims = 1;
+    int max_depth = 0;
+    std::vector<orc_kd_node> nodes;
+    uint32_t n_alloced = 0, next_free = 0;
+    std::vector<uint32_t> prim_indices;
+    std::vector<B3> prim_bounds;
+    B3 bounds;
+};
+
+static bool kd_is_leaf(const orc_kd_node& n) { return (n.flags & 3u) == 3u; }
+
+// KdAccelNode::init_leaf (kdtreeaccel.rs:476-490)
+static void kd_init_leaf(KdTree& k, uint32_t node, const uint32_t* prim_nums, uint32_t np) {
+    orc_kd_node& n = k.nodes[node];
+    n.flags = 3u | (np << 2);
+    if (np == 0) n.word = 0;
+    else if (np == 1) n.word = prim_nums[0];
+    else {
+        n.word = (uint32_t)k.prim_indices.size();
+        for (uint32_t i = 0; i < np; ++i) k.prim_indices.push_back(prim_nums[i]);
+    }
+}
+
+// build_tree (kdtreeaccel.rs:90-244), with the reference's scratch buffers:
+// prims0 is reused by the below child, prims1 + n by both children.
+static void kd_build_tree(KdTree& k, uint32_t node_num, const B3& node_bounds, const uint32_t* prim_nums,
+                          uint32_t n_primitives, int depth, std::vector<KdEdge>* edges, uint32_t* prims0,
+                          uint32_t* prims1, int bad_refines) {
+    if (k.next_free == k.n_alloced) {
+        uint32_t n_new = std::max(2 * k.n_alloced, 512u);
+        k.nodes.resize(n_new, orc_kd_node{0, 0});
+        k.n_alloced = n_new;
+    }
+    ++k.next_free;
+    if (n_primitives <= k.max_prims || depth == 0) {
+        kd_init_leaf(k, node_num, prim_nums, n_primitives);
+        return;
+    }
+    int best_axis = -1, best_offset = -1;
+    float best_cost = std::numeric_limits<float>::infinity();
+    float old_cost = (float)((uint64_t)k.isect_cost * n_primitives);
+    float total_sa = surface_area(node_bounds);
+    float inv_total_sa = 1.0f / total_sa;
+    V3 d = sub(node_bounds.mx, node_bounds.mn);
+    int axis = maximum_extent(node_bounds);
+    int retries = 0;
+    for (;;) {
+        std::vector<KdEdge>& e = edges[axis];
+        for (uint32_t i = 0; i < n_primitives; ++i) {
+            uint32_t pn = prim_nums[i];
+            const B3& b = k.prim_bounds[pn];
+            e[2 * i] = KdEdge{comp(b.mn, axis), pn, kStart};
+            e[2 * i + 1] = KdEdge{comp(b.mx, axis), pn, kEnd};
+        }
+        std::sort(e.begin(), e.begin() + 2 * n_primitives, [](const KdEdge& a, const KdEdge& b) {
+            if (a.t == b.t) {
+                if (a.type != b.type) return a.type < b.type;
+                return a.prim < b.prim;
+            }
+            return a.t < b.t;
+        });
+        uint32_t n_below = 0, n_above = n_primitives;
+        for (uint32_t i = 0; i < 2 * n_primitives; ++i) {
+            if (e[i].type == kEnd) --n_above;
+            float edge_t = e[i].t;
+            float lo = comp(node_bounds.mn, axis), hi = comp(node_bounds.mx, axis);
+            if (edge_t > lo && edge_t < hi) {
+                int a0 = (axis + 1) % 3, a1 = (axis + 2) % 3;
+                float below_sa = 2.0f * (comp(d, a0) * comp(d, a1) + (edge_t - lo) * (comp(d, a0) + comp(d, a1)));
+                float above_sa = 2.0f * (comp(d, a0) * comp(d, a1) + (hi - edge_t) * (comp(d, a0) + comp(d, a1)));
+                float p_below = below_sa * inv_total_sa;
+                float p_above = above_sa * inv_total_sa;
+                float eb = (n_above == 0 || n_below == 0) ? k.empty_bonus : 0.0f;
+                float cost = (float)k.traversal_cost +
+                             (float)k.isect_cost * (1.0f - eb) * (p_below * (float)n_below + p_above * (float)n_above);
+                if (cost < best_cost) {
+                    best_cost = cost;
+                    best_axis = axis;
+                    best_offset = (int)i;
+                }
+            }
+            if (e[i].type == kStart) ++n_below;
+        }
+        if (best_axis == -1 && retries < 2) {
+            ++retries;
+            axis = (axis + 1) % 3;
+            continue;
+        }
+        break;
+    }
+    if (best_cost > old_cost) ++bad_refines;
+    if ((best_cost > 4.0f * old_cost && n_primitives < 16) || best_axis == -1 || bad_refines == 3) {
+        kd_init_leaf(k, node_num, prim_nums, n_primitives);
+        return;
+    }
+    const std::vector<KdEdge>& e = edges[best_axis];
+    uint32_t n0 = 0, n1 = 0;
+    for (int i = 0; i < best_offset; ++i)
+        if (e[i].type == kStart) prims0[n0++] = e[i].prim;
+    for (uint32_t i = (uint32_t)best_offset + 1; i < 2 * n_primitives; ++i)
+        if (e[i].type == kEnd) prims1[n1++] = e[i].prim;
+    float t_split = e[best_offset].t;
+    B3 bounds0 = node_bounds, bounds1 = node_bounds;
+    if (best_axis == 0) { bounds0.mx.x = t_split; bounds1.mn.x = t_split; }
+    else if (best_axis == 1) { bounds0.mx.y = t_split; bounds1.mn.y = t_split; }
+    else { bounds0.mx.z = t_split; bounds1.mn.z = t_split; }
+    kd_build_tree(k, node_num + 1, bounds0, prims0, n0, depth - 1, edges, prims0, prims1 + n_primitives,
+                  bad_refines);
+    uint32_t above_child = k.next_free;
+    // KdAccelNode::init_interior (kdtreeaccel.rs:492-496)
+    std::memcpy(&k.nodes[node_num].word, &t_split, 4);
+    k.nodes[node_num].flags = (uint32_t)best_axis | (above_child << 2);
+    kd_build_tree(k, above_child, bounds1, prims1, n1, depth - 1, edges, prims0, prims1 + n_primitives,
+                  bad_refines);
+}
+
+// Bounds3::intersect_ray (geometry/bounds3.rs:253-282)
+static bool bounds_intersect_ray(const B3& b, const Ray& ray, float* hit0, float* hit1) {
+    float t0 = 0.0f, t1 = ray.t_max;
+    for (int i = 0; i < 3; ++i) {
+        float inv = 1.0f / comp(ray.d, i);
+        float t_near = (comp(b.mn, i) - comp(ray.o, i)) * inv;
+        float t_far = (comp(b.mx, i) - comp(ray.o, i)) * inv;
+        if (t_near > t_far) std::swap(t_near, t_far);
+        t_far *= 1.0f + 2.0f * gamma(3);
+        if (t_near > t0) t0 = t_near;
+        if (t_far < t1) t1 = t_far;
+        if (t0 > t1) return false;
+    }
+    *hit0 = t0;
+    *hit1 = t1;
+    return true;
+}
+
+struct KdToDo { uint32_t node; float t_min, t_max; };
+
+// KdTreeAccel::intersect / intersect_p (kdtreeaccel.rs:256-465).  The closest
+// form owns t_max as the BVH traversal does, with the same tie rule.
+static int kd_trace(const KdTree& k, const orc_ray& r, bool closest, orc_hit* hit, uint8_t* occ, uint32_t* nv,
+                    uint32_t* nt) {
+    if (hit) { hit->prim = 0xFFFFFFFFu; hit->t = r.tmax; hit->u = 0; hit->v = 0; }
+    if (occ) *occ = 0;
+    uint32_t visits = 0, tests = 0;
+    struct Count {
+        uint32_t *nv, *nt, *visits, *tests;
+        ~Count() { if (nv) *nv = *visits; if (nt) *nt = *tests; }
+    } count{nv, nt, &visits, &tests};
+    if (k.nodes.empty()) return 0;
+    Ray ray{{r.o[0], r.o[1], r.o[2]}, {r.d[0], r.d[1], r.d[2]}, r.tmax};
+    float t_min, t_max;
+    if (!bounds_intersect_ray(k.bounds, ray, &t_min, &t_max)) return 0;
+    V3 inv_dir{1.0f / ray.d.x, 1.0f / ray.d.y, 1.0f / ray.d.z};
+    KdToDo todo[64];
+    int todo_pos = 0;
+    uint32_t node = 0;
+    for (;;) {
+        if (ray.t_max < t_min) break;
+        const orc_kd_node& n = k.nodes[node];
+        ++visits;
+        if (!kd_is_leaf(n)) {
+            int axis = (int)(n.flags & 3u);
+            float split;
+            std::memcpy(&split, &n.word, 4);
+            float t_plane = (split - comp(ray.o, axis)) * comp(inv_dir, axis);
+            bool below_first = comp(ray.o, axis) < split || (comp(ray.o, axis) == split && comp(ray.d, axis) <= 0.0f);
+            uint32_t first = below_first ? node + 1 : (n.flags >> 2);
+            uint32_t second = below_first ? (n.flags >> 2) : node + 1;
+            if (t_plane > t_max || t_plane <= 0.0f) {
+                node = first;
+            } else if (t_plane < t_min) {
+                node = second;
+            } else {
+                if (todo_pos == 64) return 1;
+                todo[todo_pos++] = KdToDo{second, t_plane, t_max};
+                node = first;
+                t_max = t_plane;
+            }
+            continue;
+        }
+        uint32_t np = n.flags >> 2;
+        for (uint32_t i = 0; i < np; ++i) {
+            uint32_t prim = np == 1 ? n.word : k.prim_indices[n.word + i];
+            float t, uv[2];
+            ++tests;
+            if (prim_test(*k.scene, prim, ray, closest, &t, uv)) {
+                if (!closest) { *occ = 1; return 0; }
+                if (t < ray.t_max || (t == ray.t_max && prim < hit->prim)) {
+                    ray.t_max = t;
+                    hit->prim = prim; hit->t = t; hit->u = uv[0]; hit->v = uv[1];
+                }
+            }
+        }
+        if (todo_pos == 0) break;
+        --todo_pos;
+        node = todo[todo_pos].node;
+        t_min = todo[todo_pos].t_min;
+        t_max = todo[todo_pos].t_max;
+    }
+    return 0;
+}
+
 }  // namespace orc
 
 using namespace orc;
@@ -903,6 +1120,62 @@ int orc_trace_closest1(void* scene, const orc_ray* ray, orc_hit* hit) {
 
 int orc_trace_any1(void* scene, const orc_ray* ray, uint8_t* occluded) {
     return trace_any(*(Scene*)scene, *ray, occluded, nullptr, nullptr);
+}
+
+void* orc_kdtree_create(void* scene, int isect_cost, int traversal_cost, float empty_bonus, uint32_t max_prims,
+                        int max_depth) {
+    const Scene* s = (const Scene*)scene;
+    KdTree* k = new KdTree();
+    k->scene = s;
+    k->isect_cost = isect_cost;
+    k->traversal_cost = traversal_cost;
+    k->empty_bonus = empty_bonus;
+    k->max_prims = max_prims;
+    uint32_t np = s->nt + (uint32_t)s->spheres.size();
+    // kdtreeaccel.rs:34-46
+    if (max_depth <= 0) max_depth = np ? (int)std::lround(8.0 + 1.3 * std::log2((double)np)) : 0;
+    k->max_depth = max_depth;
+    k->prim_bounds.resize(np);
+    for (uint32_t i = 0; i < np; ++i) {
+        k->prim_bounds[i] = i < s->nt ? tri_bound(*s, i) : sphere_world_bound(s->spheres[i - s->nt]);
+        k->bounds = bunion(k->bounds, k->prim_bounds[i]);
+    }
+    if (np == 0) return k;
+    std::vector<KdEdge> edges[3];
+    for (auto& e : edges) e.resize(2 * (size_t)np);
+    std::vector<uint32_t> prims0(np), prims1(((size_t)max_depth + 1) * np), prim_nums(np);
+    for (uint32_t i = 0; i < np; ++i) prim_nums[i] = i;
+    kd_build_tree(*k, 0, k->bounds, prim_nums.data(), np, max_depth, edges, prims0.data(), prims1.data(), 0);
+    k->nodes.resize(k->next_free);
+    return k;
+}
+void orc_kdtree_destroy(void* kd) { delete (KdTree*)kd; }
+uint32_t orc_kdtree_node_count(void* kd) { return (uint32_t)((KdTree*)kd)->nodes.size(); }
+uint32_t orc_kdtree_index_count(void* kd) { return (uint32_t)((KdTree*)kd)->prim_indices.size(); }
+int orc_kdtree_max_depth(void* kd) { return ((KdTree*)kd)->max_depth; }
+void orc_kdtree_nodes(void* kd, orc_kd_node* out) {
+    KdTree* k = (KdTree*)kd;
+    if (!k->nodes.empty()) std::memcpy(out, k->nodes.data(), k->nodes.size() * sizeof(orc_kd_node));
+}
+void orc_kdtree_indices(void* kd, uint32_t* out) {
+    KdTree* k = (KdTree*)kd;
+    if (!k->prim_indices.empty()) std::memcpy(out, k->prim_indices.data(), k->prim_indices.size() * 4);
+}
+int64_t orc_kdtree_intersect(void* kd, const orc_ray* rays, uint64_t n, orc_hit* hits, uint32_t* node_visits,
+                             uint32_t* prim_tests, int nthreads) {
+    const KdTree& k = *(KdTree*)kd;
+    return parallel_rays(n, nthreads, [&](uint64_t i) {
+        return kd_trace(k, rays[i], true, &hits[i], nullptr, node_visits ? &node_visits[i] : nullptr,
+                        prim_tests ? &prim_tests[i] : nullptr);
+    });
+}
+int64_t orc_kdtree_intersect_p(void* kd, const orc_ray* rays, uint64_t n, uint8_t* occluded, uint32_t* node_visits,
+                               uint32_t* prim_tests, int nthreads) {
+    const KdTree& k = *(KdTree*)kd;
+    return parallel_rays(n, nthreads, [&](uint64_t i) {
+        return kd_trace(k, rays[i], false, nullptr, &occluded[i], node_visits ? &node_visits[i] : nullptr,
+                        prim_tests ? &prim_tests[i] : nullptr);
+    });
 }
 
 }  // extern "C"

@@ -133,6 +133,28 @@ int orc_render_pt(void* scene, const float* verts, const uint32_t* idx, uint32_t
                   uint32_t max_depth, uint32_t rr_depth, uint64_t seed, uint32_t x0, uint32_t y0,
                   uint32_t x1, uint32_t y1, int nthreads, float* rgb_out, uint64_t* ray_counts);
 
+/* KdTreeAccel (accelerators/kdtreeaccel.rs:11-596) over the scene's
+ * primitives (the scene must outlive it).  max_depth <= 0: the reference's
+ * default.  Nodes are the 8-byte KdAccelNode: word = split bits, the one
+ * primitive or the run's first slot; flags = axis or 3 (leaf), and above
+ * child or count << 2. */
+typedef struct { uint32_t word, flags; } orc_kd_node;
+void* orc_kdtree_create(void* scene, int isect_cost, int traversal_cost, float empty_bonus, uint32_t max_prims,
+                        int max_depth);
+void orc_kdtree_destroy(void* kd);
+uint32_t orc_kdtree_node_count(void* kd);
+uint32_t orc_kdtree_index_count(void* kd);
+int orc_kdtree_max_depth(void* kd);
+void orc_kdtree_nodes(void* kd, orc_kd_node* out);
+void orc_kdtree_indices(void* kd, uint32_t* out);
+/* KdTreeAccel::intersect / intersect_p over a ray batch; returns the number
+ * of rays whose 64-entry stack overflowed.  node_visits / prim_tests may be
+ * NULL; otherwise per-ray counters. */
+int64_t orc_kdtree_intersect(void* kd, const orc_ray* rays, uint64_t n, orc_hit* hits, uint32_t* node_visits,
+                             uint32_t* prim_tests, int nthreads);
+int64_t orc_kdtree_intersect_p(void* kd, const orc_ray* rays, uint64_t n, uint8_t* occluded, uint32_t* node_visits,
+                               uint32_t* prim_tests, int nthreads);
+
 /* Wall-clock seconds spent by the last orc_intersect/_p call (traversal only). */
 double orc_last_trace_seconds(void);
 

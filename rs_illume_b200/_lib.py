@@ -69,7 +69,19 @@ class ilm_build_opts(ctypes.Structure):
 class ilm_accel_info(ctypes.Structure):
     _fields_ = [("n_prims", ctypes.c_uint32), ("n_binary_nodes", ctypes.c_uint32),
                 ("n_nodes", ctypes.c_uint32), ("width", ctypes.c_uint32),
-                ("device_bytes", ctypes.c_uint64), ("build_seconds", ctypes.c_double)]
+                ("device_bytes", ctypes.c_uint64), ("build_seconds", ctypes.c_double),
+                ("n_leaf_refs", ctypes.c_uint32), ("max_depth", ctypes.c_uint32)]
+
+
+ILM_LAYOUT_KDTREE = 1
+
+
+class ilm_kdtree_opts(ctypes.Structure):
+    _fields_ = [("isect_cost", ctypes.c_int32), ("traversal_cost", ctypes.c_int32),
+                ("empty_bonus", ctypes.c_float), ("max_prims", ctypes.c_uint32), ("max_depth", ctypes.c_int32)]
+
+
+KD_NODE_DTYPE = np.dtype([("word", "<u4"), ("flags", "<u4")])
 
 
 class ilm_sphere_desc(ctypes.Structure):
@@ -162,6 +174,11 @@ SIGNATURES = {
     "ilm_host_layout_info": (_I32, [_P, ctypes.POINTER(ilm_accel_info)]),
     "ilm_host_layout_copy": (_I32, [_P, _P, _P, _P, _P, _P]),
     "ilm_host_layout_destroy": (_I32, [_P]),
+    "ilm_kdtree_build": (_I32, [_P, _P, _U32, ctypes.POINTER(ilm_kdtree_opts), ctypes.POINTER(_U32)]),
+    "ilm_accel_kd_nodes": (_I32, [_P, _U32, _P, _P]),
+    "ilm_host_kdtree_build": (_I32, [_P, _U32, _P, _U32, _P, _U32, ctypes.POINTER(ilm_kdtree_opts), _I32,
+                                     ctypes.POINTER(_P)]),
+    "ilm_host_layout_kd_index": (_I32, [_P, _P]),
     "ilm_intersect_closest": (_I32, [_P, _U32, _P, _U64, _P, _P]),
     "ilm_intersect_any": (_I32, [_P, _U32, _P, _U64, _P, _P]),
     "ilm_intersect_closest_noalloc": (_I32, [_P, _U32, _P, _U64, _P, _P]),

@@ -188,35 +188,83 @@ int32_t ilm_mesh_set_attrs(ilm_context* ctx, ilm_mesh_id mesh, const ilm_mesh_at
     return ILM_OK;
 }
 
+// The record of one quadric description; null on success, else why it is
+// rejected.
+static const char* quadric_record(const ilm_sphere_desc& d, SphereRec* out) {
+    if (!(d.radius > 0.0f) || !std::isfinite(d.radius)) return "radius must be positive and finite";
+    if (d.kind < ILM_QUADRIC_SPHERE || d.kind > ILM_QUADRIC_CONE ||
+        (d.kind == ILM_QUADRIC_CONE && !(d.height > 0.0f)) ||
+        (d.kind == ILM_QUADRIC_DISK && !(d.inner_radius >= 0.0f && d.inner_radius < d.radius)) ||
+        (d.kind == ILM_QUADRIC_CYLINDER && !(d.z_min != d.z_max)) || !std::isfinite(d.height) ||
+        !std::isfinite(d.z_min) || !std::isfinite(d.z_max))
+        return "invalid quadric parameters";
+    SphereInput in;
+    std::memcpy(in.o2w, d.object_to_world, sizeof in.o2w);
+    std::memcpy(in.w2o, d.world_to_object, sizeof in.w2o);
+    in.radius = d.radius; in.z_min = d.z_min; in.z_max = d.z_max; in.phi_max_deg = d.phi_max_deg;
+    in.reverse = d.reverse_orientation;
+    in.kind = d.kind; in.height = d.height; in.inner_radius = d.inner_radius;
+    *out = make_sphere(in);
+    return nullptr;
+}
+
 int32_t ilm_spheres_upload(ilm_context* ctx, const ilm_sphere_desc* spheres, uint32_t n, ilm_mesh_id* out) {
     if (!ctx || !out || (n > 0 && !spheres)) return ILM_ERR_INVALID_ARGUMENT;
     auto m = std::make_unique<Mesh>();
     m->is_spheres = true;
     for (uint32_t i = 0; i < n; ++i) {
-        const ilm_sphere_desc& d = spheres[i];
-        if (!(d.radius > 0.0f) || !std::isfinite(d.radius)) {
-            set_error(ctx, "ilm_spheres_upload: radius must be positive and finite");
+        SphereRec rec;
+        if (const char* why = quadric_record(spheres[i], &rec)) {
+            set_error(ctx, std::string("ilm_spheres_upload: ") + why);
             return ILM_ERR_INVALID_ARGUMENT;
         }
-        if (d.kind < ILM_QUADRIC_SPHERE || d.kind > ILM_QUADRIC_CONE ||
-            (d.kind == ILM_QUADRIC_CONE && !(d.height > 0.0f)) ||
-            (d.kind == ILM_QUADRIC_DISK && !(d.inner_radius >= 0.0f && d.inner_radius < d.radius)) ||
-            (d.kind == ILM_QUADRIC_CYLINDER && !(d.z_min != d.z_max)) || !std::isfinite(d.height) ||
-            !std::isfinite(d.z_min) || !std::isfinite(d.z_max)) {
-            set_error(ctx, "ilm_spheres_upload: invalid quadric parameters");
-            return ILM_ERR_INVALID_ARGUMENT;
-        }
-        SphereInput in;
-        std::memcpy(in.o2w, d.object_to_world, sizeof in.o2w);
-        std::memcpy(in.w2o, d.world_to_object, sizeof in.w2o);
-        in.radius = d.radius; in.z_min = d.z_min; in.z_max = d.z_max; in.phi_max_deg = d.phi_max_deg;
-        in.reverse = d.reverse_orientation;
-        in.kind = d.kind; in.height = d.height; in.inner_radius = d.inner_radius;
-        m->spheres.push_back(make_sphere(in));
+        m->spheres.push_back(rec);
     }
     m->n_prims = n;
     ilm_mesh_id id = ctx->next_mesh++;
     ctx->meshes[id] = std::move(m);
+    *out = id;
+    return ILM_OK;
+}
+
+// The shape views of `meshes`, which become fixed (their attributes can no
+// longer change).
+static int32_t mesh_views(ilm_context* ctx, const char* who, const ilm_mesh_id* meshes, uint32_t n_meshes,
+                          std::vector<MeshView>& views) {
+    for (uint32_t k = 0; k < n_meshes; ++k) {
+        auto it = ctx->meshes.find(meshes[k]);
+        if (it == ctx->meshes.end()) {
+            set_error(ctx, std::string(who) + ": unknown mesh id");
+            return ILM_ERR_NOT_FOUND;
+        }
+        const Mesh& m = *it->second;
+        views.push_back({m.is_spheres, m.xyz.data(), m.idx.data(), m.spheres.data(), m.n_prims});
+    }
+    for (uint32_t k = 0; k < n_meshes; ++k) ctx->meshes[meshes[k]]->built = true;
+    return ILM_OK;
+}
+
+// Copies a host layout to the device and registers the accel.
+static int32_t upload_accel(ilm_context* ctx, std::unique_ptr<Accel> acc, std::chrono::steady_clock::time_point t0,
+                            ilm_accel_id* out) {
+    const HostLayout& h = acc->host;
+    auto put = [&](DeviceBuffer& d, const void* src, size_t bytes, const char* what) -> int32_t {
+        if (!bytes) return ILM_OK;
+        ILM_CUDA(ctx, d.reserve(bytes), what);
+        ILM_CUDA(ctx, cudaMemcpy(d.ptr, src, bytes, cudaMemcpyHostToDevice), what);
+        return ILM_OK;
+    };
+    const size_t rb = h.records.size() * sizeof(PrimRec), sb = h.spheres.size() * sizeof(SphereRec),
+                 kb = h.kd_index.size() * sizeof(uint32_t);
+    int32_t rc;
+    if ((rc = put(acc->d_nodes, h.node_bytes.data(), h.node_bytes.size(), "upload(nodes)")) != ILM_OK) return rc;
+    if ((rc = put(acc->d_prims, h.records.data(), rb, "upload(prims)")) != ILM_OK) return rc;
+    if ((rc = put(acc->d_spheres, h.spheres.data(), sb, "upload(spheres)")) != ILM_OK) return rc;
+    if ((rc = put(acc->d_kd_index, h.kd_index.data(), kb, "upload(kd index)")) != ILM_OK) return rc;
+    acc->device_bytes = h.node_bytes.size() + rb + sb + kb;
+    acc->build_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    ilm_accel_id id = ctx->next_accel++;
+    ctx->accels[id] = std::move(acc);
     *out = id;
     return ILM_OK;
 }
@@ -229,46 +277,45 @@ int32_t ilm_accel_build(ilm_context* ctx, const ilm_mesh_id* meshes, uint32_t n_
     int max_prims = opts ? opts->max_prims_in_node : 4;
     auto t0 = std::chrono::steady_clock::now();
     std::vector<MeshView> views;
-    for (uint32_t k = 0; k < n_meshes; ++k) {
-        auto it = ctx->meshes.find(meshes[k]);
-        if (it == ctx->meshes.end()) {
-            set_error(ctx, "ilm_accel_build: unknown mesh id");
-            return ILM_ERR_NOT_FOUND;
-        }
-        const Mesh& m = *it->second;
-        views.push_back({m.is_spheres, m.xyz.data(), m.idx.data(), m.spheres.data(), m.n_prims});
-    }
+    if (int32_t rc = mesh_views(ctx, "ilm_accel_build", meshes, n_meshes, views)) return rc;
     auto acc = std::make_unique<Accel>();
     acc->mesh_ids.assign(meshes, meshes + n_meshes);
-    for (uint32_t k = 0; k < n_meshes; ++k) ctx->meshes[meshes[k]]->built = true;
     std::string msg = build_layout(views, width, max_prims, (int)std::thread::hardware_concurrency(), acc->host);
     if (!msg.empty()) {
         set_error(ctx, "ilm_accel_build: " + msg);
         return ILM_ERR_INVALID_ARGUMENT;
     }
-    const HostLayout& h = acc->host;
-    if (!h.node_bytes.empty()) {
-        ILM_CUDA(ctx, acc->d_nodes.reserve(h.node_bytes.size()), "cudaMalloc(nodes)");
-        ILM_CUDA(ctx, cudaMemcpy(acc->d_nodes.ptr, h.node_bytes.data(), h.node_bytes.size(), cudaMemcpyHostToDevice),
-                 "cudaMemcpy(nodes)");
+    return upload_accel(ctx, std::move(acc), t0, out);
+}
+
+static KdParams kd_params(const ilm_kdtree_opts* o) {
+    KdParams p;
+    if (o) {
+        p.isect_cost = o->isect_cost;
+        p.traversal_cost = o->traversal_cost;
+        p.empty_bonus = o->empty_bonus;
+        p.max_prims = o->max_prims;
+        p.max_depth = o->max_depth;
     }
-    size_t rb = h.records.size() * sizeof(PrimRec);
-    if (rb) {
-        ILM_CUDA(ctx, acc->d_prims.reserve(rb), "cudaMalloc(prims)");
-        ILM_CUDA(ctx, cudaMemcpy(acc->d_prims.ptr, h.records.data(), rb, cudaMemcpyHostToDevice), "cudaMemcpy(prims)");
+    return p;
+}
+
+int32_t ilm_kdtree_build(ilm_context* ctx, const ilm_mesh_id* meshes, uint32_t n_meshes, const ilm_kdtree_opts* opts,
+                         ilm_accel_id* out) {
+    ILM_CHECK_CTX(ctx);
+    if (!out || (n_meshes > 0 && !meshes)) return ILM_ERR_INVALID_ARGUMENT;
+    auto t0 = std::chrono::steady_clock::now();
+    std::vector<MeshView> views;
+    if (int32_t rc = mesh_views(ctx, "ilm_kdtree_build", meshes, n_meshes, views)) return rc;
+    auto acc = std::make_unique<Accel>();
+    acc->mesh_ids.assign(meshes, meshes + n_meshes);
+    std::string msg =
+        build_kd_layout(views, kd_params(opts), (int)std::thread::hardware_concurrency(), acc->host);
+    if (!msg.empty()) {
+        set_error(ctx, "ilm_kdtree_build: " + msg);
+        return ILM_ERR_INVALID_ARGUMENT;
     }
-    size_t sb = h.spheres.size() * sizeof(SphereRec);
-    if (sb) {
-        ILM_CUDA(ctx, acc->d_spheres.reserve(sb), "cudaMalloc(spheres)");
-        ILM_CUDA(ctx, cudaMemcpy(acc->d_spheres.ptr, h.spheres.data(), sb, cudaMemcpyHostToDevice),
-                 "cudaMemcpy(spheres)");
-    }
-    acc->device_bytes = h.node_bytes.size() + rb + sb;
-    acc->build_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
-    ilm_accel_id id = ctx->next_accel++;
-    ctx->accels[id] = std::move(acc);
-    *out = id;
-    return ILM_OK;
+    return upload_accel(ctx, std::move(acc), t0, out);
 }
 
 int32_t ilm_accel_destroy(ilm_context* ctx, ilm_accel_id accel) {
@@ -298,6 +345,23 @@ int32_t ilm_accel_get_info(ilm_context* ctx, ilm_accel_id accel, ilm_accel_info*
     out->width = (uint32_t)a->host.width;
     out->device_bytes = a->device_bytes;
     out->build_seconds = a->build_seconds;
+    out->n_leaf_refs = (uint32_t)a->host.kd_index.size();
+    out->max_depth = (uint32_t)a->host.kd_max_depth;
+    return ILM_OK;
+}
+
+int32_t ilm_accel_kd_nodes(ilm_context* ctx, ilm_accel_id accel, void* out_nodes, uint32_t* out_index) {
+    if (!ctx) return ILM_ERR_INVALID_ARGUMENT;
+    Accel* a = find_accel(ctx, accel);
+    if (!a) return ILM_ERR_NOT_FOUND;
+    if (a->host.width != kLayoutKdTree) {
+        set_error(ctx, "ilm_accel_kd_nodes: not a kd-tree accel");
+        return ILM_ERR_INVALID_ARGUMENT;
+    }
+    if (out_nodes && !a->host.node_bytes.empty())
+        std::memcpy(out_nodes, a->host.node_bytes.data(), a->host.node_bytes.size());
+    if (out_index && !a->host.kd_index.empty())
+        std::memcpy(out_index, a->host.kd_index.data(), a->host.kd_index.size() * 4);
     return ILM_OK;
 }
 
@@ -419,28 +483,31 @@ struct ilm_host_layout {
     double seconds = 0.0;
 };
 
-int32_t ilm_host_layout_build(const float* xyz, uint32_t nv, const uint32_t* idx, uint32_t nt,
-                              const ilm_sphere_desc* spheres, uint32_t ns, const ilm_build_opts* opts,
-                              ilm_host_layout** out) {
-    if (!out || (nv > 0 && !xyz) || (nt > 0 && !idx) || (ns > 0 && !spheres)) return ILM_ERR_INVALID_ARGUMENT;
+// Shape views of one triangle mesh followed by one quadric set, for the
+// host-only builds.
+static int32_t host_views(const float* xyz, uint32_t nv, const uint32_t* idx, uint32_t nt,
+                          const ilm_sphere_desc* spheres, uint32_t ns, std::vector<SphereRec>& sph,
+                          std::vector<MeshView>& views) {
+    if ((nv > 0 && !xyz) || (nt > 0 && !idx) || (ns > 0 && !spheres)) return ILM_ERR_INVALID_ARGUMENT;
     for (uint64_t i = 0; i < 3ull * nt; ++i)
         if (idx[i] >= nv) return ILM_ERR_INVALID_ARGUMENT;
     for (uint64_t i = 0; i < 3ull * nv; ++i)
         if (!std::isfinite(xyz[i])) return ILM_ERR_INVALID_ARGUMENT;
-    std::vector<SphereRec> sph;
-    for (uint32_t i = 0; i < ns; ++i) {
-        const ilm_sphere_desc& d = spheres[i];
-        if (!(d.radius > 0.0f) || !std::isfinite(d.radius)) return ILM_ERR_INVALID_ARGUMENT;
-        SphereInput in;
-        std::memcpy(in.o2w, d.object_to_world, sizeof in.o2w);
-        std::memcpy(in.w2o, d.world_to_object, sizeof in.w2o);
-        in.radius = d.radius; in.z_min = d.z_min; in.z_max = d.z_max; in.phi_max_deg = d.phi_max_deg;
-        in.reverse = d.reverse_orientation;
-        sph.push_back(make_sphere(in));
-    }
-    std::vector<MeshView> views;
+    sph.resize(ns);
+    for (uint32_t i = 0; i < ns; ++i)
+        if (quadric_record(spheres[i], &sph[i])) return ILM_ERR_INVALID_ARGUMENT;
     if (nt > 0) views.push_back({false, xyz, idx, nullptr, nt});
     if (ns > 0) views.push_back({true, nullptr, nullptr, sph.data(), ns});
+    return ILM_OK;
+}
+
+int32_t ilm_host_layout_build(const float* xyz, uint32_t nv, const uint32_t* idx, uint32_t nt,
+                              const ilm_sphere_desc* spheres, uint32_t ns, const ilm_build_opts* opts,
+                              ilm_host_layout** out) {
+    if (!out) return ILM_ERR_INVALID_ARGUMENT;
+    std::vector<SphereRec> sph;
+    std::vector<MeshView> views;
+    if (int32_t rc = host_views(xyz, nv, idx, nt, spheres, ns, sph, views)) return rc;
     auto t0 = std::chrono::steady_clock::now();
     std::unique_ptr<ilm_host_layout> hl(new ilm_host_layout());
     std::string msg = build_layout(views, opts ? opts->width : 8, opts ? opts->max_prims_in_node : 4,
@@ -451,6 +518,29 @@ int32_t ilm_host_layout_build(const float* xyz, uint32_t nv, const uint32_t* idx
     return ILM_OK;
 }
 
+int32_t ilm_host_kdtree_build(const float* xyz, uint32_t nv, const uint32_t* idx, uint32_t nt,
+                              const ilm_sphere_desc* spheres, uint32_t ns, const ilm_kdtree_opts* opts,
+                              int32_t threads, ilm_host_layout** out) {
+    if (!out) return ILM_ERR_INVALID_ARGUMENT;
+    std::vector<SphereRec> sph;
+    std::vector<MeshView> views;
+    if (int32_t rc = host_views(xyz, nv, idx, nt, spheres, ns, sph, views)) return rc;
+    auto t0 = std::chrono::steady_clock::now();
+    std::unique_ptr<ilm_host_layout> hl(new ilm_host_layout());
+    int nth = threads > 0 ? threads : (int)std::thread::hardware_concurrency();
+    std::string msg = build_kd_layout(views, kd_params(opts), nth, hl->h);
+    if (!msg.empty()) return ILM_ERR_INVALID_ARGUMENT;
+    hl->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    *out = hl.release();
+    return ILM_OK;
+}
+
+int32_t ilm_host_layout_kd_index(const ilm_host_layout* hl, uint32_t* out) {
+    if (!hl || !out) return ILM_ERR_INVALID_ARGUMENT;
+    if (!hl->h.kd_index.empty()) std::memcpy(out, hl->h.kd_index.data(), hl->h.kd_index.size() * 4);
+    return ILM_OK;
+}
+
 int32_t ilm_host_layout_info(const ilm_host_layout* hl, ilm_accel_info* out) {
     if (!hl || !out) return ILM_ERR_INVALID_ARGUMENT;
     const HostLayout& h = hl->h;
@@ -458,8 +548,11 @@ int32_t ilm_host_layout_info(const ilm_host_layout* hl, ilm_accel_info* out) {
     out->n_binary_nodes = (uint32_t)h.bin_nodes.size();
     out->n_nodes = h.n_nodes;
     out->width = (uint32_t)h.width;
-    out->device_bytes = h.node_bytes.size() + h.records.size() * sizeof(PrimRec) + h.spheres.size() * sizeof(SphereRec);
+    out->device_bytes = h.node_bytes.size() + h.records.size() * sizeof(PrimRec) +
+                        h.spheres.size() * sizeof(SphereRec) + h.kd_index.size() * sizeof(uint32_t);
     out->build_seconds = hl->seconds;
+    out->n_leaf_refs = (uint32_t)h.kd_index.size();
+    out->max_depth = (uint32_t)h.kd_max_depth;
     return ILM_OK;
 }
 

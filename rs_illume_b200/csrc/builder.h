@@ -68,7 +68,7 @@ struct MeshView {
 // host: the SAH binary tree, the layout for `width`, and primitive records in
 // traversal order.
 struct HostLayout {
-    int width = 8;
+    int width = 8;                      // 2, 4, 8, or kLayoutKdTree
     uint32_t n_prims = 0;
     std::vector<BinNode> bin_nodes;
     std::vector<uint32_t> prim_order;   // BVHAccel ordered_prims as primitive ids
@@ -77,7 +77,37 @@ struct HostLayout {
     std::vector<PrimRec> records;
     std::vector<SphereRec> spheres;
     float bound[6];
+    std::vector<uint32_t> kd_index;     // kd-tree: leaf primitive runs (records in id order)
+    int kd_max_depth = 0;               // kd-tree: the depth limit used
 };
+
+// KdTreeAccel::new parameters (accelerators/kdtreeaccel.rs:25-32).
+struct KdParams {
+    int isect_cost = 80;
+    int traversal_cost = 1;
+    float empty_bonus = 0.5f;
+    uint32_t max_prims = 1;
+    int max_depth = -1;                 // <= 0: round(8 + 1.3 log2(N))
+};
+
+// KdTreeAccel::build_tree (kdtreeaccel.rs:90-244) over the primitives' world
+// bounds: SAH over the sorted bound edges of one axis at a time (the largest
+// extent first, then the others when no edge lies strictly inside the node),
+// leaves below max_prims primitives, at max_depth, after three bad refines,
+// or when the best split costs over four times the leaf with fewer than 16
+// primitives.  Nodes come out depth first (below child next, as the
+// reference allocates them); subtrees near the root are built on up to
+// `threads` host threads into separate arrays and spliced in that order, so
+// the result does not depend on the thread count.  Edges at equal position
+// and type are ordered by primitive id.
+void kd_build(const std::vector<Box>& bounds, const Box& root, const KdParams& p, int threads,
+              std::vector<KdNode>& nodes, std::vector<uint32_t>& index);
+// The default depth limit round(8 + 1.3 log2(n)) (kdtreeaccel.rs:34-36).
+int kd_default_depth(uint64_t n);
+
+// KdTreeAccel::new followed by the device layout: kd nodes in node_bytes,
+// leaf runs in kd_index, one primitive record per primitive id.
+std::string build_kd_layout(const std::vector<MeshView>& meshes, const KdParams& p, int threads, HostLayout& out);
 
 // BVHAccel::new (bvh.rs:32-93) followed by the device layout.  Returns an
 // empty string on success or a description of the failure.

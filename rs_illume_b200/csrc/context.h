@@ -55,7 +55,7 @@ struct ShadingData {
 
 struct Accel {
     HostLayout host;                 // SAH tree, prim order, bound (device copies below)
-    DeviceBuffer d_nodes, d_prims, d_spheres;
+    DeviceBuffer d_nodes, d_prims, d_spheres, d_kd_index;
     uint64_t device_bytes = 0;
     double build_seconds = 0.0;
     // per-accel launch choices (ilm_accel_set_launch); -1 = context default
@@ -71,6 +71,7 @@ struct Accel {
         a.prims = static_cast<const PrimRec*>(d_prims.ptr);
         a.n_records = (uint32_t)host.records.size();
         a.spheres = static_cast<const SphereRec*>(d_spheres.ptr);
+        a.kd_index = static_cast<const uint32_t*>(d_kd_index.ptr);
         for (int k = 0; k < 6; ++k) a.bound[k] = host.bound[k];
         return a;
     }

@@ -10,12 +10,13 @@ namespace ilm {
 
 // Device view of one acceleration structure.
 struct DeviceAccel {
-    int width;                 // 2, 4, 8
-    const void* nodes;         // BinNode[] or WideNode<W>[]
+    int width;                 // 2, 4, 8, or kLayoutKdTree
+    const void* nodes;         // BinNode[], WideNode<W>[] or KdNode[]
     uint32_t n_nodes;
     const PrimRec* prims;      // traversal-ordered primitive records
     uint32_t n_records;
     const SphereRec* spheres;
+    const uint32_t* kd_index;  // kd-tree leaf runs (null for the BVH layouts)
     float bound[6];            // world bound (root box), min xyz / max xyz
 };
 
@@ -43,6 +44,7 @@ struct TraceArgs {
     uint32_t max_iter;
     unsigned long long* counter;       // persistent-schedule work counter
     float bound[6];
+    const uint32_t* kd_index;          // kd-tree leaf runs
 };
 
 // occ == nullptr: closest hit into `hits`; otherwise any-hit into `occ`.
@@ -52,6 +54,7 @@ cudaError_t launch_trace(const DeviceAccel& a, const ilm_ray* rays, uint64_t n, 
                          const unsigned long long* n_dev = nullptr);
 
 cudaError_t launch_trace_binary(const TraceArgs& t, cudaStream_t s);
+cudaError_t launch_trace_kd(const TraceArgs& t, const LaunchParams& lp, cudaStream_t s);
 cudaError_t launch_trace_wide(int width, const TraceArgs& t, const LaunchParams& lp, cudaStream_t s);
 
 }  // namespace ilm

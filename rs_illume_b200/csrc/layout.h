@@ -78,6 +78,24 @@ template <> struct WideNode<4> {           // 64 bytes
 };
 static_assert(sizeof(WideNode<4>) == 64, "WideNode<4> must be 64 bytes");
 
+// kd-tree node, the 8-byte KdAccelNode (accelerators/kdtreeaccel.rs:470-545):
+//   word : interior -> split position (float bits); leaf of one primitive ->
+//          its id; leaf of several -> first slot of its run in the index list
+//   flags: low 2 bits = split axis (0..2) or 3 for a leaf; the upper 30 bits =
+//          the above child's node index (interior) or the primitive count (leaf)
+// The below child of an interior node is the next node.
+struct KdNode {
+    uint32_t word;
+    uint32_t flags;
+};
+static_assert(sizeof(KdNode) == 8, "KdNode must be 8 bytes");
+constexpr uint32_t kKdLeaf = 3u;
+// Layout code of a kd-tree accel (the BVH layouts are their widths 2, 4, 8).
+constexpr int kLayoutKdTree = 1;
+// Deepest kd-tree accepted: the traversal keeps at most one deferred node per
+// level on its 64-entry stack.
+constexpr int kKdMaxDepth = 64;
+
 // Stack / entry encoding used by the wide traversal kernels.
 constexpr uint32_t kLeafFlag = 0x80000000u;
 constexpr uint32_t kMaxLeafPrims = 4;     // per wide-node child slot

@@ -1,4 +1,4 @@
-// Dispatch of the ray-query kernels (trace_bin.cu, trace_wide.cu).
+// Dispatch of the ray-query kernels (trace_bin.cu, trace_wide.cu, trace_kd.cu).
 #include "kernels.h"
 
 namespace ilm {
@@ -20,6 +20,8 @@ cudaError_t launch_trace(const DeviceAccel& a, const ilm_ray* rays, uint64_t n, 
     t.max_iter = lp.max_iter;
     t.counter = lp.counter;
     for (int k = 0; k < 6; ++k) t.bound[k] = a.bound[k];
+    t.kd_index = a.kd_index;
+    if (a.width == kLayoutKdTree) return launch_trace_kd(t, lp, s);
     if (a.width == 2) return launch_trace_binary(t, s);
     return launch_trace_wide(a.width, t, lp, s);
 }

@@ -1,0 +1,239 @@
+// kd-tree ray queries: KdTreeAccel::intersect / intersect_p
+// (accelerators/kdtreeaccel.rs:256-465).
+//
+// The ray's parametric range is clipped to the tree's bound
+// (Bounds3::intersect_ray, geometry/bounds3.rs:253-282); each interior node
+// sends the ray to the child on its origin's side of the split first and, when
+// the split plane falls inside the current range, defers the other child with
+// the range beyond the plane.  Traversal ends when the closest hit so far lies
+// before the next range.  Every comparison keeps the reference's form, so a
+// ray lying in a split plane (0 * inf = NaN plane distance) visits both
+// children as the reference does.
+//
+// Deferred entries hold (node, t_min) only: an entry's t_max is always the
+// t_min of the entry beneath it (the root range's end for the bottom one),
+// because the range being traversed ends where the last deferred range
+// starts.  The values restored are the reference's, bit for bit.
+//
+// Leaf runs test primitives by id (records are stored in id order).  The
+// reference's multi-primitive leaf loop reads the run's second entry n times
+// (`primitive_indices_offset + 1`, kdtreeaccel.rs:351 and 440); this loop
+// reads entry k on iteration k.
+//
+// Schedules: one thread per ray (grid), or persistent warps that claim rays in
+// chunks and refill finished lanes (the wide BVH kernels' scheme); every loop
+// iteration advances a lane by one node or one leaf.
+#include "wide_tracer.cuh"
+
+namespace ilm {
+
+namespace {
+
+// One slab of Bounds3::intersect_ray.
+__device__ __forceinline__ bool clip_slab(float lo, float hi, float o, float inv, float& t0, float& t1) {
+    float t_near = __fmul_rn(__fsub_rn(lo, o), inv);
+    float t_far = __fmul_rn(__fsub_rn(hi, o), inv);
+    if (t_near > t_far) {
+        float s = t_near;
+        t_near = t_far;
+        t_far = s;
+    }
+    t_far = __fmul_rn(t_far, kBoxRobust);
+    if (t_near > t0) t0 = t_near;
+    if (t_far < t1) t1 = t_far;
+    return !(t0 > t1);
+}
+
+__device__ __forceinline__ float pick(uint32_t axis, float x, float y, float z) {
+    return axis == 0 ? x : (axis == 1 ? y : z);
+}
+
+constexpr int kKdBlock = 128;
+
+template <bool kAny>
+struct KdTracer {
+    RayIn ray;
+    float ix, iy, iz;
+    float t_min, t_max, t_root;      // current range; end of the root range
+    float best_t, bu, bv;
+    uint32_t best, status, cur, iter;
+    int sp;
+    bool tr_ready, occluded;
+    TriRay tr;
+    uint2 stack[kKdMaxDepth];        // (node, t_min bits)
+
+    __device__ __forceinline__ void init(const RayIn& r) {
+        ray = r;
+        best_t = r.tmax; bu = 0.0f; bv = 0.0f;
+        best = ILM_MISS;
+        status = 0; cur = 0; iter = 0; sp = 0;
+        tr_ready = false; occluded = false;
+        ix = __frcp_rn(r.dx); iy = __frcp_rn(r.dy); iz = __frcp_rn(r.dz);   // == 1/d exactly
+    }
+
+    // The tree-bound clip of KdTreeAccel::intersect (kdtreeaccel.rs:258-264).
+    __device__ __forceinline__ bool enters(const float* b) {
+        t_min = 0.0f;
+        t_max = ray.tmax;
+        bool in = clip_slab(b[0], b[3], ray.ox, ix, t_min, t_max) && clip_slab(b[1], b[4], ray.oy, iy, t_min, t_max) &&
+                  clip_slab(b[2], b[5], ray.oz, iz, t_min, t_max);
+        t_root = t_max;
+        return in;
+    }
+
+    // One node or one leaf; true when the ray is finished.
+    __device__ __forceinline__ bool step(const TraceArgs& a) {
+        if ((kAny ? ray.tmax : best_t) < t_min) return true;
+        if (++iter > a.max_iter) { status = kErrIterationCap; return true; }
+        const uint2 nd = __ldg(static_cast<const uint2*>(a.nodes) + cur);
+        const uint32_t axis = nd.y & 3u;
+        if (axis != kKdLeaf) {
+            const float split = __uint_as_float(nd.x);
+            const float o = pick(axis, ray.ox, ray.oy, ray.oz);
+            const float d = pick(axis, ray.dx, ray.dy, ray.dz);
+            const float t_plane = __fmul_rn(__fsub_rn(split, o), pick(axis, ix, iy, iz));
+            const bool below_first = o < split || (o == split && d <= 0.0f);
+            const uint32_t above = nd.y >> 2;
+            const uint32_t first = below_first ? cur + 1 : above;
+            const uint32_t second = below_first ? above : cur + 1;
+            if (t_plane > t_max || t_plane <= 0.0f) {
+                cur = first;
+            } else if (t_plane < t_min) {
+                cur = second;
+            } else {
+                if (sp == kKdMaxDepth) { status = kErrStackOverflow; return true; }
+                stack[sp++] = make_uint2(second, __float_as_uint(t_plane));
+                cur = first;
+                t_max = t_plane;
+            }
+            return false;
+        }
+        const uint32_t n = nd.y >> 2;
+        for (uint32_t k = 0; k < n; ++k) {
+            const uint32_t r = n == 1 ? nd.x : __ldg(a.kd_index + nd.x + k);
+            float t, u, v;
+            uint32_t pid;
+            if (kAny) {
+                if (prim_test<false>(a.prims, a.spheres, r, tr, tr_ready, ray, ray.tmax, t, u, v, pid)) {
+                    occluded = true;
+                    return true;
+                }
+            } else if (prim_test<true>(a.prims, a.spheres, r, tr, tr_ready, ray, best_t, t, u, v, pid) &&
+                       (t < best_t || (t == best_t && pid < best))) {
+                best_t = t; best = pid; bu = u; bv = v;
+            }
+        }
+        if (sp == 0) return true;
+        --sp;
+        cur = stack[sp].x;
+        t_min = __uint_as_float(stack[sp].y);
+        t_max = sp > 0 ? __uint_as_float(stack[sp - 1].y) : t_root;
+        return false;
+    }
+
+    __device__ __forceinline__ void write(uint64_t i, const TraceArgs& a) const {
+        if (status) atomicOr(a.err, status);
+        if (kAny) {
+            a.occ[i] = status ? kHitTraversalError : (occluded ? 1u : 0u);
+        } else {
+            if (status) store_hit(a.hits, i, kHitTraversalError, ray.tmax, 0.0f, 0.0f);
+            else store_hit(a.hits, i, best, best == ILM_MISS ? ray.tmax : best_t, bu, bv);
+        }
+    }
+};
+
+template <bool kAny>
+__global__ void __launch_bounds__(kKdBlock) k_trace_kd(TraceArgs a) {
+    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= ray_count(a)) return;
+    RayIn r = load_ray(a.rays, i);
+    KdTracer<kAny> T;
+    T.init(r);
+    if (a.n_nodes == 0 || !T.enters(a.bound)) { write_miss(i, r, a.hits, a.occ); return; }
+    while (!T.step(a)) {}
+    T.write(i, a);
+}
+
+template <bool kAny, int kMinBlocks>
+__global__ void __launch_bounds__(kKdBlock, kMinBlocks) k_trace_kd_persistent(TraceArgs a) {
+    const uint64_t n = ray_count(a);
+    const unsigned chunk = n < 2ull * gridDim.x * blockDim.x ? 32u : kChunk;
+    const unsigned lane = threadIdx.x & 31u;
+    const unsigned below = (1u << lane) - 1u;
+    KdTracer<kAny> T;
+    bool active = false;
+    uint64_t id = 0;
+    unsigned long long chunk_next = 0, chunk_end = 0;   // warp-uniform
+    bool exhausted = false;                             // warp-uniform
+    for (;;) {
+        unsigned need = __ballot_sync(0xFFFFFFFFu, !active);
+        // Hand rays to idle lanes; rays missing the tree's bound are answered
+        // here.  Every pass hands out >= 1 ray or claims a chunk.
+        while (need != 0u && !exhausted) {
+            if (chunk_next == chunk_end) {
+                unsigned long long b = 0;
+                if (lane == 0) b = atomicAdd(a.counter, (unsigned long long)chunk);
+                b = __shfl_sync(0xFFFFFFFFu, b, 0);
+                if (b >= n) { exhausted = true; break; }
+                chunk_next = b;
+                chunk_end = b + chunk < n ? b + chunk : n;
+            }
+            unsigned avail = (unsigned)(chunk_end - chunk_next);
+            unsigned rank = __popc(need & below);
+            if (((need >> lane) & 1u) && rank < avail) {
+                id = chunk_next + rank;
+                RayIn r = load_ray(a.rays, id);
+                T.init(r);
+                if (a.n_nodes != 0 && T.enters(a.bound)) active = true;
+                else write_miss(id, r, a.hits, a.occ);
+            }
+            chunk_next += min((unsigned)__popc(need), avail);
+            need = __ballot_sync(0xFFFFFFFFu, !active);
+        }
+        if (!__any_sync(0xFFFFFFFFu, active)) break;   // only reached once exhausted
+        if (active && T.step(a)) {
+            T.write(id, a);
+            active = false;
+        }
+    }
+}
+
+template <int kMinBlocks>
+cudaError_t launch_persistent(const TraceArgs& t, cudaStream_t s) {
+    const unsigned block = kKdBlock;
+    auto kc = k_trace_kd_persistent<false, kMinBlocks>;
+    auto ka = k_trace_kd_persistent<true, kMinBlocks>;
+    static int per_sm[2] = {0, 0};
+    static int sms = 0;
+    const int which = t.occ ? 1 : 0;
+    if (per_sm[which] == 0) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[which], t.occ ? (const void*)ka : (const void*)kc,
+                                                      block, 0);
+        if (per_sm[which] < 1) per_sm[which] = 1;
+    }
+    uint64_t need_blocks = (t.n + block - 1) / block;
+    uint64_t grid = (uint64_t)sms * per_sm[which];
+    if (grid > need_blocks) grid = need_blocks;
+    cudaError_t e = cudaMemsetAsync(t.counter, 0, sizeof(unsigned long long), s);
+    if (e != cudaSuccess) return e;
+    if (t.occ) ka<<<(unsigned)grid, block, 0, s>>>(t);
+    else kc<<<(unsigned)grid, block, 0, s>>>(t);
+    return cudaGetLastError();
+}
+
+}  // namespace
+
+cudaError_t launch_trace_kd(const TraceArgs& t, const LaunchParams& lp, cudaStream_t s) {
+    if (lp.persistent && t.counter)
+        return lp.min_blocks >= 8 ? launch_persistent<8>(t, s) : launch_persistent<1>(t, s);
+    const unsigned block = kKdBlock;
+    unsigned grid = (unsigned)((t.n + block - 1) / block);
+    if (t.occ) k_trace_kd<true><<<grid, block, 0, s>>>(t);
+    else k_trace_kd<false><<<grid, block, 0, s>>>(t);
+    return cudaGetLastError();
+}
+
+}  // namespace ilm

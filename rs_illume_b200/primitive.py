@@ -207,15 +207,16 @@ class GpuBVHAccel:
         return bool(occ)
 
     def get_area_light(self):
-        log.error("GpuBVHAccel::get_area_light() called; should have gone to GeometricPrimitive.")
+        log.error("%s::get_area_light() called; should have gone to GeometricPrimitive.", type(self).__name__)
         return None
 
     def get_material(self):
-        log.error("GpuBVHAccel::get_material() called; should have gone to GeometricPrimitive.")
+        log.error("%s::get_material() called; should have gone to GeometricPrimitive.", type(self).__name__)
         return None
 
     def compute_scattering_function(self, *args, **kwargs):
-        log.error("GpuBVHAccel::compute_scattering_function() called; should have gone to GeometricPrimitive.")
+        log.error("%s::compute_scattering_function() called; should have gone to GeometricPrimitive.",
+                  type(self).__name__)
 
     # -- batched path ------------------------------------------------------
     def intersect_batch(self, rays, hits=None, stream=None):
@@ -254,6 +255,36 @@ class GpuBVHAccel:
         self.ctx.check(self.ctx._lib.ilm_accel_binary_nodes(self.ctx.handle, self.id, ptr(nodes), ptr(order)),
                        "ilm_accel_binary_nodes")
         return nodes, order
+
+
+class GpuKdTreeAccel(GpuBVHAccel):
+    """GPU drop-in for KdTreeAccel (accelerators/kdtreeaccel.rs:25-32): the
+    same SAH kd-tree, traversed on the B200.  Queries, surface interactions
+    and path tracing work as on GpuBVHAccel."""
+
+    def __init__(self, ctx: Context, shapes: Sequence, isect_cost: int = 80, traversal_cost: int = 1,
+                 empty_bonus: float = 0.5, max_prims: int = 1, max_depth: int = -1):
+        self.ctx = ctx
+        ids = (ctypes.c_uint32 * len(shapes))(*[s.id for s in shapes])
+        opts = _lib.ilm_kdtree_opts(isect_cost, traversal_cost, empty_bonus, max_prims, max_depth)
+        aid = ctypes.c_uint32()
+        ctx.check(ctx._lib.ilm_kdtree_build(ctx.handle, ids, len(shapes), ctypes.byref(opts), ctypes.byref(aid)),
+                  "ilm_kdtree_build")
+        self.id = aid.value
+        self.width = _lib.ILM_LAYOUT_KDTREE
+        self.n_prims = sum(s.n_prims for s in shapes)
+
+    def binary_nodes(self):
+        raise NotImplementedError("a kd-tree has no BVH nodes; see kd_nodes()")
+
+    def kd_nodes(self):
+        """(nodes as KD_NODE_DTYPE, leaf index list as uint32)."""
+        inf = self.info()
+        nodes = np.zeros(inf["n_nodes"], _lib.KD_NODE_DTYPE)
+        index = np.zeros(inf["n_leaf_refs"], np.uint32)
+        self.ctx.check(self.ctx._lib.ilm_accel_kd_nodes(self.ctx.handle, self.id, ptr(nodes), ptr(index)),
+                       "ilm_accel_kd_nodes")
+        return nodes, index
 
 
 class PathTracer:

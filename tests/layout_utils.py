@@ -42,6 +42,31 @@ def host_layout(xyz, idx, width=8, max_prims=4, spheres=()):
     return {"info": inf, "bin": bn, "order": po, "nodes": nodes, "records": recs, "bound": bound}
 
 
+def host_kdtree(xyz, idx, spheres=(), threads=0, isect_cost=80, traversal_cost=1, empty_bonus=0.5, max_prims=1,
+                max_depth=-1):
+    """The product's host-only kd-tree build: (status, dict)."""
+    lib = _lib.load()
+    xyz = np.ascontiguousarray(xyz, np.float32).reshape(-1, 3)
+    idx = np.ascontiguousarray(idx, np.uint32).reshape(-1, 3)
+    sph = (_lib.ilm_sphere_desc * max(1, len(spheres)))(*spheres)
+    h = ctypes.c_void_p()
+    opts = _lib.ilm_kdtree_opts(isect_cost, traversal_cost, empty_bonus, max_prims, max_depth)
+    st = lib.ilm_host_kdtree_build(_lib.ptr(xyz), len(xyz), _lib.ptr(idx), len(idx), ctypes.addressof(sph),
+                                   len(spheres), ctypes.byref(opts), threads, ctypes.byref(h))
+    if st != 0:
+        return st, None
+    inf = _lib.ilm_accel_info()
+    lib.ilm_host_layout_info(h, ctypes.byref(inf))
+    nodes = np.zeros(inf.n_nodes, _lib.KD_NODE_DTYPE)
+    index = np.zeros(inf.n_leaf_refs, np.uint32)
+    recs = np.zeros(inf.n_prims, _lib.PRIM_REC_DTYPE)
+    bound = np.zeros(6, np.float32)
+    lib.ilm_host_layout_copy(h, None, None, _lib.ptr(nodes), _lib.ptr(recs), _lib.ptr(bound))
+    lib.ilm_host_layout_kd_index(h, _lib.ptr(index))
+    lib.ilm_host_layout_destroy(h)
+    return 0, {"info": inf, "nodes": nodes, "index": index, "records": recs, "bound": bound}
+
+
 def dequantised_boxes(node, width):
     """(W, 2, 3) float32 child boxes of one wide node: fma(q, 2^(e-127), origin)."""
     ex = [(int(node["packed"]) >> (8 * a)) & 0xFF for a in range(3)]
