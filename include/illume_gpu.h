@@ -64,9 +64,16 @@ typedef struct { uint32_t prim; float t; float u; float v; } ilm_hit;
  *   ILM_QUADRIC_DISK     Disk::new (disk.rs:27-47): height, radius, inner_radius, phi_max_deg;
  *   ILM_QUADRIC_CYLINDER Cylinder::new (cylinder.rs:26-46): radius, z_min, z_max, phi_max_deg
  *                        (in degrees and ordered, as pbrt; the reference keeps the raw values);
- *   ILM_QUADRIC_CONE     Cone::new (cone.rs:26-41): height, radius, phi_max_deg.
+ *   ILM_QUADRIC_CONE     Cone::new (cone.rs:26-41): height, radius, phi_max_deg;
+ *   ILM_QUADRIC_PARABOLOID  Paraboloid::new (paraboloid.rs:26-47): radius, z_min, z_max
+ *                        (ordered, as pbrt), phi_max_deg;
+ *   ILM_QUADRIC_HYPERBOLOID Hyperboloid::new (hyperboloid.rs:31-77): the points p1, p2
+ *                        swept around z, phi_max_deg (pbrt's p2.z == 0 swap).
  * Zero-initialised extra fields keep the sphere layout of earlier callers. */
-enum { ILM_QUADRIC_SPHERE = 0, ILM_QUADRIC_DISK = 1, ILM_QUADRIC_CYLINDER = 2, ILM_QUADRIC_CONE = 3 };
+enum {
+    ILM_QUADRIC_SPHERE = 0, ILM_QUADRIC_DISK = 1, ILM_QUADRIC_CYLINDER = 2, ILM_QUADRIC_CONE = 3,
+    ILM_QUADRIC_PARABOLOID = 4, ILM_QUADRIC_HYPERBOLOID = 5
+};
 typedef struct {
     float object_to_world[16];
     float world_to_object[16];
@@ -74,6 +81,7 @@ typedef struct {
     int32_t reverse_orientation;
     int32_t kind;
     float height, inner_radius;
+    float p1[3], p2[3];
 } ilm_sphere_desc;
 
 typedef struct {

@@ -32,7 +32,8 @@ class orc_sphere_desc(ctypes.Structure):
     _fields_ = [("object_to_world", ctypes.c_float * 16), ("world_to_object", ctypes.c_float * 16),
                 ("radius", ctypes.c_float), ("z_min", ctypes.c_float), ("z_max", ctypes.c_float),
                 ("phi_max_deg", ctypes.c_float), ("reverse_orientation", ctypes.c_int32),
-                ("kind", ctypes.c_int32), ("height", ctypes.c_float), ("inner_radius", ctypes.c_float)]
+                ("kind", ctypes.c_int32), ("height", ctypes.c_float), ("inner_radius", ctypes.c_float),
+                ("p1", ctypes.c_float * 3), ("p2", ctypes.c_float * 3)]
 
 
 _P = ctypes.c_void_p
@@ -121,9 +122,10 @@ def rng_u32(seq: int, n: int) -> np.ndarray:
 
 def quadric_desc(kind: int, radius: float, matrix, z_min: float = 0.0, z_max: float = 0.0,
                  phi_max_deg: float = 360.0, height: float = 0.0, inner_radius: float = 0.0,
-                 reverse: bool = False) -> orc_sphere_desc:
-    """Any quadric (kind 0 sphere, 1 disk, 2 cylinder, 3 cone) under a 4x4
-    object-to-world matrix (its inverse computed in float64)."""
+                 reverse: bool = False, p1=(0.0, 0.0, 0.0), p2=(0.0, 0.0, 0.0)) -> orc_sphere_desc:
+    """Any quadric (kind 0 sphere, 1 disk, 2 cylinder, 3 cone, 4 paraboloid,
+    5 hyperboloid) under a 4x4 object-to-world matrix (its inverse computed in
+    float64)."""
     m = np.asarray(matrix, np.float64).reshape(4, 4)
     inv = np.linalg.inv(m)
     d = orc_sphere_desc()
@@ -132,6 +134,8 @@ def quadric_desc(kind: int, radius: float, matrix, z_min: float = 0.0, z_max: fl
         d.world_to_object[i] = float(np.float32(inv.flat[i]))
     d.kind, d.radius, d.z_min, d.z_max = kind, radius, z_min, z_max
     d.phi_max_deg, d.height, d.inner_radius, d.reverse_orientation = phi_max_deg, height, inner_radius, int(reverse)
+    for k in range(3):
+        d.p1[k], d.p2[k] = p1[k], p2[k]
     return d
 
 

@@ -242,7 +242,9 @@ struct Sphere {
     float m[16], mi[16];   // object_to_world, world_to_object (row-major)
     float radius, z_min, z_max, theta_min, theta_max, phi_max;
     float inner_radius, height;
-    int kind;              // 0 sphere, 1 disk, 2 cylinder, 3 cone
+    V3 p1, p2;             // hyperboloid: the swept segment (after the p2.z == 0 swap)
+    float ah, ch;          // hyperboloid: ah (x^2 + y^2) - ch z^2 = 1
+    int kind;              // 0 sphere, 1 disk, 2 cylinder, 3 cone, 4 paraboloid, 5 hyperboloid
     bool reverse;
 };
 // Sphere::new (sphere.rs:50-75; D22: made public), Disk::new (disk.rs:27-47),
@@ -275,6 +277,37 @@ static Sphere sphere_new(const orc_sphere_desc& d) {
             s.z_min = 0.0f;
             s.z_max = d.height;
             break;
+        case 4:   // paraboloid (paraboloid.rs:26-47; z range ordered as pbrt)
+            s.z_min = mn;
+            s.z_max = mx;
+            break;
+        case 5: {   // hyperboloid (hyperboloid.rs:31-77)
+            V3 p1{d.p1[0], d.p1[1], d.p1[2]}, p2{d.p2[0], d.p2[1], d.p2[2]};
+            float radius1 = std::sqrt(p1.x * p1.x + p1.y * p1.y);
+            float radius2 = std::sqrt(p2.x * p2.x + p2.y * p2.y);
+            s.radius = std::fmax(radius1, radius2);
+            s.z_min = std::fmin(p1.z, p2.z);
+            s.z_max = std::fmax(p1.z, p2.z);
+            // D33: swap when p2.z == 0 (the reference swaps when it is not),
+            // and iterate until both coefficients are finite (not only
+            // until neither is infinite), as pbrt
+            if (p2.z == 0.0f) std::swap(p1, p2);
+            V3 pp = p1;
+            float ah = std::numeric_limits<float>::infinity(), ch = ah;
+            for (int it = 0; it < 64 && !(std::isfinite(ah) && std::isfinite(ch)); ++it) {
+                pp = {pp.x + 2.0f * (p2.x - p1.x), pp.y + 2.0f * (p2.y - p1.y), pp.z + 2.0f * (p2.z - p1.z)};
+                float xy1 = pp.x * pp.x + pp.y * pp.y;
+                float xy2 = p2.x * p2.x + p2.y * p2.y;
+                ah = (1.0f / xy1 - (pp.z * pp.z) / (xy1 * p2.z * p2.z)) /
+                     (1.0f - (xy2 * pp.z * pp.z) / (xy1 * p2.z * p2.z));
+                ch = (ah * xy2 - 1.0f) / (p2.z * p2.z);
+            }
+            s.p1 = p1;
+            s.p2 = p2;
+            s.ah = ah;
+            s.ch = ch;
+            break;
+        }
         default:   // sphere
             s.z_min = clamp(mn, -d.radius, d.radius);
             s.z_max = clamp(mx, -d.radius, d.radius);
@@ -491,11 +524,94 @@ static bool cone_test(const Sphere& s, const Ray& world_ray, float* t_out, float
     return true;
 }
 
+// Paraboloid::intersect / intersect_p (paraboloid.rs:95-...): k (x^2 + y^2)
+// = z with k = z_max / r^2 in EFloat, clipped by z and phi (retry with t1).
+static bool paraboloid_test(const Sphere& s, const Ray& world_ray, float* t_out, float* uv_out) {
+    V3 o, d, oe, de;
+    transform_ray_with_error(s.mi, world_ray, &o, &d, &oe, &de);
+    EF ox = ef_new(o.x, oe.x), oy = ef_new(o.y, oe.y), oz = ef_new(o.z, oe.z);
+    EF dx = ef_new(d.x, de.x), dy = ef_new(d.y, de.y), dz = ef_new(d.z, de.z);
+    EF k = ef_div(ef_new(s.z_max, 0.0f), ef_mul(ef_new(s.radius, 0.0f), ef_new(s.radius, 0.0f)));
+    EF a = ef_mul(k, ef_add(ef_mul(dx, dx), ef_mul(dy, dy)));
+    // D23: the reference's `* 2.0` builds an interval as wide as the value; exact 2
+    EF b = ef_sub(ef_mul(ef_mul(k, ef_add(ef_mul(dx, ox), ef_mul(dy, oy))), ef_new(2.0f, 0.0f)), dz);
+    EF c = ef_sub(ef_mul(k, ef_add(ef_mul(ox, ox), ef_mul(oy, oy))), oz);
+    EF t0, t1, th;
+    if (!ef_quadratic(a, b, c, &t0, &t1)) return false;
+    if (!nearest_root(t0, t1, world_ray.t_max, &th)) return false;
+    V3 p;
+    float phi;
+    auto hit_point = [&](float t) {
+        p = {o.x + d.x * t, o.y + d.y * t, o.z + d.z * t};
+        phi = std::atan2(p.y, p.x);
+        if (phi < 0.0f) phi += 2.0f * kPi;
+    };
+    auto clipped = [&]() { return p.z < s.z_min || p.z > s.z_max || phi > s.phi_max; };
+    hit_point(th.v);
+    if (clipped()) {
+        if (th.v == t1.v) return false;
+        if (t1.high > world_ray.t_max) return false;
+        th = t1;
+        hit_point(th.v);
+        if (clipped()) return false;
+    }
+    *t_out = th.v;
+    uv_out[0] = phi / s.phi_max;
+    uv_out[1] = (p.z - s.z_min) / (s.z_max - s.z_min);
+    return true;
+}
+
+// Hyperboloid::intersect / intersect_p (hyperboloid.rs:128-...): ah (x^2 +
+// y^2) - ch z^2 = 1, clipped by z and phi (retry with t1); phi is measured
+// from the swept point pr = (1 - v) p1 + v p2 at the hit's height.
+// D34: c = ah ox^2 + ah oy^2 - ch oz^2 - 1 (line 149 has - oz^2 - ch).
+// D35: the first phi is atan2(pr.x py - px pr.y, px pr.x + py pr.y) (line 169
+// applies atan2 to pr.y alone; line 180 has it right).
+static bool hyperboloid_test(const Sphere& s, const Ray& world_ray, float* t_out, float* uv_out) {
+    V3 o, d, oe, de;
+    transform_ray_with_error(s.mi, world_ray, &o, &d, &oe, &de);
+    EF ox = ef_new(o.x, oe.x), oy = ef_new(o.y, oe.y), oz = ef_new(o.z, oe.z);
+    EF dx = ef_new(d.x, de.x), dy = ef_new(d.y, de.y), dz = ef_new(d.z, de.z);
+    EF ah = ef_new(s.ah, 0.0f), ch = ef_new(s.ch, 0.0f);
+    EF a = ef_sub(ef_add(ef_mul(ef_mul(dx, dx), ah), ef_mul(ef_mul(dy, dy), ah)), ef_mul(ef_mul(dz, dz), ch));
+    EF b = ef_mul(ef_new(2.0f, 0.0f),
+                  ef_sub(ef_add(ef_mul(ef_mul(dx, ox), ah), ef_mul(ef_mul(dy, oy), ah)), ef_mul(ef_mul(dz, oz), ch)));
+    EF c = ef_sub(ef_sub(ef_add(ef_mul(ef_mul(ox, ox), ah), ef_mul(ef_mul(oy, oy), ah)), ef_mul(ef_mul(oz, oz), ch)),
+                  ef_new(1.0f, 0.0f));
+    EF t0, t1, th;
+    if (!ef_quadratic(a, b, c, &t0, &t1)) return false;
+    if (!nearest_root(t0, t1, world_ray.t_max, &th)) return false;
+    V3 p;
+    float phi, v;
+    auto hit_point = [&](float t) {
+        p = {o.x + d.x * t, o.y + d.y * t, o.z + d.z * t};
+        v = (p.z - s.p1.z) / (s.p2.z - s.p1.z);
+        V3 pr{s.p1.x * (1.0f - v) + s.p2.x * v, s.p1.y * (1.0f - v) + s.p2.y * v, 0.0f};
+        phi = std::atan2(pr.x * p.y - p.x * pr.y, p.x * pr.x + p.y * pr.y);
+        if (phi < 0.0f) phi += 2.0f * kPi;
+    };
+    auto clipped = [&]() { return p.z < s.z_min || p.z > s.z_max || phi > s.phi_max; };
+    hit_point(th.v);
+    if (clipped()) {
+        if (th.v == t1.v) return false;
+        if (t1.high > world_ray.t_max) return false;
+        th = t1;
+        hit_point(th.v);
+        if (clipped()) return false;
+    }
+    *t_out = th.v;
+    uv_out[0] = phi / s.phi_max;
+    uv_out[1] = v;
+    return true;
+}
+
 static bool quadric_test(const Sphere& s, const Ray& ray, float* t_out, float* uv_out) {
     switch (s.kind) {
         case 1: return disk_test(s, ray, t_out, uv_out);
         case 2: return cylinder_test(s, ray, t_out, uv_out);
         case 3: return cone_test(s, ray, t_out, uv_out);
+        case 4: return paraboloid_test(s, ray, t_out, uv_out);
+        case 5: return hyperboloid_test(s, ray, t_out, uv_out);
         default: return sphere_test(s, ray, t_out, uv_out);
     }
 }

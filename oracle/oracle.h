@@ -33,7 +33,9 @@ typedef struct { uint32_t prim; float t; float u; float v; } orc_hit;
  * (m[i][j] at [4*i+j]).  kind 0: Sphere (shapes/sphere.rs:15-75; radius,
  * z_min, z_max, phi_max); 1: Disk (disk.rs:27-47; height, radius,
  * inner_radius, phi_max); 2: Cylinder (cylinder.rs:26-46; radius, z_min,
- * z_max, phi_max); 3: Cone (cone.rs:26-41; height, radius, phi_max). */
+ * z_max, phi_max); 3: Cone (cone.rs:26-41; height, radius, phi_max);
+ * 4: Paraboloid (paraboloid.rs:26-47; radius, z_min, z_max, phi_max);
+ * 5: Hyperboloid (hyperboloid.rs:31-77; p1, p2, phi_max). */
 typedef struct {
     float object_to_world[16];
     float world_to_object[16];
@@ -41,6 +43,7 @@ typedef struct {
     int32_t reverse_orientation;
     int32_t kind;
     float height, inner_radius;
+    float p1[3], p2[3];
 } orc_sphere_desc;
 
 /* 32-byte flattened BVH node (accelerators/bvh.rs:665-673, 32 B per D6). */

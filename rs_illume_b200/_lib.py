@@ -88,10 +88,11 @@ class ilm_sphere_desc(ctypes.Structure):
     _fields_ = [("object_to_world", ctypes.c_float * 16), ("world_to_object", ctypes.c_float * 16),
                 ("radius", ctypes.c_float), ("z_min", ctypes.c_float), ("z_max", ctypes.c_float),
                 ("phi_max_deg", ctypes.c_float), ("reverse_orientation", ctypes.c_int32),
-                ("kind", ctypes.c_int32), ("height", ctypes.c_float), ("inner_radius", ctypes.c_float)]
+                ("kind", ctypes.c_int32), ("height", ctypes.c_float), ("inner_radius", ctypes.c_float),
+                ("p1", ctypes.c_float * 3), ("p2", ctypes.c_float * 3)]
 
 
-QUADRICS = {"sphere": 0, "disk": 1, "cylinder": 2, "cone": 3}
+QUADRICS = {"sphere": 0, "disk": 1, "cylinder": 2, "cone": 3, "paraboloid": 4, "hyperboloid": 5}
 
 
 class ilm_pt_scene_desc(ctypes.Structure):

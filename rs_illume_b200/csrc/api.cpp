@@ -191,12 +191,16 @@ int32_t ilm_mesh_set_attrs(ilm_context* ctx, ilm_mesh_id mesh, const ilm_mesh_at
 // The record of one quadric description; null on success, else why it is
 // rejected.
 static const char* quadric_record(const ilm_sphere_desc& d, SphereRec* out) {
-    if (!(d.radius > 0.0f) || !std::isfinite(d.radius)) return "radius must be positive and finite";
-    if (d.kind < ILM_QUADRIC_SPHERE || d.kind > ILM_QUADRIC_CONE ||
+    const bool hyper = d.kind == ILM_QUADRIC_HYPERBOLOID;
+    if (!hyper && (!(d.radius > 0.0f) || !std::isfinite(d.radius))) return "radius must be positive and finite";
+    for (int k = 0; k < 3; ++k)
+        if (!std::isfinite(d.p1[k]) || !std::isfinite(d.p2[k])) return "invalid quadric parameters";
+    if (d.kind < ILM_QUADRIC_SPHERE || d.kind > ILM_QUADRIC_HYPERBOLOID ||
         (d.kind == ILM_QUADRIC_CONE && !(d.height > 0.0f)) ||
         (d.kind == ILM_QUADRIC_DISK && !(d.inner_radius >= 0.0f && d.inner_radius < d.radius)) ||
-        (d.kind == ILM_QUADRIC_CYLINDER && !(d.z_min != d.z_max)) || !std::isfinite(d.height) ||
-        !std::isfinite(d.z_min) || !std::isfinite(d.z_max))
+        (d.kind == ILM_QUADRIC_CYLINDER && !(d.z_min != d.z_max)) ||
+        (d.kind == ILM_QUADRIC_PARABOLOID && !(d.z_min != d.z_max && std::fmax(d.z_min, d.z_max) > 0.0f)) ||
+        !std::isfinite(d.height) || !std::isfinite(d.z_min) || !std::isfinite(d.z_max))
         return "invalid quadric parameters";
     SphereInput in;
     std::memcpy(in.o2w, d.object_to_world, sizeof in.o2w);
@@ -204,7 +208,8 @@ static const char* quadric_record(const ilm_sphere_desc& d, SphereRec* out) {
     in.radius = d.radius; in.z_min = d.z_min; in.z_max = d.z_max; in.phi_max_deg = d.phi_max_deg;
     in.reverse = d.reverse_orientation;
     in.kind = d.kind; in.height = d.height; in.inner_radius = d.inner_radius;
-    *out = make_sphere(in);
+    for (int k = 0; k < 3; ++k) { in.p1[k] = d.p1[k]; in.p2[k] = d.p2[k]; }
+    if (!make_sphere(in, out)) return "hyperboloid points give no finite implicit form";
     return nullptr;
 }
 

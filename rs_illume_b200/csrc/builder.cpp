@@ -232,6 +232,12 @@ bool triangle_degenerate(const float* p0, const float* p1, const float* p2) {
 
 SphereRec make_sphere(const SphereInput& in) {
     SphereRec s;
+    make_sphere(in, &s);
+    return s;
+}
+
+bool make_sphere(const SphereInput& in, SphereRec* out) {
+    SphereRec& s = *out;
     std::memset(&s, 0, sizeof s);
     std::memcpy(s.o2w, in.o2w, sizeof s.o2w);
     std::memcpy(s.w2o, in.w2o, sizeof s.w2o);
@@ -255,13 +261,44 @@ SphereRec make_sphere(const SphereInput& in) {
             s.z_min = 0.0f;
             s.z_max = in.height;
             break;
+        case kQuadricParaboloid:   // Paraboloid::new (paraboloid.rs:26-47), z range ordered as pbrt
+            s.z_min = mn;
+            s.z_max = mx;
+            break;
+        case kQuadricHyperboloid: {   // Hyperboloid::new (hyperboloid.rs:31-77)
+            float p1[3] = {in.p1[0], in.p1[1], in.p1[2]}, p2[3] = {in.p2[0], in.p2[1], in.p2[2]};
+            float r1 = std::sqrt(p1[0] * p1[0] + p1[1] * p1[1]);
+            float r2 = std::sqrt(p2[0] * p2[0] + p2[1] * p2[1]);
+            s.radius = r1 > r2 ? r1 : r2;
+            s.z_min = std::fmin(p1[2], p2[2]);
+            s.z_max = std::fmax(p1[2], p2[2]);
+            // the implicit coefficients need p2.z != 0: swap when it is 0
+            // (hyperboloid.rs:42-47 swaps on the opposite test; pbrt's rule)
+            if (p2[2] == 0.0f) for (int k = 0; k < 3; ++k) std::swap(p1[k], p2[k]);
+            float pp[3] = {p1[0], p1[1], p1[2]};
+            float ah = INFINITY, ch = INFINITY;
+            // step pp away from p1 until both coefficients are finite numbers
+            // (the reference's loop tests infinities only; pbrt's also NaN)
+            for (int it = 0; it < 64 && !(std::isfinite(ah) && std::isfinite(ch)); ++it) {
+                for (int k = 0; k < 3; ++k) pp[k] = pp[k] + 2.0f * (p2[k] - p1[k]);
+                float xy1 = pp[0] * pp[0] + pp[1] * pp[1];
+                float xy2 = p2[0] * p2[0] + p2[1] * p2[1];
+                ah = (1.0f / xy1 - (pp[2] * pp[2]) / (xy1 * p2[2] * p2[2])) /
+                     (1.0f - (xy2 * pp[2] * pp[2]) / (xy1 * p2[2] * p2[2]));
+                ch = (ah * xy2 - 1.0f) / (p2[2] * p2[2]);
+            }
+            for (int k = 0; k < 3; ++k) { s.aux[k] = p1[k]; s.aux[3 + k] = p2[k]; }
+            s.aux[6] = ah;
+            s.aux[7] = ch;
+            return std::isfinite(ah) && std::isfinite(ch) && s.z_min < s.z_max;
+        }
         default:   // Sphere::new (sphere.rs:50-75)
             s.z_min = clamp(mn, -in.radius, in.radius);
             s.z_max = clamp(mx, -in.radius, in.radius);
             s.theta_min = std::acos(clamp(mn / in.radius, -1.0f, 1.0f));
             s.theta_max = std::acos(clamp(mx / in.radius, -1.0f, 1.0f));
     }
-    return s;
+    return true;
 }
 
 Box sphere_bound(const SphereRec& s) {

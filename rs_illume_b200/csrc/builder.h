@@ -51,7 +51,10 @@ struct SphereInput {
     int32_t reverse;
     int32_t kind = 0;              // kQuadric*
     float height = 0.0f, inner_radius = 0.0f;
+    float p1[3] = {0, 0, 0}, p2[3] = {0, 0, 0};
 };
+// False when a hyperboloid's implicit coefficients do not come out finite.
+bool make_sphere(const SphereInput& in, SphereRec* out);
 SphereRec make_sphere(const SphereInput& in);
 Box sphere_bound(const SphereRec& s);
 

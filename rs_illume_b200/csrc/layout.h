@@ -32,18 +32,23 @@ enum : uint32_t {
 };
 
 // Sphere record (shapes/sphere.rs:15-75) with Sphere::new's derived values.
-// A sphere or another quadric (kind).  z_min / z_max bound the object box in
-// z for every kind; a disk keeps its height in z_min (= z_max) and its inner
-// radius in theta_min, a cone its height in z_max (z_min = 0).
-enum : int32_t { kQuadricSphere = 0, kQuadricDisk = 1, kQuadricCylinder = 2, kQuadricCone = 3 };
+// A sphere or another quadric (kind).  radius and z_min / z_max bound the
+// object box for every kind; a disk keeps its height in z_min (= z_max) and
+// its inner radius in theta_min, a cone its height in z_max (z_min = 0), a
+// hyperboloid its largest radius in radius and p1, p2, ah, ch in aux.
+enum : int32_t {
+    kQuadricSphere = 0, kQuadricDisk = 1, kQuadricCylinder = 2, kQuadricCone = 3,
+    kQuadricParaboloid = 4, kQuadricHyperboloid = 5
+};
 struct SphereRec {
     float o2w[16];
     float w2o[16];
     float radius, z_min, z_max, theta_min, theta_max, phi_max;
     int32_t reverse;
     int32_t kind;
+    float aux[8];
 };
-static_assert(sizeof(SphereRec) == 160, "SphereRec must be 160 bytes");
+static_assert(sizeof(SphereRec) == 192, "SphereRec must be 192 bytes");
 
 // Compressed wide node.  Child boxes are quantised to 8 bits per plane on a
 // per-node grid: plane = fma(q, 2^(e-127), origin), with q rounded outward at

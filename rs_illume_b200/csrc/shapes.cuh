@@ -383,6 +383,92 @@ __device__ __forceinline__ bool cone_test(const SphereRec& s, const ObjRay& r, f
     return true;
 }
 
+// Paraboloid::intersect / intersect_p (paraboloid.rs:95-...):
+// k (x^2 + y^2) = z with k = z_max / r^2, clipped by z and phi (retry with t1).
+// b = k (dx ox + dy oy) * 2 - dz with the 2 exact.
+__device__ __forceinline__ bool paraboloid_test(const SphereRec& s, const ObjRay& r, float tmax, float& t_out,
+                                                float& u_out, float& v_out) {
+    EF eox = ef_new(r.ox, r.oex), eoy = ef_new(r.oy, r.oey), eoz = ef_new(r.oz, r.oez);
+    EF edx = ef_new(r.dx, r.dex), edy = ef_new(r.dy, r.dey), edz = ef_new(r.dz, r.dez);
+    EF rr = EF{s.radius, s.radius, s.radius};
+    EF k = ef_div(EF{s.z_max, s.z_max, s.z_max}, ef_mul(rr, rr));
+    EF a = ef_mul(k, ef_add(ef_mul(edx, edx), ef_mul(edy, edy)));
+    EF b = ef_sub(ef_mul(ef_mul(k, ef_add(ef_mul(edx, eox), ef_mul(edy, eoy))), EF{2.0f, 2.0f, 2.0f}), edz);
+    EF c = ef_sub(ef_mul(k, ef_add(ef_mul(eox, eox), ef_mul(eoy, eoy))), eoz);
+    EF t0, t1, th;
+    if (!ef_quadratic(a, b, c, t0, t1)) return false;
+    if (!nearest_root(t0, t1, tmax, th)) return false;
+    float px, py, pz, phi;
+    auto hit_point = [&](float t) {
+        px = __fadd_rn(r.ox, __fmul_rn(r.dx, t));
+        py = __fadd_rn(r.oy, __fmul_rn(r.dy, t));
+        pz = __fadd_rn(r.oz, __fmul_rn(r.dz, t));
+        phi = phi_of(py, px);
+    };
+    auto clipped = [&]() { return pz < s.z_min || pz > s.z_max || phi > s.phi_max; };
+    hit_point(th.v);
+    if (clipped()) {
+        if (th.v == t1.v) return false;
+        if (t1.hi > tmax) return false;
+        th = t1;
+        hit_point(th.v);
+        if (clipped()) return false;
+    }
+    t_out = th.v;
+    u_out = __fdiv_rn(phi, s.phi_max);
+    v_out = __fdiv_rn(__fsub_rn(pz, s.z_min), __fsub_rn(s.z_max, s.z_min));
+    return true;
+}
+
+// Hyperboloid::intersect / intersect_p (hyperboloid.rs:128-...):
+// ah (x^2 + y^2) - ch z^2 = 1 through p1, p2 (aux[0..5]; ah, ch in aux[6..7]),
+// clipped by z and phi, where phi is the angle between the hit and the swept
+// point at its height.  Repaired as pbrt: c = ah ox^2 + ah oy^2 - ch oz^2 - 1
+// (hyperboloid.rs:149 subtracts oz^2 and ch), and the first phi is
+// atan2(pr.x py - px pr.y, px pr.x + py pr.y) (line 169 applies atan2 to pr.y
+// alone).
+__device__ __forceinline__ bool hyperboloid_test(const SphereRec& s, const ObjRay& r, float tmax, float& t_out,
+                                                 float& u_out, float& v_out) {
+    const float p1x = s.aux[0], p1y = s.aux[1], p1z = s.aux[2], p2x = s.aux[3], p2y = s.aux[4], p2z = s.aux[5];
+    const EF ah = EF{s.aux[6], s.aux[6], s.aux[6]}, ch = EF{s.aux[7], s.aux[7], s.aux[7]};
+    EF eox = ef_new(r.ox, r.oex), eoy = ef_new(r.oy, r.oey), eoz = ef_new(r.oz, r.oez);
+    EF edx = ef_new(r.dx, r.dex), edy = ef_new(r.dy, r.dey), edz = ef_new(r.dz, r.dez);
+    EF a = ef_sub(ef_add(ef_mul(ef_mul(edx, edx), ah), ef_mul(ef_mul(edy, edy), ah)), ef_mul(ef_mul(edz, edz), ch));
+    EF b = ef_mul(EF{2.0f, 2.0f, 2.0f}, ef_sub(ef_add(ef_mul(ef_mul(edx, eox), ah), ef_mul(ef_mul(edy, eoy), ah)),
+                                                 ef_mul(ef_mul(edz, eoz), ch)));
+    EF c = ef_sub(ef_sub(ef_add(ef_mul(ef_mul(eox, eox), ah), ef_mul(ef_mul(eoy, eoy), ah)),
+                         ef_mul(ef_mul(eoz, eoz), ch)),
+                  EF{1.0f, 1.0f, 1.0f});
+    EF t0, t1, th;
+    if (!ef_quadratic(a, b, c, t0, t1)) return false;
+    if (!nearest_root(t0, t1, tmax, th)) return false;
+    float px, py, pz, phi, v;
+    auto hit_point = [&](float t) {
+        px = __fadd_rn(r.ox, __fmul_rn(r.dx, t));
+        py = __fadd_rn(r.oy, __fmul_rn(r.dy, t));
+        pz = __fadd_rn(r.oz, __fmul_rn(r.dz, t));
+        v = __fdiv_rn(__fsub_rn(pz, p1z), __fsub_rn(p2z, p1z));
+        float w = __fsub_rn(1.0f, v);
+        float prx = __fadd_rn(__fmul_rn(p1x, w), __fmul_rn(p2x, v));
+        float pry = __fadd_rn(__fmul_rn(p1y, w), __fmul_rn(p2y, v));
+        phi = phi_of(__fsub_rn(__fmul_rn(prx, py), __fmul_rn(px, pry)),
+                     __fadd_rn(__fmul_rn(px, prx), __fmul_rn(py, pry)));
+    };
+    auto clipped = [&]() { return pz < s.z_min || pz > s.z_max || phi > s.phi_max; };
+    hit_point(th.v);
+    if (clipped()) {
+        if (th.v == t1.v) return false;
+        if (t1.hi > tmax) return false;
+        th = t1;
+        hit_point(th.v);
+        if (clipped()) return false;
+    }
+    t_out = th.v;
+    u_out = __fdiv_rn(phi, s.phi_max);
+    v_out = v;
+    return true;
+}
+
 // The quadric record's test (SphereRec::kind), in its object space.
 static __device__ __noinline__ bool quadric_test(const SphereRec& s, float rox, float roy, float roz, float rdx,
                                                  float rdy, float rdz, float tmax, float& t_out, float& u_out,
@@ -392,6 +478,8 @@ static __device__ __noinline__ bool quadric_test(const SphereRec& s, float rox, 
         case kQuadricDisk: return disk_test(s, r, tmax, t_out, u_out, v_out);
         case kQuadricCylinder: return cylinder_test(s, r, tmax, t_out, u_out, v_out);
         case kQuadricCone: return cone_test(s, r, tmax, t_out, u_out, v_out);
+        case kQuadricParaboloid: return paraboloid_test(s, r, tmax, t_out, u_out, v_out);
+        case kQuadricHyperboloid: return hyperboloid_test(s, r, tmax, t_out, u_out, v_out);
         default: return sphere_test(s, r, tmax, t_out, u_out, v_out);
     }
 }

@@ -143,6 +143,26 @@ def sphere_desc(radius: float, translate=(0.0, 0.0, 0.0), scale: float = 1.0, z_
     return d
 
 
+def quadric_desc(kind, radius: float, matrix, z_min: float = 0.0, z_max: float = 0.0, phi_max_deg: float = 360.0,
+                 height: float = 0.0, inner_radius: float = 0.0, reverse: bool = False, p1=(0.0, 0.0, 0.0),
+                 p2=(0.0, 0.0, 0.0)) -> ilm_sphere_desc:
+    """Arguments of Sphere / Disk / Cylinder / Cone / Paraboloid / Hyperboloid
+    ::new (shapes/*.rs) for any 4x4 object-to-world matrix (its inverse taken
+    in float64).  `kind` is a name of _lib.QUADRICS or its number."""
+    d = ilm_sphere_desc()
+    m = np.asarray(matrix, np.float64).reshape(4, 4)
+    inv = np.linalg.inv(m)
+    for i in range(16):
+        d.object_to_world[i] = float(np.float32(m.flat[i]))
+        d.world_to_object[i] = float(np.float32(inv.flat[i]))
+    d.kind = _lib.QUADRICS[kind] if isinstance(kind, str) else int(kind)
+    d.radius, d.z_min, d.z_max, d.phi_max_deg = radius, z_min, z_max, phi_max_deg
+    d.height, d.inner_radius, d.reverse_orientation = height, inner_radius, int(reverse)
+    for k in range(3):
+        d.p1[k], d.p2[k] = p1[k], p2[k]
+    return d
+
+
 class Spheres:
     """A set of Sphere shapes (shapes/sphere.rs)."""
 

@@ -67,7 +67,7 @@ def test_context_without_device_fails_loudly():
 
 def test_record_layouts():
     assert _lib.RAY_DTYPE.itemsize == 32 and _lib.HIT_DTYPE.itemsize == 16
-    assert ctypes.sizeof(_lib.ilm_sphere_desc) == 160   # sphere fields + kind, height, inner radius
+    assert ctypes.sizeof(_lib.ilm_sphere_desc) == 184   # sphere fields + kind, height, inner radius, p1, p2
     assert ctypes.sizeof(_lib.ilm_config) == 20
     r = rb.rays_array([rb.Ray((1, 2, 3), (0, 0, 1), 5.0)])
     assert r["o"][0].tolist() == [1, 2, 3] and r["tmax"][0] == 5.0
