@@ -28,6 +28,7 @@
 #ifndef ILLUME_GPU_H
 #define ILLUME_GPU_H
 
+#include <stddef.h>
 #include <stdint.h>
 
 #ifdef __cplusplus
@@ -354,9 +355,11 @@ typedef struct {
     const float* emission;          /* emitted radiance along the triangle normal
                                        normalize((p0-p2) x (p1-p2)), 3 per material */
     uint32_t n_materials;
-    float eye[3];                   /* pinhole camera at eye, looking +z, up +y */
+    float eye[3];                   /* pinhole camera at eye, looking +z, up +y (in camera space) */
     float fov_deg;                  /* vertical field of view */
     uint32_t width, height;
+    float camera_to_world[9];       /* row-major 3x3 taking camera-space directions to world space
+                                       (a LookAt frame, possibly mirrored); all zero = identity */
 } ilm_pt_scene_desc;
 
 typedef struct {
@@ -476,6 +479,75 @@ int32_t ilm_read_pfm(const char* path, float* rgb, uint32_t* width, uint32_t* he
 /* One filter value at film offset (x, y) from the sample. */
 int32_t ilm_filter_evaluate(const ilm_filter_desc* filter, float x, float y, float* out);
 int32_t ilm_filter_table(const ilm_filter_desc* filter, float* table /* 16 x 16 */);
+
+/* ------------------------------------------------------ scene files (host) */
+/* pbrt-v3 scene files, the format whose syntax tree core/parser/ast.rs
+ * defines (the reference parses to that tree and constructs no scene,
+ * core/parser/mod.rs:36-46; its parser module is missing).  Loading runs the
+ * directives against pbrt's graphics state -- the current transform and its
+ * named copies, AttributeBegin/End and TransformBegin/End stacks, materials,
+ * area lights, ReverseOrientation, object instancing, Include -- and keeps:
+ *  - Shape "trianglemesh" (P, indices, N, S, uv/st) with world-space vertices;
+ *    a shape whose orientation is reversed (ReverseOrientation, or a
+ *    transform that swaps handedness) has its triangles' last two indices
+ *    swapped, so (p0-p2)x(p1-p2) is the normal pbrt's Triangle reports;
+ *  - Shape "sphere", "disk", "cylinder", "cone", "paraboloid", "hyperboloid"
+ *    with their pbrt parameters and defaults, under the current transform;
+ *  - Material "matte" Kd (other types: their Kd, else 0.5, with a warning),
+ *    MakeNamedMaterial / NamedMaterial, AreaLightSource "diffuse" L x scale;
+ *  - Camera "perspective" fov (of the shorter image axis) under LookAt or any
+ *    transform, Film xresolution / yresolution, Sampler pixelsamples (or
+ *    xsamples x ysamples; rounded up to a square), Integrator maxdepth,
+ *    PixelFilter box / triangle / gaussian / mitchell / sinc, Accelerator
+ *    "bvh" maxnodeprims or "kdtree" with its costs.
+ * Directives this library cannot represent (point / spot / distant /
+ * infinite lights, textures, media, plymesh, curves, other cameras) are
+ * skipped with a warning.  Syntax errors fail with a "file:line: message". */
+typedef struct ilm_scene_file ilm_scene_file;
+typedef struct {
+    uint32_t n_meshes, n_triangles, n_vertices, n_quadrics;
+    uint32_t n_materials;      /* distinct (albedo, emission) pairs */
+    uint32_t n_emissive;       /* triangles under an area light */
+    uint32_t width, height;    /* Film */
+    uint32_t spp;              /* Sampler, a perfect square */
+    uint32_t max_depth;        /* Integrator "path" maxdepth (pbrt default 5) */
+    float eye[3];              /* camera position */
+    float camera_to_world[9];  /* row-major 3x3 */
+    float fov_deg;             /* vertical field of view for ilm_pt_scene_desc */
+    ilm_filter_desc filter;
+    int32_t accelerator;       /* 0 = "bvh", 1 = "kdtree" */
+    ilm_build_opts bvh;
+    ilm_kdtree_opts kdtree;
+    uint32_t n_warnings;
+} ilm_scene_file_info;
+/* Loads `path`; on failure *out is NULL and `error` (error_len bytes, may be
+ * NULL) holds the message. */
+int32_t ilm_scene_file_load(const char* path, char* error, size_t error_len, ilm_scene_file** out);
+/* The same from text in memory; Include paths are relative to base_dir. */
+int32_t ilm_scene_file_parse(const char* text, const char* base_dir, char* error, size_t error_len,
+                             ilm_scene_file** out);
+int32_t ilm_scene_file_info_get(const ilm_scene_file* sf, ilm_scene_file_info* out);
+/* Warnings, one per line (valid until the scene file is destroyed). */
+const char* ilm_scene_file_warnings(const ilm_scene_file* sf);
+/* Triangle mesh k: vertex count and triangle count (nv, nt may be NULL), and
+ * copies of its arrays into any non-NULL output: xyz (3 nv), idx (3 nt),
+ * n / s (3 nv; *has_n / *has_s say whether the file gave them), uv (2 nv;
+ * *has_uv), material (the mesh's material index). */
+int32_t ilm_scene_file_mesh(const ilm_scene_file* sf, uint32_t k, uint32_t* nv, uint32_t* nt, float* xyz,
+                            uint32_t* idx, float* n, float* s, float* uv, int32_t* has_n, int32_t* has_s,
+                            int32_t* has_uv, uint32_t* material);
+/* The quadrics (n_quadrics descriptions) and their material indices. */
+int32_t ilm_scene_file_quadrics(const ilm_scene_file* sf, ilm_sphere_desc* out, uint32_t* material);
+/* The material table: albedo and emission, 3 floats each per material. */
+int32_t ilm_scene_file_materials(const ilm_scene_file* sf, float* albedo, float* emission);
+/* Uploads the shapes to ctx (one mesh per trianglemesh, with its N / S / uv,
+ * then one quadric set) and builds the accelerator the file names.
+ * Primitive ids run over the meshes in file order, then the quadrics.  With
+ * pt_out non-NULL and triangles only, also creates the path-tracing scene
+ * (camera, film size, materials); with quadrics present *pt_out is 0. */
+int32_t ilm_scene_file_build(ilm_context* ctx, const ilm_scene_file* sf, ilm_accel_id* accel_out,
+                             ilm_pt_scene_id* pt_out);
+int32_t ilm_scene_file_destroy(ilm_scene_file* sf);
 
 /* Device error word accumulated by the kernels since the last reset
  * (bit 0: traversal stack overflow, bit 1: iteration cap).  Synchronises. */

@@ -58,7 +58,7 @@ _SIG = {
     "orc_render_pt_filtered": (ctypes.c_int, [_P, _P, _P, ctypes.c_uint32, _P, _P, _P, _P, ctypes.c_float,
                                               ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32,
                                               ctypes.c_uint32, ctypes.c_uint64, _P, ctypes.c_float, ctypes.c_float,
-                                              ctypes.c_int, _P, _P]),
+                                              ctypes.c_int, _P, _P, _P]),
     "orc_sphere_intersect": (ctypes.c_int, [_P, _P, ctypes.c_int, _P]),
     "orc_sphere_world_bound": (None, [_P, _P]),
     "orc_last_trace_seconds": (ctypes.c_double, []),
@@ -279,7 +279,7 @@ def render_pt(scene: "Scene", xyz, idx, mat, albedo, emission, eye, fov_deg, wid
 
 
 def render_pt_filtered(scene: "Scene", xyz, idx, mat, albedo, emission, eye, fov_deg, width, height, spp,
-                       table, radius, max_depth=8, rr_depth=3, seed=3, threads=0):
+                       table, radius, max_depth=8, rr_depth=3, seed=3, threads=0, camera_to_world=None):
     """Full-frame render through a filtered film (16 x 16 weight table,
     radius (rx, ry)).  Returns (rgb[h, w, 3], (closest rays, shadow rays))."""
     xyz = np.ascontiguousarray(xyz, np.float32)
@@ -291,9 +291,10 @@ def render_pt_filtered(scene: "Scene", xyz, idx, mat, albedo, emission, eye, fov
     table = np.ascontiguousarray(table, np.float32)
     out = np.zeros((height, width, 3), np.float32)
     counts = np.zeros(2, np.uint64)
+    cam = None if camera_to_world is None else np.ascontiguousarray(camera_to_world, np.float32).reshape(9)
     st = load().orc_render_pt_filtered(scene.h, _p(xyz), _p(idx), len(idx.reshape(-1, 3)), _p(mat), _p(albedo),
                                        _p(emission), _p(eye), fov_deg, width, height, spp, max_depth, rr_depth, seed,
-                                       _p(table), radius[0], radius[1], threads, _p(out), _p(counts))
+                                       _p(table), radius[0], radius[1], threads, _p(out), _p(counts), _p(cam))
     assert st == 0
     return out, (int(counts[0]), int(counts[1]))
 

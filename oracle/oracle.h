@@ -109,12 +109,15 @@ int orc_surface_interaction(const float* p, const float* n, const float* s, cons
                             const orc_ray* r, orc_si* out);
 /* Full-frame render through a filtered film: each sample's L is splatted
  * with the 16 x 16 filter table (table[y*16 + x], radius rx, ry) as
- * FilmTile::add_sample does (film.rs:288-333, D20 repaired). */
+ * FilmTile::add_sample does (film.rs:288-333, D20 repaired).  camera_to_world
+ * (row-major 3x3, may be NULL) turns the camera-space direction into world
+ * space. */
 int orc_render_pt_filtered(void* scene, const float* verts, const uint32_t* idx, uint32_t nt,
                            const uint32_t* prim_material, const float* albedo, const float* emission,
                            const float eye[3], float fov_deg, uint32_t width, uint32_t height, uint32_t spp,
                            uint32_t max_depth, uint32_t rr_depth, uint64_t seed, const float* table, float rx,
-                           float ry, int nthreads, float* rgb_out, uint64_t* ray_counts);
+                           float ry, int nthreads, float* rgb_out, uint64_t* ray_counts,
+                           const float* camera_to_world);
 /* out = {t, u, v}. */
 int orc_sphere_intersect(const orc_sphere_desc* s, const orc_ray* r, int closest, float* out);
 void orc_sphere_world_bound(const orc_sphere_desc* s, float out[6]);

@@ -352,7 +352,7 @@ extern "C" int orc_render_pt_filtered(void* scene, const float* verts, const uin
                                       const float eye[3], float fov_deg, uint32_t width, uint32_t height,
                                       uint32_t spp, uint32_t max_depth, uint32_t rr_depth, uint64_t seed,
                                       const float* table, float rx, float ry, int nthreads, float* rgb_out,
-                                      uint64_t* ray_counts) {
+                                      uint64_t* ray_counts, const float* camera_to_world) {
     uint32_t ns = (uint32_t)std::lround(std::sqrt((double)spp));
     if (ns * ns != spp || width == 0 || height == 0 || !(rx > 0.0f) || !(ry > 0.0f)) return -1;
     PtScene s;
@@ -391,6 +391,11 @@ extern "C" int orc_render_pt_filtered(void* scene, const float* verts, const uin
                     float sx = (fx / (float)width * 2.0f - 1.0f) * th * aspect;
                     float sy = (1.0f - fy / (float)height * 2.0f) * th;
                     V d = normalize(V{sx, sy, 1.0f});
+                    if (camera_to_world) {   // camera-space direction to world space
+                        const float* m = camera_to_world;
+                        d = V{m[0] * d.x + m[1] * d.y + m[2] * d.z, m[3] * d.x + m[4] * d.y + m[5] * d.z,
+                              m[6] * d.x + m[7] * d.y + m[8] * d.z};
+                    }
                     RGB L = li(s, V{eye[0], eye[1], eye[2]}, d, rng, max_depth, rr_depth, cnt);
                     if (std::isnan(L.r) || std::isnan(L.g) || std::isnan(L.b) || luminance(L) < -1e-5f ||
                         std::isinf(luminance(L)))

@@ -98,12 +98,21 @@ QUADRICS = {"sphere": 0, "disk": 1, "cylinder": 2, "cone": 3, "paraboloid": 4, "
 class ilm_pt_scene_desc(ctypes.Structure):
     _fields_ = [("prim_material", ctypes.c_void_p), ("albedo", ctypes.c_void_p), ("emission", ctypes.c_void_p),
                 ("n_materials", ctypes.c_uint32), ("eye", ctypes.c_float * 3), ("fov_deg", ctypes.c_float),
-                ("width", ctypes.c_uint32), ("height", ctypes.c_uint32)]
+                ("width", ctypes.c_uint32), ("height", ctypes.c_uint32), ("camera_to_world", ctypes.c_float * 9)]
 
 
 class ilm_filter_desc(ctypes.Structure):
     _fields_ = [("kind", ctypes.c_int32), ("radius", ctypes.c_float * 2), ("a", ctypes.c_float),
                 ("b", ctypes.c_float)]
+
+
+class ilm_scene_file_info(ctypes.Structure):
+    _fields_ = [("n_meshes", ctypes.c_uint32), ("n_triangles", ctypes.c_uint32), ("n_vertices", ctypes.c_uint32),
+                ("n_quadrics", ctypes.c_uint32), ("n_materials", ctypes.c_uint32), ("n_emissive", ctypes.c_uint32),
+                ("width", ctypes.c_uint32), ("height", ctypes.c_uint32), ("spp", ctypes.c_uint32),
+                ("max_depth", ctypes.c_uint32), ("eye", ctypes.c_float * 3), ("camera_to_world", ctypes.c_float * 9),
+                ("fov_deg", ctypes.c_float), ("filter", ilm_filter_desc), ("accelerator", ctypes.c_int32),
+                ("bvh", ilm_build_opts), ("kdtree", ilm_kdtree_opts), ("n_warnings", ctypes.c_uint32)]
 
 
 class ilm_pt_opts(ctypes.Structure):
@@ -180,6 +189,16 @@ SIGNATURES = {
     "ilm_host_kdtree_build": (_I32, [_P, _U32, _P, _U32, _P, _U32, ctypes.POINTER(ilm_kdtree_opts), _I32,
                                      ctypes.POINTER(_P)]),
     "ilm_host_layout_kd_index": (_I32, [_P, _P]),
+    "ilm_scene_file_load": (_I32, [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_size_t, ctypes.POINTER(_P)]),
+    "ilm_scene_file_parse": (_I32, [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_size_t,
+                                    ctypes.POINTER(_P)]),
+    "ilm_scene_file_info_get": (_I32, [_P, ctypes.POINTER(ilm_scene_file_info)]),
+    "ilm_scene_file_warnings": (ctypes.c_char_p, [_P]),
+    "ilm_scene_file_mesh": (_I32, [_P, _U32, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
+    "ilm_scene_file_quadrics": (_I32, [_P, _P, _P]),
+    "ilm_scene_file_materials": (_I32, [_P, _P, _P]),
+    "ilm_scene_file_build": (_I32, [_P, _P, ctypes.POINTER(_U32), ctypes.POINTER(_U32)]),
+    "ilm_scene_file_destroy": (_I32, [_P]),
     "ilm_intersect_closest": (_I32, [_P, _U32, _P, _U64, _P, _P]),
     "ilm_intersect_any": (_I32, [_P, _U32, _P, _U64, _P, _P]),
     "ilm_intersect_closest_noalloc": (_I32, [_P, _U32, _P, _U64, _P, _P]),

@@ -35,6 +35,7 @@
 // batch and the network takes one training step on the recorded vertices.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <memory>
@@ -77,6 +78,7 @@ struct PtArgs {
     int fbox;                 // 1: box of radius 0.5, each sample to its own pixel with weight 1
     uint32_t width, height, npix, spp, ns;
     float eye_x, eye_y, eye_z, tan_half, aspect;
+    float cam[9];                  // camera-to-world 3x3, row-major
     uint32_t max_depth, rr_depth;
     unsigned long long seed;
     ilm_ray* rays[2];
@@ -274,7 +276,11 @@ __global__ void k_pt_camera(PtArgs a, unsigned long long p0, uint32_t count) {
     float fy = (float)py + ((float)(sample / a.ns) + jy) / (float)a.ns;
     float sx = (fx / (float)a.width * 2.0f - 1.0f) * a.tan_half * a.aspect;
     float sy = (1.0f - fy / (float)a.height * 2.0f) * a.tan_half;
-    float3 d = normalize3(make_float3(sx, sy, 1.0f));
+    float3 c = normalize3(make_float3(sx, sy, 1.0f));
+    // camera-to-world (exact for the identity: 1*x + 0*y + 0*z == x)
+    float3 d = make_float3(__fadd_rn(__fadd_rn(__fmul_rn(a.cam[0], c.x), __fmul_rn(a.cam[1], c.y)), __fmul_rn(a.cam[2], c.z)),
+                           __fadd_rn(__fadd_rn(__fmul_rn(a.cam[3], c.x), __fmul_rn(a.cam[4], c.y)), __fmul_rn(a.cam[5], c.z)),
+                           __fadd_rn(__fadd_rn(__fmul_rn(a.cam[6], c.x), __fmul_rn(a.cam[7], c.y)), __fmul_rn(a.cam[8], c.z)));
     put_ray(a.rays[0], k, make_float3(a.eye_x, a.eye_y, a.eye_z), d, INFINITY);
     a.beta[0][k] = make_float4(1.0f, 1.0f, 1.0f, __uint_as_float(id));
     if (!a.fbox) splat(a, fx, fy, make_float3(0.0f, 0.0f, 0.0f), true);   // the sample's filter weights
@@ -684,6 +690,9 @@ int32_t setup_render(ilm_context* ctx, PtScene& sc, uint32_t spp, uint32_t max_d
     a.eye_x = d.eye[0]; a.eye_y = d.eye[1]; a.eye_z = d.eye[2];
     a.tan_half = std::tan(0.5f * d.fov_deg * 3.14159265358979323846f / 180.0f);
     a.aspect = (float)d.width / (float)d.height;
+    bool zero = true;
+    for (int q = 0; q < 9; ++q) zero = zero && d.camera_to_world[q] == 0.0f;
+    for (int q = 0; q < 9; ++q) a.cam[q] = zero ? (q % 4 == 0 ? 1.0f : 0.0f) : d.camera_to_world[q];
     a.max_depth = max_depth; a.rr_depth = rr_depth; a.seed = seed;
     for (int q = 0; q < 2; ++q) {
         a.rays[q] = static_cast<ilm_ray*>(b.rays[q].ptr);
@@ -769,7 +778,8 @@ int32_t ilm_pt_scene_create(ilm_context* ctx, ilm_accel_id accel, const ilm_pt_s
     if (!acc) { set_error(ctx, "ilm_pt_scene_create: unknown accel id"); return ILM_ERR_NOT_FOUND; }
     const HostLayout& h = acc->host;
     if (!desc->prim_material || !desc->albedo || !desc->emission || desc->n_materials == 0 || desc->width == 0 ||
-        desc->height == 0 || !(desc->fov_deg > 0.0f && desc->fov_deg < 180.0f)) {
+        desc->height == 0 || !(desc->fov_deg > 0.0f && desc->fov_deg < 180.0f) ||
+        !std::all_of(desc->camera_to_world, desc->camera_to_world + 9, [](float v) { return std::isfinite(v); })) {
         set_error(ctx, "ilm_pt_scene_create: invalid scene description");
         return ILM_ERR_INVALID_ARGUMENT;
     }

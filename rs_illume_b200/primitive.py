@@ -310,10 +310,12 @@ class GpuKdTreeAccel(GpuBVHAccel):
 class PathTracer:
     """Wavefront path tracer over a triangle GpuBVHAccel (ilm_pt_scene_create /
     ilm_render_pt): Lambertian materials, one-sided diffuse emitters, a pinhole
-    camera looking +z."""
+    camera looking +z in its own frame (camera_to_world places it)."""
 
     def __init__(self, accel: GpuBVHAccel, prim_material, albedo, emission, eye, fov_deg: float, width: int,
-                 height: int):
+                 height: int, camera_to_world=None):
+        """camera_to_world: 3x3 taking camera-space directions (looking +z,
+        up +y) to world space; None = identity."""
         self.accel = accel
         ctx = accel.ctx
         self._mat = np.ascontiguousarray(prim_material, np.uint32)
@@ -328,6 +330,9 @@ class PathTracer:
             d.eye[k] = eye[k]
         d.fov_deg = fov_deg
         d.width, d.height = width, height
+        if camera_to_world is not None:
+            for k, v in enumerate(np.asarray(camera_to_world, np.float32).reshape(9)):
+                d.camera_to_world[k] = float(v)
         sid = ctypes.c_uint32()
         ctx.check(ctx._lib.ilm_pt_scene_create(ctx.handle, accel.id, ctypes.byref(d), ctypes.byref(sid)),
                   "ilm_pt_scene_create")
