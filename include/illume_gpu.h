@@ -142,6 +142,12 @@ int32_t ilm_context_create(ilm_context** out, const ilm_config* cfg);
 int32_t ilm_context_destroy(ilm_context* ctx);
 /* Last error message on ctx (static string for ctx == NULL). Never NULL. */
 const char* ilm_last_error_string(const ilm_context* ctx);
+/* Rays per chunk when host ray / result buffers are copied through device
+ * staging: copy-in and copy-out run on their own streams (the host link
+ * carries both directions at once) and a ring of four slots traces on four
+ * streams; the first and last chunks ramp from chunk/8.  4096 .. 2^24,
+ * default 524288. */
+int32_t ilm_context_set_stage_chunk(ilm_context* ctx, uint64_t rays);
 
 /* ----------------------------------------------------------------- shapes */
 /* TriangleMesh::new (shapes/triangle.rs:36-73) with world-space vertices:

@@ -170,6 +170,7 @@ SIGNATURES = {
     "ilm_context_create": (_I32, [ctypes.POINTER(_P), ctypes.POINTER(ilm_config)]),
     "ilm_context_destroy": (_I32, [_P]),
     "ilm_last_error_string": (ctypes.c_char_p, [_P]),
+    "ilm_context_set_stage_chunk": (_I32, [_P, _U64]),
     "ilm_mesh_upload": (_I32, [_P, _P, _U32, _P, _U32, ctypes.POINTER(_U32)]),
     "ilm_spheres_upload": (_I32, [_P, _P, _U32, ctypes.POINTER(_U32)]),
     "ilm_mesh_set_attrs": (_I32, [_P, _U32, ctypes.POINTER(ilm_mesh_attrs)]),

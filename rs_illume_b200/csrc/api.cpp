@@ -3,6 +3,7 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -42,6 +43,31 @@ cudaError_t DeviceBuffer::reserve(size_t n) {
     cudaError_t e = cudaMalloc(&ptr, n);
     if (e == cudaSuccess) bytes = n;
     return e;
+}
+
+std::vector<uint64_t> stage_plan(uint64_t n, uint64_t c) {
+    std::vector<uint64_t> plan;
+    const uint64_t ramp = c / 8 + c / 4 + c / 2;
+    if (n < 2 * ramp + c) {
+        // equal chunks, at least four when the batch allows
+        uint64_t k = std::max<uint64_t>(1, std::min<uint64_t>(4, (n + 4095) / 4096));
+        k = std::max(k, (n + c - 1) / c);
+        for (uint64_t off = 0, i = 0; i < k; ++i) {
+            uint64_t cnt = (n - off) / (k - i);
+            plan.push_back(cnt);
+            off += cnt;
+        }
+        return plan;
+    }
+    for (uint64_t d : {c / 8, c / 4, c / 2}) plan.push_back(d);
+    uint64_t middle = n - 2 * ramp, k = (middle + c - 1) / c;
+    for (uint64_t off = 0, i = 0; i < k; ++i) {
+        uint64_t cnt = (middle - off) / (k - i);
+        plan.push_back(cnt);
+        off += cnt;
+    }
+    for (uint64_t d : {c / 2, c / 4, c / 8}) plan.push_back(d);
+    return plan;
 }
 
 PtrKind classify(const void* p) {
@@ -108,9 +134,26 @@ int32_t ilm_context_create(ilm_context** out, const ilm_config* cfg) {
     for (auto& s : ctx->pipe)
         if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) return ILM_ERR_CUDA;
     if (cudaEventCreateWithFlags(&ctx->fence, cudaEventDisableTiming) != cudaSuccess) return ILM_ERR_CUDA;
+    for (auto& st : ctx->stage) {
+        if (cudaStreamCreateWithFlags(&st.run, cudaStreamNonBlocking) != cudaSuccess) return ILM_ERR_CUDA;
+        for (cudaEvent_t* e : {&st.in, &st.ran, &st.out_done})
+            if (cudaEventCreateWithFlags(e, cudaEventDisableTiming) != cudaSuccess) return ILM_ERR_CUDA;
+    }
     if (ctx->err_word.reserve(sizeof(uint32_t)) != cudaSuccess) return ILM_ERR_OUT_OF_MEMORY;
     if (cudaMemset(ctx->err_word.ptr, 0, sizeof(uint32_t)) != cudaSuccess) return ILM_ERR_CUDA;
     *out = ctx.release();
+    return ILM_OK;
+}
+
+int32_t ilm_context_set_stage_chunk(ilm_context* ctx, uint64_t rays) {
+    ILM_CHECK_CTX(ctx);
+    if (rays < 4096 || rays > (1ull << 24)) {
+        set_error(ctx, "ilm_context_set_stage_chunk: chunk must be 4096 .. 2^24 rays");
+        return ILM_ERR_INVALID_ARGUMENT;
+    }
+    cudaError_t e = cudaDeviceSynchronize();   // no staging buffer may be in use
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaDeviceSynchronize");
+    ctx->stage_chunk = rays;
     return ILM_OK;
 }
 
@@ -120,7 +163,12 @@ int32_t ilm_context_destroy(ilm_context* ctx) {
     cudaDeviceSynchronize();
     ctx->pt_scenes.clear();
     ctx->accels.clear();
-    for (auto& st : ctx->stage) { st.rays.release(); st.out.release(); }
+    for (auto& st : ctx->stage) {
+        st.rays.release();
+        st.out.release();
+        for (cudaEvent_t e : {st.in, st.ran, st.out_done}) if (e) cudaEventDestroy(e);
+        if (st.run) cudaStreamDestroy(st.run);
+    }
     ctx->err_word.release();
     ctx->scratch_release();
     if (ctx->fence) cudaEventDestroy(ctx->fence);
@@ -436,36 +484,50 @@ static int32_t intersect_impl(ilm_context* ctx, ilm_accel_id accel, const ilm_ra
             }
         }
     }
-    // Host buffers: pipelined chunks over three streams (copy-in, trace,
-    // copy-out of consecutive chunks overlap).
-    const uint64_t chunk = ctx->stage_chunk;
+    // Host buffers: chunks staged through a ring of device slots.  Copy-in and
+    // copy-out have a stream each, so the host link carries rays in and
+    // results out at once; each slot traces on its own stream, so traces of
+    // consecutive chunks overlap.  A slot is refilled once its trace (rays)
+    // and copy-out (results) are done.
     const size_t out_rec = occ ? sizeof(uint32_t) : sizeof(ilm_hit);
+    const std::vector<uint64_t> plan = stage_plan(n, ctx->stage_chunk);
+    const uint64_t biggest = *std::max_element(plan.begin(), plan.end());
     for (auto& st : ctx->stage) {
-        ILM_CUDA(ctx, st.rays.reserve(chunk * sizeof(ilm_ray)), "cudaMalloc(stage rays)");
-        ILM_CUDA(ctx, st.out.reserve(chunk * sizeof(ilm_hit)), "cudaMalloc(stage out)");
+        ILM_CUDA(ctx, st.rays.reserve(biggest * sizeof(ilm_ray)), "cudaMalloc(stage rays)");
+        ILM_CUDA(ctx, st.out.reserve(biggest * sizeof(ilm_hit)), "cudaMalloc(stage out)");
     }
+    cudaStream_t in_s = ctx->pipe[0], out_s = ctx->pipe[1];
     ILM_CUDA(ctx, cudaEventRecord(ctx->fence, user), "cudaEventRecord");
     for (auto& s : ctx->pipe) ILM_CUDA(ctx, cudaStreamWaitEvent(s, ctx->fence, 0), "cudaStreamWaitEvent");
-    uint64_t c = 0;
-    for (uint64_t off = 0; off < n; off += chunk, ++c) {
-        uint64_t cnt = n - off < chunk ? n - off : chunk;
-        int slot = (int)(c % kPipeDepth);
-        cudaStream_t s = ctx->pipe[slot];
-        Stage& st = ctx->stage[slot];
-        ILM_CUDA(ctx, cudaMemcpyAsync(st.rays.ptr, rays + off, cnt * sizeof(ilm_ray), cudaMemcpyHostToDevice, s),
+    for (auto& st : ctx->stage) ILM_CUDA(ctx, cudaStreamWaitEvent(st.run, ctx->fence, 0), "cudaStreamWaitEvent");
+    uint64_t off = 0;
+    for (size_t c = 0; c < plan.size(); ++c) {
+        const uint64_t cnt = plan[c];
+        Stage& st = ctx->stage[c % kStageSlots];
+        const bool reused = c >= (size_t)kStageSlots;
+        if (reused) ILM_CUDA(ctx, cudaStreamWaitEvent(in_s, st.ran, 0), "cudaStreamWaitEvent");
+        ILM_CUDA(ctx, cudaMemcpyAsync(st.rays.ptr, rays + off, cnt * sizeof(ilm_ray), cudaMemcpyHostToDevice, in_s),
                  "cudaMemcpyAsync(rays)");
-        lp.counter = counter(s);
+        ILM_CUDA(ctx, cudaEventRecord(st.in, in_s), "cudaEventRecord");
+        ILM_CUDA(ctx, cudaStreamWaitEvent(st.run, st.in, 0), "cudaStreamWaitEvent");
+        if (reused) ILM_CUDA(ctx, cudaStreamWaitEvent(st.run, st.out_done, 0), "cudaStreamWaitEvent");
+        lp.counter = counter(st.run);
         if (persistent && !lp.counter) return ILM_ERR_OUT_OF_MEMORY;
         ILM_CUDA(ctx,
                  launch_trace(da, static_cast<const ilm_ray*>(st.rays.ptr), cnt,
                               occ ? nullptr : static_cast<ilm_hit*>(st.out.ptr),
-                              occ ? static_cast<uint32_t*>(st.out.ptr) : nullptr, err, lp, s),
+                              occ ? static_cast<uint32_t*>(st.out.ptr) : nullptr, err, lp, st.run),
                  "trace launch");
+        ILM_CUDA(ctx, cudaEventRecord(st.ran, st.run), "cudaEventRecord");
+        ILM_CUDA(ctx, cudaStreamWaitEvent(out_s, st.ran, 0), "cudaStreamWaitEvent");
         void* dst = occ ? (void*)(occ + off) : (void*)(hits + off);
-        ILM_CUDA(ctx, cudaMemcpyAsync(dst, st.out.ptr, cnt * out_rec, cudaMemcpyDeviceToHost, s),
+        ILM_CUDA(ctx, cudaMemcpyAsync(dst, st.out.ptr, cnt * out_rec, cudaMemcpyDeviceToHost, out_s),
                  "cudaMemcpyAsync(results)");
+        ILM_CUDA(ctx, cudaEventRecord(st.out_done, out_s), "cudaEventRecord");
+        off += cnt;
     }
     for (auto& s : ctx->pipe) ILM_CUDA(ctx, cudaStreamSynchronize(s), "cudaStreamSynchronize");
+    for (auto& st : ctx->stage) ILM_CUDA(ctx, cudaStreamSynchronize(st.run), "cudaStreamSynchronize");
     return ILM_OK;
 }
 

@@ -77,11 +77,23 @@ struct Accel {
     }
 };
 
-constexpr int kPipeDepth = 3;
+// Host-buffer queries: a copy-in and a copy-out stream and a ring of staging
+// slots, each with its own trace stream (traces of consecutive chunks overlap,
+// since a small trace lasts as long as its slowest ray) and the events that
+// hand the slot from one stream to the next.
+constexpr int kPipeStreams = 2;
+constexpr int kStageSlots = 4;
 
 struct Stage {
     DeviceBuffer rays, out;
+    cudaStream_t run = nullptr;
+    cudaEvent_t in = nullptr, ran = nullptr, out_done = nullptr;
 };
+
+// Chunk sizes for n rays with a steady chunk of c: the first and last chunks
+// ramp (c/8, c/4, c/2) so the copy-in of the first chunk and the trace and
+// copy-out of the last one are short; small batches use equal chunks.
+std::vector<uint64_t> stage_plan(uint64_t n, uint64_t c);
 
 enum class PtrKind { kHost, kDevice };
 
@@ -96,10 +108,10 @@ struct ilm_context {
     int flags = 0;
     uint32_t max_iter = 1u << 20;
     cudaStream_t stream = nullptr;
-    cudaStream_t pipe[ilm::kPipeDepth] = {nullptr, nullptr, nullptr};
+    cudaStream_t pipe[ilm::kPipeStreams] = {nullptr, nullptr};
     cudaEvent_t fence = nullptr;
-    ilm::Stage stage[ilm::kPipeDepth];
-    uint64_t stage_chunk = 1ull << 18;
+    ilm::Stage stage[ilm::kStageSlots];
+    uint64_t stage_chunk = 1ull << 19;
     ilm::DeviceBuffer err_word;
     std::string last_error;
     std::map<ilm_mesh_id, std::unique_ptr<ilm::Mesh>> meshes;
