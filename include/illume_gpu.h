@@ -499,6 +499,8 @@ int32_t ilm_filter_table(const ilm_filter_desc* filter, float* table /* 16 x 16 
  *    swapped, so (p0-p2)x(p1-p2) is the normal pbrt's Triangle reports;
  *  - Shape "sphere", "disk", "cylinder", "cone", "paraboloid", "hyperboloid"
  *    with their pbrt parameters and defaults, under the current transform;
+ *  - Shape "loopsubdiv" (levels, indices, P) as the subdivided triangle mesh
+ *    with its limit normals;
  *  - Material "matte" Kd (other types: their Kd, else 0.5, with a warning),
  *    MakeNamedMaterial / NamedMaterial, AreaLightSource "diffuse" L x scale;
  *  - Camera "perspective" fov (of the shorter image axis) under LookAt or any
@@ -509,6 +511,16 @@ int32_t ilm_filter_table(const ilm_filter_desc* filter, float* table /* 16 x 16 
  * Directives this library cannot represent (point / spot / distant /
  * infinite lights, textures, media, plymesh, curves, other cameras) are
  * skipped with a warning.  Syntax errors fail with a "file:line: message". */
+/* Loop subdivision surface (shapes/loop_subdiv.rs, pbrt-v3's LoopSubdivide):
+ * `levels` (0 .. 10) refinements of a triangle mesh by Loop's vertex and edge
+ * rules, vertices then moved to the limit surface, with limit normals.  Call
+ * with out_xyz == NULL to get *out_nv and *out_nt; call again with those
+ * counts in *out_nv / *out_nt and buffers of 3 * nv floats (out_xyz, out_n,
+ * out_n may be NULL) and 3 * nt indices.  Non-manifold input or buffers
+ * smaller than the result fail with ILM_ERR_INVALID_ARGUMENT. */
+int32_t ilm_loop_subdivide(const float* xyz, uint32_t nv, const uint32_t* idx, uint32_t nt, uint32_t levels,
+                           uint32_t* out_nv, uint32_t* out_nt, float* out_xyz, uint32_t* out_idx, float* out_n);
+
 typedef struct ilm_scene_file ilm_scene_file;
 typedef struct {
     uint32_t n_meshes, n_triangles, n_vertices, n_quadrics;

@@ -8,12 +8,12 @@ aggregate interface on top of that ABI.
 from ._lib import (HIT_DTYPE, ILM_MISS, ILM_TRAVERSAL_ERROR, RAY_DTYPE, IllumeError, LIB_PATH, load)
 from .image import filter_desc, filter_table, read_pfm, write_pfm
 from .primitive import (Bounds3f, Context, GpuBVHAccel, GpuKdTreeAccel, Hit, PathTracer, Ray, Scene, Spheres,
-                        TriangleMesh, quadric_desc, rays_array, sphere_desc)
+                        TriangleMesh, loop_subdivide, quadric_desc, rays_array, sphere_desc)
 from .scene_file import SceneFile
 
 __all__ = [
     "HIT_DTYPE", "ILM_MISS", "ILM_TRAVERSAL_ERROR", "RAY_DTYPE", "IllumeError", "LIB_PATH", "load",
     "Bounds3f", "Context", "GpuBVHAccel", "GpuKdTreeAccel", "Hit", "PathTracer", "Ray", "Scene", "Spheres",
     "TriangleMesh", "rays_array",
-    "SceneFile", "sphere_desc", "quadric_desc", "filter_desc", "filter_table", "read_pfm", "write_pfm",
+    "SceneFile", "loop_subdivide", "sphere_desc", "quadric_desc", "filter_desc", "filter_table", "read_pfm", "write_pfm",
 ]

@@ -190,6 +190,7 @@ SIGNATURES = {
     "ilm_host_kdtree_build": (_I32, [_P, _U32, _P, _U32, _P, _U32, ctypes.POINTER(ilm_kdtree_opts), _I32,
                                      ctypes.POINTER(_P)]),
     "ilm_host_layout_kd_index": (_I32, [_P, _P]),
+    "ilm_loop_subdivide": (_I32, [_P, _U32, _P, _U32, _U32, ctypes.POINTER(_U32), ctypes.POINTER(_U32), _P, _P, _P]),
     "ilm_scene_file_load": (_I32, [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_size_t, ctypes.POINTER(_P)]),
     "ilm_scene_file_parse": (_I32, [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_size_t,
                                     ctypes.POINTER(_P)]),

@@ -112,6 +112,13 @@ int kd_default_depth(uint64_t n);
 // leaf runs in kd_index, one primitive record per primitive id.
 std::string build_kd_layout(const std::vector<MeshView>& meshes, const KdParams& p, int threads, HostLayout& out);
 
+// Loop subdivision (shapes/loop_subdiv.rs, pbrt-v3's LoopSubdivide): `levels`
+// refinements of the triangle mesh (p: 3 floats per vertex, idx: 3 per face),
+// vertices moved to the limit surface, limit normals (unnormalised) per vertex.
+// Throws std::runtime_error on an invalid or non-manifold mesh.
+void loop_subdivide(const std::vector<float>& p, const std::vector<uint32_t>& idx, int levels,
+                    std::vector<float>& p_out, std::vector<uint32_t>& idx_out, std::vector<float>& n_out);
+
 // BVHAccel::new (bvh.rs:32-93) followed by the device layout.  Returns an
 // empty string on success or a description of the failure.
 std::string build_layout(const std::vector<MeshView>& meshes, int width, int max_prims_in_node, int threads,

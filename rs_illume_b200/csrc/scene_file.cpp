@@ -28,6 +28,7 @@
 #include <string>
 #include <vector>
 
+#include "builder.h"
 #include "illume_gpu.h"
 
 namespace {
@@ -534,6 +535,9 @@ private:
         if (type == "trianglemesh") {
             emit_mesh(t, ps, x, reverse, material);
             return;
+        } else if (type == "loopsubdiv") {
+            emit_loop(t, ps, x, reverse, material);
+            return;
         } else if (type == "sphere") {
             kind = ILM_QUADRIC_SPHERE;
             q.radius = (float)ps.one_float("radius", 1.0);
@@ -579,6 +583,36 @@ private:
             }
         out_->quadrics.push_back(q);
         out_->quadric_material.push_back(material);
+    }
+
+    // Shape "loopsubdiv" (pbrt-v3 CreateLoopSubdiv): the control mesh
+    // subdivided `levels` times (3), then placed like a trianglemesh with the
+    // limit normals as N.
+    void emit_loop(const Token& t, const Params& ps, const Xform& x, bool reverse, uint32_t material) {
+        const Param* P = ps.need_num("P", {"point"}, 3);
+        const Param* I = ps.need_num("indices", {"integer"}, 3);
+        if (!P || !I) fail(t, "loopsubdiv needs \"point P\" and \"integer indices\"");
+        long levels = ps.one_int("levels", ps.one_int("nlevels", 3));
+        std::vector<float> p(P->num.begin(), P->num.end()), po, no;
+        std::vector<uint32_t> idx, io;
+        for (double v : I->num) {
+            if (v < 0 || v >= (double)(P->num.size() / 3) || v != std::floor(v))
+                fail_at(ps.file, I->line, "loopsubdiv index out of range");
+            idx.push_back((uint32_t)v);
+        }
+        try {
+            ilm::loop_subdivide(p, idx, (int)levels, po, io, no);
+        } catch (const std::exception& e) {
+            fail(t, e.what());
+        }
+        Params mesh;
+        mesh.file = ps.file;
+        Param pp, ip, np;
+        pp.type = "point"; pp.name = "P"; pp.num.assign(po.begin(), po.end()); pp.line = t.line;
+        ip.type = "integer"; ip.name = "indices"; ip.num.assign(io.begin(), io.end()); ip.line = t.line;
+        np.type = "normal"; np.name = "N"; np.num.assign(no.begin(), no.end()); np.line = t.line;
+        mesh.items = {pp, ip, np};
+        emit_mesh(t, mesh, x, reverse, material);
     }
 
     // TriangleMesh::new (shapes/triangle.rs:36-73) with the Shape's transform
@@ -1066,6 +1100,30 @@ int32_t ilm_scene_file_build(ilm_context* ctx, const ilm_scene_file* sf, ilm_acc
     d.height = in.height;
     std::memcpy(d.camera_to_world, in.camera_to_world, sizeof d.camera_to_world);
     return ilm_pt_scene_create(ctx, *accel_out, &d, pt_out);
+}
+
+int32_t ilm_loop_subdivide(const float* xyz, uint32_t nv, const uint32_t* idx, uint32_t nt, uint32_t levels,
+                           uint32_t* out_nv, uint32_t* out_nt, float* out_xyz, uint32_t* out_idx, float* out_n) {
+    if ((nv && !xyz) || (nt && !idx) || !out_nv || !out_nt) return ILM_ERR_INVALID_ARGUMENT;
+    for (uint64_t i = 0; i < 3ull * nv; ++i)
+        if (!std::isfinite(xyz[i])) return ILM_ERR_INVALID_ARGUMENT;
+    std::vector<float> p(xyz, xyz + 3ull * nv), po, no;
+    std::vector<uint32_t> ix(idx, idx + 3ull * nt), io;
+    try {
+        ilm::loop_subdivide(p, ix, (int)levels, po, io, no);
+    } catch (const std::exception&) {
+        return ILM_ERR_INVALID_ARGUMENT;
+    }
+    const uint32_t onv = (uint32_t)(po.size() / 3), ont = (uint32_t)(io.size() / 3);
+    if (out_xyz) {
+        if (*out_nv < onv || *out_nt < ont) return ILM_ERR_INVALID_ARGUMENT;
+        std::memcpy(out_xyz, po.data(), po.size() * 4);
+        if (out_idx) std::memcpy(out_idx, io.data(), io.size() * 4);
+        if (out_n) std::memcpy(out_n, no.data(), no.size() * 4);
+    }
+    *out_nv = onv;
+    *out_nt = ont;
+    return ILM_OK;
 }
 
 int32_t ilm_scene_file_destroy(ilm_scene_file* sf) {

@@ -163,6 +163,28 @@ def quadric_desc(kind, radius: float, matrix, z_min: float = 0.0, z_max: float =
     return d
 
 
+def loop_subdivide(xyz, idx, levels: int = 3):
+    """Loop subdivision surface (shapes/loop_subdiv.rs): (xyz[nv, 3],
+    idx[nt, 3], n[nv, 3]) of the mesh refined `levels` times, on its limit
+    surface with limit normals (unnormalised)."""
+    lib = _lib.load()
+    xyz = np.ascontiguousarray(xyz, np.float32).reshape(-1, 3)
+    idx = np.ascontiguousarray(idx, np.uint32).reshape(-1, 3)
+    nv, nt = ctypes.c_uint32(), ctypes.c_uint32()
+    st = lib.ilm_loop_subdivide(ptr(xyz), len(xyz), ptr(idx), len(idx), levels, ctypes.byref(nv), ctypes.byref(nt),
+                                None, None, None)
+    if st != _lib.ILM_OK:
+        raise IllumeError(st, "ilm_loop_subdivide")
+    p = np.empty((nv.value, 3), np.float32)
+    i = np.empty((nt.value, 3), np.uint32)
+    n = np.empty((nv.value, 3), np.float32)
+    st = lib.ilm_loop_subdivide(ptr(xyz), len(xyz), ptr(idx), len(idx), levels, ctypes.byref(nv), ctypes.byref(nt),
+                                ptr(p), ptr(i), ptr(n))
+    if st != _lib.ILM_OK:
+        raise IllumeError(st, "ilm_loop_subdivide")
+    return p, i, n
+
+
 class Spheres:
     """A set of Sphere shapes (shapes/sphere.rs)."""
 
