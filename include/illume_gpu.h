@@ -149,6 +149,23 @@ const char* ilm_last_error_string(const ilm_context* ctx);
  * default 524288. */
 int32_t ilm_context_set_stage_chunk(ilm_context* ctx, uint64_t rays);
 
+/* One segment of a cubic Bezier curve (shapes/curve.rs:14-91): the curve's
+ * object-space control points and widths at u = 0 and 1, the part
+ * [u_min, u_max] this primitive covers (pbrt splits a curve into 2^splitdepth
+ * segments), and for ribbons the normals at u = 0 and 1.  Flat and cylinder
+ * curves intersect alike (they differ only in shading). */
+enum { ILM_CURVE_FLAT = 0, ILM_CURVE_CYLINDER = 1, ILM_CURVE_RIBBON = 2 };
+typedef struct {
+    float object_to_world[16];
+    float world_to_object[16];
+    float cp[12];
+    float width[2];
+    float n[6];
+    float u_min, u_max;
+    int32_t type;
+    int32_t reverse_orientation;
+} ilm_curve_desc;
+
 /* ----------------------------------------------------------------- shapes */
 /* TriangleMesh::new (shapes/triangle.rs:36-73) with world-space vertices:
  * xyz holds 3*nv floats, idx holds 3*nt vertex indices.  Host memory is
@@ -158,6 +175,11 @@ int32_t ilm_mesh_upload(ilm_context* ctx, const float* xyz, uint32_t nv,
 /* A set of spheres and other quadrics (shapes/{sphere,disk,cylinder,cone}.rs). */
 int32_t ilm_spheres_upload(ilm_context* ctx, const ilm_sphere_desc* spheres, uint32_t n,
                            ilm_mesh_id* out);
+/* A set of curve segments (Curve::intersect, shapes/curve.rs:278-375: the
+ * segment projected into the ray's frame and refined by recursive Bezier
+ * subdivision to a depth set by its flatness; hits report t, u along the
+ * curve and v across it).  Widths must be positive, u_min < u_max in [0, 1]. */
+int32_t ilm_curves_upload(ilm_context* ctx, const ilm_curve_desc* curves, uint32_t n, ilm_mesh_id* out);
 
 /* ----------------------------------------------------------------- accel */
 /* BVHAccel::new (accelerators/bvh.rs:32-93): SAH recursive build with 12
@@ -501,6 +523,9 @@ int32_t ilm_filter_table(const ilm_filter_desc* filter, float* table /* 16 x 16 
  *    with their pbrt parameters and defaults, under the current transform;
  *  - Shape "loopsubdiv" (levels, indices, P) as the subdivided triangle mesh
  *    with its limit normals;
+ *  - Shape "curve" (P: 4 control points, width / width0 / width1, type flat /
+ *    cylinder / ribbon with N at both ends, splitdepth 3) as 2^splitdepth
+ *    curve segments under the current transform;
  *  - Material "matte" Kd (other types: their Kd, else 0.5, with a warning),
  *    MakeNamedMaterial / NamedMaterial, AreaLightSource "diffuse" L x scale;
  *  - Camera "perspective" fov (of the shorter image axis) under LookAt or any
@@ -537,6 +562,7 @@ typedef struct {
     ilm_build_opts bvh;
     ilm_kdtree_opts kdtree;
     uint32_t n_warnings;
+    uint32_t n_curves;         /* curve segments */
 } ilm_scene_file_info;
 /* Loads `path`; on failure *out is NULL and `error` (error_len bytes, may be
  * NULL) holds the message. */
@@ -556,13 +582,16 @@ int32_t ilm_scene_file_mesh(const ilm_scene_file* sf, uint32_t k, uint32_t* nv, 
                             int32_t* has_uv, uint32_t* material);
 /* The quadrics (n_quadrics descriptions) and their material indices. */
 int32_t ilm_scene_file_quadrics(const ilm_scene_file* sf, ilm_sphere_desc* out, uint32_t* material);
+/* The curve segments (n_curves descriptions) and their material indices. */
+int32_t ilm_scene_file_curves(const ilm_scene_file* sf, ilm_curve_desc* out, uint32_t* material);
 /* The material table: albedo and emission, 3 floats each per material. */
 int32_t ilm_scene_file_materials(const ilm_scene_file* sf, float* albedo, float* emission);
 /* Uploads the shapes to ctx (one mesh per trianglemesh, with its N / S / uv,
  * then one quadric set) and builds the accelerator the file names.
- * Primitive ids run over the meshes in file order, then the quadrics.  With
- * pt_out non-NULL and triangles only, also creates the path-tracing scene
- * (camera, film size, materials); with quadrics present *pt_out is 0. */
+ * Primitive ids run over the meshes in file order, then the quadrics, then
+ * the curve segments.  With pt_out non-NULL and triangles only, also creates
+ * the path-tracing scene (camera, film size, materials); with quadrics or
+ * curves present *pt_out is 0. */
 int32_t ilm_scene_file_build(ilm_context* ctx, const ilm_scene_file* sf, ilm_accel_id* accel_out,
                              ilm_pt_scene_id* pt_out);
 int32_t ilm_scene_file_destroy(ilm_scene_file* sf);

@@ -36,6 +36,13 @@ class orc_sphere_desc(ctypes.Structure):
                 ("p1", ctypes.c_float * 3), ("p2", ctypes.c_float * 3)]
 
 
+class orc_curve_desc(ctypes.Structure):
+    _fields_ = [("object_to_world", ctypes.c_float * 16), ("world_to_object", ctypes.c_float * 16),
+                ("cp", ctypes.c_float * 12), ("width", ctypes.c_float * 2), ("n", ctypes.c_float * 6),
+                ("u_min", ctypes.c_float), ("u_max", ctypes.c_float), ("type", ctypes.c_int32),
+                ("reverse_orientation", ctypes.c_int32)]
+
+
 _P = ctypes.c_void_p
 _SIG = {
     "orc_gamma": (ctypes.c_float, [ctypes.c_int]),
@@ -46,6 +53,9 @@ _SIG = {
     "orc_rng_floats_advanced": (None, [ctypes.c_uint64, ctypes.c_int64, ctypes.c_uint64, _P]),
     "orc_scene_create": (_P, [_P, ctypes.c_uint32, _P, ctypes.c_uint32, _P, ctypes.c_uint32, ctypes.c_int]),
     "orc_scene_destroy": (None, [_P]),
+    "orc_scene_create_curves": (_P, [_P, ctypes.c_uint32, _P, ctypes.c_uint32, _P, ctypes.c_uint32, _P,
+                                     ctypes.c_uint32, ctypes.c_int]),
+    "orc_curve_intersect": (ctypes.c_int, [_P, _P, _P]),
     "orc_scene_node_count": (ctypes.c_uint32, [_P]),
     "orc_scene_nodes": (None, [_P, _P]),
     "orc_scene_prim_order": (None, [_P, _P]),
@@ -159,14 +169,16 @@ def sphere_desc(radius: float, translate=(0.0, 0.0, 0.0), scale: float = 1.0, z_
 class Scene:
     """BVHAccel over triangles (ids 0..nt-1) followed by spheres."""
 
-    def __init__(self, xyz, idx, spheres=(), max_prims_in_node: int = 4):
+    def __init__(self, xyz, idx, spheres=(), max_prims_in_node: int = 4, curves=()):
         lib = load()
         self._xyz = np.ascontiguousarray(xyz, np.float32).reshape(-1, 3)
         self._idx = np.ascontiguousarray(idx, np.uint32).reshape(-1, 3)
         sph = (orc_sphere_desc * max(1, len(spheres)))(*spheres)
-        self.n_prims = len(self._idx) + len(spheres)
-        self.h = lib.orc_scene_create(_p(self._xyz), len(self._xyz), _p(self._idx), len(self._idx),
-                                      ctypes.addressof(sph), len(spheres), max_prims_in_node)
+        cur = (orc_curve_desc * max(1, len(curves)))(*curves)
+        self.n_prims = len(self._idx) + len(spheres) + len(curves)
+        self.h = lib.orc_scene_create_curves(_p(self._xyz), len(self._xyz), _p(self._idx), len(self._idx),
+                                             ctypes.addressof(sph), len(spheres), ctypes.addressof(cur), len(curves),
+                                             max_prims_in_node)
 
     def __del__(self):
         if getattr(self, "h", None):
@@ -334,6 +346,40 @@ def surface_interaction(p, o, d, tmax=float("inf"), n=None, s=None, uv=None, rev
     hit = load().orc_surface_interaction(_p(p), *(_p(a) if a is not None else None for a in arrs), int(reverse),
                                          _p(r), _p(out))
     return out[0] if hit else None
+
+
+def curve_desc(cp, width, matrix=None, curve_type: int = 0, normals=None, u_range=(0.0, 1.0),
+               reverse: bool = False) -> orc_curve_desc:
+    """One curve segment: cp 4x3 control points, width (w0, w1), optional
+    4x4 object-to-world (inverse taken in float64), type 0 flat, 1 cylinder,
+    2 ribbon (normals 2x3)."""
+    m = np.eye(4) if matrix is None else np.asarray(matrix, np.float64).reshape(4, 4)
+    inv = np.linalg.inv(m)
+    d = orc_curve_desc()
+    for i in range(16):
+        d.object_to_world[i] = float(np.float32(m.flat[i]))
+        d.world_to_object[i] = float(np.float32(inv.flat[i]))
+    for i, v in enumerate(np.asarray(cp, np.float32).reshape(12)):
+        d.cp[i] = float(v)
+    d.width[0], d.width[1] = width
+    if normals is not None:
+        for i, v in enumerate(np.asarray(normals, np.float32).reshape(6)):
+            d.n[i] = float(v)
+    d.u_min, d.u_max = u_range
+    d.type = curve_type
+    d.reverse_orientation = int(reverse)
+    return d
+
+
+def curve_intersect(desc: orc_curve_desc, o, d, tmax=float("inf")):
+    """Returns (t, u, v) or None."""
+    r = np.zeros(1, RAY_DTYPE)
+    r["o"][0] = o
+    r["d"][0] = d
+    r["tmax"][0] = tmax
+    out = np.zeros(3, np.float32)
+    ok = load().orc_curve_intersect(ctypes.byref(desc), _p(r), _p(out))
+    return tuple(float(x) for x in out) if ok else None
 
 
 def sphere_intersect(desc: orc_sphere_desc, o, d, tmax=float("inf")):

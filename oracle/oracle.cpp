@@ -244,9 +244,60 @@ struct Sphere {
     float inner_radius, height;
     V3 p1, p2;             // hyperboloid: the swept segment (after the p2.z == 0 swap)
     float ah, ch;          // hyperboloid: ah (x^2 + y^2) - ch z^2 = 1
-    int kind;              // 0 sphere, 1 disk, 2 cylinder, 3 cone, 4 paraboloid, 5 hyperboloid
+    int kind;              // 0 sphere, 1 disk, 2 cylinder, 3 cone, 4 paraboloid, 5 hyperboloid, 6 curve
     bool reverse;
+    // curve segment: the curve's control points and end widths, the segment's
+    // u range, the type and the ribbon normals (CurveCommon, curve.rs:20-61)
+    V3 ccp[4];
+    float width[2], u_min, u_max;
+    int ctype;
+    V3 n[2];
+    float normal_angle, inv_sin_normal_angle;
 };
+
+static inline float lerpf(float t, float a, float b) { return a * (1.0f - t) + b * t; }   // pbrt.rs:41-47
+static inline V3 lerp3(float t, const V3& a, const V3& b) {
+    return {lerpf(t, a.x, b.x), lerpf(t, a.y, b.y), lerpf(t, a.z, b.z)};
+}
+// blossom_bezier (curve.rs:406-412)
+static V3 blossom_bezier(const V3* p, float u0, float u1, float u2) {
+    V3 a[3] = {lerp3(u0, p[0], p[1]), lerp3(u0, p[1], p[2]), lerp3(u0, p[2], p[3])};
+    V3 b[2] = {lerp3(u1, a[0], a[1]), lerp3(u1, a[1], a[2])};
+    return lerp3(u2, b[0], b[1]);
+}
+// The segment's control points (curve.rs:256-261 and 290-295).
+static void segment_cp(const Sphere& s, V3* cp) {
+    cp[0] = blossom_bezier(s.ccp, s.u_min, s.u_min, s.u_min);
+    cp[1] = blossom_bezier(s.ccp, s.u_min, s.u_min, s.u_max);
+    cp[2] = blossom_bezier(s.ccp, s.u_min, s.u_max, s.u_max);
+    cp[3] = blossom_bezier(s.ccp, s.u_max, s.u_max, s.u_max);
+}
+// Curve::new with CurveCommon::new (curve.rs:30-91).
+static Sphere curve_new(const orc_curve_desc& d) {
+    Sphere s;
+    std::memset(&s, 0, sizeof s);
+    std::memcpy(s.m, d.object_to_world, sizeof s.m);
+    std::memcpy(s.mi, d.world_to_object, sizeof s.mi);
+    s.kind = 6;
+    s.reverse = d.reverse_orientation != 0;
+    for (int i = 0; i < 4; ++i) s.ccp[i] = {d.cp[3 * i], d.cp[3 * i + 1], d.cp[3 * i + 2]};
+    s.width[0] = d.width[0];
+    s.width[1] = d.width[1];
+    s.u_min = d.u_min;
+    s.u_max = d.u_max;
+    s.ctype = d.type;
+    if (d.type == 2) {
+        for (int e = 0; e < 2; ++e) {
+            V3 v{d.n[3 * e], d.n[3 * e + 1], d.n[3 * e + 2]};
+            float inv = 1.0f / std::sqrt(v.x * v.x + v.y * v.y + v.z * v.z);
+            s.n[e] = {v.x * inv, v.y * inv, v.z * inv};
+        }
+        float dot = s.n[0].x * s.n[1].x + s.n[0].y * s.n[1].y + s.n[0].z * s.n[1].z;
+        s.normal_angle = std::acos(dot < 0.0f ? 0.0f : (dot > 1.0f ? 1.0f : dot));
+        s.inv_sin_normal_angle = 1.0f / std::sin(s.normal_angle);
+    }
+    return s;
+}
 // Sphere::new (sphere.rs:50-75; D22: made public), Disk::new (disk.rs:27-47),
 // Cylinder::new (cylinder.rs:26-46; D29: phi_max in radians of the clamped
 // degrees and z_min <= z_max, as pbrt), Cone::new (cone.rs:26-41).
@@ -321,6 +372,18 @@ static B3 sphere_world_bound(const Sphere& s) {
     B3 ob;
     ob.mn = {-s.radius, -s.radius, s.z_min};
     ob.mx = {s.radius, s.radius, s.z_max};
+    if (s.kind == 6) {   // Curve::object_bound (curve.rs:255-268)
+        V3 cp[4];
+        segment_cp(s, cp);
+        B3 b;
+        b = bunion_pt(b, cp[0]);
+        b = bunion_pt(b, cp[1]);
+        b = bunion_pt(b, cp[2]);
+        b = bunion_pt(b, cp[3]);
+        float w = std::fmax(lerpf(s.u_min, s.width[0], s.width[1]), lerpf(s.u_max, s.width[0], s.width[1])) * 0.5f;
+        ob.mn = {b.mn.x - w, b.mn.y - w, b.mn.z - w};
+        ob.mx = {b.mx.x + w, b.mx.y + w, b.mx.z + w};
+    }
     float bmin[3] = {s.m[3], s.m[7], s.m[11]}, bmax[3] = {s.m[3], s.m[7], s.m[11]};
     for (int i = 0; i < 3; ++i)
         for (int j = 0; j < 3; ++j) {
@@ -605,8 +668,155 @@ static bool hyperboloid_test(const Sphere& s, const Ray& world_ray, float* t_out
     return true;
 }
 
+// ---------------------------------------------------------------- curve.rs
+static inline V3 add3(const V3& a, const V3& b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+static inline V3 scl3(const V3& a, float s) { return {a.x * s, a.y * s, a.z * s}; }
+static inline float dot3(const V3& a, const V3& b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+static inline V3 norm3(const V3& a) { return scl3(a, 1.0f / std::sqrt(dot3(a, a))); }   // vector3.rs:85-95
+
+// subdivide_bezier (curve.rs:414-423)
+static void subdivide_bezier(const V3* cp, V3* out) {
+    out[0] = cp[0];
+    out[1] = scl3(add3(cp[0], cp[1]), 0.5f);
+    out[2] = scl3(add3(add3(cp[0], scl3(cp[1], 2.0f)), cp[2]), 0.25f);
+    out[3] = scl3(add3(add3(add3(cp[0], scl3(cp[1], 3.0f)), scl3(cp[2], 3.0f)), cp[3]), 0.125f);
+    out[4] = scl3(add3(add3(cp[1], scl3(cp[2], 2.0f)), cp[3]), 0.25f);
+    out[5] = scl3(add3(cp[2], cp[3]), 0.5f);
+    out[6] = cp[3];
+}
+// eval_bezier (curve.rs:425-446)
+static V3 eval_bezier(const V3* cp, float u, V3* deriv) {
+    V3 c1[3] = {lerp3(u, cp[0], cp[1]), lerp3(u, cp[1], cp[2]), lerp3(u, cp[2], cp[3])};
+    V3 c2[2] = {lerp3(u, c1[0], c1[1]), lerp3(u, c1[1], c1[2])};
+    V3 dd = sub(c2[1], c2[0]);
+    *deriv = dot3(dd, dd) > 0.0f ? scl3(dd, 3.0f) : sub(cp[3], cp[0]);
+    return lerp3(u, c2[0], c2[1]);
+}
+// The segment against the ray's beam, padded by half its width (curve.rs:116-140).
+static bool beam_overlaps(const V3* c, float max_width, float z_max) {
+    float hw = 0.5f * max_width;
+    if (std::fmax(std::fmax(c[0].y, c[1].y), std::fmax(c[2].y, c[3].y)) + hw < 0.0f ||
+        std::fmin(std::fmin(c[0].y, c[1].y), std::fmin(c[2].y, c[3].y)) - hw > 0.0f)
+        return false;
+    if (std::fmax(std::fmax(c[0].x, c[1].x), std::fmax(c[2].x, c[3].x)) + hw < 0.0f ||
+        std::fmin(std::fmin(c[0].x, c[1].x), std::fmin(c[2].x, c[3].x)) - hw > 0.0f)
+        return false;
+    return !(std::fmax(std::fmax(c[0].z, c[1].z), std::fmax(c[2].z, c[3].z)) + hw < 0.0f ||
+             std::fmin(std::fmin(c[0].z, c[1].z), std::fmin(c[2].z, c[3].z)) - hw > z_max);
+}
+
+struct CurveHit { float t, u, v; bool hit; };
+
+// Curve::recursive_intersect (curve.rs:94-252), t / u / v only.  Repairs:
+// the halves come from the subdivided points (the reference slices the
+// parent's four points), and the nearer of the halves' hits is kept (the
+// reference keeps the last one found); later halves are tested against the
+// nearest hit so far.
+static void recursive_intersect(const Sphere& s, const V3* cp, const V3& d, float ray_len, float u0, float u1,
+                                int depth, float* z_max, CurveHit* best) {
+    if (depth > 0) {
+        V3 split[7];
+        subdivide_bezier(cp, split);
+        float u[3] = {u0, (u0 + u1) * 0.5f, u1};
+        for (int seg = 0; seg < 2; ++seg) {
+            const V3* cps = split + 3 * seg;
+            float mw = std::fmax(lerpf(u[seg], s.width[0], s.width[1]), lerpf(u[seg + 1], s.width[0], s.width[1]));
+            if (!beam_overlaps(cps, mw, *z_max)) continue;
+            recursive_intersect(s, cps, d, ray_len, u[seg], u[seg + 1], depth - 1, z_max, best);
+        }
+        return;
+    }
+    float edge = (cp[1].y - cp[0].y) * -cp[0].y + cp[0].x * (cp[0].x - cp[1].x);
+    if (edge < 0.0f) return;
+    edge = (cp[2].y - cp[3].y) * -cp[3].y + cp[3].x * (cp[3].x - cp[2].x);
+    if (edge < 0.0f) return;
+    float sx = cp[3].x - cp[0].x, sy = cp[3].y - cp[0].y;
+    float denom = sx * sx + sy * sy;
+    if (denom == 0.0f) return;
+    float w = (-cp[0].x * sx + -cp[0].y * sy) / denom;
+    float u = std::fmin(std::fmax(lerpf(w, u0, u1), u0), u1);
+    float hit_width = lerpf(u, s.width[0], s.width[1]);
+    if (s.ctype == 2) {
+        // D38: parallel normals (angle 0) give 0 * inf = NaN weights in the
+        // reference (curve.rs:185-191); the ribbon then keeps n0
+        V3 nh = s.n[0];
+        if (s.normal_angle != 0.0f) {
+            float sin0 = std::sin((1.0f - u) * s.normal_angle) * s.inv_sin_normal_angle;
+            float sin1 = std::sin(u * s.normal_angle) * s.inv_sin_normal_angle;
+            nh = add3(scl3(s.n[0], sin0), scl3(s.n[1], sin1));
+        }
+        hit_width *= std::fabs(dot3(nh, d)) / ray_len;
+    }
+    V3 dpcdw;
+    V3 pc = eval_bezier(cp, std::fmin(std::fmax(w, 0.0f), 1.0f), &dpcdw);
+    float dist2 = pc.x * pc.x + pc.y * pc.y;
+    if (dist2 > hit_width * hit_width * 0.25f) return;
+    if (pc.z < 0.0f || pc.z > *z_max) return;
+    float dist = std::sqrt(dist2);
+    float edge_func = dpcdw.x * -pc.y + pc.x * dpcdw.y;
+    float v = edge_func > 0.0f ? 0.5f + dist / hit_width : 0.5f - dist / hit_width;
+    float t = pc.z / ray_len;
+    if (!best->hit || t < best->t) {
+        *best = CurveHit{t, u, v, true};
+        *z_max = pc.z;
+    }
+}
+
+// Curve::intersect (curve.rs:278-375).  The ray frame is the reference's
+// look_at(o, o + d, up) with its inverse applied as the transpose of the
+// orthonormal frame; Vector3::cross is evaluated in f64 (vector3.rs:67-83).
+static bool curve_test(const Sphere& s, const Ray& world_ray, float* t_out, float* uv_out) {
+    V3 o, d, oe, de;
+    transform_ray_with_error(s.mi, world_ray, &o, &d, &oe, &de);
+    V3 cp_obj[4];
+    segment_cp(s, cp_obj);
+    V3 dx = cross64(d, sub(cp_obj[3], cp_obj[0]));
+    if (length_sq(dx) == 0.0f) {   // coordinate_system (vector3.rs:520-545)
+        if (std::fabs(d.x) > std::fabs(d.y)) {
+            float len = std::sqrt(d.x * d.x + d.z * d.z);
+            dx = {-d.z / len, 0.0f, d.x / len};
+        } else {
+            float len = std::sqrt(d.y * d.y + d.z * d.z);
+            dx = {0.0f, d.z / len, -d.y / len};
+        }
+    }
+    V3 dir = norm3(sub(add3(o, d), o));
+    V3 right = norm3(cross64(norm3(dx), dir));
+    V3 new_up = cross64(dir, right);
+    V3 cp[4];
+    for (int i = 0; i < 4; ++i) {
+        V3 q = sub(cp_obj[i], o);
+        cp[i] = {dot3(right, q), dot3(new_up, q), dot3(dir, q)};
+    }
+    float ray_len = std::sqrt(dot3(d, d));
+    float z_max = ray_len * world_ray.t_max;
+    float max_width = std::fmax(lerpf(s.u_min, s.width[0], s.width[1]), lerpf(s.u_max, s.width[0], s.width[1]));
+    if (!beam_overlaps(cp, max_width, z_max)) return false;
+    float l0 = 0.0f;
+    for (int i = 0; i < 2; ++i)
+        l0 = std::fmax(l0, std::fmax(std::fmax(std::fabs(cp[i].x - 2.0f * cp[i + 1].x + cp[i + 2].x),
+                                               std::fabs(cp[i].y - 2.0f * cp[i + 1].y + cp[i + 2].y)),
+                                     std::fabs(cp[i].z - 2.0f * cp[i + 1].z + cp[i + 2].z)));
+    float eps = std::fmax(s.width[0], s.width[1]) * 0.05f;
+    auto log2i = [](float v) -> int {   // curve.rs:340-350
+        if (v < 1.0f) return 0;
+        uint32_t bits = f2u(v);
+        return (int)(bits >> 23) - 127 + ((bits & (1u << 22)) ? 1 : 0);
+    };
+    int r0 = log2i(1.41421356237f * 6.0f * l0 / (8.0f * eps)) / 2;
+    int max_depth = r0 < 0 ? 0 : (r0 > 10 ? 10 : r0);
+    CurveHit best{0, 0, 0, false};
+    recursive_intersect(s, cp, d, ray_len, s.u_min, s.u_max, max_depth, &z_max, &best);
+    if (!best.hit) return false;
+    *t_out = best.t;
+    uv_out[0] = best.u;
+    uv_out[1] = best.v;
+    return true;
+}
+
 static bool quadric_test(const Sphere& s, const Ray& ray, float* t_out, float* uv_out) {
     switch (s.kind) {
+        case 6: return curve_test(s, ray, t_out, uv_out);
         case 1: return disk_test(s, ray, t_out, uv_out);
         case 2: return cylinder_test(s, ray, t_out, uv_out);
         case 3: return cone_test(s, ray, t_out, uv_out);
@@ -1133,6 +1343,12 @@ void orc_rng_floats_advanced(uint64_t seq, int64_t delta, uint64_t n, float* out
 
 void* orc_scene_create(const float* verts, uint32_t nv, const uint32_t* idx, uint32_t nt,
                        const orc_sphere_desc* spheres, uint32_t ns, int max_prims_in_node) {
+    return orc_scene_create_curves(verts, nv, idx, nt, spheres, ns, nullptr, 0, max_prims_in_node);
+}
+
+void* orc_scene_create_curves(const float* verts, uint32_t nv, const uint32_t* idx, uint32_t nt,
+                              const orc_sphere_desc* spheres, uint32_t ns, const orc_curve_desc* curves,
+                              uint32_t nc, int max_prims_in_node) {
     auto t0 = std::chrono::steady_clock::now();
     Scene* s = new Scene();
     s->verts.resize(nv);
@@ -1140,7 +1356,8 @@ void* orc_scene_create(const float* verts, uint32_t nv, const uint32_t* idx, uin
     s->idx.assign(idx, idx + 3 * (size_t)nt);
     s->nt = nt;
     for (uint32_t i = 0; i < ns; ++i) s->spheres.push_back(sphere_new(spheres[i]));
-    uint32_t np = nt + ns;
+    for (uint32_t i = 0; i < nc; ++i) s->spheres.push_back(curve_new(curves[i]));
+    uint32_t np = nt + ns + nc;
     if (np > 0) {
         // BVHPrimitiveInfo per primitive (bvh.rs:50-53, 730-737)
         std::vector<PrimInfo> info(np);
@@ -1218,6 +1435,15 @@ int orc_sphere_intersect(const orc_sphere_desc* sd, const orc_ray* r, int closes
     Ray ray{{r->o[0], r->o[1], r->o[2]}, {r->d[0], r->d[1], r->d[2]}, r->tmax};
     float t, uv[2];
     if (!quadric_test(s, ray, &t, uv)) return 0;
+    out[0] = t; out[1] = uv[0]; out[2] = uv[1];
+    return 1;
+}
+
+int orc_curve_intersect(const orc_curve_desc* cd, const orc_ray* r, float* out) {
+    Sphere s = curve_new(*cd);
+    Ray ray{{r->o[0], r->o[1], r->o[2]}, {r->d[0], r->d[1], r->d[2]}, r->tmax};
+    float t, uv[2];
+    if (!curve_test(s, ray, &t, uv)) return 0;
     out[0] = t; out[1] = uv[0]; out[2] = uv[1];
     return 1;
 }

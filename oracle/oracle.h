@@ -46,6 +46,20 @@ typedef struct {
     float p1[3], p2[3];
 } orc_sphere_desc;
 
+/* One segment of a cubic Bezier curve (shapes/curve.rs:14-91): control
+ * points, widths at u = 0 and 1, normals at u = 0 and 1 (ribbons), the
+ * segment's u range, type 0 flat, 1 cylinder, 2 ribbon. */
+typedef struct {
+    float object_to_world[16];
+    float world_to_object[16];
+    float cp[12];
+    float width[2];
+    float n[6];
+    float u_min, u_max;
+    int32_t type;
+    int32_t reverse_orientation;
+} orc_curve_desc;
+
 /* 32-byte flattened BVH node (accelerators/bvh.rs:665-673, 32 B per D6). */
 typedef struct {
     float bmin[3], bmax[3];
@@ -72,6 +86,11 @@ void orc_rng_floats_advanced(uint64_t seq, int64_t delta, uint64_t n, float* out
 void* orc_scene_create(const float* verts, uint32_t nv, const uint32_t* idx,
                        uint32_t nt, const orc_sphere_desc* spheres, uint32_t ns,
                        int max_prims_in_node);
+/* The same with curve segments after the quadrics (their primitive ids
+ * follow the quadrics'). */
+void* orc_scene_create_curves(const float* verts, uint32_t nv, const uint32_t* idx, uint32_t nt,
+                              const orc_sphere_desc* spheres, uint32_t ns, const orc_curve_desc* curves,
+                              uint32_t nc, int max_prims_in_node);
 void orc_scene_destroy(void* scene);
 uint32_t orc_scene_node_count(void* scene);
 void orc_scene_nodes(void* scene, orc_bvh_node* out);
@@ -121,6 +140,8 @@ int orc_render_pt_filtered(void* scene, const float* verts, const uint32_t* idx,
 /* out = {t, u, v}. */
 int orc_sphere_intersect(const orc_sphere_desc* s, const orc_ray* r, int closest, float* out);
 void orc_sphere_world_bound(const orc_sphere_desc* s, float out[6]);
+/* Curve::intersect (curve.rs:278-375): out = {t, u, v}; 1 on a hit. */
+int orc_curve_intersect(const orc_curve_desc* c, const orc_ray* r, float* out);
 
 /* Single-ray forms (used by the path-tracer restatement). Return 1 on stack overflow. */
 int orc_trace_closest1(void* scene, const orc_ray* ray, orc_hit* hit);

@@ -7,13 +7,14 @@ aggregate interface on top of that ABI.
 """
 from ._lib import (HIT_DTYPE, ILM_MISS, ILM_TRAVERSAL_ERROR, RAY_DTYPE, IllumeError, LIB_PATH, load)
 from .image import filter_desc, filter_table, read_pfm, write_pfm
-from .primitive import (Bounds3f, Context, GpuBVHAccel, GpuKdTreeAccel, Hit, PathTracer, Ray, Scene, Spheres,
-                        TriangleMesh, loop_subdivide, quadric_desc, rays_array, sphere_desc)
+from .primitive import (Bounds3f, Context, Curves, GpuBVHAccel, GpuKdTreeAccel, Hit, PathTracer, Ray, Scene, Spheres,
+                        TriangleMesh, curve_segments, loop_subdivide, quadric_desc, rays_array, sphere_desc)
 from .scene_file import SceneFile
 
 __all__ = [
     "HIT_DTYPE", "ILM_MISS", "ILM_TRAVERSAL_ERROR", "RAY_DTYPE", "IllumeError", "LIB_PATH", "load",
-    "Bounds3f", "Context", "GpuBVHAccel", "GpuKdTreeAccel", "Hit", "PathTracer", "Ray", "Scene", "Spheres",
+    "Bounds3f", "Context", "Curves", "GpuBVHAccel", "GpuKdTreeAccel", "Hit", "PathTracer", "Ray", "Scene", "Spheres",
     "TriangleMesh", "rays_array",
-    "SceneFile", "loop_subdivide", "sphere_desc", "quadric_desc", "filter_desc", "filter_table", "read_pfm", "write_pfm",
+    "SceneFile", "curve_segments", "loop_subdivide", "sphere_desc", "quadric_desc", "filter_desc", "filter_table",
+    "read_pfm", "write_pfm",
 ]

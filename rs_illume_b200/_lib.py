@@ -92,6 +92,14 @@ class ilm_sphere_desc(ctypes.Structure):
                 ("p1", ctypes.c_float * 3), ("p2", ctypes.c_float * 3)]
 
 
+class ilm_curve_desc(ctypes.Structure):
+    _fields_ = [("object_to_world", ctypes.c_float * 16), ("world_to_object", ctypes.c_float * 16),
+                ("cp", ctypes.c_float * 12), ("width", ctypes.c_float * 2), ("n", ctypes.c_float * 6),
+                ("u_min", ctypes.c_float), ("u_max", ctypes.c_float), ("type", ctypes.c_int32),
+                ("reverse_orientation", ctypes.c_int32)]
+
+
+CURVE_TYPES = {"flat": 0, "cylinder": 1, "ribbon": 2}
 QUADRICS = {"sphere": 0, "disk": 1, "cylinder": 2, "cone": 3, "paraboloid": 4, "hyperboloid": 5}
 
 
@@ -112,7 +120,8 @@ class ilm_scene_file_info(ctypes.Structure):
                 ("width", ctypes.c_uint32), ("height", ctypes.c_uint32), ("spp", ctypes.c_uint32),
                 ("max_depth", ctypes.c_uint32), ("eye", ctypes.c_float * 3), ("camera_to_world", ctypes.c_float * 9),
                 ("fov_deg", ctypes.c_float), ("filter", ilm_filter_desc), ("accelerator", ctypes.c_int32),
-                ("bvh", ilm_build_opts), ("kdtree", ilm_kdtree_opts), ("n_warnings", ctypes.c_uint32)]
+                ("bvh", ilm_build_opts), ("kdtree", ilm_kdtree_opts), ("n_warnings", ctypes.c_uint32),
+                ("n_curves", ctypes.c_uint32)]
 
 
 class ilm_pt_opts(ctypes.Structure):
@@ -173,6 +182,7 @@ SIGNATURES = {
     "ilm_context_set_stage_chunk": (_I32, [_P, _U64]),
     "ilm_mesh_upload": (_I32, [_P, _P, _U32, _P, _U32, ctypes.POINTER(_U32)]),
     "ilm_spheres_upload": (_I32, [_P, _P, _U32, ctypes.POINTER(_U32)]),
+    "ilm_curves_upload": (_I32, [_P, _P, _U32, ctypes.POINTER(_U32)]),
     "ilm_mesh_set_attrs": (_I32, [_P, _U32, ctypes.POINTER(ilm_mesh_attrs)]),
     "ilm_surface_interactions": (_I32, [_P, _U32, _P, _P, _U64, _P, _P]),
     "ilm_accel_build": (_I32, [_P, _P, _U32, ctypes.POINTER(ilm_build_opts), ctypes.POINTER(_U32)]),
@@ -199,6 +209,7 @@ SIGNATURES = {
     "ilm_scene_file_mesh": (_I32, [_P, _U32, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
     "ilm_scene_file_quadrics": (_I32, [_P, _P, _P]),
     "ilm_scene_file_materials": (_I32, [_P, _P, _P]),
+    "ilm_scene_file_curves": (_I32, [_P, _P, _P]),
     "ilm_scene_file_build": (_I32, [_P, _P, ctypes.POINTER(_U32), ctypes.POINTER(_U32)]),
     "ilm_scene_file_destroy": (_I32, [_P]),
     "ilm_intersect_closest": (_I32, [_P, _U32, _P, _U64, _P, _P]),

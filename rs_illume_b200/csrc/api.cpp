@@ -322,6 +322,45 @@ static int32_t upload_accel(ilm_context* ctx, std::unique_ptr<Accel> acc, std::c
     return ILM_OK;
 }
 
+int32_t ilm_curves_upload(ilm_context* ctx, const ilm_curve_desc* curves, uint32_t n, ilm_mesh_id* out) {
+    if (!ctx || !out || (n > 0 && !curves)) return ILM_ERR_INVALID_ARGUMENT;
+    auto m = std::make_unique<Mesh>();
+    m->is_spheres = true;
+    for (uint32_t i = 0; i < n; ++i) {
+        const ilm_curve_desc& d = curves[i];
+        bool ok = d.type >= ILM_CURVE_FLAT && d.type <= ILM_CURVE_RIBBON && d.width[0] > 0.0f && d.width[1] > 0.0f &&
+                  std::isfinite(d.width[0]) && std::isfinite(d.width[1]) && d.u_min >= 0.0f && d.u_min < d.u_max &&
+                  d.u_max <= 1.0f;
+        for (float v : d.cp) ok = ok && std::isfinite(v);
+        if (d.type == ILM_CURVE_RIBBON)
+            for (int e = 0; e < 2; ++e) {
+                const float* nv = d.n + 3 * e;
+                ok = ok && std::isfinite(nv[0]) && std::isfinite(nv[1]) && std::isfinite(nv[2]) &&
+                     (nv[0] != 0.0f || nv[1] != 0.0f || nv[2] != 0.0f);
+            }
+        if (!ok) {
+            set_error(ctx, "ilm_curves_upload: invalid curve (type, widths, u range, control points or normals)");
+            return ILM_ERR_INVALID_ARGUMENT;
+        }
+        CurveInput in;
+        std::memcpy(in.o2w, d.object_to_world, sizeof in.o2w);
+        std::memcpy(in.w2o, d.world_to_object, sizeof in.w2o);
+        std::memcpy(in.cp, d.cp, sizeof in.cp);
+        std::memcpy(in.width, d.width, sizeof in.width);
+        std::memcpy(in.n, d.n, sizeof in.n);
+        in.u_min = d.u_min;
+        in.u_max = d.u_max;
+        in.type = d.type;
+        in.reverse = d.reverse_orientation;
+        m->spheres.push_back(make_curve(in));
+    }
+    m->n_prims = n;
+    ilm_mesh_id id = ctx->next_mesh++;
+    ctx->meshes[id] = std::move(m);
+    *out = id;
+    return ILM_OK;
+}
+
 int32_t ilm_accel_build(ilm_context* ctx, const ilm_mesh_id* meshes, uint32_t n_meshes, const ilm_build_opts* opts,
                         ilm_accel_id* out) {
     ILM_CHECK_CTX(ctx);

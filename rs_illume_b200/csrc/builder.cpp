@@ -301,8 +301,63 @@ bool make_sphere(const SphereInput& in, SphereRec* out) {
     return true;
 }
 
+namespace {
+// lerp(t, a, b) = a (1 - t) + b t (core/pbrt.rs:41-47)
+inline float lerpf(float t, float a, float b) { return a * (1.0f - t) + b * t; }
+// blossom_bezier (curve.rs:406-412)
+void blossom(const float* p, float u0, float u1, float u2, float* out) {
+    float a[3][3], b[2][3];
+    for (int k = 0; k < 3; ++k) {
+        for (int i = 0; i < 3; ++i) a[i][k] = lerpf(u0, p[3 * i + k], p[3 * (i + 1) + k]);
+        for (int i = 0; i < 2; ++i) b[i][k] = lerpf(u1, a[i][k], a[i + 1][k]);
+        out[k] = b[0][k] * (1.0f - u2) + b[1][k] * u2;
+    }
+}
+}  // namespace
+
+SphereRec make_curve(const CurveInput& in) {
+    SphereRec s;
+    std::memset(&s, 0, sizeof s);
+    std::memcpy(s.o2w, in.o2w, sizeof s.o2w);
+    std::memcpy(s.w2o, in.w2o, sizeof s.w2o);
+    s.kind = kQuadricCurve;
+    s.theta_min = (float)in.type;
+    s.reverse = in.reverse;
+    blossom(in.cp, in.u_min, in.u_min, in.u_min, &s.aux[0]);
+    blossom(in.cp, in.u_min, in.u_min, in.u_max, &s.aux[3]);
+    blossom(in.cp, in.u_min, in.u_max, in.u_max, &s.aux[6]);
+    blossom(in.cp, in.u_max, in.u_max, in.u_max, &s.aux[9]);
+    s.aux[12] = in.width[0];
+    s.aux[13] = in.width[1];
+    s.aux[14] = in.u_min;
+    s.aux[15] = in.u_max;
+    if (in.type == 2) {   // CurveCommon::new with normals (curve.rs:39-52)
+        float n[6];
+        for (int e = 0; e < 2; ++e) {
+            const float* v = in.n + 3 * e;
+            float inv = 1.0f / std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+            for (int k = 0; k < 3; ++k) n[3 * e + k] = v[k] * inv;
+        }
+        float dot = n[0] * n[3] + n[1] * n[4] + n[2] * n[5];
+        float angle = std::acos(dot < 0.0f ? 0.0f : (dot > 1.0f ? 1.0f : dot));
+        std::memcpy(&s.aux[16], n, sizeof n);
+        s.aux[22] = angle;
+        s.aux[23] = 1.0f / std::sin(angle);
+    }
+    return s;
+}
+
 Box sphere_bound(const SphereRec& s) {
     float omn[3] = {-s.radius, -s.radius, s.z_min}, omx[3] = {s.radius, s.radius, s.z_max};
+    if (s.kind == kQuadricCurve) {
+        const float* c = s.aux;
+        for (int k = 0; k < 3; ++k) {
+            omn[k] = std::fmin(std::fmin(c[k], c[3 + k]), std::fmin(c[6 + k], c[9 + k]));
+            omx[k] = std::fmax(std::fmax(c[k], c[3 + k]), std::fmax(c[6 + k], c[9 + k]));
+        }
+        float w = std::fmax(lerpf(s.aux[14], s.aux[12], s.aux[13]), lerpf(s.aux[15], s.aux[12], s.aux[13])) * 0.5f;
+        for (int k = 0; k < 3; ++k) { omn[k] -= w; omx[k] += w; }
+    }
     float bmin[3] = {s.o2w[3], s.o2w[7], s.o2w[11]}, bmax[3] = {s.o2w[3], s.o2w[7], s.o2w[11]};
     for (int i = 0; i < 3; ++i)
         for (int j = 0; j < 3; ++j) {

@@ -56,6 +56,22 @@ struct SphereInput {
 // False when a hyperboloid's implicit coefficients do not come out finite.
 bool make_sphere(const SphereInput& in, SphereRec* out);
 SphereRec make_sphere(const SphereInput& in);
+// Curve::new for one segment (shapes/curve.rs:30-91): the segment's control
+// points blossomed from the curve's for [u_min, u_max], the ribbon normals'
+// angle; type 0 flat, 1 cylinder, 2 ribbon.
+struct CurveInput {
+    float o2w[16], w2o[16];
+    float cp[12];
+    float width[2];
+    float n[6];
+    float u_min, u_max;
+    int32_t type;
+    int32_t reverse;
+};
+SphereRec make_curve(const CurveInput& in);
+// World bound of a quadric or curve record (geometry/bounds3.rs:320-356 on
+// the object box; a curve's box is its segment's control points padded by
+// half the larger end width, curve.rs:255-268).
 Box sphere_bound(const SphereRec& s);
 
 // One shape list entry: a triangle mesh (world-space vertices) or a sphere set.

@@ -36,9 +36,11 @@ enum : uint32_t {
 // object box for every kind; a disk keeps its height in z_min (= z_max) and
 // its inner radius in theta_min, a cone its height in z_max (z_min = 0), a
 // hyperboloid its largest radius in radius and p1, p2, ah, ch in aux.
+// A curve segment (kQuadricCurve) keeps its control points, widths, u range
+// and ribbon normals in aux and its type in theta_min (shapes.cuh).
 enum : int32_t {
     kQuadricSphere = 0, kQuadricDisk = 1, kQuadricCylinder = 2, kQuadricCone = 3,
-    kQuadricParaboloid = 4, kQuadricHyperboloid = 5
+    kQuadricParaboloid = 4, kQuadricHyperboloid = 5, kQuadricCurve = 6
 };
 struct SphereRec {
     float o2w[16];
@@ -46,9 +48,9 @@ struct SphereRec {
     float radius, z_min, z_max, theta_min, theta_max, phi_max;
     int32_t reverse;
     int32_t kind;
-    float aux[8];
+    float aux[24];
 };
-static_assert(sizeof(SphereRec) == 192, "SphereRec must be 192 bytes");
+static_assert(sizeof(SphereRec) == 256, "SphereRec must be 256 bytes");
 
 // Compressed wide node.  Child boxes are quantised to 8 bits per plane on a
 // per-node grid: plane = fma(q, 2^(e-127), origin), with q rounded outward at

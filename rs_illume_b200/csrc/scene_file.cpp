@@ -325,6 +325,8 @@ struct ilm_scene_file {
     std::vector<MeshOut> meshes;
     std::vector<ilm_sphere_desc> quadrics;
     std::vector<uint32_t> quadric_material;
+    std::vector<ilm_curve_desc> curves;
+    std::vector<uint32_t> curve_material;
     std::vector<MaterialKey> materials;
     ilm_scene_file_info info{};
     std::string warnings;
@@ -383,11 +385,13 @@ public:
             const MaterialKey& k = out_->materials[m.material];
             if (k.emission[0] > 0 || k.emission[1] > 0 || k.emission[2] > 0) ne += m.idx.size() / 3;
         }
-        if (nt + out_->quadrics.size() >= (1ull << 28)) throw std::runtime_error("more than 2^28 primitives");
+        if (nt + out_->quadrics.size() + out_->curves.size() >= (1ull << 28))
+            throw std::runtime_error("more than 2^28 primitives");
         in.n_triangles = (uint32_t)nt;
         in.n_vertices = (uint32_t)nv;
         in.n_emissive = (uint32_t)ne;
         in.n_quadrics = (uint32_t)out_->quadrics.size();
+        in.n_curves = (uint32_t)out_->curves.size();
         in.n_materials = (uint32_t)out_->materials.size();
         in.width = (uint32_t)width_;
         in.height = (uint32_t)height_;
@@ -538,6 +542,9 @@ private:
         } else if (type == "loopsubdiv") {
             emit_loop(t, ps, x, reverse, material);
             return;
+        } else if (type == "curve") {
+            emit_curve(t, ps, x, reverse, material);
+            return;
         } else if (type == "sphere") {
             kind = ILM_QUADRIC_SPHERE;
             q.radius = (float)ps.one_float("radius", 1.0);
@@ -583,6 +590,52 @@ private:
             }
         out_->quadrics.push_back(q);
         out_->quadric_material.push_back(material);
+    }
+
+    // Shape "curve" (pbrt-v3 CreateCurveShape): one cubic Bezier in object
+    // space split into 2^splitdepth segments over equal u ranges.
+    void emit_curve(const Token& t, const Params& ps, const Xform& x, bool reverse, uint32_t material) {
+        const Param* P = ps.need_num("P", {"point"}, 3);
+        if (!P || P->num.size() != 12) fail(t, "curve needs 4 control points in \"point P\"");
+        double w = ps.one_float("width", 1.0);
+        double w0 = ps.one_float("width0", w), w1 = ps.one_float("width1", w);
+        if (!(w0 > 0 && w1 > 0)) fail(t, "curve widths must be positive");
+        std::string type = ps.one_string("type", "flat");
+        int ct = type == "flat" ? ILM_CURVE_FLAT : type == "cylinder" ? ILM_CURVE_CYLINDER
+                 : type == "ribbon" ? ILM_CURVE_RIBBON : -1;
+        if (ct < 0) {
+            warn(t, "curve type \"" + type + "\" unknown; flat");
+            ct = ILM_CURVE_FLAT;
+        }
+        const Param* N = ps.need_num("N", {"normal"}, 3);
+        if (N && ct != ILM_CURVE_RIBBON) {
+            warn(t, "curve normals are only used with ribbon curves");
+            N = nullptr;
+        }
+        if (ct == ILM_CURVE_RIBBON && (!N || N->num.size() != 6)) fail(t, "ribbon curves need two normals in \"normal N\"");
+        long sd = ps.one_int("splitdepth", 3);
+        if (sd < 0 || sd > 10) fail(t, "splitdepth must be 0 .. 10");
+        const int nseg = 1 << sd;
+        for (int k = 0; k < nseg; ++k) {
+            ilm_curve_desc c;
+            std::memset(&c, 0, sizeof c);
+            for (int r = 0; r < 4; ++r)
+                for (int q = 0; q < 4; ++q) {
+                    c.object_to_world[4 * r + q] = (float)x.m.m[r][q];
+                    c.world_to_object[4 * r + q] = (float)x.inv.m[r][q];
+                }
+            for (int i = 0; i < 12; ++i) c.cp[i] = (float)P->num[i];
+            c.width[0] = (float)w0;
+            c.width[1] = (float)w1;
+            if (N)
+                for (int i = 0; i < 6; ++i) c.n[i] = (float)N->num[i];
+            c.u_min = (float)k / (float)nseg;
+            c.u_max = (float)(k + 1) / (float)nseg;
+            c.type = ct;
+            c.reverse_orientation = reverse ? 1 : 0;
+            out_->curves.push_back(c);
+            out_->curve_material.push_back(material);
+        }
     }
 
     // Shape "loopsubdiv" (pbrt-v3 CreateLoopSubdiv): the control mesh
@@ -1046,6 +1099,14 @@ int32_t ilm_scene_file_quadrics(const ilm_scene_file* sf, ilm_sphere_desc* out, 
     return ILM_OK;
 }
 
+int32_t ilm_scene_file_curves(const ilm_scene_file* sf, ilm_curve_desc* out, uint32_t* material) {
+    if (!sf) return ILM_ERR_INVALID_ARGUMENT;
+    if (out && !sf->curves.empty()) std::memcpy(out, sf->curves.data(), sf->curves.size() * sizeof(ilm_curve_desc));
+    if (material && !sf->curve_material.empty())
+        std::memcpy(material, sf->curve_material.data(), sf->curve_material.size() * 4);
+    return ILM_OK;
+}
+
 int32_t ilm_scene_file_materials(const ilm_scene_file* sf, float* albedo, float* emission) {
     if (!sf) return ILM_ERR_INVALID_ARGUMENT;
     for (size_t i = 0; i < sf->materials.size(); ++i)
@@ -1081,11 +1142,16 @@ int32_t ilm_scene_file_build(ilm_context* ctx, const ilm_scene_file* sf, ilm_acc
         if ((rc = ilm_spheres_upload(ctx, sf->quadrics.data(), (uint32_t)sf->quadrics.size(), &id)) != ILM_OK) return rc;
         ids.push_back(id);
     }
+    if (!sf->curves.empty()) {
+        ilm_mesh_id id;
+        if ((rc = ilm_curves_upload(ctx, sf->curves.data(), (uint32_t)sf->curves.size(), &id)) != ILM_OK) return rc;
+        ids.push_back(id);
+    }
     const ilm_scene_file_info& in = sf->info;
     rc = in.accelerator == 1 ? ilm_kdtree_build(ctx, ids.data(), (uint32_t)ids.size(), &in.kdtree, accel_out)
                              : ilm_accel_build(ctx, ids.data(), (uint32_t)ids.size(), &in.bvh, accel_out);
     if (rc != ILM_OK) return rc;
-    if (!pt_out || !sf->quadrics.empty() || sf->meshes.empty()) return ILM_OK;
+    if (!pt_out || !sf->quadrics.empty() || !sf->curves.empty() || sf->meshes.empty()) return ILM_OK;
     std::vector<float> albedo(3 * sf->materials.size()), emission(3 * sf->materials.size());
     ilm_scene_file_materials(sf, albedo.data(), emission.data());
     ilm_pt_scene_desc d;

@@ -469,6 +469,195 @@ __device__ __forceinline__ bool hyperboloid_test(const SphereRec& s, const ObjRa
     return true;
 }
 
+// ------------------------------------------------------------------ curves
+// Curve::intersect (shapes/curve.rs:278-375 and recursive_intersect 94-252).
+// Curve records (kind kQuadricCurve): aux[0..11] the segment's cubic Bezier
+// control points (blossomed on the host for [u_min, u_max]), aux[12..13] the
+// curve's widths at u = 0 and 1, aux[14..15] u_min and u_max, aux[16..21] the
+// ribbon normals n0, n1 (unit), aux[22] their angle, aux[23] 1 / sin(angle);
+// theta_min holds the curve type (0 flat, 1 cylinder, 2 ribbon).  Every
+// operation is a round-to-nearest intrinsic, so nothing contracts to an FMA.
+struct CP3 {
+    float x, y, z;
+};
+__device__ __forceinline__ CP3 cp_add(CP3 a, CP3 b) { return {__fadd_rn(a.x, b.x), __fadd_rn(a.y, b.y), __fadd_rn(a.z, b.z)}; }
+__device__ __forceinline__ CP3 cp_sub(CP3 a, CP3 b) { return {__fsub_rn(a.x, b.x), __fsub_rn(a.y, b.y), __fsub_rn(a.z, b.z)}; }
+__device__ __forceinline__ CP3 cp_scale(CP3 a, float s) { return {__fmul_rn(a.x, s), __fmul_rn(a.y, s), __fmul_rn(a.z, s)}; }
+__device__ __forceinline__ float cp_dot(CP3 a, CP3 b) {
+    return __fadd_rn(__fadd_rn(__fmul_rn(a.x, b.x), __fmul_rn(a.y, b.y)), __fmul_rn(a.z, b.z));
+}
+// Vector3::cross in f64 (geometry/vector3.rs:67-83), rounded once to float.
+__device__ __forceinline__ CP3 cp_cross(CP3 a, CP3 b) {
+    return {__double2float_rn(__dsub_rn(__dmul_rn((double)a.y, (double)b.z), __dmul_rn((double)a.z, (double)b.y))),
+            __double2float_rn(__dsub_rn(__dmul_rn((double)a.z, (double)b.x), __dmul_rn((double)a.x, (double)b.z))),
+            __double2float_rn(__dsub_rn(__dmul_rn((double)a.x, (double)b.y), __dmul_rn((double)a.y, (double)b.x)))};
+}
+// Vector3::normalize (vector3.rs:85-95): times 1 / length.
+__device__ __forceinline__ CP3 cp_normalize(CP3 a) { return cp_scale(a, __fdiv_rn(1.0f, __fsqrt_rn(cp_dot(a, a)))); }
+// lerp(t, a, b) = a (1 - t) + b t (core/pbrt.rs:41-47)
+__device__ __forceinline__ float cp_lerpf(float t, float a, float b) {
+    return __fadd_rn(__fmul_rn(a, __fsub_rn(1.0f, t)), __fmul_rn(b, t));
+}
+__device__ __forceinline__ CP3 cp_lerp(float t, CP3 a, CP3 b) {
+    return {cp_lerpf(t, a.x, b.x), cp_lerpf(t, a.y, b.y), cp_lerpf(t, a.z, b.z)};
+}
+
+// eval_bezier (curve.rs:425-446): the point at u and the derivative.
+__device__ __forceinline__ CP3 cp_eval(const CP3* cp, float u, CP3& deriv) {
+    CP3 a0 = cp_lerp(u, cp[0], cp[1]), a1 = cp_lerp(u, cp[1], cp[2]), a2 = cp_lerp(u, cp[2], cp[3]);
+    CP3 b0 = cp_lerp(u, a0, a1), b1 = cp_lerp(u, a1, a2);
+    CP3 db = cp_sub(b1, b0);
+    deriv = cp_dot(db, db) > 0.0f ? cp_scale(db, 3.0f) : cp_sub(cp[3], cp[0]);
+    return cp_lerp(u, b0, b1);
+}
+
+// subdivide_bezier (curve.rs:414-423): the two halves share out[3].
+__device__ __forceinline__ void cp_split(const CP3* cp, CP3* out) {
+    out[0] = cp[0];
+    out[1] = cp_scale(cp_add(cp[0], cp[1]), 0.5f);
+    out[2] = cp_scale(cp_add(cp_add(cp[0], cp_scale(cp[1], 2.0f)), cp[2]), 0.25f);
+    out[3] = cp_scale(cp_add(cp_add(cp_add(cp[0], cp_scale(cp[1], 3.0f)), cp_scale(cp[2], 3.0f)), cp[3]), 0.125f);
+    out[4] = cp_scale(cp_add(cp_add(cp[1], cp_scale(cp[2], 2.0f)), cp[3]), 0.25f);
+    out[5] = cp_scale(cp_add(cp[2], cp[3]), 0.5f);
+    out[6] = cp[3];
+}
+
+// The bound test of a segment against the ray's zero-width beam, padded by
+// half the width (curve.rs:116-140).
+__device__ __forceinline__ bool cp_overlaps(const CP3* c, float half_w, float z_max) {
+    float ymax = fmaxf(fmaxf(c[0].y, c[1].y), fmaxf(c[2].y, c[3].y));
+    float ymin = fminf(fminf(c[0].y, c[1].y), fminf(c[2].y, c[3].y));
+    if (__fadd_rn(ymax, half_w) < 0.0f || __fsub_rn(ymin, half_w) > 0.0f) return false;
+    float xmax = fmaxf(fmaxf(c[0].x, c[1].x), fmaxf(c[2].x, c[3].x));
+    float xmin = fminf(fminf(c[0].x, c[1].x), fminf(c[2].x, c[3].x));
+    if (__fadd_rn(xmax, half_w) < 0.0f || __fsub_rn(xmin, half_w) > 0.0f) return false;
+    float zmax = fmaxf(fmaxf(c[0].z, c[1].z), fmaxf(c[2].z, c[3].z));
+    float zmin = fminf(fminf(c[0].z, c[1].z), fminf(c[2].z, c[3].z));
+    return !(__fadd_rn(zmax, half_w) < 0.0f || __fsub_rn(zmin, half_w) > z_max);
+}
+
+// Integer log2 rounded to nearest for v >= 1, else 0 (curve.rs:340-350).
+__device__ __forceinline__ int curve_log2(float v) {
+    if (v < 1.0f) return 0;
+    uint32_t bits = __float_as_uint(v);
+    return (int)(bits >> 23) - 127 + ((bits & (1u << 22)) ? 1 : 0);
+}
+
+static __device__ __noinline__ bool curve_test(const SphereRec& s, const ObjRay& r, float tmax, float& t_out,
+                                        float& u_out, float& v_out) {
+    const CP3 d{r.dx, r.dy, r.dz}, o{r.ox, r.oy, r.oz};
+    CP3 obj[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) obj[i] = CP3{s.aux[3 * i], s.aux[3 * i + 1], s.aux[3 * i + 2]};
+    const float w0 = s.aux[12], w1 = s.aux[13], u_min = s.aux[14], u_max = s.aux[15];
+    const int type = (int)s.theta_min;
+    // the ray's frame: z along the ray, y towards the chord (curve.rs:305-320)
+    CP3 up = cp_cross(d, cp_sub(obj[3], obj[0]));
+    if (cp_dot(up, up) == 0.0f) {   // coordinate_system(d) (vector3.rs:520-545)
+        if (fabsf(d.x) > fabsf(d.y)) {
+            float len = __fsqrt_rn(__fadd_rn(__fmul_rn(d.x, d.x), __fmul_rn(d.z, d.z)));
+            up = CP3{__fdiv_rn(-d.z, len), 0.0f, __fdiv_rn(d.x, len)};
+        } else {
+            float len = __fsqrt_rn(__fadd_rn(__fmul_rn(d.y, d.y), __fmul_rn(d.z, d.z)));
+            up = CP3{0.0f, __fdiv_rn(d.z, len), __fdiv_rn(-d.y, len)};
+        }
+    }
+    // Transform::look_at(o, o + d, up) (transform.rs:181-209); its inverse is
+    // applied as the transpose of the orthonormal frame
+    CP3 dir = cp_normalize(cp_sub(cp_add(o, d), o));
+    CP3 right = cp_normalize(cp_cross(cp_normalize(up), dir));
+    CP3 new_up = cp_cross(dir, right);
+    CP3 c[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        CP3 q = cp_sub(obj[i], o);
+        c[i] = CP3{cp_dot(right, q), cp_dot(new_up, q), cp_dot(dir, q)};
+    }
+    const float ray_len = __fsqrt_rn(cp_dot(d, d));
+    float z_max = __fmul_rn(ray_len, tmax);
+    const float max_w = fmaxf(cp_lerpf(u_min, w0, w1), cp_lerpf(u_max, w0, w1));
+    if (!cp_overlaps(c, __fmul_rn(0.5f, max_w), z_max)) return false;
+    // refinement depth (curve.rs:332-357)
+    float l0 = 0.0f;
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+        float lx = fabsf(__fadd_rn(__fsub_rn(c[i].x, __fmul_rn(2.0f, c[i + 1].x)), c[i + 2].x));
+        float ly = fabsf(__fadd_rn(__fsub_rn(c[i].y, __fmul_rn(2.0f, c[i + 1].y)), c[i + 2].y));
+        float lz = fabsf(__fadd_rn(__fsub_rn(c[i].z, __fmul_rn(2.0f, c[i + 1].z)), c[i + 2].z));
+        l0 = fmaxf(l0, fmaxf(fmaxf(lx, ly), lz));
+    }
+    const float eps = __fmul_rn(fmaxf(w0, w1), 0.05f);
+    int r0 = curve_log2(__fdiv_rn(__fmul_rn(__fmul_rn(1.41421356237f, 6.0f), l0), __fmul_rn(8.0f, eps))) / 2;
+    const int max_depth = r0 < 0 ? 0 : (r0 > 10 ? 10 : r0);
+    // depth-first over the halves, first half first; the nearest hit of the
+    // whole curve is kept (curve.rs:146-153 keeps the last one found)
+    struct Seg {
+        CP3 cp[4];
+        float u0, u1;
+        int depth;
+    };
+    Seg stack[11];
+    int sp = 0;
+    stack[sp++] = Seg{{c[0], c[1], c[2], c[3]}, u_min, u_max, max_depth};
+    bool hit = false;
+    while (sp > 0) {
+        Seg g = stack[--sp];
+        if (g.depth > 0) {
+            CP3 sp7[7];
+            cp_split(g.cp, sp7);
+            const float um = __fmul_rn(__fadd_rn(g.u0, g.u1), 0.5f);
+            const float us[3] = {g.u0, um, g.u1};
+            for (int seg = 1; seg >= 0; --seg) {   // pushed second half first
+                const CP3* cps = sp7 + 3 * seg;
+                float mw = fmaxf(cp_lerpf(us[seg], w0, w1), cp_lerpf(us[seg + 1], w0, w1));
+                if (!cp_overlaps(cps, __fmul_rn(0.5f, mw), z_max)) continue;
+                stack[sp++] = Seg{{cps[0], cps[1], cps[2], cps[3]}, us[seg], us[seg + 1], g.depth - 1};
+            }
+            continue;
+        }
+        const CP3* cp = g.cp;
+        // the sample point must lie between the end tangents' perpendiculars
+        float edge = __fadd_rn(__fmul_rn(__fsub_rn(cp[1].y, cp[0].y), -cp[0].y),
+                               __fmul_rn(cp[0].x, __fsub_rn(cp[0].x, cp[1].x)));
+        if (edge < 0.0f) continue;
+        edge = __fadd_rn(__fmul_rn(__fsub_rn(cp[2].y, cp[3].y), -cp[3].y), __fmul_rn(cp[3].x, __fsub_rn(cp[3].x, cp[2].x)));
+        if (edge < 0.0f) continue;
+        const float sdx = __fsub_rn(cp[3].x, cp[0].x), sdy = __fsub_rn(cp[3].y, cp[0].y);
+        const float denom = __fadd_rn(__fmul_rn(sdx, sdx), __fmul_rn(sdy, sdy));
+        if (denom == 0.0f) continue;
+        const float w = __fdiv_rn(__fadd_rn(__fmul_rn(-cp[0].x, sdx), __fmul_rn(-cp[0].y, sdy)), denom);
+        const float u = fminf(fmaxf(cp_lerpf(w, g.u0, g.u1), g.u0), g.u1);
+        float hit_w = cp_lerpf(u, w0, w1);
+        if (type == 2) {   // ribbon: the width seen along the ray
+            // parallel normals (angle 0) keep n0 instead of 0 * inf weights
+            CP3 nh = CP3{s.aux[16], s.aux[17], s.aux[18]};
+            if (s.aux[22] != 0.0f) {
+                float sin0 = __fmul_rn(sinf(__fmul_rn(__fsub_rn(1.0f, u), s.aux[22])), s.aux[23]);
+                float sin1 = __fmul_rn(sinf(__fmul_rn(u, s.aux[22])), s.aux[23]);
+                nh = cp_add(cp_scale(nh, sin0), cp_scale(CP3{s.aux[19], s.aux[20], s.aux[21]}, sin1));
+            }
+            hit_w = __fmul_rn(hit_w, __fdiv_rn(fabsf(cp_dot(nh, d)), ray_len));
+        }
+        CP3 dpcdw;
+        const CP3 pc = cp_eval(cp, fminf(fmaxf(w, 0.0f), 1.0f), dpcdw);
+        const float dist2 = __fadd_rn(__fmul_rn(pc.x, pc.x), __fmul_rn(pc.y, pc.y));
+        if (dist2 > __fmul_rn(__fmul_rn(hit_w, hit_w), 0.25f)) continue;
+        if (pc.z < 0.0f || pc.z > z_max) continue;
+        const float dist = __fsqrt_rn(dist2);
+        const float edge_fn = __fadd_rn(__fmul_rn(dpcdw.x, -pc.y), __fmul_rn(pc.x, dpcdw.y));
+        const float v = edge_fn > 0.0f ? __fadd_rn(0.5f, __fdiv_rn(dist, hit_w)) : __fsub_rn(0.5f, __fdiv_rn(dist, hit_w));
+        const float t = __fdiv_rn(pc.z, ray_len);
+        if (!hit || t < t_out) {
+            t_out = t;
+            u_out = u;
+            v_out = v;
+            hit = true;
+            z_max = pc.z;   // later segments must come nearer
+        }
+    }
+    return hit;
+}
+
 // The quadric record's test (SphereRec::kind), in its object space.
 static __device__ __noinline__ bool quadric_test(const SphereRec& s, float rox, float roy, float roz, float rdx,
                                                  float rdy, float rdz, float tmax, float& t_out, float& u_out,
@@ -480,6 +669,7 @@ static __device__ __noinline__ bool quadric_test(const SphereRec& s, float rox, 
         case kQuadricCone: return cone_test(s, r, tmax, t_out, u_out, v_out);
         case kQuadricParaboloid: return paraboloid_test(s, r, tmax, t_out, u_out, v_out);
         case kQuadricHyperboloid: return hyperboloid_test(s, r, tmax, t_out, u_out, v_out);
+        case kQuadricCurve: return curve_test(s, r, tmax, t_out, u_out, v_out);
         default: return sphere_test(s, r, tmax, t_out, u_out, v_out);
     }
 }

@@ -185,6 +185,46 @@ def loop_subdivide(xyz, idx, levels: int = 3):
     return p, i, n
 
 
+def curve_segments(cp, width, matrix=None, curve_type="flat", normals=None, split_depth: int = 3,
+                   reverse: bool = False):
+    """A cubic Bezier curve (shapes/curve.rs) as 2^split_depth ilm_curve_desc
+    segments over equal u ranges, as pbrt's curve shape splits it.  cp: 4x3
+    control points; width (w0, w1); normals 2x3 for ribbons."""
+    m = np.eye(4) if matrix is None else np.asarray(matrix, np.float64).reshape(4, 4)
+    inv = np.linalg.inv(m)
+    n_seg = 1 << split_depth
+    out = []
+    for k in range(n_seg):
+        d = _lib.ilm_curve_desc()
+        for i in range(16):
+            d.object_to_world[i] = float(np.float32(m.flat[i]))
+            d.world_to_object[i] = float(np.float32(inv.flat[i]))
+        for i, v in enumerate(np.asarray(cp, np.float32).reshape(12)):
+            d.cp[i] = float(v)
+        d.width[0], d.width[1] = width
+        if normals is not None:
+            for i, v in enumerate(np.asarray(normals, np.float32).reshape(6)):
+                d.n[i] = float(v)
+        d.u_min, d.u_max = k / n_seg, (k + 1) / n_seg
+        d.type = _lib.CURVE_TYPES[curve_type] if isinstance(curve_type, str) else int(curve_type)
+        d.reverse_orientation = int(reverse)
+        out.append(d)
+    return out
+
+
+class Curves:
+    """A set of curve segments (shapes/curve.rs), one primitive each."""
+
+    def __init__(self, ctx: Context, descs):
+        arr = (_lib.ilm_curve_desc * len(descs))(*descs)
+        mid = ctypes.c_uint32()
+        ctx.check(ctx._lib.ilm_curves_upload(ctx.handle, ctypes.addressof(arr), len(descs), ctypes.byref(mid)),
+                  "ilm_curves_upload")
+        self.id = mid.value
+        self.n_prims = len(descs)
+        self.descs = list(descs)
+
+
 class Spheres:
     """A set of Sphere shapes (shapes/sphere.rs)."""
 

@@ -84,6 +84,14 @@ class SceneFile:
         self._check(self._lib.ilm_scene_file_quadrics(self.handle, ctypes.addressof(arr), ptr(mat)))
         return list(arr)[:n], mat
 
+    def curves(self):
+        """(list of ilm_curve_desc segments, material index per segment)."""
+        n = self.info.n_curves
+        arr = (_lib.ilm_curve_desc * max(1, n))()
+        mat = np.zeros(n, np.uint32)
+        self._check(self._lib.ilm_scene_file_curves(self.handle, ctypes.addressof(arr), ptr(mat)))
+        return list(arr)[:n], mat
+
     def materials(self):
         """(albedo[m, 3], emission[m, 3])."""
         m = self.info.n_materials
@@ -109,7 +117,7 @@ class SceneFile:
         acc = cls.__new__(cls)
         acc.ctx, acc.id = ctx, aid.value
         acc.width = _lib.ILM_LAYOUT_KDTREE if self.info.accelerator == 1 else self.info.bvh.width
-        acc.n_prims = self.info.n_triangles + self.info.n_quadrics
+        acc.n_prims = self.info.n_triangles + self.info.n_quadrics + self.info.n_curves
         pt: Optional[PathTracer] = None
         if pid.value:
             pt = PathTracer.__new__(PathTracer)
