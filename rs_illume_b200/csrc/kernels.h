@@ -56,5 +56,8 @@ cudaError_t launch_trace(const DeviceAccel& a, const ilm_ray* rays, uint64_t n, 
 cudaError_t launch_trace_binary(const TraceArgs& t, cudaStream_t s);
 cudaError_t launch_trace_kd(const TraceArgs& t, const LaunchParams& lp, cudaStream_t s);
 cudaError_t launch_trace_wide(int width, const TraceArgs& t, const LaunchParams& lp, cudaStream_t s);
+// Rays that one wave of the one-thread-per-ray wide kernel holds resident on
+// the current device (0 when unknown).
+uint64_t wide_grid_wave(int width, int stack_depth);
 
 }  // namespace ilm

@@ -75,11 +75,11 @@ __device__ __forceinline__ TraceArgs args_of(const BatchTable& t, uint32_t b) {
     return a;
 }
 
-template <int W, int kStack, bool kAny>
+template <int W, int kStack, bool kAny, bool kAnalytic>
 __global__ void __launch_bounds__(128, 8) k_trace_batched(BatchTable tab) {
     const unsigned lane = threadIdx.x & 31u;
     const unsigned below = (1u << lane) - 1u;
-    WideTracer<W, kStack, kAny> T;
+    WideTracer<W, kStack, kAny, kAnalytic> T;
     TraceArgs a;
     bool active = false;
     uint64_t id = 0;
@@ -120,11 +120,11 @@ __global__ void __launch_bounds__(128, 8) k_trace_batched(BatchTable tab) {
     }
 }
 
-template <int W, int kStack>
-cudaError_t launch_batched(const BatchTable& t, bool any, cudaStream_t s) {
+template <int W, int kStack, bool kAnalytic>
+cudaError_t launch_batched_variant(const BatchTable& t, bool any, cudaStream_t s) {
     const unsigned block = 128;
-    auto kc = k_trace_batched<W, kStack, false>;
-    auto ka = k_trace_batched<W, kStack, true>;
+    auto kc = k_trace_batched<W, kStack, false, kAnalytic>;
+    auto ka = k_trace_batched<W, kStack, true, kAnalytic>;
     int dev = 0, sms = 148, per_sm = 1;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -139,6 +139,13 @@ cudaError_t launch_batched(const BatchTable& t, bool any, cudaStream_t s) {
     return cudaGetLastError();
 }
 
+// Tables without quadric or curve records run the triangle-only variant.
+template <int W, int kStack>
+cudaError_t launch_batched(const BatchTable& t, bool any, bool analytic, cudaStream_t s) {
+    return analytic ? launch_batched_variant<W, kStack, true>(t, any, s)
+                    : launch_batched_variant<W, kStack, false>(t, any, s);
+}
+
 }  // namespace
 }  // namespace ilm
 
@@ -148,6 +155,7 @@ using namespace ilm;
 struct ilm_batch_plan {
     struct Group {
         int width;
+        bool analytic = false;   // some accel holds quadric or curve records
         DeviceBuffer table, counter;
         BatchTable t;
     };
@@ -169,8 +177,11 @@ cudaError_t launch_plan(const ilm_batch_plan& p, cudaStream_t s) {
     for (const auto& g : p.groups) {
         cudaError_t e;
         bool deep = p.stack_depth > 32;
-        if (g->width == 8) e = deep ? launch_batched<8, 64>(g->t, p.any, s) : launch_batched<8, 32>(g->t, p.any, s);
-        else e = deep ? launch_batched<4, 64>(g->t, p.any, s) : launch_batched<4, 32>(g->t, p.any, s);
+        const bool an = g->analytic;
+        if (g->width == 8)
+            e = deep ? launch_batched<8, 64>(g->t, p.any, an, s) : launch_batched<8, 32>(g->t, p.any, an, s);
+        else
+            e = deep ? launch_batched<4, 64>(g->t, p.any, an, s) : launch_batched<4, 32>(g->t, p.any, an, s);
         if (e != cudaSuccess) return e;
     }
     return cudaSuccess;
@@ -220,6 +231,7 @@ int32_t build_plan(ilm_context* ctx, const ilm_batch_desc* batches, uint32_t n, 
         for (auto& e : v) { e.first = first; first += e.n; }
         auto g = std::make_unique<ilm_batch_plan::Group>();
         g->width = k ? 8 : 4;
+        for (const auto& e : v) g->analytic = g->analytic || e.spheres != nullptr;
         cudaError_t ce = g->table.reserve(v.size() * sizeof(BatchEntry));
         if (ce == cudaSuccess) ce = g->counter.reserve(sizeof(unsigned long long));
         if (ce == cudaSuccess) ce = cudaMemcpy(g->table.ptr, v.data(), v.size() * sizeof(BatchEntry), cudaMemcpyHostToDevice);

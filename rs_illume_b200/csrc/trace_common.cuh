@@ -39,7 +39,11 @@ __device__ __forceinline__ uint64_t ray_count(const TraceArgs& a) {
 
 // Tests primitive record `r` (index in traversal order).  The shear constants
 // of the triangle test are set up on the first primitive a ray reaches.
-template <bool kClosest>
+// kAnalytic = false compiles the triangle test alone, for accels without
+// quadric or curve records: the call into the analytic shapes' tests costs a
+// kernel registers (spills at the 64-register occupancy target) even when it
+// never runs.
+template <bool kClosest, bool kAnalytic = true>
 __device__ __forceinline__ bool prim_test(const PrimRec* __restrict__ prims, const SphereRec* __restrict__ spheres,
                                           uint32_t r, TriRay& tr, bool& tr_ready, const RayIn& ray, float tmax,
                                           float& t, float& u, float& v, uint32_t& prim_id) {
@@ -47,7 +51,7 @@ __device__ __forceinline__ bool prim_test(const PrimRec* __restrict__ prims, con
     float4 a = __ldg(p), b = __ldg(p + 1), c = __ldg(p + 2);
     uint32_t flags = __float_as_uint(b.w);
     prim_id = __float_as_uint(a.w);
-    if (flags & kPrimSphere) {
+    if (kAnalytic && (flags & kPrimSphere)) {
         return quadric_test(spheres[__float_as_uint(c.w)], ray.ox, ray.oy, ray.oz, ray.dx, ray.dy, ray.dz,
                             tmax, t, u, v);
     }

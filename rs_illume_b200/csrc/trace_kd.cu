@@ -50,7 +50,7 @@ __device__ __forceinline__ float pick(uint32_t axis, float x, float y, float z) 
 
 constexpr int kKdBlock = 128;
 
-template <bool kAny>
+template <bool kAny, bool kAnalytic>
 struct KdTracer {
     RayIn ray;
     float ix, iy, iz;
@@ -114,11 +114,11 @@ struct KdTracer {
             float t, u, v;
             uint32_t pid;
             if (kAny) {
-                if (prim_test<false>(a.prims, a.spheres, r, tr, tr_ready, ray, ray.tmax, t, u, v, pid)) {
+                if (prim_test<false, kAnalytic>(a.prims, a.spheres, r, tr, tr_ready, ray, ray.tmax, t, u, v, pid)) {
                     occluded = true;
                     return true;
                 }
-            } else if (prim_test<true>(a.prims, a.spheres, r, tr, tr_ready, ray, best_t, t, u, v, pid) &&
+            } else if (prim_test<true, kAnalytic>(a.prims, a.spheres, r, tr, tr_ready, ray, best_t, t, u, v, pid) &&
                        (t < best_t || (t == best_t && pid < best))) {
                 best_t = t; best = pid; bu = u; bv = v;
             }
@@ -142,25 +142,25 @@ struct KdTracer {
     }
 };
 
-template <bool kAny>
+template <bool kAny, bool kAnalytic>
 __global__ void __launch_bounds__(kKdBlock) k_trace_kd(TraceArgs a) {
     uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= ray_count(a)) return;
     RayIn r = load_ray(a.rays, i);
-    KdTracer<kAny> T;
+    KdTracer<kAny, kAnalytic> T;
     T.init(r);
     if (a.n_nodes == 0 || !T.enters(a.bound)) { write_miss(i, r, a.hits, a.occ); return; }
     while (!T.step(a)) {}
     T.write(i, a);
 }
 
-template <bool kAny, int kMinBlocks>
+template <bool kAny, int kMinBlocks, bool kAnalytic>
 __global__ void __launch_bounds__(kKdBlock, kMinBlocks) k_trace_kd_persistent(TraceArgs a) {
     const uint64_t n = ray_count(a);
     const unsigned chunk = n < 2ull * gridDim.x * blockDim.x ? 32u : kChunk;
     const unsigned lane = threadIdx.x & 31u;
     const unsigned below = (1u << lane) - 1u;
-    KdTracer<kAny> T;
+    KdTracer<kAny, kAnalytic> T;
     bool active = false;
     uint64_t id = 0;
     unsigned long long chunk_next = 0, chunk_end = 0;   // warp-uniform
@@ -198,11 +198,11 @@ __global__ void __launch_bounds__(kKdBlock, kMinBlocks) k_trace_kd_persistent(Tr
     }
 }
 
-template <int kMinBlocks>
+template <int kMinBlocks, bool kAnalytic>
 cudaError_t launch_persistent(const TraceArgs& t, cudaStream_t s) {
     const unsigned block = kKdBlock;
-    auto kc = k_trace_kd_persistent<false, kMinBlocks>;
-    auto ka = k_trace_kd_persistent<true, kMinBlocks>;
+    auto kc = k_trace_kd_persistent<false, kMinBlocks, kAnalytic>;
+    auto ka = k_trace_kd_persistent<true, kMinBlocks, kAnalytic>;
     static int per_sm[2] = {0, 0};
     static int sms = 0;
     const int which = t.occ ? 1 : 0;
@@ -224,16 +224,22 @@ cudaError_t launch_persistent(const TraceArgs& t, cudaStream_t s) {
     return cudaGetLastError();
 }
 
-}  // namespace
-
-cudaError_t launch_trace_kd(const TraceArgs& t, const LaunchParams& lp, cudaStream_t s) {
+template <bool kAnalytic>
+cudaError_t launch_kd(const TraceArgs& t, const LaunchParams& lp, cudaStream_t s) {
     if (lp.persistent && t.counter)
-        return lp.min_blocks >= 8 ? launch_persistent<8>(t, s) : launch_persistent<1>(t, s);
+        return lp.min_blocks >= 8 ? launch_persistent<8, kAnalytic>(t, s) : launch_persistent<1, kAnalytic>(t, s);
     const unsigned block = kKdBlock;
     unsigned grid = (unsigned)((t.n + block - 1) / block);
-    if (t.occ) k_trace_kd<true><<<grid, block, 0, s>>>(t);
-    else k_trace_kd<false><<<grid, block, 0, s>>>(t);
+    if (t.occ) k_trace_kd<true, kAnalytic><<<grid, block, 0, s>>>(t);
+    else k_trace_kd<false, kAnalytic><<<grid, block, 0, s>>>(t);
     return cudaGetLastError();
+}
+
+}  // namespace
+
+// Trees without quadric or curve records run the triangle-only variants.
+cudaError_t launch_trace_kd(const TraceArgs& t, const LaunchParams& lp, cudaStream_t s) {
+    return t.spheres ? launch_kd<true>(t, lp, s) : launch_kd<false>(t, lp, s);
 }
 
 }  // namespace ilm

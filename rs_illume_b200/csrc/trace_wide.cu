@@ -16,12 +16,12 @@ namespace ilm {
 
 namespace {
 
-template <int W, int kStack, bool kAny>
+template <int W, int kStack, bool kAny, bool kAnalytic>
 __global__ void __launch_bounds__(128) k_trace_wide(TraceArgs a) {
     uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= ray_count(a)) return;
     RayIn r = load_ray(a.rays, i);
-    WideTracer<W, kStack, kAny> T;
+    WideTracer<W, kStack, kAny, kAnalytic> T;
     T.init(r);
     if (a.n_nodes == 0 || !T.enters(a.bound)) { write_miss(i, r, a.hits, a.occ); return; }
     while (!T.step(a)) {}
@@ -30,7 +30,7 @@ __global__ void __launch_bounds__(128) k_trace_wide(TraceArgs a) {
 
 // kMinBlocks > 0 asks the compiler for that many resident 128-thread blocks
 // per SM (64 registers at 8), trading a few spills for more warps in flight.
-template <int W, int kStack, bool kAny, int kMinBlocks>
+template <int W, int kStack, bool kAny, int kMinBlocks, bool kAnalytic>
 __global__ void __launch_bounds__(128, kMinBlocks) k_trace_wide_persistent(TraceArgs a) {
     const uint64_t n = ray_count(a);
     // A short queue (fewer than two rays per resident lane) is claimed one ray
@@ -38,7 +38,7 @@ __global__ void __launch_bounds__(128, kMinBlocks) k_trace_wide_persistent(Trace
     const unsigned chunk = n < 2ull * gridDim.x * blockDim.x ? 32u : kChunk;
     const unsigned lane = threadIdx.x & 31u;
     const unsigned below = (1u << lane) - 1u;
-    WideTracer<W, kStack, kAny> T;
+    WideTracer<W, kStack, kAny, kAnalytic> T;
     bool active = false;
     uint64_t id = 0;
     unsigned long long chunk_next = 0, chunk_end = 0;   // warp-uniform
@@ -76,12 +76,12 @@ __global__ void __launch_bounds__(128, kMinBlocks) k_trace_wide_persistent(Trace
     }
 }
 
-template <int W, int kStack, int kMinBlocks>
+template <int W, int kStack, int kMinBlocks, bool kAnalytic>
 cudaError_t launch_persistent(const TraceArgs& t, cudaStream_t s) {
     const unsigned block = 128;
     {
-        auto kc = k_trace_wide_persistent<W, kStack, false, kMinBlocks>;
-        auto ka = k_trace_wide_persistent<W, kStack, true, kMinBlocks>;
+        auto kc = k_trace_wide_persistent<W, kStack, false, kMinBlocks, kAnalytic>;
+        auto ka = k_trace_wide_persistent<W, kStack, true, kMinBlocks, kAnalytic>;
         static int per_sm[2] = {0, 0};
         static int sms = 0;
         int which = t.occ ? 1 : 0;
@@ -104,18 +104,42 @@ cudaError_t launch_persistent(const TraceArgs& t, cudaStream_t s) {
     }
 }
 
-template <int W, int kStack>
-cudaError_t launch(const TraceArgs& t, const LaunchParams& lp, cudaStream_t s) {
+template <int W, int kStack, bool kAnalytic>
+cudaError_t launch_variant(const TraceArgs& t, const LaunchParams& lp, cudaStream_t s) {
     const unsigned block = 128;
     if (lp.persistent && t.counter)
-        return lp.min_blocks >= 8 ? launch_persistent<W, kStack, 8>(t, s) : launch_persistent<W, kStack, 1>(t, s);
+        return lp.min_blocks >= 8 ? launch_persistent<W, kStack, 8, kAnalytic>(t, s)
+                                  : launch_persistent<W, kStack, 1, kAnalytic>(t, s);
     unsigned grid = (unsigned)((t.n + block - 1) / block);
-    if (t.occ) k_trace_wide<W, kStack, true><<<grid, block, 0, s>>>(t);
-    else k_trace_wide<W, kStack, false><<<grid, block, 0, s>>>(t);
+    if (t.occ) k_trace_wide<W, kStack, true, kAnalytic><<<grid, block, 0, s>>>(t);
+    else k_trace_wide<W, kStack, false, kAnalytic><<<grid, block, 0, s>>>(t);
     return cudaGetLastError();
 }
 
+// Accels without quadric or curve records run the triangle-only variants.
+template <int W, int kStack>
+cudaError_t launch(const TraceArgs& t, const LaunchParams& lp, cudaStream_t s) {
+    return t.spheres ? launch_variant<W, kStack, true>(t, lp, s) : launch_variant<W, kStack, false>(t, lp, s);
+}
+
 }  // namespace
+
+uint64_t wide_grid_wave(int width, int stack_depth) {
+    static uint64_t cache[2][2] = {{0, 0}, {0, 0}};
+    const int wi = width == 8, di = stack_depth > 32;
+    if (cache[wi][di]) return cache[wi][di];
+    const void* k = wi ? (di ? (const void*)k_trace_wide<8, 64, false, true> : (const void*)k_trace_wide<8, 32, false, true>)
+                       : (di ? (const void*)k_trace_wide<4, 64, false, true> : (const void*)k_trace_wide<4, 32, false, true>);
+    int dev = 0, sms = 0, per_sm = 0;
+    cudaGetDevice(&dev);
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, 128, 0) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    cache[wi][di] = (uint64_t)sms * (uint64_t)per_sm * 128u;
+    return cache[wi][di];
+}
 
 cudaError_t launch_trace_wide(int width, const TraceArgs& t, const LaunchParams& lp, cudaStream_t s) {
     bool deep = lp.stack_depth > 32;

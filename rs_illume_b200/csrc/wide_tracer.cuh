@@ -126,7 +126,7 @@ __device__ __forceinline__ void sort_keys(uint32_t* k) {
 }
 
 // Per-lane traversal state of one ray.
-template <int W, int kStack, bool kAny>
+template <int W, int kStack, bool kAny, bool kAnalytic = true>
 struct WideTracer {
     RayIn ray;
     float ix, iy, iz;
@@ -208,11 +208,13 @@ struct WideTracer {
             float t, u, v;
             uint32_t pid;
             if (kAny) {
-                if (prim_test<false>(prims, spheres, start + k, tr, tr_ready, ray, ray.tmax, t, u, v, pid)) {
+                if (prim_test<false, kAnalytic>(prims, spheres, start + k, tr, tr_ready, ray, ray.tmax, t, u, v,
+                                                pid)) {
                     occluded = true;
                     return;
                 }
-            } else if (prim_test<true>(prims, spheres, start + k, tr, tr_ready, ray, best_t, t, u, v, pid) &&
+            } else if (prim_test<true, kAnalytic>(prims, spheres, start + k, tr, tr_ready, ray, best_t, t, u, v,
+                                                  pid) &&
                        (t < best_t || (t == best_t && pid < best))) {
                 best_t = t; best = pid; bu = u; bv = v;
             }
