@@ -450,21 +450,34 @@ struct Collapser {
     }
 };
 
-// Smallest scale 2^e covering the node extent in 255 steps, with every child
-// plane rounded outward in float arithmetic identical to the kernel's
-// fmaf(q, scale, origin).
-bool quantize_axis(float origin, const std::vector<Entry>& ch, int axis, int e, uint8_t* qlo,
-                   uint8_t* qhi) {
-    float s = std::ldexp(1.0f, e);
+// Dequantised plane q of an axis with scale s and biased origin b, exactly as
+// the kernel computes it: fmaf(2^23 + q, s, b).  2^23 + q is the float whose
+// low mantissa byte is q, which the kernel forms with one byte permute.
+float dequant(int q, float s, float b) { return std::fma((float)(8388608 + q), s, b); }
+
+// Biased origin for grid start `mn`: the largest float b with
+// 2^23 * s + b <= mn, so that dequant(0) <= mn.
+float biased_origin(float mn, float s) {
+    double d = (double)mn - std::ldexp((double)s, 23);
+    float b = (float)d;
+    if ((double)b > d) b = std::nextafter(b, -INFINITY);
+    return b;
+}
+
+// Every child plane of one axis rounded outward on the grid (scale s, biased
+// origin b), checked with the kernel's arithmetic; false when 255 steps do not
+// reach a plane.
+bool quantize_axis(float b, float s, const std::vector<Entry>& ch, int axis, uint8_t* qlo, uint8_t* qhi) {
+    const double base = (double)dequant(0, s, b);
     for (size_t c = 0; c < ch.size(); ++c) {
         float lo = ch[c].box.mn[axis], hi = ch[c].box.mx[axis];
-        double fl = std::floor(((double)lo - (double)origin) / (double)s);
-        double fh = std::ceil(((double)hi - (double)origin) / (double)s);
+        double fl = std::floor(((double)lo - base) / (double)s);
+        double fh = std::ceil(((double)hi - base) / (double)s);
         int ql = (int)std::max(0.0, std::min(255.0, fl));
         int qh = (int)std::max(0.0, std::min(256.0, fh));
-        while (ql > 0 && std::fma((float)ql, s, origin) > lo) --ql;
-        while (qh <= 255 && std::fma((float)qh, s, origin) < hi) ++qh;
-        if (qh > 255 || std::fma((float)ql, s, origin) > lo) return false;
+        while (ql > 0 && dequant(ql, s, b) > lo) --ql;
+        while (qh <= 255 && dequant(qh, s, b) < hi) ++qh;
+        if (qh > 255 || dequant(ql, s, b) > lo) return false;
         qlo[c] = (uint8_t)ql;
         qhi[c] = (uint8_t)qh;
     }
@@ -512,12 +525,19 @@ void collapse_wide(const std::vector<BinNode>& bin, const std::vector<BuildPrim>
         if (prim_off > kMaxPrimsPerNode) throw std::runtime_error("wide node holds too many primitives");
         float origin[3];
         for (int a = 0; a < 3; ++a) {
-            origin[a] = nbx.mn[a];
+            // 254 steps over the extent leave one for the biased origin's
+            // rounding below the node's lower plane
             double ext = (double)nbx.mx[a] - (double)nbx.mn[a];
             int e2 = -126;
-            if (ext > 0.0) e2 = std::max(-126, (int)std::ceil(std::log2(ext / 255.0)));
-            while (!quantize_axis(origin[a], ch, a, e2, qlo[a], qhi[a])) {
-                if (++e2 > 127) throw std::runtime_error("cannot quantise node bounds");
+            if (ext > 0.0) e2 = std::max(-126, (int)std::ceil(std::log2(ext / 254.0)));
+            // a step far below the plane's float spacing only spends passes
+            float mag = std::max(std::fabs(nbx.mn[a]), std::fabs(nbx.mx[a]));
+            if (mag > 0.0f) e2 = std::max(e2, std::ilogb(mag) - 23 - 8);
+            for (;;) {
+                float sc = std::ldexp(1.0f, e2);
+                origin[a] = biased_origin(nbx.mn[a], sc);
+                if (std::isfinite(origin[a]) && quantize_axis(origin[a], sc, ch, a, qlo[a], qhi[a])) break;
+                if (++e2 > 104) throw std::runtime_error("cannot quantise node bounds");
             }
             ex[a] = (uint8_t)(e2 + 127);
         }

@@ -53,8 +53,10 @@ struct SphereRec {
 static_assert(sizeof(SphereRec) == 256, "SphereRec must be 256 bytes");
 
 // Compressed wide node.  Child boxes are quantised to 8 bits per plane on a
-// per-node grid: plane = fma(q, 2^(e-127), origin), with q rounded outward at
-// build time so every dequantised box contains its child's exact box.
+// per-node grid: plane = fma(2^23 + q, 2^(e-127), origin), where origin is the
+// grid start biased by -2^23 * 2^(e-127) (so the kernel forms 2^23 + q with
+// one byte permute and subtracts nothing), with q rounded outward at build
+// time so every dequantised box contains its child's exact box.
 //   word 0: origin x, y, z (float), packed = ex | ey<<8 | ez<<16 | imask<<24
 //   word 1: child_base, prim_base, meta[W] ...
 //   then qlo_x[W], qlo_y[W], qlo_z[W], qhi_x[W], qhi_y[W], qhi_z[W] (bytes)

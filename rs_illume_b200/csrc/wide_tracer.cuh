@@ -20,13 +20,13 @@ __device__ __forceinline__ uint32_t byte_of(uint32_t lo, uint32_t hi, int i) {
     return __byte_perm(i < 4 ? lo : hi, 0u, (uint32_t)(i & 3) | 0x4440u);
 }
 
-// The same byte as an exact float, without an integer-to-float conversion
-// (those issue on the narrow XU pipe, which the 48 conversions per node
-// saturate): the byte becomes the low mantissa bits of 2^23, and 2^23 is
-// subtracted again.  Both steps are exact, so the value equals (float)byte.
+// The float 2^23 + byte, formed by one byte permute that writes the byte into
+// the low mantissa bits of 2^23 (no integer-to-float conversion: those issue
+// on the narrow XU pipe, which 48 conversions per node saturate).  Nodes
+// store their origin biased by -2^23 * scale, so fma(2^23 + q, scale, origin)
+// is the dequantised plane with no subtraction of the bias.
 __device__ __forceinline__ float byte_float(uint32_t lo, uint32_t hi, int i) {
-    uint32_t bits = __byte_perm(i < 4 ? lo : hi, 0x4B000000u, (uint32_t)(i & 3) | 0x7650u);
-    return __fsub_rn(__uint_as_float(bits), 8388608.0f);
+    return __uint_as_float(__byte_perm(i < 4 ? lo : hi, 0x4B000000u, (uint32_t)(i & 3) | 0x7650u));
 }
 
 // Decoded node, with near/far planes already swapped for the ray octant.

@@ -68,12 +68,14 @@ def host_kdtree(xyz, idx, spheres=(), threads=0, isect_cost=80, traversal_cost=1
 
 
 def dequantised_boxes(node, width):
-    """(W, 2, 3) float32 child boxes of one wide node: fma(q, 2^(e-127), origin)."""
+    """(W, 2, 3) float32 child boxes of one wide node: fma(2^23 + q, 2^(e-127),
+    origin), the origin biased by -2^23 * 2^(e-127).  The sum is exact in
+    float64, so one cast to float32 rounds as the fma does."""
     ex = [(int(node["packed"]) >> (8 * a)) & 0xFF for a in range(3)]
     out = np.zeros((width, 2, 3), np.float32)
     for a in range(3):
         s = 2.0 ** (ex[a] - 127)
         o = float(node["origin"][a])
-        out[:, 0, a] = (o + node["qlo"][a].astype(np.float64) * s).astype(np.float32)
-        out[:, 1, a] = (o + node["qhi"][a].astype(np.float64) * s).astype(np.float32)
+        out[:, 0, a] = (o + (8388608.0 + node["qlo"][a].astype(np.float64)) * s).astype(np.float32)
+        out[:, 1, a] = (o + (8388608.0 + node["qhi"][a].astype(np.float64)) * s).astype(np.float32)
     return out
