@@ -595,6 +595,21 @@ int32_t ilm_scene_file_materials(const ilm_scene_file* sf, float* albedo, float*
 int32_t ilm_scene_file_build(ilm_context* ctx, const ilm_scene_file* sf, ilm_accel_id* accel_out,
                              ilm_pt_scene_id* pt_out);
 int32_t ilm_scene_file_destroy(ilm_scene_file* sf);
+/* The directive tree of a scene description, read by the loader's tokenizer
+ * and argument grammar but not run: what the reference's parse_to_ast
+ * returns (core/parser/mod.rs:19-34; grammar of core/parser/parsers/).  JSON:
+ * {"directives": [node...], "comments": [text after '#'...]}, a node being
+ * {"directive", "file", "line", "num": [numeric arguments], "str": [quoted
+ * arguments or ActiveTransform's word], "params": [{"type", "name", "num",
+ * "str"}...]} plus "children" for AttributeBegin, TransformBegin,
+ * ObjectBegin and WorldBegin blocks (the matching end closes the block and
+ * is not listed).  Include is replaced by the named file's directives, its
+ * path relative to the including file or, from text, to base_dir.
+ * *json_len = the JSON's length; up to json_cap - 1 bytes of it and a NUL
+ * are written to json (json_cap = 0 only measures).  On a syntax error
+ * returns ILM_ERR_INVALID_ARGUMENT with the message in `error`. */
+int32_t ilm_scene_syntax(const char* text, const char* base_dir, char* json, size_t json_cap, size_t* json_len,
+                         char* error, size_t error_len);
 
 /* Device error word accumulated by the kernels since the last reset
  * (bit 0: traversal stack overflow, bit 1: iteration cap).  Synchronises. */

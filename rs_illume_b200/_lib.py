@@ -212,6 +212,8 @@ SIGNATURES = {
     "ilm_scene_file_curves": (_I32, [_P, _P, _P]),
     "ilm_scene_file_build": (_I32, [_P, _P, ctypes.POINTER(_U32), ctypes.POINTER(_U32)]),
     "ilm_scene_file_destroy": (_I32, [_P]),
+    "ilm_scene_syntax": (_I32, [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_size_t,
+                                ctypes.POINTER(ctypes.c_size_t), ctypes.c_char_p, ctypes.c_size_t]),
     "ilm_intersect_closest": (_I32, [_P, _U32, _P, _U64, _P, _P]),
     "ilm_intersect_any": (_I32, [_P, _U32, _P, _U64, _P, _P]),
     "ilm_intersect_closest_noalloc": (_I32, [_P, _U32, _P, _U64, _P, _P]),

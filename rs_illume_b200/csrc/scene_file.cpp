@@ -1,13 +1,17 @@
 // pbrt-v3 scene files -> shapes, materials, camera and render settings.
 //
-// The reference defines the syntax tree of these files (core/parser/ast.rs:
-// directives, parameter lists, transform, attribute, world and object blocks)
-// and a ParamSet for typed parameter lookup (core/paramset.rs:303-511), but
-// its parse() constructs nothing (core/parser/mod.rs:36-46) and its parser
-// module is missing.  This file tokenises the text, runs each directive
-// against pbrt's graphics state and keeps what the ray-query and path-tracing
-// library can represent; directive semantics and parameter defaults follow
-// pbrt-v3 (api.cpp and the shape / material / camera factories).
+// The reference parses these files into a syntax tree (parse_to_ast,
+// core/parser/mod.rs:19-34, with the grammar of core/parser/parsers/ and the
+// tree of core/parser/ast.rs) and has a ParamSet for typed parameter lookup
+// (core/paramset.rs:303-511), but its parse() constructs nothing from the
+// tree (core/parser/mod.rs:36-46).  This file tokenises the text, reads each
+// directive's arguments with one grammar table (Reader::read_directive), runs
+// the directive against pbrt's graphics state and keeps what the ray-query
+// and path-tracing library can represent; directive semantics and parameter
+// defaults follow pbrt-v3 (api.cpp and the shape / material / camera
+// factories).  ilm_scene_syntax returns the directive tree that the same
+// reader produces, without running it, for comparison with the reference's
+// parser tests.
 //
 // Transforms are kept in double precision as (matrix, inverse) pairs and
 // rounded to float when a shape takes them.  Normals go through the inverse
@@ -175,7 +179,10 @@ struct Token {
     throw std::runtime_error(file + ":" + std::to_string(line) + ": " + msg);
 }
 
-void tokenize(const std::string& src, int file, const std::string& fname, std::vector<Token>& out) {
+// Whitespace and '#' comments separate tokens; a comment runs to the end of
+// its line.  `comments`, when given, receives each comment's text after '#'.
+void tokenize(const std::string& src, int file, const std::string& fname, std::vector<Token>& out,
+              std::vector<std::string>* comments = nullptr) {
     int line = 1;
     size_t i = 0, n = src.size();
     while (i < n) {
@@ -183,7 +190,10 @@ void tokenize(const std::string& src, int file, const std::string& fname, std::v
         if (c == '\n') { ++line; ++i; continue; }
         if (std::isspace((unsigned char)c)) { ++i; continue; }
         if (c == '#') {
-            while (i < n && src[i] != '\n') ++i;
+            size_t j = i + 1;
+            while (j < n && src[j] != '\n') ++j;
+            if (comments) comments->push_back(src.substr(i + 1, j - i - 1));
+            i = j;
             continue;
         }
         Token t;
@@ -351,7 +361,184 @@ struct GState {
     double le[3] = {0, 0, 0};
 };
 
-class Parser {
+// ------------------------------------------------------------------ reader
+// A directive as read from the token stream: its name token, the arguments
+// its grammar fixes (numbers, quoted strings, or one bare word) and its
+// parameter list.
+struct Directive {
+    Token tok;
+    std::vector<double> num;
+    std::vector<std::string> str;
+    Params params;
+};
+
+// Argument grammar of one directive: `numbers` numbers (bracketed or not),
+// `quoted` quoted strings and up to `more_quoted` further ones, or one bare
+// `word`; `params` when a parameter list follows.  The directives and their
+// arguments are those of core/parser/parsers/directives.rs and transforms.rs
+// (pbrt-v3's file format).
+struct Grammar {
+    int numbers = 0, quoted = 0, more_quoted = 0;
+    bool word = false, params = false;
+};
+
+const std::map<std::string, Grammar>& grammar() {
+    static const std::map<std::string, Grammar> g = [] {
+        std::map<std::string, Grammar> m;
+        auto nums = [](int k) { Grammar x; x.numbers = k; return x; };
+        auto names = [](int k, bool params) { Grammar x; x.quoted = k; x.params = params; return x; };
+        for (const char* d : {"Identity", "ReverseOrientation", "WorldBegin", "WorldEnd", "AttributeBegin",
+                              "AttributeEnd", "TransformBegin", "TransformEnd", "ObjectEnd"})
+            m[d] = Grammar();
+        m["Translate"] = nums(3);
+        m["Scale"] = nums(3);
+        m["Rotate"] = nums(4);
+        m["LookAt"] = nums(9);
+        m["Transform"] = nums(16);
+        m["ConcatTransform"] = nums(16);
+        m["TransformTimes"] = nums(2);
+        Grammar w;
+        w.word = true;
+        m["ActiveTransform"] = w;
+        for (const char* d : {"CoordinateSystem", "CoordSysTransform", "ObjectBegin", "ObjectInstance",
+                              "NamedMaterial", "Include"})
+            m[d] = names(1, false);
+        for (const char* d : {"Shape", "Material", "MakeNamedMaterial", "AreaLightSource", "LightSource", "Camera",
+                              "Film", "Sampler", "Integrator", "PixelFilter", "Accelerator", "MakeNamedMedium"})
+            m[d] = names(1, true);
+        m["Texture"] = names(3, true);
+        Grammar mi = names(1, false);
+        mi.more_quoted = 1;
+        m["MediumInterface"] = mi;
+        return m;
+    }();
+    return g;
+}
+
+// Token-level reading shared by the loader and the syntax dump.
+class Reader {
+public:
+    // The next directive and its arguments, by the grammar table.
+    Directive read_directive(const std::vector<Token>& toks, size_t& i) const {
+        Directive D;
+        D.tok = toks[i++];
+        const Token& d = D.tok;
+        if (d.quoted || d.text == "[" || d.text == "]") fail(d, "expected a directive, found \"" + d.text + "\"");
+        auto it = grammar().find(d.text);
+        if (it == grammar().end()) fail(d, "unknown directive \"" + d.text + "\"");
+        const Grammar& g = it->second;
+        if (g.numbers) D.num = numbers(toks, i, d, (size_t)g.numbers);
+        for (int k = 0; k < g.quoted; ++k) D.str.push_back(quoted(toks, i, d));
+        for (int k = 0; k < g.more_quoted && i < toks.size() && toks[i].quoted; ++k) D.str.push_back(toks[i++].text);
+        if (g.word) {
+            const Token& w = next(toks, i, d);
+            if (w.quoted || (w.text != "StartTime" && w.text != "EndTime" && w.text != "All"))
+                fail(w, d.text + " takes StartTime, EndTime or All");
+            D.str.push_back(w.text);
+        }
+        if (g.params) D.params = params(toks, i);
+        return D;
+    }
+
+protected:
+    std::vector<std::string> files_;
+
+    const std::string& fname(const Token& t) const { return files_[t.file]; }
+
+    [[noreturn]] void fail(const Token& t, const std::string& msg) const { fail_at(fname(t), t.line, msg); }
+
+    const Token& next(const std::vector<Token>& toks, size_t& i, const Token& ctx) const {
+        if (i >= toks.size()) fail(ctx, "unexpected end of input after " + ctx.text);
+        return toks[i++];
+    }
+
+    double number(const Token& t) const {
+        if (t.quoted || t.text == "[" || t.text == "]") fail(t, "expected a number, found \"" + t.text + "\"");
+        char* end = nullptr;
+        errno = 0;
+        double v = std::strtod(t.text.c_str(), &end);
+        if (end != t.text.c_str() + t.text.size() || errno == ERANGE || !std::isfinite(v))
+            fail(t, "expected a number, found \"" + t.text + "\"");
+        return v;
+    }
+
+    std::vector<double> numbers(const std::vector<Token>& toks, size_t& i, const Token& dir, size_t count) const {
+        std::vector<double> v;
+        bool bracket = i < toks.size() && !toks[i].quoted && toks[i].text == "[";
+        if (bracket) ++i;
+        while (v.size() < count) v.push_back(number(next(toks, i, dir)));
+        if (bracket) {
+            const Token& t = next(toks, i, dir);
+            if (t.quoted || t.text != "]") fail(t, dir.text + " takes " + std::to_string(count) + " numbers");
+        }
+        return v;
+    }
+
+    std::string quoted(const std::vector<Token>& toks, size_t& i, const Token& dir) const {
+        const Token& t = next(toks, i, dir);
+        if (!t.quoted) fail(t, dir.text + " expects a quoted string, found " + t.text);
+        return t.text;
+    }
+
+    // "type name" value | "type name" [ values ]
+    Params params(const std::vector<Token>& toks, size_t& i) const {
+        Params ps;
+        while (i < toks.size() && toks[i].quoted) {
+            const Token& decl = toks[i++];
+            std::istringstream ds(decl.text);
+            Param p;
+            ds >> p.type >> p.name;
+            std::string extra;
+            if (p.type.empty() || p.name.empty() || (ds >> extra))
+                fail(decl, "malformed parameter declaration \"" + decl.text + "\"");
+            if (p.type == "point3") p.type = "point";
+            if (p.type == "vector3") p.type = "vector";
+            if (p.type == "normal3") p.type = "normal";
+            static const std::set<std::string> known = {"integer", "float", "point2", "vector2", "point", "vector",
+                                                        "normal", "rgb", "color", "xyz", "spectrum", "blackbody",
+                                                        "bool", "string", "texture"};
+            if (!known.count(p.type)) fail(decl, "unknown parameter type \"" + p.type + "\"");
+            p.is_string = p.type == "string" || p.type == "bool" || p.type == "texture" ||
+                          (p.type == "spectrum" && i < toks.size() && (toks[i].quoted ||
+                           (toks[i].text == "[" && i + 1 < toks.size() && toks[i + 1].quoted)));
+            p.line = decl.line;
+            const Token& first = next(toks, i, decl);
+            // integers are -?digits and booleans "true" or "false", as the
+            // reference's grammar reads them (parse_int, values.rs;
+            // parse_boolean_parameter, parameters.rs)
+            auto take = [&](const Token& t) {
+                if (p.is_string) {
+                    if (!t.quoted) fail(t, "parameter \"" + p.name + "\" takes quoted strings");
+                    if (p.type == "bool" && t.text != "true" && t.text != "false")
+                        fail(t, "parameter \"" + p.name + "\" takes \"true\" or \"false\"");
+                    p.str.push_back(t.text);
+                } else {
+                    if (p.type == "integer") {
+                        size_t k = !t.quoted && !t.text.empty() && t.text[0] == '-' ? 1 : 0;
+                        bool digits = !t.quoted && k < t.text.size();
+                        for (size_t j = k; j < t.text.size(); ++j) digits = digits && std::isdigit((unsigned char)t.text[j]);
+                        if (!digits) fail(t, "parameter \"" + p.name + "\" takes integers, found \"" + t.text + "\"");
+                    }
+                    p.num.push_back(number(t));
+                }
+            };
+            if (!first.quoted && first.text == "[") {
+                for (;;) {
+                    const Token& t = next(toks, i, decl);
+                    if (!t.quoted && t.text == "]") break;
+                    take(t);
+                }
+            } else {
+                take(first);
+            }
+            ps.items.push_back(std::move(p));
+        }
+        ps.file = i > 0 ? files_[toks[i - 1].file] : std::string();
+        return ps;
+    }
+};
+
+class Parser : public Reader {
 public:
     explicit Parser(ilm_scene_file* out) : out_(out) {}
 
@@ -415,88 +602,6 @@ public:
     }
 
 private:
-    const std::string& fname(const Token& t) const { return files_[t.file]; }
-
-    [[noreturn]] void fail(const Token& t, const std::string& msg) const { fail_at(fname(t), t.line, msg); }
-
-    const Token& next(const std::vector<Token>& toks, size_t& i, const Token& ctx) const {
-        if (i >= toks.size()) fail(ctx, "unexpected end of input after " + ctx.text);
-        return toks[i++];
-    }
-
-    double number(const Token& t) const {
-        if (t.quoted || t.text == "[" || t.text == "]") fail(t, "expected a number, found \"" + t.text + "\"");
-        char* end = nullptr;
-        errno = 0;
-        double v = std::strtod(t.text.c_str(), &end);
-        if (end != t.text.c_str() + t.text.size() || errno == ERANGE || !std::isfinite(v))
-            fail(t, "expected a number, found \"" + t.text + "\"");
-        return v;
-    }
-
-    std::vector<double> numbers(const std::vector<Token>& toks, size_t& i, const Token& dir, size_t count) const {
-        std::vector<double> v;
-        bool bracket = i < toks.size() && !toks[i].quoted && toks[i].text == "[";
-        if (bracket) ++i;
-        while (v.size() < count) v.push_back(number(next(toks, i, dir)));
-        if (bracket) {
-            const Token& t = next(toks, i, dir);
-            if (t.quoted || t.text != "]") fail(t, dir.text + " takes " + std::to_string(count) + " numbers");
-        }
-        return v;
-    }
-
-    std::string quoted(const std::vector<Token>& toks, size_t& i, const Token& dir) const {
-        const Token& t = next(toks, i, dir);
-        if (!t.quoted) fail(t, dir.text + " expects a quoted string, found " + t.text);
-        return t.text;
-    }
-
-    // "type name" value | "type name" [ values ]
-    Params params(const std::vector<Token>& toks, size_t& i) const {
-        Params ps;
-        while (i < toks.size() && toks[i].quoted) {
-            const Token& decl = toks[i++];
-            std::istringstream ds(decl.text);
-            Param p;
-            ds >> p.type >> p.name;
-            std::string extra;
-            if (p.type.empty() || p.name.empty() || (ds >> extra))
-                fail(decl, "malformed parameter declaration \"" + decl.text + "\"");
-            if (p.type == "point3") p.type = "point";
-            if (p.type == "vector3") p.type = "vector";
-            if (p.type == "normal3") p.type = "normal";
-            static const std::set<std::string> known = {"integer", "float", "point2", "vector2", "point", "vector",
-                                                        "normal", "rgb", "color", "xyz", "spectrum", "blackbody",
-                                                        "bool", "string", "texture"};
-            if (!known.count(p.type)) fail(decl, "unknown parameter type \"" + p.type + "\"");
-            p.is_string = p.type == "string" || p.type == "bool" || p.type == "texture" ||
-                          (p.type == "spectrum" && i < toks.size() && (toks[i].quoted ||
-                           (toks[i].text == "[" && i + 1 < toks.size() && toks[i + 1].quoted)));
-            p.line = decl.line;
-            const Token& first = next(toks, i, decl);
-            auto take = [&](const Token& t) {
-                if (p.is_string) {
-                    if (!t.quoted) fail(t, "parameter \"" + p.name + "\" takes quoted strings");
-                    p.str.push_back(t.text);
-                } else {
-                    p.num.push_back(number(t));
-                }
-            };
-            if (!first.quoted && first.text == "[") {
-                for (;;) {
-                    const Token& t = next(toks, i, decl);
-                    if (!t.quoted && t.text == "]") break;
-                    take(t);
-                }
-            } else {
-                take(first);
-            }
-            ps.items.push_back(std::move(p));
-        }
-        ps.file = i > 0 ? files_[toks[i - 1].file] : std::string();
-        return ps;
-    }
 
     void warn(const Token& t, const std::string& msg) { warn_.push_back(fname(t) + ":" + std::to_string(t.line) + ": " + msg); }
 
@@ -725,32 +830,30 @@ private:
         out_->meshes.push_back(std::move(m));
     }
 
-    void directive(const std::vector<Token>& toks, size_t& i) {
-        const Token& d = toks[i++];
-        if (d.quoted || d.text == "[" || d.text == "]") fail(d, "expected a directive, found \"" + d.text + "\"");
+    void directive(const std::vector<Token>& toks, size_t& i) { execute(read_directive(toks, i)); }
+
+    void execute(const Directive& D) {
+        const Token& d = D.tok;
         const std::string& n = d.text;
+        const std::vector<double>& v = D.num;
+        const Params& ps = D.params;
         auto done = [&](const Params& ps, const std::string& what) { ps.report_unused(what, warn_); };
         if (n == "Identity") {
             st_.ctm = Xform();
         } else if (n == "Translate") {
-            auto v = numbers(toks, i, d, 3);
             apply(translate(v[0], v[1], v[2]));
         } else if (n == "Scale") {
-            auto v = numbers(toks, i, d, 3);
             if (v[0] == 0 || v[1] == 0 || v[2] == 0) fail(d, "Scale by zero");
             apply(scale(v[0], v[1], v[2]));
         } else if (n == "Rotate") {
-            auto v = numbers(toks, i, d, 4);
             if (v[1] == 0 && v[2] == 0 && v[3] == 0) fail(d, "Rotate about a zero axis");
             apply(rotate(v[0], v[1], v[2], v[3]));
         } else if (n == "LookAt") {
-            auto v = numbers(toks, i, d, 9);
             Xform la;
             if (!look_at(&v[0], &v[3], &v[6], &la)) warn(d, "LookAt with up parallel to the view direction; ignored");
             else apply(la);
         } else if (n == "Transform" || n == "ConcatTransform") {
             // 16 numbers, the matrix's columns (pbrt-v3 transposes them)
-            auto v = numbers(toks, i, d, 16);
             Mat4 m;
             for (int r = 0; r < 4; ++r)
                 for (int c = 0; c < 4; ++c) m.m[c][r] = v[4 * r + c];
@@ -760,18 +863,15 @@ private:
             if (n == "Transform") st_.ctm = x;
             else apply(x);
         } else if (n == "CoordinateSystem") {
-            named_[quoted(toks, i, d)] = st_.ctm;
+            named_[D.str[0]] = st_.ctm;
         } else if (n == "CoordSysTransform") {
-            std::string name = quoted(toks, i, d);
+            const std::string& name = D.str[0];
             auto it = named_.find(name);
             if (it == named_.end()) warn(d, "coordinate system \"" + name + "\" not declared; ignored");
             else st_.ctm = it->second;
         } else if (n == "ActiveTransform") {
-            const Token& w = next(toks, i, d);
-            if (w.text != "StartTime" && w.text != "EndTime" && w.text != "All") fail(w, "ActiveTransform takes StartTime, EndTime or All");
-            if (w.text != "All") warn(d, "motion transforms are not supported; both times get every transform");
+            if (D.str[0] != "All") warn(d, "motion transforms are not supported; both times get every transform");
         } else if (n == "TransformTimes") {
-            numbers(toks, i, d, 2);
             warn(d, "TransformTimes ignored (no motion blur)");
         } else if (n == "ReverseOrientation") {
             st_.reverse = !st_.reverse;
@@ -791,7 +891,7 @@ private:
             if (f.transform_only) st_.ctm = f.state.ctm;
             else st_ = f.state;
         } else if (n == "ObjectBegin") {
-            std::string name = quoted(toks, i, d);
+            const std::string& name = D.str[0];
             if (in_object_) fail(d, "ObjectBegin inside an object");
             stack_.push_back({st_, false});
             in_object_ = true;
@@ -804,14 +904,13 @@ private:
             st_ = stack_.back().state;
             stack_.pop_back();
         } else if (n == "ObjectInstance") {
-            std::string name = quoted(toks, i, d);
+            const std::string& name = D.str[0];
             auto it = objects_.find(name);
             if (it == objects_.end()) fail(d, "object \"" + name + "\" not defined");
             for (const ShapeRecord& r : it->second)
                 emit_shape(d, r.type, r.params, compose(st_.ctm, r.ctm), r.reverse, r.material);
         } else if (n == "Shape") {
-            std::string type = quoted(toks, i, d);
-            Params ps = params(toks, i);
+            const std::string& type = D.str[0];
             if (in_object_) {
                 if (st_.emits) warn(d, "area lights inside object instances are not supported; shape not emissive");
                 GState g = st_;
@@ -823,13 +922,11 @@ private:
                 done(ps, "shape \"" + type + "\"");
             }
         } else if (n == "Material") {
-            std::string type = quoted(toks, i, d);
-            Params ps = params(toks, i);
+            const std::string& type = D.str[0];
             set_material(d, type, ps, st_);
             done(ps, "material \"" + type + "\"");
         } else if (n == "MakeNamedMaterial") {
-            std::string name = quoted(toks, i, d);
-            Params ps = params(toks, i);
+            const std::string& name = D.str[0];
             std::string type = ps.one_string("type", "");
             if (type.empty()) fail(d, "MakeNamedMaterial needs \"string type\"");
             GState g;
@@ -837,13 +934,12 @@ private:
             std::copy(g.kd, g.kd + 3, named_mats_[name].kd);
             done(ps, "material \"" + name + "\"");
         } else if (n == "NamedMaterial") {
-            std::string name = quoted(toks, i, d);
+            const std::string& name = D.str[0];
             auto it = named_mats_.find(name);
             if (it == named_mats_.end()) fail(d, "named material \"" + name + "\" not defined");
             std::copy(it->second.kd, it->second.kd + 3, st_.kd);
         } else if (n == "AreaLightSource") {
-            std::string type = quoted(toks, i, d);
-            Params ps = params(toks, i);
+            const std::string& type = D.str[0];
             if (type != "diffuse") {
                 warn(d, "area light \"" + type + "\" is not supported; shapes stay non-emissive");
                 for (const Param& p : ps.items) p.used = true;
@@ -860,13 +956,11 @@ private:
                 done(ps, "area light");
             }
         } else if (n == "LightSource") {
-            std::string type = quoted(toks, i, d);
-            Params ps = params(toks, i);
+            const std::string& type = D.str[0];
             for (const Param& p : ps.items) p.used = true;
             warn(d, "light \"" + type + "\" is not supported (area lights only); skipped");
         } else if (n == "Camera") {
-            std::string type = quoted(toks, i, d);
-            Params ps = params(toks, i);
+            const std::string& type = D.str[0];
             if (type != "perspective") warn(d, "camera \"" + type + "\" is rendered as a perspective camera");
             camera_ = st_.ctm;
             named_["camera"] = Xform{st_.ctm.inv, st_.ctm.m};
@@ -881,8 +975,6 @@ private:
             ps.one_float("shutterclose", 1.0);
             done(ps, "camera");
         } else if (n == "Film") {
-            std::string type = quoted(toks, i, d);
-            Params ps = params(toks, i);
             width_ = ps.one_int("xresolution", 640);
             height_ = ps.one_int("yresolution", 480);
             if (width_ <= 0 || height_ <= 0 || width_ > 65536 || height_ > 65536) fail(d, "film resolution out of range");
@@ -893,8 +985,7 @@ private:
             ps.one_float("maxsampleluminance", INFINITY);
             done(ps, "film");
         } else if (n == "Sampler") {
-            std::string type = quoted(toks, i, d);
-            Params ps = params(toks, i);
+            const std::string& type = D.str[0];
             long want;
             if (type == "stratified") {
                 want = ps.one_int("xsamples", 4) * ps.one_int("ysamples", 4);
@@ -909,8 +1000,7 @@ private:
             ps.one_int("dimensions", 4);
             done(ps, "sampler");
         } else if (n == "Integrator") {
-            std::string type = quoted(toks, i, d);
-            Params ps = params(toks, i);
+            const std::string& type = D.str[0];
             if (type != "path") warn(d, "integrator \"" + type + "\" is rendered by the path integrator");
             max_depth_ = ps.one_int("maxdepth", 5);
             if (max_depth_ < 0) fail(d, "maxdepth must be non-negative");
@@ -919,8 +1009,7 @@ private:
             if (ps.find("pixelbounds", {"integer"})) warn(d, "pixelbounds ignored");
             done(ps, "integrator");
         } else if (n == "PixelFilter") {
-            std::string type = quoted(toks, i, d);
-            Params ps = params(toks, i);
+            const std::string& type = D.str[0];
             ilm_filter_desc f{};
             double w = type == "box" ? 0.5 : (type == "sinc" ? 4.0 : 2.0);
             f.radius[0] = (float)ps.one_float("xwidth", w);
@@ -938,8 +1027,7 @@ private:
             filter_ = f;
             done(ps, "filter");
         } else if (n == "Accelerator") {
-            std::string type = quoted(toks, i, d);
-            Params ps = params(toks, i);
+            const std::string& type = D.str[0];
             if (type == "bvh") {
                 kdtree_ = false;
                 bvh_.max_prims_in_node = (int32_t)std::min(255L, ps.one_int("maxnodeprims", 4));
@@ -957,20 +1045,14 @@ private:
             }
             done(ps, "accelerator");
         } else if (n == "Texture") {
-            quoted(toks, i, d);
-            quoted(toks, i, d);
-            std::string cls = quoted(toks, i, d);
-            Params ps = params(toks, i);
+            const std::string& cls = D.str[2];
             for (const Param& p : ps.items) p.used = true;
             warn(d, "texture \"" + cls + "\" is not supported; materials use their constant defaults");
         } else if (n == "MakeNamedMedium" || n == "MediumInterface") {
-            quoted(toks, i, d);
-            if (n == "MediumInterface" && i < toks.size() && toks[i].quoted) ++i;
-            Params ps = params(toks, i);
             for (const Param& p : ps.items) p.used = true;
             warn(d, "participating media are not supported; " + n + " skipped");
         } else if (n == "Include") {
-            std::string path = quoted(toks, i, d);
+            const std::string& path = D.str[0];
             std::string dir = fname(d);
             size_t cut = dir.find_last_of('/');
             std::string base = cut == std::string::npos ? base_dir_ : dir.substr(0, cut);
@@ -990,7 +1072,6 @@ private:
     };
 
     ilm_scene_file* out_;
-    std::vector<std::string> files_;
     std::vector<std::string> warn_;
     int depth_ = 0;
     GState st_;
@@ -1026,6 +1107,165 @@ void put_error(char* error, size_t error_len, const std::string& msg) {
     std::snprintf(error, error_len, "%s", msg.c_str());
 }
 
+// ------------------------------------------------------------ syntax dump
+// The directive tree of a scene description, read with the loader's tokenizer
+// and Reader::read_directive but not run: the tree parse_to_ast returns
+// (core/parser/mod.rs:19-34).  AttributeBegin, TransformBegin, ObjectBegin and
+// WorldBegin open a block that holds the directives up to its matching end
+// (ast.rs's Attribute, Transform, Object and World directives); Include is
+// replaced by the directives of the file it names (many_with_include,
+// core/parser/parsers/directives.rs).
+class SyntaxDump : public Reader {
+public:
+    std::string base_dir_;
+
+    std::string run(const std::string& text) {
+        std::vector<Node> top;
+        std::vector<Block> open;
+        read_text(text, "<text>", top, open);
+        if (!open.empty()) {
+            const Node& b = open.back().node;
+            fail(b.d.tok, b.d.tok.text + " without a matching end");
+        }
+        std::string out = "{\"directives\":";
+        list(top, out);
+        out += ",\"comments\":[";
+        for (size_t k = 0; k < comments_.size(); ++k) {
+            if (k) out += ',';
+            str(comments_[k], out);
+        }
+        out += "]}";
+        return out;
+    }
+
+private:
+    struct Node {
+        Directive d;
+        bool block = false;
+        std::vector<Node> children;
+    };
+    struct Block {
+        Node node;
+        std::string end;
+    };
+
+    std::vector<std::string> comments_;
+    int depth_ = 0;
+
+    void read_text(const std::string& text, const std::string& name, std::vector<Node>& top, std::vector<Block>& open) {
+        if (++depth_ > 16) throw std::runtime_error(name + ": Include nested more than 16 deep");
+        files_.push_back(name);
+        std::vector<Token> toks;
+        tokenize(text, (int)files_.size() - 1, name, toks, &comments_);
+        size_t i = 0;
+        while (i < toks.size()) {
+            Node n;
+            n.d = read_directive(toks, i);
+            const std::string& w = n.d.tok.text;
+            static const std::map<std::string, std::string> ends = {{"AttributeBegin", "AttributeEnd"},
+                                                                    {"TransformBegin", "TransformEnd"},
+                                                                    {"ObjectBegin", "ObjectEnd"},
+                                                                    {"WorldBegin", "WorldEnd"}};
+            auto e = ends.find(w);
+            if (e != ends.end()) {
+                n.block = true;
+                open.push_back({std::move(n), e->second});
+            } else if (w == "AttributeEnd" || w == "TransformEnd" || w == "ObjectEnd" || w == "WorldEnd") {
+                if (open.empty() || open.back().end != w) fail(n.d.tok, "unmatched " + w);
+                Node b = std::move(open.back().node);
+                open.pop_back();
+                (open.empty() ? top : open.back().node.children).push_back(std::move(b));
+            } else if (w == "Include") {
+                std::string dir = fname(n.d.tok);
+                size_t cut = dir.find_last_of('/');
+                std::string base = cut == std::string::npos ? base_dir_ : dir.substr(0, cut);
+                const std::string& path = n.d.str[0];
+                std::string full = !path.empty() && path[0] == '/' ? path : (base.empty() ? path : base + "/" + path);
+                std::ifstream f(full, std::ios::binary);
+                if (!f) throw std::runtime_error(full + ": cannot open");
+                std::stringstream ss;
+                ss << f.rdbuf();
+                read_text(ss.str(), full, top, open);
+            } else {
+                (open.empty() ? top : open.back().node.children).push_back(std::move(n));
+            }
+        }
+        --depth_;
+    }
+
+    static void str(const std::string& v, std::string& out) {
+        out += '"';
+        for (unsigned char c : v) {
+            if (c == '"' || c == '\\') {
+                out += '\\';
+                out += (char)c;
+            } else if (c < 0x20) {
+                char buf[8];
+                std::snprintf(buf, sizeof buf, "\\u%04x", c);
+                out += buf;
+            } else {
+                out += (char)c;
+            }
+        }
+        out += '"';
+    }
+    static void nums(const std::vector<double>& v, std::string& out) {
+        out += '[';
+        for (size_t k = 0; k < v.size(); ++k) {
+            char buf[32];
+            std::snprintf(buf, sizeof buf, "%s%.17g", k ? "," : "", v[k]);
+            out += buf;
+        }
+        out += ']';
+    }
+    static void strs(const std::vector<std::string>& v, std::string& out) {
+        out += '[';
+        for (size_t k = 0; k < v.size(); ++k) {
+            if (k) out += ',';
+            str(v[k], out);
+        }
+        out += ']';
+    }
+    void node(const Node& n, std::string& out) const {
+        out += "{\"directive\":";
+        str(n.d.tok.text, out);
+        out += ",\"file\":";
+        str(fname(n.d.tok), out);
+        out += ",\"line\":" + std::to_string(n.d.tok.line) + ",\"num\":";
+        nums(n.d.num, out);
+        out += ",\"str\":";
+        strs(n.d.str, out);
+        out += ",\"params\":[";
+        for (size_t k = 0; k < n.d.params.items.size(); ++k) {
+            const Param& p = n.d.params.items[k];
+            if (k) out += ',';
+            out += "{\"type\":";
+            str(p.type, out);
+            out += ",\"name\":";
+            str(p.name, out);
+            out += ",\"num\":";
+            nums(p.num, out);
+            out += ",\"str\":";
+            strs(p.str, out);
+            out += '}';
+        }
+        out += ']';
+        if (n.block) {
+            out += ",\"children\":";
+            list(n.children, out);
+        }
+        out += '}';
+    }
+    void list(const std::vector<Node>& v, std::string& out) const {
+        out += '[';
+        for (size_t k = 0; k < v.size(); ++k) {
+            if (k) out += ',';
+            node(v[k], out);
+        }
+        out += ']';
+    }
+};
+
 }  // namespace
 
 extern "C" {
@@ -1057,6 +1297,26 @@ int32_t ilm_scene_file_parse(const char* text, const char* base_dir, char* error
         p.base_dir_ = base_dir ? base_dir : "";
         p.run_text(text, "<text>");
         return finish_load(p, sf, out);
+    } catch (const std::exception& e) {
+        put_error(error, error_len, e.what());
+        return ILM_ERR_INVALID_ARGUMENT;
+    }
+}
+
+int32_t ilm_scene_syntax(const char* text, const char* base_dir, char* json, size_t json_cap, size_t* json_len,
+                         char* error, size_t error_len) {
+    if (!text || !json_len || (json_cap && !json)) return ILM_ERR_INVALID_ARGUMENT;
+    try {
+        SyntaxDump d;
+        d.base_dir_ = base_dir ? base_dir : "";
+        std::string out = d.run(text);
+        *json_len = out.size();
+        if (json_cap) {
+            size_t k = std::min(out.size(), json_cap - 1);
+            std::memcpy(json, out.data(), k);
+            json[k] = '\0';
+        }
+        return ILM_OK;
     } catch (const std::exception& e) {
         put_error(error, error_len, e.what());
         return ILM_ERR_INVALID_ARGUMENT;

@@ -1,13 +1,15 @@
 """pbrt-v3 scene files on the GPU path (ilm_scene_file_*).
 
-The reference parses these files to a syntax tree (core/parser/ast.rs) and
-stops there (core/parser/mod.rs:36-46); this module loads them into the
-shapes, materials, camera and render settings that the B200 accelerators and
-path tracer take.
+The reference parses these files to a syntax tree (parse_to_ast,
+core/parser/mod.rs:19-34) and stops there (core/parser/mod.rs:36-46); this
+module loads them into the shapes, materials, camera and render settings that
+the B200 accelerators and path tracer take.  `syntax` returns the directive
+tree itself, read by the loader's own tokenizer and argument grammar.
 """
 from __future__ import annotations
 
 import ctypes
+import json
 from typing import Optional
 
 import numpy as np
@@ -15,6 +17,25 @@ import numpy as np
 from . import _lib
 from ._lib import IllumeError, ptr
 from .primitive import Context, GpuBVHAccel, GpuKdTreeAccel, PathTracer
+
+
+def syntax(text: str, base_dir: str = "") -> dict:
+    """The directive tree of `text` without running it (ilm_scene_syntax):
+    {"directives": [...], "comments": [...]}, each directive a dict with
+    "directive", "file", "line", "num", "str", "params" and, for blocks,
+    "children".  Raises IllumeError on a syntax error."""
+    lib = _lib.load()
+    err = ctypes.create_string_buffer(1024)
+    n = ctypes.c_size_t()
+    src, base = text.encode(), base_dir.encode()
+    st = lib.ilm_scene_syntax(src, base, None, 0, ctypes.byref(n), err, len(err))
+    if st != 0:
+        raise IllumeError(st, "reading scene syntax", err.value.decode(errors="replace"))
+    buf = ctypes.create_string_buffer(n.value + 1)
+    st = lib.ilm_scene_syntax(src, base, buf, len(buf), ctypes.byref(n), err, len(err))
+    if st != 0:
+        raise IllumeError(st, "reading scene syntax", err.value.decode(errors="replace"))
+    return json.loads(buf.raw[:n.value].decode())
 
 
 class SceneFile:
