@@ -19,7 +19,9 @@
  *    host memory (pageable or pinned; the call stages through device buffers
  *    and returns when the results are back in host memory).
  *  - `stream` is a cudaStream_t passed as void*; NULL selects the context's
- *    own stream.
+ *    own (non-blocking) stream, which is not ordered with other streams.  A
+ *    caller whose buffers come from work on the legacy default stream passes
+ *    cudaStreamLegacy, or cudaStreamPerThread for the per-thread one.
  *  - Primitive ids: meshes and sphere sets passed to ilm_accel_build are
  *    numbered in list order; triangles of a mesh (or spheres of a set) take
  *    consecutive ids.  This matches BVHAccel's `primitives` vector order.

@@ -26,6 +26,9 @@ ILM_FLAG_VALIDATE_RAYS = 1
 ILM_FLAG_GRID_SCHEDULE = 2
 ILM_FLAG_HIGH_OCCUPANCY = 4
 ILM_MISS = 0xFFFFFFFF
+# cudaStreamLegacy: the explicit handle of the legacy default stream (a NULL
+# stream argument selects the context's own stream instead)
+CUDA_STREAM_LEGACY = 0x1
 ILM_TRAVERSAL_ERROR = 0xFFFFFFFE
 
 STATUS_NAMES = {

@@ -60,4 +60,9 @@ cudaError_t launch_trace_wide(int width, const TraceArgs& t, const LaunchParams&
 // the current device (0 when unknown).
 uint64_t wide_grid_wave(int width, int stack_depth);
 
+// SMs x resident blocks per SM of `kernel` at `block` threads on the current
+// device (at least one block per SM), cached per (device, kernel) and safe to
+// call from several host threads; 0 when the query fails.
+uint64_t resident_blocks(const void* kernel, int block);
+
 }  // namespace ilm

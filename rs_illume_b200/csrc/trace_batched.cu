@@ -125,12 +125,9 @@ cudaError_t launch_batched_variant(const BatchTable& t, bool any, cudaStream_t s
     const unsigned block = 128;
     auto kc = k_trace_batched<W, kStack, false, kAnalytic>;
     auto ka = k_trace_batched<W, kStack, true, kAnalytic>;
-    int dev = 0, sms = 148, per_sm = 1;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, any ? (const void*)ka : (const void*)kc, block, 0);
-    if (per_sm < 1) per_sm = 1;
-    uint64_t grid = std::min<uint64_t>((uint64_t)sms * per_sm, (t.total + block - 1) / block);
+    const uint64_t resident = resident_blocks(any ? (const void*)ka : (const void*)kc, (int)block);
+    if (resident == 0) return cudaErrorInvalidConfiguration;
+    uint64_t grid = std::min<uint64_t>(resident, (t.total + block - 1) / block);
     if (grid == 0) return cudaSuccess;
     cudaError_t e = cudaMemsetAsync(t.counter, 0, sizeof(unsigned long long), s);
     if (e != cudaSuccess) return e;

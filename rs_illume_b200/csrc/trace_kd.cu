@@ -203,19 +203,9 @@ cudaError_t launch_persistent(const TraceArgs& t, cudaStream_t s) {
     const unsigned block = kKdBlock;
     auto kc = k_trace_kd_persistent<false, kMinBlocks, kAnalytic>;
     auto ka = k_trace_kd_persistent<true, kMinBlocks, kAnalytic>;
-    static int per_sm[2] = {0, 0};
-    static int sms = 0;
-    const int which = t.occ ? 1 : 0;
-    if (per_sm[which] == 0) {
-        int dev = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[which], t.occ ? (const void*)ka : (const void*)kc,
-                                                      block, 0);
-        if (per_sm[which] < 1) per_sm[which] = 1;
-    }
-    uint64_t need_blocks = (t.n + block - 1) / block;
-    uint64_t grid = (uint64_t)sms * per_sm[which];
+    uint64_t grid = resident_blocks(t.occ ? (const void*)ka : (const void*)kc, (int)block);
+    if (grid == 0) return cudaErrorInvalidConfiguration;
+    const uint64_t need_blocks = (t.n + block - 1) / block;
     if (grid > need_blocks) grid = need_blocks;
     cudaError_t e = cudaMemsetAsync(t.counter, 0, sizeof(unsigned long long), s);
     if (e != cudaSuccess) return e;

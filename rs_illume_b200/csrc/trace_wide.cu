@@ -79,29 +79,17 @@ __global__ void __launch_bounds__(128, kMinBlocks) k_trace_wide_persistent(Trace
 template <int W, int kStack, int kMinBlocks, bool kAnalytic>
 cudaError_t launch_persistent(const TraceArgs& t, cudaStream_t s) {
     const unsigned block = 128;
-    {
-        auto kc = k_trace_wide_persistent<W, kStack, false, kMinBlocks, kAnalytic>;
-        auto ka = k_trace_wide_persistent<W, kStack, true, kMinBlocks, kAnalytic>;
-        static int per_sm[2] = {0, 0};
-        static int sms = 0;
-        int which = t.occ ? 1 : 0;
-        if (per_sm[which] == 0) {
-            int dev = 0;
-            cudaGetDevice(&dev);
-            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[which], t.occ ? (const void*)ka : (const void*)kc,
-                                                          block, 0);
-            if (per_sm[which] < 1) per_sm[which] = 1;
-        }
-        uint64_t need_blocks = (t.n + block - 1) / block;
-        uint64_t grid = (uint64_t)sms * per_sm[which];
-        if (grid > need_blocks) grid = need_blocks;
-        cudaError_t e = cudaMemsetAsync(t.counter, 0, sizeof(unsigned long long), s);
-        if (e != cudaSuccess) return e;
-        if (t.occ) ka<<<(unsigned)grid, block, 0, s>>>(t);
-        else kc<<<(unsigned)grid, block, 0, s>>>(t);
-        return cudaGetLastError();
-    }
+    auto kc = k_trace_wide_persistent<W, kStack, false, kMinBlocks, kAnalytic>;
+    auto ka = k_trace_wide_persistent<W, kStack, true, kMinBlocks, kAnalytic>;
+    uint64_t grid = resident_blocks(t.occ ? (const void*)ka : (const void*)kc, (int)block);
+    if (grid == 0) return cudaErrorInvalidConfiguration;
+    const uint64_t need_blocks = (t.n + block - 1) / block;
+    if (grid > need_blocks) grid = need_blocks;
+    cudaError_t e = cudaMemsetAsync(t.counter, 0, sizeof(unsigned long long), s);
+    if (e != cudaSuccess) return e;
+    if (t.occ) ka<<<(unsigned)grid, block, 0, s>>>(t);
+    else kc<<<(unsigned)grid, block, 0, s>>>(t);
+    return cudaGetLastError();
 }
 
 template <int W, int kStack, bool kAnalytic>
@@ -125,20 +113,10 @@ cudaError_t launch(const TraceArgs& t, const LaunchParams& lp, cudaStream_t s) {
 }  // namespace
 
 uint64_t wide_grid_wave(int width, int stack_depth) {
-    static uint64_t cache[2][2] = {{0, 0}, {0, 0}};
-    const int wi = width == 8, di = stack_depth > 32;
-    if (cache[wi][di]) return cache[wi][di];
-    const void* k = wi ? (di ? (const void*)k_trace_wide<8, 64, false, true> : (const void*)k_trace_wide<8, 32, false, true>)
-                       : (di ? (const void*)k_trace_wide<4, 64, false, true> : (const void*)k_trace_wide<4, 32, false, true>);
-    int dev = 0, sms = 0, per_sm = 0;
-    cudaGetDevice(&dev);
-    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, 128, 0) != cudaSuccess) {
-        cudaGetLastError();
-        return 0;
-    }
-    cache[wi][di] = (uint64_t)sms * (uint64_t)per_sm * 128u;
-    return cache[wi][di];
+    const bool w8 = width == 8, deep = stack_depth > 32;
+    const void* k = w8 ? (deep ? (const void*)k_trace_wide<8, 64, false, true> : (const void*)k_trace_wide<8, 32, false, true>)
+                       : (deep ? (const void*)k_trace_wide<4, 64, false, true> : (const void*)k_trace_wide<4, 32, false, true>);
+    return resident_blocks(k, 128) * 128u;
 }
 
 cudaError_t launch_trace_wide(int width, const TraceArgs& t, const LaunchParams& lp, cudaStream_t s) {

@@ -10,7 +10,7 @@ import ctypes
 import numpy as np
 
 from . import _lib
-from ._lib import ptr
+from ._lib import CUDA_STREAM_LEGACY, ptr
 from .primitive import Context
 
 N_PARAMS = 30720
@@ -61,7 +61,7 @@ class RadianceCache:
         if out is None:
             out = np.empty((n, 3), np.float32)
         self.ctx.check(self.ctx._lib.ilm_nrc_infer(self.ctx.handle, self.handle, ptr(inputs), n, ptr(out),
-                                                   _stream(stream)), "ilm_nrc_infer")
+                                                   _stream(stream, inputs)), "ilm_nrc_infer")
         return out
 
     def train_step(self, inputs, targets, stream=None, with_loss: bool = True):
@@ -70,7 +70,7 @@ class RadianceCache:
         loss = ctypes.c_float()
         self.ctx.check(self.ctx._lib.ilm_nrc_train_step(self.ctx.handle, self.handle, ptr(inputs), ptr(targets),
                                                         _rows(inputs), ctypes.byref(loss) if with_loss else None,
-                                                        _stream(stream)),
+                                                        _stream(stream, inputs)),
                        "ilm_nrc_train_step")
         return loss.value if with_loss else None
 
@@ -108,7 +108,16 @@ def _rows(a) -> int:
     return a.shape[0]
 
 
-def _stream(stream):
+def _stream(stream, buf=None):
+    """As primitive._stream: torch's current stream for torch CUDA tensors
+    when no stream is given, NULL (the context's stream) for host arrays."""
     if stream is None:
+        if getattr(buf, "is_cuda", False):
+            import torch
+            h = torch.cuda.current_stream(buf.device).cuda_stream
+            # torch's default stream is the legacy default stream, handle 0;
+            # the C ABI reads NULL as the context's stream, so name it by
+            # its explicit handle, cudaStreamLegacy (0x1)
+            return h if h else CUDA_STREAM_LEGACY
         return None
     return stream if isinstance(stream, int) else stream.cuda_stream

@@ -19,7 +19,7 @@ from typing import Optional, Sequence
 import numpy as np
 
 from . import _lib
-from ._lib import (HIT_DTYPE, ILM_MISS, RAY_DTYPE, IllumeError, ilm_accel_info, ilm_build_opts,
+from ._lib import (CUDA_STREAM_LEGACY, HIT_DTYPE, ILM_MISS, RAY_DTYPE, IllumeError, ilm_accel_info, ilm_build_opts,
                    ilm_config, ilm_sphere_desc, ptr)
 
 log = logging.getLogger("rs_illume_b200")
@@ -263,7 +263,7 @@ class GpuBVHAccel:
         n = len(rays) if isinstance(rays, np.ndarray) else _count(rays, RAY_DTYPE.itemsize)
         if out is None:
             out = np.empty(n, _lib.SURFACE_INTERACTION_DTYPE)
-        s = None if stream is None else (stream if isinstance(stream, int) else stream.cuda_stream)
+        s = _stream(stream, rays)
         self.ctx.check(self.ctx._lib.ilm_surface_interactions(self.ctx.handle, self.id, ptr(rays), ptr(hits), n,
                                                               ptr(out), s), "ilm_surface_interactions")
         return out
@@ -304,14 +304,15 @@ class GpuBVHAccel:
     def intersect_batch(self, rays, hits=None, stream=None):
         """Closest hit for every ray.  `rays` is a RAY_DTYPE numpy array (host)
         or a torch uint8/float tensor on the device holding 32-byte records;
-        `hits` likewise (16-byte records).  Host arrays return a HIT_DTYPE array."""
+        `hits` likewise (16-byte records).  Host arrays return a HIT_DTYPE array.
+        Device tensors run on `stream`, by default torch's current stream."""
         n = _count(rays, 32)
         if hits is None:
             if not isinstance(rays, np.ndarray):
                 raise ValueError("device rays need a device `hits` buffer")
             hits = np.empty(n, HIT_DTYPE)
         self.ctx.check(self.ctx._lib.ilm_intersect_closest(self.ctx.handle, self.id, ptr(rays), n, ptr(hits),
-                                                           _stream(stream)), "ilm_intersect_closest")
+                                                           _stream(stream, rays)), "ilm_intersect_closest")
         return hits
 
     def intersect_p_batch(self, rays, occluded=None, stream=None):
@@ -321,7 +322,7 @@ class GpuBVHAccel:
                 raise ValueError("device rays need a device `occluded` buffer")
             occluded = np.empty(n, np.uint32)
         self.ctx.check(self.ctx._lib.ilm_intersect_any(self.ctx.handle, self.id, ptr(rays), n, ptr(occluded),
-                                                       _stream(stream)), "ilm_intersect_any")
+                                                       _stream(stream, rays)), "ilm_intersect_any")
         return occluded
 
     def info(self) -> dict:
@@ -458,8 +459,19 @@ def _count(buf, rec: int) -> int:
     return buf.numel() * buf.element_size() // rec
 
 
-def _stream(stream):
+def _stream(stream, buf=None):
+    """The cudaStream_t to pass.  With no stream given, a call on torch CUDA
+    tensors runs on torch's current stream of their device, so it is ordered
+    after the torch work that produced them; a call on host arrays passes NULL
+    (the context's own stream)."""
     if stream is None:
+        if getattr(buf, "is_cuda", False):
+            import torch
+            h = torch.cuda.current_stream(buf.device).cuda_stream
+            # torch's default stream is the legacy default stream, handle 0;
+            # the C ABI reads NULL as the context's stream, so name it by
+            # its explicit handle, cudaStreamLegacy (0x1)
+            return h if h else CUDA_STREAM_LEGACY
         return None
     if isinstance(stream, int):
         return stream

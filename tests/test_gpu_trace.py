@@ -285,3 +285,34 @@ def test_mixed_pointer_kinds_rejected(ctx):
     with pytest.raises(rb.IllumeError) as e:
         acc.intersect_batch(rays, d_hits)
     assert e.value.status == -1
+
+
+@pytest.mark.parametrize("grid", [False, True])
+def test_batch_beyond_32_bit_offsets(incoherent, grid):
+    """138,412,032 rays (4.4 GB of ray records, 2.2 GB of hits): the incoherent
+    rays tiled 33 times on the device.  Every copy must answer exactly as the
+    first, so ray indices, byte offsets and the persistent schedule's claim
+    counter stay correct past 2^32 bytes, for closest and any hit."""
+    import torch
+    xyz, idx, rays, _ = incoherent
+    ctx = rb.Context(0, high_occupancy=True, grid_schedule=grid)
+    acc = rb.GpuBVHAccel(ctx, [rb.TriangleMesh(ctx, xyz, idx)], width=8)
+    reps = 33
+    one = torch.from_numpy(rays.view(np.uint8)).cuda()
+    d_rays = one.repeat(reps)
+    n = len(rays) * reps
+    assert n * 32 > (1 << 32) and n * 16 > (1 << 31)
+    d_hits = torch.empty(n * 16, dtype=torch.uint8, device="cuda")
+    d_occ = torch.empty(n * 4, dtype=torch.uint8, device="cuda")
+    # no stream given: the calls run on torch's current stream, after repeat()
+    acc.intersect_batch(d_rays, d_hits)
+    acc.intersect_p_batch(d_rays, d_occ)
+    torch.cuda.synchronize()
+    del d_rays
+    hits = d_hits.view(reps, -1)
+    occ = d_occ.view(reps, -1)
+    assert bool((hits == hits[0]).all()) and bool((occ == occ[0]).all())
+    want = acc.intersect_batch(rays)
+    assert hits[0].cpu().numpy().tobytes() == want.tobytes()
+    assert ctx.device_errors() == 0
+    ctx.close()
