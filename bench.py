@@ -452,7 +452,8 @@ def kdtree_leg(rb, wl, ctx, torch, dev, steps, warmup, scene=None):
             "n_leaf_refs": int(info["n_leaf_refs"]), "max_depth": int(info["max_depth"]),
             "device_bytes": int(info["device_bytes"]),
             "config": "KdTreeAccel 80/1/0.5/1 over the headline scene; the headline's 2,097,152 closest and "
-                      "2,097,152 any-hit rays; one thread per ray; L2 flushed between launches"}
+                      "2,097,152 any-hit rays; persistent schedule, 8 blocks of 128 per SM; L2 flushed between "
+                      "launches"}
 
 
 def run_reference(args):
