@@ -310,8 +310,9 @@ def mlp_leg(rb, ctx, torch, dev, cache=None):
             "infer_frac": round(inf_tf / peak, 4), "train_step_ms_16384": round(1e3 * t_train, 4),
             "train_tflops": round(3 * 16384 * flops_row / t_train / 1e12, 2),
             "peak_tflops": peak, "flop_per_row_forward": flops_row,
-            "kernels": "inference: tcgen05.mma kind::f16 (bf16, FP32 accumulators in TMEM), M 128 N 64 K 16; "
-                       "training: mma.sync m16n8k16 bf16, FP32 accumulate"}
+            "kernels": "inference and the training forward / backward: tcgen05.mma kind::f16 (bf16, FP32 "
+                       "accumulators in TMEM), M 128 N 64 K 16; weight gradients: mma.sync m16n8k16 bf16, "
+                       "FP32 accumulate (split-K over the batch rows)"}
 
 
 def batched_leg(rb, wl, ctx, torch, dev, steps):

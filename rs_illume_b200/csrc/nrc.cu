@@ -1,5 +1,6 @@
-// Neural radiance cache: input encoding, a 5 x 64 ReLU MLP on BF16 tensor
-// cores (mma.sync m16n8k16, FP32 accumulation), relative-L2 loss and Adam.
+// Neural radiance cache: input encoding, a 5 x 64 ReLU MLP on the BF16
+// tensor cores (tcgen05.mma, FP32 accumulators in TMEM; the weight gradients
+// on mma.sync), relative-L2 loss and Adam.
 // No counterpart in the reference (a learned component added on top of the
 // path tracer); the method follows published neural radiance caching:
 //   inputs: position (12-frequency sin/cos per axis, 72), outgoing direction
@@ -10,19 +11,19 @@
 //   loss = mean over samples and channels of (p - y)^2 / (sg(p)^2 + 0.01).
 //
 // Kernels
-//   k_mlp_fwd      one warp per 16 rows: the encoding is computed straight
-//                  into layer 0's A fragments (each lane evaluates the 8
-//                  features its fragment holds), every layer's output
-//                  fragments become the next layer's A fragments in
-//                  registers; weights in shared memory (rows padded against
-//                  bank conflicts); training stores the encoding and the
-//                  bf16 activations
-//   k_mlp_bwd      loss gradient, then back through the layers the same way
-//                  (transposed weights in shared memory), storing dOut
+//   k_mlp_fwd_tc<train>  forward pass: per 128-row tile a warpgroup encodes its
+//                  rows straight into layer 0's A operand in shared memory,
+//                  one thread issues the MMAs, each layer's accumulator comes
+//                  back through tcgen05.ld as the next layer's A; training
+//                  also stores the encoding and the bf16 activations
+//   k_mlp_bwd_tc   loss gradient, then back through the layers the same way
+//                  (transposed weights), storing dOut
 //   k_wgrad_all    dW_l = dOut_l^T * in_l for all six layers: each CTA takes
 //                  64-row chunks (16-byte cp.async into padded shared tiles),
 //                  ldmatrix.trans gives both operands' fragments, warps own
-//                  output tiles; one FP32 partial sum per CTA, no atomics
+//                  output tiles; one FP32 partial sum per CTA, no atomics.
+//                  A split-K over the batch rows with 64 x 64 outputs: about
+//                  1 GFLOP per step, bound by latency, not by the MMAs
 //   k_reduce_adam  sums the CTA partials, Adam on the FP32 master weights,
 //                  bf16 weight packs and the inference moving average
 //   k_nrc_encode   the encoding alone (for inspection)
@@ -59,23 +60,17 @@ constexpr int kParams = kHid * kIn + 4 * kHid * kHid + kOut * kHid;   // 30720
 __host__ __device__ constexpr int tc_index(int l, int o, int i) {
     return param_off(l) + ((o >> 3) * (in_dim(l) >> 3) + (i >> 3)) * 64 + (o & 7) * 8 + (i & 7);
 }
-// bf16 packs: forward W_l rows padded to in+8; backward W_l^T (l >= 1) rows
-// padded to out+8
-__host__ __device__ constexpr int fwd_stride(int l) { return in_dim(l) + 8; }
-__host__ __device__ constexpr int fwd_off(int l) {
-    return l == 0 ? 0 : kHid * (kIn + 8) + (l - 1) * kHid * (kHid + 8);
+// Transposed bf16 pack for the backward pass, the same canonical layout:
+// layer l >= 1 as W_l^T ([in][out], N = in, K = out), core matrix (i/8, o/8)
+// at (i/8 * out/8 + o/8) * 64 elements from tcb_off(l).
+__host__ __device__ constexpr int tcb_off(int l) { return (l - 1) * kHid * kHid; }   // l = 1..5
+__host__ __device__ constexpr int tcb_index(int l, int o, int i) {
+    return tcb_off(l) + ((i >> 3) * (out_dim(l) >> 3) + (o >> 3)) * 64 + (i & 7) * 8 + (o & 7);
 }
-constexpr int kFwdElems = kHid * (kIn + 8) + 4 * kHid * (kHid + 8) + kOut * (kHid + 8);   // 33408
-__host__ __device__ constexpr int bwd_stride(int l) { return out_dim(l) + 8; }
-__host__ __device__ constexpr int bwd_off(int l) { return (l - 1) * kHid * (kHid + 8); }   // l = 1..5
-constexpr int kBwdElems = 4 * kHid * (kHid + 8) + kHid * (kOut + 8);                        // 19968
+constexpr int kTcbElems = 4 * kHid * kHid + kHid * kOut;   // 17408
 constexpr float kLossEps = 0.01f;
 constexpr int kMaxPartials = 148;   // CTAs of k_wgrad_all (one FP32 partial gradient each)
 constexpr int kChunk = 64;          // rows per k_wgrad_all staging step
-// Warps per CTA of the forward / backward kernels: the CTA's weights in shared
-// memory (67 / 40 KB) are shared by all its warps, so more warps per CTA means
-// more warps per SM (3 CTAs fit either way).
-constexpr int kMlpWarps = 8;
 
 struct Enc {   // position normalisation: q = (p - origin) * scale
     float x0, y0, z0, sx, sy, sz;
@@ -212,132 +207,10 @@ __global__ void k_nrc_encode(const float* __restrict__ raw, uint32_t n, Enc ec, 
     encode_row<0>(v, reinterpret_cast<uint32_t*>(enc + (size_t)i * kIn));
 }
 
-// ---------------------------------------------------------------- forward
-// C fragments of 8 n-tiles (64 columns) -> ReLU'd bf16 A fragments of 4 k-steps.
-__device__ __forceinline__ void to_a_frags(const float (&c)[8][4], uint32_t (&a)[4][4], bool relu) {
-#pragma unroll
-    for (int j = 0; j < 4; ++j) {
-        float v[8];
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            v[q] = c[2 * j][q];
-            v[4 + q] = c[2 * j + 1][q];
-        }
-        if (relu)
-#pragma unroll
-            for (int q = 0; q < 8; ++q) v[q] = fmaxf(v[q], 0.0f);
-        a[j][0] = pack(v[0], v[1]);
-        a[j][1] = pack(v[2], v[3]);
-        a[j][2] = pack(v[4], v[5]);
-        a[j][3] = pack(v[6], v[7]);
-    }
-}
-
-// Stores 4 k-steps of A fragments as a [rows][64] bf16 tile (row stride 32 words).
-__device__ __forceinline__ void store_frags(uint32_t* base, uint32_t row0, uint32_t nrows, const uint32_t (&a)[4][4]) {
-    const unsigned lane = threadIdx.x & 31u, g = lane >> 2, t = lane & 3u;
-    uint32_t r0 = row0 + g, r1 = row0 + g + 8;
-#pragma unroll
-    for (int j = 0; j < 4; ++j) {
-        if (r0 < nrows) { base[r0 * 32 + 8 * j + t] = a[j][0]; base[r0 * 32 + 8 * j + 4 + t] = a[j][2]; }
-        if (r1 < nrows) { base[r1 * 32 + 8 * j + t] = a[j][1]; base[r1 * 32 + 8 * j + 4 + t] = a[j][3]; }
-    }
-}
-
-// Multiplies A fragments (16 x 64, four k-steps) by a 64-wide weight block in
-// shared memory: out[nt] += A * B where B[k][n] = w[n * stride + k].
-template <int NT>
-__device__ __forceinline__ void gemm64(float (&acc)[NT][4], const uint32_t (&a)[4][4], const __nv_bfloat16* w,
-                                       int stride) {
-    const unsigned lane = threadIdx.x & 31u, g = lane >> 2, t = lane & 3u;
-#pragma unroll
-    for (int nt = 0; nt < NT; ++nt)
-#pragma unroll
-        for (int q = 0; q < 4; ++q) acc[nt][q] = 0.0f;
-#pragma unroll
-    for (int ks = 0; ks < 4; ++ks)
-#pragma unroll
-        for (int nt = 0; nt < NT; ++nt) {
-            const __nv_bfloat16* p = w + (nt * 8 + g) * stride + ks * 16 + 2 * t;
-            uint32_t b0 = *reinterpret_cast<const uint32_t*>(p);
-            uint32_t b1 = *reinterpret_cast<const uint32_t*>(p + 8);
-            mma(acc[nt], a[ks], b0, b1);
-        }
-}
-
-// Layer 0, k-steps KS..12: A fragments evaluated from the rows' inputs;
-// optionally stored as the encoding ([rows][208] bf16, 104 words per row).
-template <int KS, bool kStore>
-__device__ __forceinline__ void layer0(float (&acc)[8][4], const RowIn& v0, const RowIn& v1, bool ok0, bool ok1,
-                                       const __nv_bfloat16* sw, uint32_t* enc, uint32_t r0, uint32_t r1) {
-    const unsigned lane = threadIdx.x & 31u, g = lane >> 2, t = lane & 3u;
-    uint32_t a[4];
-    a[0] = ok0 ? feat2<KS * 16>(v0, t) : 0u;
-    a[1] = ok1 ? feat2<KS * 16>(v1, t) : 0u;
-    a[2] = ok0 ? feat2<KS * 16 + 8>(v0, t) : 0u;
-    a[3] = ok1 ? feat2<KS * 16 + 8>(v1, t) : 0u;
-    if (kStore) {
-        if (ok0) { enc[(size_t)r0 * 104 + 8 * KS + t] = a[0]; enc[(size_t)r0 * 104 + 8 * KS + 4 + t] = a[2]; }
-        if (ok1) { enc[(size_t)r1 * 104 + 8 * KS + t] = a[1]; enc[(size_t)r1 * 104 + 8 * KS + 4 + t] = a[3]; }
-    }
-#pragma unroll
-    for (int nt = 0; nt < 8; ++nt) {
-        const __nv_bfloat16* p = sw + fwd_off(0) + (nt * 8 + g) * fwd_stride(0) + KS * 16 + 2 * t;
-        mma(acc[nt], a, *reinterpret_cast<const uint32_t*>(p), *reinterpret_cast<const uint32_t*>(p + 8));
-    }
-    if constexpr (KS + 1 < kIn / 16) layer0<KS + 1, kStore>(acc, v0, v1, ok0, ok1, sw, enc, r0, r1);
-}
-
-// Forward pass from raw inputs.  kTrain stores the encoding ([n][208]) and the
-// five hidden activations (layer l at acts + l * ld * 64, [n][64] bf16).
-template <bool kTrain>
-__global__ void __launch_bounds__(32 * kMlpWarps) k_mlp_fwd(const float* __restrict__ raw, NrcCount cnt, Enc ec,
-                                                            uint32_t ld,
-                                                 const __nv_bfloat16* __restrict__ wfwd, float* __restrict__ out,
-                                                 __nv_bfloat16* __restrict__ acts, __nv_bfloat16* __restrict__ enc) {
-    extern __shared__ __align__(16) __nv_bfloat16 sw[];
-    stage(sw, wfwd, kFwdElems);
-    __syncthreads();
-    const uint32_t n = rows_of(cnt);
-    const unsigned lane = threadIdx.x & 31u, g = lane >> 2, t = lane & 3u, warp = threadIdx.x >> 5;
-    for (uint32_t tile = blockIdx.x * kMlpWarps + warp; tile * 16 < n; tile += gridDim.x * kMlpWarps) {
-        const uint32_t row0 = tile * 16, r0 = row0 + g, r1 = row0 + g + 8;
-        const bool ok0 = r0 < n, ok1 = r1 < n;
-        RowIn v0 = {}, v1 = {};
-        if (ok0) v0 = load_row(raw, r0, ec);
-        if (ok1) v1 = load_row(raw, r1, ec);
-        float acc[8][4];
-#pragma unroll
-        for (int nt = 0; nt < 8; ++nt)
-#pragma unroll
-            for (int q = 0; q < 4; ++q) acc[nt][q] = 0.0f;
-        layer0<0, kTrain>(acc, v0, v1, ok0, ok1, sw, reinterpret_cast<uint32_t*>(enc), r0, r1);
-        uint32_t af[4][4];
-        to_a_frags(acc, af, true);
-        if (kTrain) store_frags(reinterpret_cast<uint32_t*>(acts), row0, n, af);
-#pragma unroll 1
-        for (int l = 1; l <= 4; ++l) {
-            gemm64<8>(acc, af, sw + fwd_off(l), fwd_stride(l));
-            to_a_frags(acc, af, true);
-            if (kTrain) store_frags(reinterpret_cast<uint32_t*>(acts + (size_t)l * ld * kHid), row0, n, af);
-        }
-        float o[2][4];
-        gemm64<2>(o, af, sw + fwd_off(5), fwd_stride(5));
-        // columns 0..2 of n-tile 0: lanes t = 0 (cols 0, 1) and t = 1 (col 2)
-        if (t == 0) {
-            if (ok0) { out[3 * (size_t)r0] = o[0][0]; out[3 * (size_t)r0 + 1] = o[0][1]; }
-            if (ok1) { out[3 * (size_t)r1] = o[0][2]; out[3 * (size_t)r1 + 1] = o[0][3]; }
-        } else if (t == 1) {
-            if (ok0) out[3 * (size_t)r0 + 2] = o[0][0];
-            if (ok1) out[3 * (size_t)r1 + 2] = o[0][2];
-        }
-    }
-}
-
-
-// ---------------------------------------------------------------- inference on tcgen05
-// k_mlp_infer_tc: the forward pass on the 5th-generation tensor cores.
-// A CTA of kTcGroups warpgroups; each warpgroup owns 128-row tiles (thread t
+// ---------------------------------------------------------------- forward on tcgen05
+// k_mlp_fwd_tc: the forward pass on the 5th-generation tensor cores.
+// A CTA of 1, 2 or 4 warpgroups (blockDim / 128; few per CTA for small
+// batches, so that the tiles spread over the SMs); each warpgroup owns 128-row tiles (thread t
 // = row t), its own A operand buffer in shared memory, 64 TMEM columns of
 // FP32 accumulator (rows = TMEM lanes) and an mbarrier.  Per tile:
 //   layer 0 in two K halves (features 0-111, 112-207): the threads evaluate
@@ -345,16 +218,19 @@ __global__ void __launch_bounds__(32 * kMlpWarps) k_mlp_fwd(const float* __restr
 //     (M 128, N 64, K 16, bf16 x bf16 -> f32) and commits to the mbarrier;
 //   layers 1-4: tcgen05.ld of the accumulator, ReLU, bf16 into A, MMA;
 //   layer 5: N = 16, the first 3 columns are the output.
+// Training also stores each row's encoding ([n][208] bf16) and its five
+// ReLU'd activations (layer l at acts + l * ld * 64, [n][64] bf16), the bf16
+// values that go into the next layer's A operand.
 // The weights (61,440 bytes, all layers) are staged once per CTA.  Operands
 // use the canonical K-major layout without swizzle: 8x8 core matrices of 128
 // contiguous bytes; LBO = 128 bytes (next core matrix along K), SBO = the
 // stride between 8-row groups.  Every mbarrier wait is bounded; a timeout
 // sets kErrMlpTimeout in *err and the warpgroup stops.
-constexpr int kTcGroups = 4;
+constexpr int kTcGroups = 4;                                   // warpgroups per CTA, at most
 constexpr int kTcHalfCols = 14;                                // core-matrix columns of an A buffer (112 features)
 constexpr int kTcABytes = 128 / 8 * kTcHalfCols * 128;         // 28,672
 constexpr int kTcWBytes = kParams * 2;                         // 61,440
-constexpr int kTcSmem = kTcWBytes + kTcGroups * kTcABytes;     // 176,128
+constexpr int kTcSmem = kTcWBytes + kTcGroups * kTcABytes;     // 176,128 at 4 warpgroups
 constexpr uint32_t kErrMlpTimeout = 4u;
 constexpr uint32_t kTcWaitCap = 1u << 22;   // try_wait polls before a wait gives up
 
@@ -411,20 +287,22 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
     for (int k = 0; k < 16; ++k) v[k] = __uint_as_float(r[k]);
 }
 
-// Row t's 8 features F..F+7 (F = 8 * KC) into core-matrix column c of an A buffer.
+// Row t's 8 features F..F+7 (F = 8 * KC) into core-matrix column c of an A
+// buffer, and into the row's stored encoding when genc is set.
 template <int KC>
-__device__ __forceinline__ void put_features(uint8_t* a, int c, int row, const RowIn& v) {
+__device__ __forceinline__ void put_features(uint8_t* a, int c, int row, const RowIn& v, uint4* genc) {
     uint4 q;
     q.x = feat2<8 * KC>(v, 0);
     q.y = feat2<8 * KC>(v, 1);
     q.z = feat2<8 * KC>(v, 2);
     q.w = feat2<8 * KC>(v, 3);
     *reinterpret_cast<uint4*>(a + ((row >> 3) * kTcHalfCols + c) * 128 + (row & 7) * 16) = q;
+    if (genc) genc[KC] = q;
 }
 template <int KC, int KEND>
-__device__ __forceinline__ void encode_cols(uint8_t* a, int c0, int row, const RowIn& v) {
-    put_features<KC>(a, KC - c0, row, v);
-    if constexpr (KC + 1 < KEND) encode_cols<KC + 1, KEND>(a, c0, row, v);
+__device__ __forceinline__ void encode_cols(uint8_t* a, int c0, int row, const RowIn& v, uint4* genc) {
+    put_features<KC>(a, KC - c0, row, v, genc);
+    if constexpr (KC + 1 < KEND) encode_cols<KC + 1, KEND>(a, c0, row, v, genc);
 }
 
 // One warpgroup's MMA batch: layer with `ksteps` K-steps of 16, A from
@@ -455,8 +333,9 @@ __device__ __forceinline__ bool mma_batch(int g, int t, uint32_t tmem_d, uint32_
     return *fail == 0;
 }
 
-// Accumulator row t (64 columns) -> ReLU -> bf16 A operand (K = 64, SBO 1024).
-__device__ __forceinline__ void acc_to_a(uint32_t tmem_row, uint8_t* a, int row) {
+// Accumulator row t (64 columns) -> ReLU -> bf16 A operand (K = 64, SBO 1024),
+// and into the row's stored activation ([64] bf16) when gact is set.
+__device__ __forceinline__ void acc_to_a(uint32_t tmem_row, uint8_t* a, int row, uint4* gact) {
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
         float v[16];
@@ -469,13 +348,53 @@ __device__ __forceinline__ void acc_to_a(uint32_t tmem_row, uint8_t* a, int row)
             w.z = pack(fmaxf(v[8 * h + 4], 0.0f), fmaxf(v[8 * h + 5], 0.0f));
             w.w = pack(fmaxf(v[8 * h + 6], 0.0f), fmaxf(v[8 * h + 7], 0.0f));
             *reinterpret_cast<uint4*>(a + ((row >> 3) * 8 + 2 * q + h) * 128 + (row & 7) * 16) = w;
+            if (gact) gact[2 * q + h] = w;
         }
     }
 }
 
-__global__ void __launch_bounds__(128 * kTcGroups, 1) k_mlp_infer_tc(const float* __restrict__ raw, NrcCount cnt,
-                                                                     Enc ec, const __nv_bfloat16* __restrict__ wtc,
-                                                                     float* __restrict__ out, uint32_t* err) {
+// TMEM, barriers and failure flags of a tcgen05 MLP kernel: allocation of
+// 64 columns per warpgroup (64, 128 or 256: powers of two) by warp 0 and the
+// fences that publish them.
+__device__ __forceinline__ void tc_setup(uint64_t* mbar, int* fail, uint32_t* tmem_base) {
+    const uint32_t groups = blockDim.x >> 7;
+    if (threadIdx.x < groups) {
+        mbar_init(smem_u32(&mbar[threadIdx.x]));
+        fail[threadIdx.x] = 0;
+    }
+    if ((threadIdx.x >> 5) == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_base)),
+                     "r"(64u * groups));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    fence_proxy_async();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+}
+
+// Reports a timed-out wait and frees the TMEM (every warpgroup has stopped
+// issuing by then: its last batch was committed and waited for, or it gave up
+// waiting, and the CTA barrier below follows every warpgroup's exit).
+__device__ __forceinline__ void tc_teardown(const int* fail, uint32_t tmem_base, uint32_t* err) {
+    const int g = threadIdx.x >> 7;
+    if ((threadIdx.x & 127) == 0 && fail[g]) atomicOr(err, kErrMlpTimeout);
+    tc_fence_before();
+    __syncthreads();
+    if ((threadIdx.x >> 5) == 0) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base),
+                     "r"(64u * (blockDim.x >> 7)));
+    }
+}
+
+template <bool kTrain>
+__global__ void __launch_bounds__(128 * kTcGroups, 1) k_mlp_fwd_tc(const float* __restrict__ raw, NrcCount cnt,
+                                                                   Enc ec, const __nv_bfloat16* __restrict__ wtc,
+                                                                   float* __restrict__ out, uint32_t* err,
+                                                                   uint32_t ld, __nv_bfloat16* __restrict__ acts,
+                                                                   __nv_bfloat16* __restrict__ enc) {
     extern __shared__ __align__(1024) uint8_t tc_smem[];
     __shared__ __align__(8) uint64_t mbar[kTcGroups];
     __shared__ int fail[kTcGroups];
@@ -487,20 +406,7 @@ __global__ void __launch_bounds__(128 * kTcGroups, 1) k_mlp_infer_tc(const float
         uint4* dst = reinterpret_cast<uint4*>(tc_smem);
         for (int k = threadIdx.x; k < kTcWBytes / 16; k += blockDim.x) dst[k] = src[k];
     }
-    if (threadIdx.x < kTcGroups) {
-        mbar_init(smem_u32(&mbar[threadIdx.x]));
-        fail[threadIdx.x] = 0;
-    }
-    if (warp == 0) {
-        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base)),
-                     "r"(64u * kTcGroups));
-        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
-    }
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    fence_proxy_async();
-    tc_fence_before();
-    __syncthreads();
-    tc_fence_after();
+    tc_setup(mbar, fail, &tmem_base);
     const uint32_t n = rows_of(cnt);
     const uint32_t tmem_d = tmem_base + 64u * g;                          // this warpgroup's columns
     const uint32_t tmem_row = tmem_d + ((uint32_t)(32 * (warp & 3)) << 16);   // this warp's lanes
@@ -509,23 +415,27 @@ __global__ void __launch_bounds__(128 * kTcGroups, 1) k_mlp_infer_tc(const float
     const uint32_t mb = smem_u32(&mbar[g]);
     uint32_t phase = 0;
     const uint32_t tiles = (n + 127) / 128;
-    for (uint32_t tile = blockIdx.x * kTcGroups + g; tile < tiles; tile += gridDim.x * kTcGroups) {
+    const uint32_t groups = blockDim.x >> 7;
+    for (uint32_t tile = blockIdx.x * groups + g; tile < tiles; tile += gridDim.x * groups) {
         const uint32_t row = tile * 128 + t;
+        const bool keep = kTrain && row < n;
         RowIn v = {};
         if (row < n) v = load_row(raw, row, ec);
+        uint4* genc = keep ? reinterpret_cast<uint4*>(enc + (size_t)row * kIn) : nullptr;
         // layer 0, features 0-111 (K-steps 0-6)
-        encode_cols<0, kTcHalfCols>(a, 0, t, v);
+        encode_cols<0, kTcHalfCols>(a, 0, t, v, genc);
         if (!mma_batch(g, t, tmem_d, a_base, kTcHalfCols * 128, w_base + 2 * param_off(0), 26 * 128, 0, 7, 64,
                        false, mb, phase, &fail[g]))
             break;
         // features 112-207 (K-steps 7-12), accumulated
-        encode_cols<kTcHalfCols, 26>(a, kTcHalfCols, t, v);
+        encode_cols<kTcHalfCols, 26>(a, kTcHalfCols, t, v, genc);
         if (!mma_batch(g, t, tmem_d, a_base, kTcHalfCols * 128, w_base + 2 * param_off(0), 26 * 128, 7, 6, 64,
                        true, mb, phase, &fail[g]))
             break;
         bool ok = true;
         for (int l = 1; l <= 5 && ok; ++l) {
-            acc_to_a(tmem_row, a, t);
+            acc_to_a(tmem_row, a, t,
+                     keep ? reinterpret_cast<uint4*>(acts + (size_t)(l - 1) * ld * kHid + (size_t)row * kHid) : nullptr);
             ok = mma_batch(g, t, tmem_d, a_base, 8 * 128, w_base + 2 * param_off(l), 8 * 128, 0, 4, l == 5 ? 16 : 64,
                            false, mb, phase, &fail[g]);
         }
@@ -538,90 +448,111 @@ __global__ void __launch_bounds__(128 * kTcGroups, 1) k_mlp_infer_tc(const float
             out[3 * (size_t)row + 2] = o[2];
         }
     }
-    if (t == 0 && fail[g]) atomicOr(err, kErrMlpTimeout);
-    tc_fence_before();
-    __syncthreads();
-    if (warp == 0) {
-        tc_fence_after();
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base), "r"(64u * kTcGroups));
-    }
+    tc_teardown(fail, tmem_base, err);
 }
 
-// ---------------------------------------------------------------- backward
-// Loss gradient (mean over the n rows and 3 channels) and dOut of every layer
-// (layer l at douts + l * ld * 64: layers 0-4 [n][64], layer 5 [n][16]);
-// accumulates the loss sum.
-__global__ void __launch_bounds__(32 * kMlpWarps) k_mlp_bwd(const float* __restrict__ pred,
-                                                            const float* __restrict__ target,
-                                                 NrcCount cnt, uint32_t ld, const __nv_bfloat16* __restrict__ acts,
-                                                 const __nv_bfloat16* __restrict__ wbwd,
-                                                 __nv_bfloat16* __restrict__ douts, float* __restrict__ loss_sum) {
-    extern __shared__ __align__(16) __nv_bfloat16 sw[];
-    stage(sw, wbwd, kBwdElems);
-    __syncthreads();
+// ---------------------------------------------------------------- backward on tcgen05
+// k_mlp_bwd_tc: loss gradient (mean over the n rows and 3 channels), then
+// dOut of every layer back to the input (layer l at douts + l * ld * 64:
+// layers 0-4 [n][64], layer 5 [n][16]); accumulates the loss sum.  The tile
+// scheme of k_mlp_fwd_tc: thread t of a warpgroup owns row t, writes its
+// dOut_l into the A operand (K-major, no swizzle) and one thread issues
+// dAct_{l-1} = dOut_l * W_l with B = W_l^T from the transposed pack (N = 64
+// inputs, K = the layer's outputs: 16 for layer 5, else 64).  dOut_l is
+// dAct_l where layer l's stored activation is positive (ReLU), else 0.
+constexpr int kTcbWBytes = kTcbElems * 2;                       // 34,816
+constexpr int kTcbABytes = 128 / 8 * 8 * 128;                  // 16,384 (K = 64)
+constexpr int kTcbSmem = kTcbWBytes + kTcGroups * kTcbABytes;   // 100,352 at 4 warpgroups
+
+__global__ void __launch_bounds__(128 * kTcGroups, 1) k_mlp_bwd_tc(const float* __restrict__ pred,
+                                                                   const float* __restrict__ target, NrcCount cnt,
+                                                                   uint32_t ld, const __nv_bfloat16* __restrict__ acts,
+                                                                   const __nv_bfloat16* __restrict__ wtcb,
+                                                                   __nv_bfloat16* __restrict__ douts,
+                                                                   float* __restrict__ loss_sum, uint32_t* err) {
+    extern __shared__ __align__(1024) uint8_t tc_smem[];
+    __shared__ __align__(8) uint64_t mbar[kTcGroups];
+    __shared__ int fail[kTcGroups];
+    __shared__ uint32_t tmem_base;
+    const int warp = threadIdx.x >> 5, g = warp >> 2, t = threadIdx.x & 127;
+    {
+        const uint4* src = reinterpret_cast<const uint4*>(wtcb);
+        uint4* dst = reinterpret_cast<uint4*>(tc_smem);
+        for (int k = threadIdx.x; k < kTcbWBytes / 16; k += blockDim.x) dst[k] = src[k];
+    }
+    tc_setup(mbar, fail, &tmem_base);
     const uint32_t n = rows_of(cnt);
-    if (n == 0) return;
-    const float scale = 1.0f / (3.0f * (float)n);
-    const unsigned lane = threadIdx.x & 31u, g = lane >> 2, t = lane & 3u, warp = threadIdx.x >> 5;
+    const float scale = n > 0 ? 1.0f / (3.0f * (float)n) : 0.0f;
+    const uint32_t tmem_d = tmem_base + 64u * g;
+    const uint32_t tmem_row = tmem_d + ((uint32_t)(32 * (warp & 3)) << 16);
+    uint8_t* a = tc_smem + kTcbWBytes + g * kTcbABytes;
+    const uint32_t a_base = smem_u32(a), w_base = smem_u32(tc_smem);
+    const uint32_t mb = smem_u32(&mbar[g]);
+    uint32_t phase = 0;
     float loss = 0.0f;
-    for (uint32_t tile = blockIdx.x * kMlpWarps + warp; tile * 16 < n; tile += gridDim.x * kMlpWarps) {
-        const uint32_t row0 = tile * 16, r0 = row0 + g, r1 = row0 + g + 8;
-        // dL/dpred for this lane's output columns 2t, 2t+1 (only 0..2 exist)
-        float d[2][2] = {{0.0f, 0.0f}, {0.0f, 0.0f}};
+    const uint32_t tiles = (n + 127) / 128;
+    const uint32_t groups = blockDim.x >> 7;
+    for (uint32_t tile = blockIdx.x * groups + g; tile < tiles; tile += gridDim.x * groups) {
+        const uint32_t row = tile * 128 + t;
+        const bool ok = row < n;
+        // dL/dpred of the row's 3 channels -> dOut5 (K = 16: two core-matrix columns)
+        float d[3] = {0.0f, 0.0f, 0.0f};
+        if (ok) {
 #pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            uint32_t r = h ? r1 : r0;
+            for (int c = 0; c < 3; ++c) {
+                const float p = pred[3 * (size_t)row + c], y = target[3 * (size_t)row + c];
+                const float den = p * p + kLossEps, e = p - y;
+                loss += e * e / den;
+                d[c] = 2.0f * e / den * scale;
+            }
+        }
+        const uint4 q0 = make_uint4(pack(d[0], d[1]), pack(d[2], 0.0f), 0u, 0u), q1 = make_uint4(0u, 0u, 0u, 0u);
+        if (ok) {
+            uint4* g5 = reinterpret_cast<uint4*>(douts + (size_t)5 * ld * kHid + (size_t)row * kOut);
+            g5[0] = q0;
+            g5[1] = q1;
+        }
+        *reinterpret_cast<uint4*>(a + ((t >> 3) * 2) * 128 + (t & 7) * 16) = q0;
+        *reinterpret_cast<uint4*>(a + ((t >> 3) * 2 + 1) * 128 + (t & 7) * 16) = q1;
+        // dAct4 = dOut5 * W5
+        if (!mma_batch(g, t, tmem_d, a_base, 2 * 128, w_base + 2 * tcb_off(5), 2 * 128, 0, 1, 64, false, mb, phase,
+                       &fail[g]))
+            break;
+        bool go = true;
+        for (int l = 4; l >= 0 && go; --l) {
+            const uint4* gact = reinterpret_cast<const uint4*>(acts + (size_t)l * ld * kHid + (size_t)row * kHid);
+            uint4* gd = reinterpret_cast<uint4*>(douts + (size_t)l * ld * kHid + (size_t)row * kHid);
 #pragma unroll
-            for (int q = 0; q < 2; ++q) {
-                uint32_t c = 2 * t + q;
-                if (r < n && c < 3) {
-                    float p = pred[3 * (size_t)r + c], y = target[3 * (size_t)r + c];
-                    float den = p * p + kLossEps;
-                    float e = p - y;
-                    loss += e * e / den;
-                    d[h][q] = 2.0f * e / den * scale;
+            for (int q = 0; q < 4; ++q) {
+                float v[16];
+                tmem_ld16(tmem_row + 16 * q, v);
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const uint4 m = ok ? gact[2 * q + h] : make_uint4(0u, 0u, 0u, 0u);
+                    const uint32_t mw[4] = {m.x, m.y, m.z, m.w};
+                    uint32_t w[4];
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) {
+                        const float lo = lo_of(mw[k]) > 0.0f ? v[8 * h + 2 * k] : 0.0f;
+                        const float hi = hi_of(mw[k]) > 0.0f ? v[8 * h + 2 * k + 1] : 0.0f;
+                        w[k] = pack(lo, hi);
+                    }
+                    const uint4 wv = make_uint4(w[0], w[1], w[2], w[3]);
+                    if (ok) gd[2 * q + h] = wv;
+                    *reinterpret_cast<uint4*>(a + ((t >> 3) * 8 + 2 * q + h) * 128 + (t & 7) * 16) = wv;
                 }
             }
-        }
-        uint32_t a5[4] = {pack(d[0][0], d[0][1]), pack(d[1][0], d[1][1]), 0u, 0u};
-        // store dOut5 ([n][16], 8 words per row)
-        uint32_t* d5 = reinterpret_cast<uint32_t*>(douts + (size_t)5 * ld * kHid);
-        if (r0 < n) { d5[r0 * 8 + t] = a5[0]; d5[r0 * 8 + 4 + t] = 0u; }
-        if (r1 < n) { d5[r1 * 8 + t] = a5[1]; d5[r1 * 8 + 4 + t] = 0u; }
-        // dAct4 = dOut5 * W5 (K = 16): B[k][n] = W5[k][n] = W5^T[n][k]
-        float acc[8][4];
-#pragma unroll
-        for (int nt = 0; nt < 8; ++nt) {
-#pragma unroll
-            for (int q = 0; q < 4; ++q) acc[nt][q] = 0.0f;
-            const __nv_bfloat16* p = sw + bwd_off(5) + (nt * 8 + g) * bwd_stride(5) + 2 * t;
-            mma(acc[nt], a5, *reinterpret_cast<const uint32_t*>(p), *reinterpret_cast<const uint32_t*>(p + 8));
-        }
-#pragma unroll 1
-        for (int l = 4; l >= 0; --l) {
-            // ReLU mask from the stored activation of layer l
-            const uint32_t* act = reinterpret_cast<const uint32_t*>(acts + (size_t)l * ld * kHid);
-#pragma unroll
-            for (int nt = 0; nt < 8; ++nt) {
-                uint32_t m0 = r0 < n ? act[r0 * 32 + 4 * nt + t] : 0u;
-                uint32_t m1 = r1 < n ? act[r1 * 32 + 4 * nt + t] : 0u;
-                acc[nt][0] = lo_of(m0) > 0.0f ? acc[nt][0] : 0.0f;
-                acc[nt][1] = hi_of(m0) > 0.0f ? acc[nt][1] : 0.0f;
-                acc[nt][2] = lo_of(m1) > 0.0f ? acc[nt][2] : 0.0f;
-                acc[nt][3] = hi_of(m1) > 0.0f ? acc[nt][3] : 0.0f;
-            }
-            uint32_t af[4][4];
-            to_a_frags(acc, af, false);
-            store_frags(reinterpret_cast<uint32_t*>(douts + (size_t)l * ld * kHid), row0, n, af);
             if (l == 0) break;
-            // dAct_{l-1} = dOut_l * W_l: B[k][n] = W_l[k][n] = W_l^T[n][k]
-            gemm64<8>(acc, af, sw + bwd_off(l), bwd_stride(l));
+            // dAct_{l-1} = dOut_l * W_l
+            go = mma_batch(g, t, tmem_d, a_base, 8 * 128, w_base + 2 * tcb_off(l), 8 * 128, 0, 4, 64, false, mb,
+                           phase, &fail[g]);
         }
+        if (!go) break;
     }
-    // warp-reduce the loss, one atomic per warp
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) loss += __shfl_xor_sync(0xFFFFFFFFu, loss, o);
-    if (lane == 0) atomicAdd(loss_sum, loss);
+    if ((threadIdx.x & 31) == 0 && loss != 0.0f) atomicAdd(loss_sum, loss);
+    tc_teardown(fail, tmem_base, err);
 }
 
 // ---------------------------------------------------------------- weight gradient
@@ -723,13 +654,14 @@ __device__ __forceinline__ void param_coords(int p, int& l, int& o, int& i) {
 
 // grad = sum of the CTA partials; with do_step, Adam on the FP32 master
 // weights (bias corrections 1 - beta^step; rows 3..15 of the output layer and
-// the padded inputs stay zero), the bf16 forward / transposed packs, and the
-// inference pack: with ema_a > 0, ema = ema_a * ema + (1 - ema_a) * w (ema
+// the padded inputs stay zero), the bf16 training packs (forward and
+// transposed, both in the tensor cores' canonical layout), and the inference
+// pack: with ema_a > 0, ema = ema_a * ema + (1 - ema_a) * w (ema
 // starts at 0) and the pack holds ema / (1 - ema_a^ema_steps), else w.
 __global__ void k_reduce_adam(const float* __restrict__ partial, int n_part, NrcCount cnt, float* __restrict__ grad,
                               float* __restrict__ w, float* __restrict__ m, float* __restrict__ v, AdamArgs ar,
-                              const StepState* __restrict__ st, int do_step, __nv_bfloat16* __restrict__ wfwd,
-                              __nv_bfloat16* __restrict__ wbwd, float* __restrict__ ema,
+                              const StepState* __restrict__ st, int do_step, __nv_bfloat16* __restrict__ wtc,
+                              __nv_bfloat16* __restrict__ wtcb, float* __restrict__ ema,
                               __nv_bfloat16* __restrict__ winf) {
     int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= kParams) return;
@@ -752,8 +684,8 @@ __global__ void k_reduce_adam(const float* __restrict__ partial, int n_part, Nrc
         w[p] = x;
     }
     __nv_bfloat16 h = __float2bfloat16_rn(x);
-    wfwd[fwd_off(l) + o * fwd_stride(l) + i] = h;
-    if (l >= 1) wbwd[bwd_off(l) + i * bwd_stride(l) + o] = h;
+    wtc[tc_index(l, o, i)] = h;
+    if (l >= 1) wtcb[tcb_index(l, o, i)] = h;
     float xi = x;
     if (ar.ema_a > 0.0f) {
         float e = ar.ema_a * ema[p] + (1.0f - ar.ema_a) * x;
@@ -765,8 +697,8 @@ __global__ void k_reduce_adam(const float* __restrict__ partial, int n_part, Nrc
 
 // Packs the master weights (after creation or replacement) and restarts the
 // moving average: the inference pack holds w.
-__global__ void k_pack(const float* __restrict__ w, __nv_bfloat16* __restrict__ wfwd,
-                       __nv_bfloat16* __restrict__ wbwd, float* __restrict__ ema, __nv_bfloat16* __restrict__ winf,
+__global__ void k_pack(const float* __restrict__ w, __nv_bfloat16* __restrict__ wtc,
+                       __nv_bfloat16* __restrict__ wtcb, float* __restrict__ ema, __nv_bfloat16* __restrict__ winf,
                        StepState* st) {
     int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p == 0) st->ema_steps = 0;
@@ -774,9 +706,9 @@ __global__ void k_pack(const float* __restrict__ w, __nv_bfloat16* __restrict__ 
     int l, o, i;
     param_coords(p, l, o, i);
     __nv_bfloat16 h = __float2bfloat16_rn(w[p]);
-    wfwd[fwd_off(l) + o * fwd_stride(l) + i] = h;
+    wtc[tc_index(l, o, i)] = h;
     winf[tc_index(l, o, i)] = h;
-    if (l >= 1) wbwd[bwd_off(l) + i * bwd_stride(l) + o] = h;
+    if (l >= 1) wtcb[tcb_index(l, o, i)] = h;
     ema[p] = 0.0f;
 }
 
@@ -789,7 +721,7 @@ using namespace ilm::nrc;
 struct ilm_nrc {
     ilm_nrc_config cfg;
     DeviceBuffer state;                          // StepState
-    DeviceBuffer w, m, v, grad, wfwd, wbwd;      // params and packs
+    DeviceBuffer w, m, v, grad, wtc, wtcb;       // params and their training packs
     DeviceBuffer ema, winf;                      // moving average and its inference pack
     DeviceBuffer partial;                        // k_wgrad_all partial sums
     DeviceBuffer err;                            // device error word (kErrMlpTimeout)
@@ -802,12 +734,22 @@ struct ilm_nrc {
 
 namespace {
 
-// Grid for n rows at rows_per_block, at most the CTAs that are resident at
-// once (3 per SM for the forward / backward kernels' shared memory): each CTA
-// stages its weights once and strides over row tiles.
-int blocks_for(uint32_t n, int rows_per_block) {
-    int b = (int)((n + rows_per_block - 1) / rows_per_block);
-    return b < 1 ? 1 : (b > 148 * 3 ? 148 * 3 : b);
+// Launch shape of a tcgen05 MLP kernel for n rows: one 128-row tile per
+// warpgroup in flight, 4 warpgroups per CTA when the tiles fill the SMs that
+// way, else 2 or 1 so that they spread over more SMs (up to 2 CTAs per SM:
+// TMEM and shared memory allow it); each CTA stages the weights once and
+// strides over tiles.
+struct TcLaunch {
+    unsigned grid, threads;
+    size_t smem;
+};
+TcLaunch tc_launch(uint32_t n, int w_bytes, int a_bytes) {
+    const uint32_t tiles = (n + 127) / 128;
+    const uint32_t groups = tiles >= 4u * 148u ? 4u : (tiles >= 2u * 148u ? 2u : 1u);
+    uint32_t grid = (tiles + groups - 1) / groups;
+    const uint32_t cap = groups == 4 ? 148u : 296u;
+    grid = grid < 1 ? 1 : (grid > cap ? cap : grid);
+    return {grid, 128u * groups, (size_t)w_bytes + groups * (size_t)a_bytes};
 }
 
 Enc enc_params(const ilm_nrc* h) {
@@ -818,8 +760,8 @@ Enc enc_params(const ilm_nrc* h) {
 
 cudaError_t pack(ilm_nrc* h, cudaStream_t s) {
     k_pack<<<(kParams + 255) / 256, 256, 0, s>>>(
-        static_cast<const float*>(h->w.ptr), static_cast<__nv_bfloat16*>(h->wfwd.ptr),
-        static_cast<__nv_bfloat16*>(h->wbwd.ptr), static_cast<float*>(h->ema.ptr),
+        static_cast<const float*>(h->w.ptr), static_cast<__nv_bfloat16*>(h->wtc.ptr),
+        static_cast<__nv_bfloat16*>(h->wtcb.ptr), static_cast<float*>(h->ema.ptr),
         static_cast<__nv_bfloat16*>(h->winf.ptr), static_cast<StepState*>(h->state.ptr));
     return cudaGetLastError();
 }
@@ -835,23 +777,20 @@ cudaError_t reserve_train(ilm_nrc* h, uint32_t rows) {
     return h->douts.reserve((size_t)rows * 6 * kHid * 2);
 }
 
+// Training runs on the current weights and stores the encoding and the
+// activations (layer stride = the batch's row cap); inference runs on the
+// moving-average pack.
 cudaError_t forward(ilm_nrc* h, const float* raw, NrcCount cnt, bool train, float* out, cudaStream_t s) {
-    size_t smem = (size_t)kFwdElems * 2;
     const uint32_t rows = batch_cap(cnt);
-    int blocks = blocks_for(rows, 16 * kMlpWarps);
+    uint32_t* err = static_cast<uint32_t*>(h->err.ptr);
+    const TcLaunch L = tc_launch(rows, kTcWBytes, kTcABytes);
     if (train)
-        k_mlp_fwd<true><<<blocks, 32 * kMlpWarps, smem, s>>>(raw, cnt, enc_params(h), rows,
-                                                  static_cast<const __nv_bfloat16*>(h->wfwd.ptr), out,
-                                                  static_cast<__nv_bfloat16*>(h->acts.ptr),
-                                                  static_cast<__nv_bfloat16*>(h->enc.ptr));
-    else {   // inference: tcgen05 kernel on the moving-average pack
-        uint32_t tiles = (rows + 127) / 128;
-        uint32_t grid = (tiles + kTcGroups - 1) / kTcGroups;
-        grid = grid < 1 ? 1 : (grid > 148 ? 148 : grid);
-        k_mlp_infer_tc<<<grid, 128 * kTcGroups, kTcSmem, s>>>(raw, cnt, enc_params(h),
-                                                             static_cast<const __nv_bfloat16*>(h->winf.ptr), out,
-                                                             static_cast<uint32_t*>(h->err.ptr));
-    }
+        k_mlp_fwd_tc<true><<<L.grid, L.threads, L.smem, s>>>(
+            raw, cnt, enc_params(h), static_cast<const __nv_bfloat16*>(h->wtc.ptr), out, err, rows,
+            static_cast<__nv_bfloat16*>(h->acts.ptr), static_cast<__nv_bfloat16*>(h->enc.ptr));
+    else
+        k_mlp_fwd_tc<false><<<L.grid, L.threads, L.smem, s>>>(
+            raw, cnt, enc_params(h), static_cast<const __nv_bfloat16*>(h->winf.ptr), out, err, 0u, nullptr, nullptr);
     return cudaGetLastError();
 }
 
@@ -867,9 +806,10 @@ cudaError_t train_rows(ilm_nrc* h, const float* raw, const float* target, NrcCou
     if ((e = forward(h, raw, cnt, true, pred, s)) != cudaSuccess) return e;
     const __nv_bfloat16* acts = static_cast<const __nv_bfloat16*>(h->acts.ptr);
     __nv_bfloat16* douts = static_cast<__nv_bfloat16*>(h->douts.ptr);
-    k_mlp_bwd<<<blocks_for(cap, 16 * kMlpWarps), 32 * kMlpWarps, (size_t)kBwdElems * 2, s>>>(
-        pred, target, cnt, cap, acts, static_cast<const __nv_bfloat16*>(h->wbwd.ptr), douts,
-        static_cast<float*>(h->loss.ptr));
+    const TcLaunch L = tc_launch(cap, kTcbWBytes, kTcbABytes);
+    k_mlp_bwd_tc<<<L.grid, L.threads, L.smem, s>>>(
+        pred, target, cnt, cap, acts, static_cast<const __nv_bfloat16*>(h->wtcb.ptr), douts,
+        static_cast<float*>(h->loss.ptr), static_cast<uint32_t*>(h->err.ptr));
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     int n_part = (int)std::min<uint32_t>(kMaxPartials, std::max<uint32_t>(1, (cap + kChunk - 1) / kChunk));
     StepState* st = static_cast<StepState*>(h->state.ptr);
@@ -881,7 +821,7 @@ cudaError_t train_rows(ilm_nrc* h, const float* raw, const float* target, NrcCou
     k_reduce_adam<<<(kParams + 255) / 256, 256, 0, s>>>(
         static_cast<const float*>(h->partial.ptr), n_part, cnt, static_cast<float*>(h->grad.ptr),
         static_cast<float*>(h->w.ptr), static_cast<float*>(h->m.ptr), static_cast<float*>(h->v.ptr), ar, st, do_step,
-        static_cast<__nv_bfloat16*>(h->wfwd.ptr), static_cast<__nv_bfloat16*>(h->wbwd.ptr),
+        static_cast<__nv_bfloat16*>(h->wtc.ptr), static_cast<__nv_bfloat16*>(h->wtcb.ptr),
         static_cast<float*>(h->ema.ptr), static_cast<__nv_bfloat16*>(h->winf.ptr));
     return cudaGetLastError();
 }
@@ -924,9 +864,9 @@ int32_t ilm_nrc_create(ilm_context* ctx, const ilm_nrc_config* cfg, ilm_nrc** ou
     for (DeviceBuffer* b : {&h->w, &h->m, &h->v, &h->grad, &h->ema})
         if ((e = b->reserve(kParams * 4)) != cudaSuccess) return cuda_fail(ctx, e, "nrc");
     if ((e = h->partial.reserve((size_t)kMaxPartials * kParams * 4)) != cudaSuccess) return cuda_fail(ctx, e, "nrc");
-    if ((e = h->wfwd.reserve(kFwdElems * 2)) != cudaSuccess) return cuda_fail(ctx, e, "nrc");
-    if ((e = h->winf.reserve(kFwdElems * 2)) != cudaSuccess) return cuda_fail(ctx, e, "nrc");
-    if ((e = h->wbwd.reserve(kBwdElems * 2)) != cudaSuccess) return cuda_fail(ctx, e, "nrc");
+    if ((e = h->wtc.reserve(kParams * 2)) != cudaSuccess) return cuda_fail(ctx, e, "nrc");
+    if ((e = h->winf.reserve(kParams * 2)) != cudaSuccess) return cuda_fail(ctx, e, "nrc");
+    if ((e = h->wtcb.reserve(kTcbElems * 2)) != cudaSuccess) return cuda_fail(ctx, e, "nrc");
     if ((e = h->loss.reserve(4)) != cudaSuccess) return cuda_fail(ctx, e, "nrc");
     if ((e = h->err.reserve(4)) != cudaSuccess) return cuda_fail(ctx, e, "nrc");
     cudaMemset(h->err.ptr, 0, 4);
@@ -948,11 +888,12 @@ int32_t ilm_nrc_create(ilm_context* ctx, const ilm_nrc_config* cfg, ilm_nrc** ou
     cudaMemcpy(h->w.ptr, w.data(), kParams * 4, cudaMemcpyHostToDevice);
     cudaMemset(h->m.ptr, 0, kParams * 4);
     cudaMemset(h->v.ptr, 0, kParams * 4);
-    cudaMemset(h->wfwd.ptr, 0, kFwdElems * 2);
-    cudaMemset(h->winf.ptr, 0, kFwdElems * 2);
-    cudaMemset(h->wbwd.ptr, 0, kBwdElems * 2);
-    cudaFuncSetAttribute(k_mlp_fwd<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kFwdElems * 2);
-    cudaFuncSetAttribute(k_mlp_infer_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem);
+    cudaMemset(h->wtc.ptr, 0, kParams * 2);
+    cudaMemset(h->winf.ptr, 0, kParams * 2);
+    cudaMemset(h->wtcb.ptr, 0, kTcbElems * 2);
+    cudaFuncSetAttribute(k_mlp_fwd_tc<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem);
+    cudaFuncSetAttribute(k_mlp_fwd_tc<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem);
+    cudaFuncSetAttribute(k_mlp_bwd_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcbSmem);
     if ((e = pack(h.get(), h->stream)) != cudaSuccess) return cuda_fail(ctx, e, "nrc pack");
     if ((e = cudaStreamSynchronize(h->stream)) != cudaSuccess) return cuda_fail(ctx, e, "nrc");
     *out = h.release();
