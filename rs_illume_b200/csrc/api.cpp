@@ -124,7 +124,7 @@ int32_t ilm_context_create(ilm_context** out, const ilm_config* cfg) {
     ctx->flags = cfg ? cfg->flags : 0;
     if (cfg && cfg->max_iterations) ctx->max_iter = cfg->max_iterations;
     if (cudaSetDevice(dev) != cudaSuccess) return ILM_ERR_NO_DEVICE;
-    // Fail early when this build's kernels cannot run on the device.
+    // Fail early when the library's kernels cannot run on the device.
     cudaFuncAttributes fa;
     if (!kernels_loadable(&fa)) {
         cudaGetLastError();
