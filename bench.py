@@ -67,7 +67,7 @@ BYTES_PER_RAY_ANY = 32 + 4 + 32 * N_NODE_ANY + 36 * N_TRI_ANY
 # DRAM bytes (read + write) of one closest-hit launch on this workload, from the
 # ncu capture summarised in profiles/closest_incoherent_w8.md, per
 # (width, schedule, occupancy, stack depth).
-DRAM_TRAFFIC = {(8, "persistent", "high", 64): 250579456}
+DRAM_TRAFFIC = {(8, "persistent", "high", 64): 250215936}
 WORKLOAD = ("incoherent closest-hit: displaced icosphere level 8 (1,310,720 tris, seed 2), "
             "2,097,152 closest rays of 4,194,304 ball rays (radius 3, uniform directions)")
 METRIC = "closest-hit Mrays/s"
