@@ -289,25 +289,32 @@ int32_t ilm_intersect_any(ilm_context* ctx, ilm_accel_id accel, const ilm_ray* r
  * callers that must not call cudaMalloc/cudaFree once set up: a render loop
  * with a fixed memory budget, a process whose device memory is owned by a
  * caching allocator, or a thread that must not stall the device (cudaMalloc
- * and cudaFree can synchronise it).  Same results as ilm_intersect_closest.
+ * and cudaFree can synchronise it).  Same results as ilm_intersect_closest:
+ * the same kernel with the same launch choices (the accel's own stack depth,
+ * schedule and occupancy from ilm_accel_set_launch / ilm_autotune, else the
+ * context's), and the same ILM_FLAG_VALIDATE_RAYS check of host rays.
  * Its scratch is one fixed array that the library holds on every GPU that
- * loads it, until exit: 3 MiB + 256 B (a work counter, an error word and
- * staging for up to ILM_NOALLOC_MAX_RAYS rays and hits).
+ * loads it, until exit: 3 MiB + 256 B (a work counter and staging for up to
+ * ILM_NOALLOC_MAX_RAYS rays and hits).
  *  - n > ILM_NOALLOC_MAX_RAYS fails with ILM_ERR_INVALID_ARGUMENT.
  *  - The first call on a device resolves the array's address on that device;
- *    make that first call before any stream capture.
+ *    make that first call before any stream capture.  The address is kept
+ *    for the life of the process: do not reset the device (cudaDeviceReset)
+ *    while the library is loaded.
  *  - All calls share the array: calls that overlap on the GPU race.
  *    Serialise them (one stream, or wait between calls).
- *  - Host buffers: returns with the hits in host memory, and
- *    ILM_ERR_TRAVERSAL_LIMIT if a ray hit the traversal limits.  Device
- *    buffers: stream-ordered; such rays are only marked in their records. */
+ *  - Rays that reach a traversal limit are marked in their records and set
+ *    the context's error word (read it with ilm_device_errors), as with
+ *    ilm_intersect_closest.  Host buffers: returns with the hits in host
+ *    memory, and ILM_ERR_TRAVERSAL_LIMIT if this call marked a record.
+ *    Device buffers: stream-ordered. */
 #define ILM_NOALLOC_MAX_RAYS 65536
 int32_t ilm_intersect_closest_noalloc(ilm_context* ctx, ilm_accel_id accel, const ilm_ray* rays,
                                       uint64_t n, ilm_hit* hits, void* stream);
 
 /* ------------------------------------------------------- batched queries */
 /* Many scenes with ray batches of any size, traced by one persistent launch
- * per BVH width (4 or 8): BVHAccel::intersect / intersect_p of each batch's
+ * per BVH width (2, 4 or 8): BVHAccel::intersect / intersect_p of each batch's
  * accel over its rays.  All buffers are device memory. */
 typedef struct {
     ilm_accel_id accel;

@@ -72,6 +72,12 @@ _SIG = {
     "orc_sphere_intersect": (ctypes.c_int, [_P, _P, ctypes.c_int, _P]),
     "orc_sphere_world_bound": (None, [_P, _P]),
     "orc_last_trace_seconds": (ctypes.c_double, []),
+    "orc_wl_icosphere_counts": (None, [ctypes.c_uint32, _P, _P]),
+    "orc_wl_icosphere": (None, [ctypes.c_uint32, ctypes.c_uint64, ctypes.c_float, ctypes.c_float, _P, _P, _P]),
+    "orc_wl_ball_rays": (None, [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_float,
+                                ctypes.c_float, ctypes.c_float, _P]),
+    "orc_wl_soup": (None, [ctypes.c_uint64, ctypes.c_uint32, ctypes.c_float, _P, _P]),
+    "orc_wl_camera_rays": (None, [ctypes.c_uint32, ctypes.c_uint32, _P, ctypes.c_float, _P]),
     "orc_kdtree_create": (_P, [_P, ctypes.c_int, ctypes.c_int, ctypes.c_float, ctypes.c_uint32, ctypes.c_int]),
     "orc_kdtree_destroy": (None, [_P]),
     "orc_kdtree_node_count": (ctypes.c_uint32, [_P]),
@@ -272,8 +278,10 @@ class KdTree:
 
 
 def render_pt(scene: "Scene", xyz, idx, mat, albedo, emission, eye, fov_deg, width, height, spp, max_depth=8,
-              rr_depth=3, seed=3, window=None, threads=0):
-    """Path-traced image (oracle/pt.cpp).  Returns (rgb[h, w, 3], (closest rays, shadow rays))."""
+              rr_depth=3, seed=3, window=None, threads=0, traversal_counts=False):
+    """Path-traced image (oracle/pt.cpp).  Returns (rgb[h, w, 3], (closest rays, shadow rays)), and with
+    traversal_counts a third item: (closest node visits, closest triangle tests, shadow node visits,
+    shadow triangle tests), summed over the rays on the binary SAH BVH."""
     x0, y0, x1, y1 = window if window else (0, 0, width, height)
     xyz = np.ascontiguousarray(xyz, np.float32)
     idx = np.ascontiguousarray(idx, np.uint32)
@@ -282,11 +290,13 @@ def render_pt(scene: "Scene", xyz, idx, mat, albedo, emission, eye, fov_deg, wid
     emission = np.ascontiguousarray(emission, np.float32)
     eye = np.asarray(eye, np.float32)
     out = np.zeros((y1 - y0, x1 - x0, 3), np.float32)
-    counts = np.zeros(2, np.uint64)
+    counts = np.zeros(6, np.uint64)
     st = load().orc_render_pt(scene.h, _p(xyz), _p(idx), len(idx), _p(mat), _p(albedo), _p(emission), _p(eye),
                               fov_deg, width, height, spp, max_depth, rr_depth, seed, x0, y0, x1, y1, threads,
                               _p(out), _p(counts))
     assert st == 0, "invalid render arguments"
+    if traversal_counts:
+        return out, (int(counts[0]), int(counts[1])), tuple(int(c) for c in counts[2:])
     return out, (int(counts[0]), int(counts[1]))
 
 
@@ -391,3 +401,48 @@ def sphere_intersect(desc: orc_sphere_desc, o, d, tmax=float("inf")):
     out = np.zeros(3, np.float32)
     ok = load().orc_sphere_intersect(ctypes.byref(desc), _p(r), 1, _p(out))
     return tuple(float(x) for x in out) if ok else None
+
+
+# --- the oracle's own copy of the benchmark inputs (oracle/workloads.cpp) ---
+
+def icosphere(level: int, seed: int, amplitude: float = 0.05, radius: float = 1.0, centre=(0.0, 0.0, 0.0)):
+    nv, nt = ctypes.c_uint32(), ctypes.c_uint32()
+    load().orc_wl_icosphere_counts(level, ctypes.byref(nv), ctypes.byref(nt))
+    xyz = np.empty((nv.value, 3), np.float32)
+    idx = np.empty((nt.value, 3), np.uint32)
+    c = np.asarray(centre, np.float32)
+    load().orc_wl_icosphere(level, seed, amplitude, radius, _p(c), _p(xyz), _p(idx))
+    return xyz, idx
+
+
+def ball_rays(seed: int, skip: int, n: int, n_closest: int, radius: float = 3.0, tmax_lo: float = 0.1,
+              tmax_hi: float = 4.0) -> np.ndarray:
+    out = np.empty(n, RAY_DTYPE)
+    load().orc_wl_ball_rays(seed, skip, n, n_closest, radius, tmax_lo, tmax_hi, _p(out))
+    return out
+
+
+def soup(seed: int = 1, n: int = 32768, spread: float = 0.02):
+    xyz = np.empty((3 * n, 3), np.float32)
+    idx = np.empty((n, 3), np.uint32)
+    load().orc_wl_soup(seed, n, spread, _p(xyz), _p(idx))
+    return xyz, idx
+
+
+def camera_rays(width: int = 256, height: int = 256, eye=(0.5, 0.5, -1.5), fov_deg: float = 45.0) -> np.ndarray:
+    out = np.empty(width * height, RAY_DTYPE)
+    e = np.asarray(eye, np.float32)
+    load().orc_wl_camera_rays(width, height, _p(e), fov_deg, _p(out))
+    return out
+
+
+def incoherent_workload(n_rays: int = 4194304, level: int = 8):
+    """Displaced icosphere (seed 2) + ball rays (first half closest, second half shadow)."""
+    xyz, idx = icosphere(level, 2, 0.05, 1.0)
+    return xyz, idx, ball_rays(2, 4, n_rays, n_rays // 2, 3.0, 0.1, 4.0)
+
+
+def coherent_workload():
+    """32,768-triangle soup (seed 1) + 256x256 primary rays."""
+    xyz, idx = soup(1, 32768, 0.02)
+    return xyz, idx, camera_rays(256, 256, (0.5, 0.5, -1.5), 45.0)

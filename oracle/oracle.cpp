@@ -1464,6 +1464,14 @@ int orc_trace_any1(void* scene, const orc_ray* ray, uint8_t* occluded) {
     return trace_any(*(Scene*)scene, *ray, occluded, nullptr, nullptr);
 }
 
+int orc_trace_closest1_counted(void* scene, const orc_ray* ray, orc_hit* hit, uint32_t* nv, uint32_t* nt) {
+    return trace_closest(*(Scene*)scene, *ray, hit, nv, nt);
+}
+
+int orc_trace_any1_counted(void* scene, const orc_ray* ray, uint8_t* occluded, uint32_t* nv, uint32_t* nt) {
+    return trace_any(*(Scene*)scene, *ray, occluded, nv, nt);
+}
+
 void* orc_kdtree_create(void* scene, int isect_cost, int traversal_cost, float empty_bonus, uint32_t max_prims,
                         int max_depth) {
     const Scene* s = (const Scene*)scene;

@@ -146,6 +146,9 @@ int orc_curve_intersect(const orc_curve_desc* c, const orc_ray* r, float* out);
 /* Single-ray forms (used by the path-tracer restatement). Return 1 on stack overflow. */
 int orc_trace_closest1(void* scene, const orc_ray* ray, orc_hit* hit);
 int orc_trace_any1(void* scene, const orc_ray* ray, uint8_t* occluded);
+// The same, also returning the ray's node visits and primitive tests.
+int orc_trace_closest1_counted(void* scene, const orc_ray* ray, orc_hit* hit, uint32_t* nv, uint32_t* nt);
+int orc_trace_any1_counted(void* scene, const orc_ray* ray, uint8_t* occluded, uint32_t* nv, uint32_t* nt);
 
 /* Path tracer (oracle/pt.cpp): renders pixels [x0,x1) x [y0,y1) of a
  * width x height pinhole image (eye, looking +z, up +y, vertical fov) with
@@ -153,7 +156,9 @@ int orc_trace_any1(void* scene, const orc_ray* ray, uint8_t* occluded);
  * (albedo[3*material]) and one-sided diffuse emitters (emission[3*material]),
  * max_depth bounces, Russian roulette from bounce rr_depth.  `scene` must have
  * been created from the same triangles.  rgb_out: 3 floats per pixel, row-major
- * over the window; ray_counts: {closest-hit rays, shadow rays}. */
+ * over the window; ray_counts (6 entries): closest-hit rays, shadow rays, and
+ * their binary-BVH node visits and primitive tests (closest: [2], [3];
+ * shadow: [4], [5]). */
 int orc_render_pt(void* scene, const float* verts, const uint32_t* idx, uint32_t nt,
                   const uint32_t* prim_material, const float* albedo, const float* emission,
                   const float eye[3], float fov_deg, uint32_t width, uint32_t height, uint32_t spp,

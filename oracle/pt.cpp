@@ -187,20 +187,30 @@ Bsdf make_bsdf(const PtScene& s, const Isect& it) {
     return b;
 }
 
-struct Counters { uint64_t ext = 0, shadow = 0; };
+// Rays traced, and their binary-BVH node visits and primitive tests.
+struct Counters {
+    uint64_t ext = 0, shadow = 0;
+    uint64_t ext_nodes = 0, ext_tris = 0, shadow_nodes = 0, shadow_tris = 0;
+};
 
 bool occluded(const PtScene& s, V o, V d, float tmax, Counters& c) {
     orc_ray r{{o.x, o.y, o.z}, 0.0f, {d.x, d.y, d.z}, tmax};
     uint8_t occ = 0;
-    orc_trace_any1(s.scene, &r, &occ);
+    uint32_t nv = 0, nt = 0;
+    orc_trace_any1_counted(s.scene, &r, &occ, &nv, &nt);
     ++c.shadow;
+    c.shadow_nodes += nv;
+    c.shadow_tris += nt;
     return occ != 0;
 }
 
 bool closest(const PtScene& s, V o, V d, orc_hit* h, Counters& c) {
     orc_ray r{{o.x, o.y, o.z}, 0.0f, {d.x, d.y, d.z}, INFINITY};
-    orc_trace_closest1(s.scene, &r, h);
+    uint32_t nv = 0, nt = 0;
+    orc_trace_closest1_counted(s.scene, &r, h, &nv, &nt);
     ++c.ext;
+    c.ext_nodes += nv;
+    c.ext_tris += nt;
     return h->prim != 0xFFFFFFFFu;
 }
 
@@ -449,7 +459,7 @@ extern "C" int orc_render_pt(void* scene, const float* verts, const uint32_t* id
     const uint32_t w = x1 - x0, hgt = y1 - y0;
     if (nthreads <= 0) nthreads = (int)std::thread::hardware_concurrency();
     std::atomic<uint32_t> next_row{0};
-    std::atomic<uint64_t> ext{0}, sh{0};
+    std::atomic<uint64_t> ext{0}, sh{0}, ext_nodes{0}, ext_tris{0}, sh_nodes{0}, sh_tris{0};
     auto worker = [&]() {
         Counters cnt;
         for (;;) {
@@ -482,10 +492,18 @@ extern "C" int orc_render_pt(void* scene, const float* verts, const uint32_t* id
         }
         ext += cnt.ext;
         sh += cnt.shadow;
+        ext_nodes += cnt.ext_nodes;
+        ext_tris += cnt.ext_tris;
+        sh_nodes += cnt.shadow_nodes;
+        sh_tris += cnt.shadow_tris;
     };
     std::vector<std::thread> th_;
     for (int i = 0; i < nthreads; ++i) th_.emplace_back(worker);
     for (auto& t : th_) t.join();
-    if (ray_counts) { ray_counts[0] = ext.load(); ray_counts[1] = sh.load(); }
+    if (ray_counts) {
+        ray_counts[0] = ext.load(); ray_counts[1] = sh.load();
+        ray_counts[2] = ext_nodes.load(); ray_counts[3] = ext_tris.load();
+        ray_counts[4] = sh_nodes.load(); ray_counts[5] = sh_tris.load();
+    }
     return 0;
 }

@@ -1,7 +1,8 @@
 """Batched multi-scene queries and the autotuner (include/illume_gpu.h).
 
 ``BatchPlan`` traces many scenes' ray batches of uneven sizes in one
-persistent launch per BVH width, captured once as a CUDA graph and replayed.
+persistent launch per BVH width (2, 4, 8) and stack depth, captured once as a
+CUDA graph and replayed; ``tuned_plan`` autotunes every scene first.
 ``autotune`` times BVH width, stack depth, schedule and occupancy variant on
 a sample of rays and returns the fastest; ``tuned_accel`` builds the accel
 with that choice applied.  Tuning results are cached in the context and can
@@ -90,6 +91,24 @@ def tuned_accel(ctx: Context, shapes: Sequence, sample, any_hit: bool = False, c
     if choice["width"] != 2:
         apply_launch(acc, choice)
     return acc, choice
+
+
+def tuned_plan(ctx: Context, scenes: Sequence, any_hit: bool = False, sample_rays: int = 1 << 16,
+               cache_path: str | None = None):
+    """Autotunes every scene on a sample of its rays and builds one plan over
+    all of them: scenes: sequence of (shapes, host rays RAY_DTYPE, device rays,
+    device output).  Each accel gets its own width (2, 4 or 8) and launch
+    choices; the plan groups the scenes by width and stack depth, one
+    persistent launch per group.  Returns (plan, accels, choices)."""
+    accs, choices, entries = [], [], []
+    for shapes, host_rays, d_rays, out in scenes:
+        step = max(1, len(host_rays) // sample_rays)
+        sample = host_rays[::step][:sample_rays].copy()
+        acc, choice = tuned_accel(ctx, shapes, sample, any_hit, cache_path)
+        accs.append(acc)
+        choices.append(choice)
+        entries.append((acc, d_rays, out))
+    return BatchPlan(ctx, entries, any_hit), accs, choices
 
 
 def cache_key(shapes, sample, any_hit: bool) -> str:

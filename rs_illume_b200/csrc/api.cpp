@@ -83,6 +83,25 @@ Accel* find_accel(ilm_context* ctx, ilm_accel_id id) {
     return it == ctx->accels.end() ? nullptr : it->second.get();
 }
 
+int32_t validate_host_rays(ilm_context* ctx, const ilm_ray* rays, uint64_t n) {
+    if (!(ctx->flags & ILM_FLAG_VALIDATE_RAYS)) return ILM_OK;
+    for (uint64_t i = 0; i < n; ++i) {
+        const ilm_ray& r = rays[i];
+        bool ok = std::isfinite(r.o[0]) && std::isfinite(r.o[1]) && std::isfinite(r.o[2]) &&
+                  std::isfinite(r.d[0]) && std::isfinite(r.d[1]) && std::isfinite(r.d[2]) &&
+                  !(r.d[0] == 0.0f && r.d[1] == 0.0f && r.d[2] == 0.0f) && !(r.tmax < 0.0f) &&
+                  !std::isnan(r.tmax);
+        if (!ok) {
+            char buf[128];
+            std::snprintf(buf, sizeof buf, "ray %llu is invalid (non-finite, zero direction or tmax < 0)",
+                          (unsigned long long)i);
+            set_error(ctx, buf);
+            return ILM_ERR_INVALID_ARGUMENT;
+        }
+    }
+    return ILM_OK;
+}
+
 }  // namespace ilm
 
 #define ILM_CHECK_CTX(ctx)                                   \
@@ -487,17 +506,15 @@ static int32_t intersect_impl(ilm_context* ctx, ilm_accel_id accel, const ilm_ra
         return ILM_ERR_NOT_FOUND;
     }
     DeviceAccel da = a->view();
-    int persistent = a->schedule >= 0 ? (a->schedule == 0) : !(ctx->flags & ILM_FLAG_GRID_SCHEDULE);
+    LaunchParams lp = accel_launch(ctx, a);
+    int persistent = lp.persistent;
     // By default a batch that one wave of the one-thread-per-ray kernel holds
     // runs that kernel: every ray is resident at once, so the persistent
     // schedule's claiming buys nothing (measured: 440 against 361 Mrays/s for
     // 65,536 camera rays).
     if (a->schedule < 0 && persistent && da.width != 2 && da.width != kLayoutKdTree &&
-        n <= wide_grid_wave(da.width, a->stack_depth > 0 ? a->stack_depth : ctx->stack_depth))
-        persistent = 0;
-    const int high_occ = a->high_occupancy >= 0 ? a->high_occupancy : (ctx->flags & ILM_FLAG_HIGH_OCCUPANCY) != 0;
-    LaunchParams lp{a->stack_depth > 0 ? a->stack_depth : ctx->stack_depth, ctx->block_size, ctx->max_iter,
-                    persistent, nullptr, high_occ ? 8 : 0};
+        n <= wide_grid_wave(da.width, lp.stack_depth))
+        persistent = lp.persistent = 0;
     uint32_t* err = static_cast<uint32_t*>(ctx->err_word.ptr);
     cudaStream_t user = stream ? static_cast<cudaStream_t>(stream) : ctx->stream;
     PtrKind kr = classify(rays), ko = classify(out);
@@ -514,22 +531,7 @@ static int32_t intersect_impl(ilm_context* ctx, ilm_accel_id accel, const ilm_ra
         ILM_CUDA(ctx, launch_trace(da, rays, n, hits, occ, err, lp, user), "trace launch");
         return ILM_OK;
     }
-    if (ctx->flags & ILM_FLAG_VALIDATE_RAYS) {
-        for (uint64_t i = 0; i < n; ++i) {
-            const ilm_ray& r = rays[i];
-            bool ok = std::isfinite(r.o[0]) && std::isfinite(r.o[1]) && std::isfinite(r.o[2]) &&
-                      std::isfinite(r.d[0]) && std::isfinite(r.d[1]) && std::isfinite(r.d[2]) &&
-                      !(r.d[0] == 0.0f && r.d[1] == 0.0f && r.d[2] == 0.0f) && !(r.tmax < 0.0f) &&
-                      !std::isnan(r.tmax);
-            if (!ok) {
-                char buf[128];
-                std::snprintf(buf, sizeof buf, "ray %llu is invalid (non-finite, zero direction or tmax < 0)",
-                              (unsigned long long)i);
-                set_error(ctx, buf);
-                return ILM_ERR_INVALID_ARGUMENT;
-            }
-        }
-    }
+    if (int32_t rc = validate_host_rays(ctx, rays, n)) return rc;
     // Host buffers: chunks staged through a ring of device slots.  Copy-in and
     // copy-out have a stream each, so the host link carries rays in and
     // results out at once; each slot traces on its own stream, so traces of

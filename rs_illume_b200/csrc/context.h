@@ -144,6 +144,20 @@ void set_error(ilm_context* ctx, const std::string& msg);
 int32_t cuda_fail(ilm_context* ctx, cudaError_t e, const char* what);
 PtrKind classify(const void* p);
 Accel* find_accel(ilm_context* ctx, ilm_accel_id id);
+
+// Launch choices of a query on accel `a`: the accel's own (ilm_accel_set_launch,
+// ilm_autotune) where it has them, else the context's.  The work counter is
+// left null for the caller to supply.
+inline LaunchParams accel_launch(const ilm_context* ctx, const Accel* a) {
+    const int persistent = a->schedule >= 0 ? (a->schedule == 0) : !(ctx->flags & ILM_FLAG_GRID_SCHEDULE);
+    const int high_occ = a->high_occupancy >= 0 ? a->high_occupancy : (ctx->flags & ILM_FLAG_HIGH_OCCUPANCY) != 0;
+    return LaunchParams{a->stack_depth > 0 ? a->stack_depth : ctx->stack_depth, ctx->block_size, ctx->max_iter,
+                        persistent, nullptr, high_occ ? 8 : 0};
+}
+
+// ILM_FLAG_VALIDATE_RAYS on host rays: ILM_OK, or ILM_ERR_INVALID_ARGUMENT with
+// the first bad ray named in the context's error string.
+int32_t validate_host_rays(ilm_context* ctx, const ilm_ray* rays, uint64_t n);
 // True when this library's kernels have an image for the current device.
 bool kernels_loadable(cudaFuncAttributes* attr);
 }  // namespace ilm

@@ -9,10 +9,14 @@
 // buffers need staging space; this entry point instead uses one fixed
 // scratch array that the library holds on every GPU that loads it.
 //
-// The kernel is the persistent closest-hit traversal of trace_wide.cu (or the
-// binary traversal for width-2 accels).  Its scratch -- the work counter, the
-// error word and, for host buffers, the staging copies of rays and hits -- lives
-// in g_noalloc_scratch below.
+// The kernel is the closest-hit traversal of the accel's layout, with the
+// launch choices ilm_intersect_closest makes for the accel (its own stack
+// depth, schedule and occupancy, else the context's).  Its scratch -- the
+// persistent schedule's work counter and, for host buffers, the staging
+// copies of rays and hits -- lives in g_noalloc_scratch below.  Rays that hit
+// a traversal limit set the context's error word, which the context
+// allocated when it was created, so ilm_device_errors reports them for both
+// entry points.
 #include <cuda_runtime.h>
 
 #include <cstdio>
@@ -26,12 +30,14 @@ namespace ilm {
 namespace {
 
 constexpr uint64_t kMaxRays = ILM_NOALLOC_MAX_RAYS;
-constexpr size_t kHeader = 256;   // work counter (8 B) + error word (4 B), padded
+constexpr size_t kHeader = 256;   // work counter (8 B), padded
 constexpr size_t kScratchBytes = kHeader + kMaxRays * (sizeof(ilm_ray) + sizeof(ilm_hit));
 
 // The scratch: 3 MiB + 256 B on every GPU that loads the library, until exit.
 // In host code this name is only a handle for cudaGetSymbolAddress, never a
-// device address.
+// device address.  The address is resolved once per device and cached for
+// the life of the process, so the device must not be reset (cudaDeviceReset)
+// while the library is loaded.
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 
 constexpr int kMaxDevices = 64;
@@ -85,23 +91,26 @@ extern "C" int32_t ilm_intersect_closest_noalloc(ilm_context* ctx, ilm_accel_id 
     e = scratch_address(ctx->device, &scratch);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaGetSymbolAddress(noalloc scratch)");
     unsigned long long* counter = reinterpret_cast<unsigned long long*>(scratch);
-    uint32_t* err = reinterpret_cast<uint32_t*>(scratch + 8);
     ilm_ray* d_rays = reinterpret_cast<ilm_ray*>(scratch + kHeader);
     ilm_hit* d_hits = reinterpret_cast<ilm_hit*>(scratch + kHeader + kMaxRays * sizeof(ilm_ray));
+    uint32_t* err = static_cast<uint32_t*>(ctx->err_word.ptr);
 
     PtrKind kr = classify(rays), kh = classify(hits);
     if (kr != kh) {
         set_error(ctx, "ilm_intersect_closest_noalloc: rays and hits must both be device or both host memory");
         return ILM_ERR_INVALID_ARGUMENT;
     }
+    if (kr == PtrKind::kHost) {
+        if (int32_t rc = validate_host_rays(ctx, rays, n)) return rc;
+    }
     cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : ctx->stream;
-    const int persistent = (ctx->flags & ILM_FLAG_GRID_SCHEDULE) ? 0 : 1;
-    LaunchParams lp{ctx->stack_depth, ctx->block_size, ctx->max_iter, persistent, counter,
-                    (ctx->flags & ILM_FLAG_HIGH_OCCUPANCY) ? 8 : 0};
+    LaunchParams lp = accel_launch(ctx, a);
+    lp.counter = counter;
     DeviceAccel da = a->view();
-    // The array keeps the previous call's contents: the counter and the error
-    // word must start at zero.
-    e = cudaMemsetAsync(scratch, 0, 16, s);
+    // The array keeps the previous call's contents: the work counter must
+    // start at zero (the persistent launch zeroes it too; this keeps the
+    // array's state independent of the schedule).
+    e = cudaMemsetAsync(counter, 0, sizeof(unsigned long long), s);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaMemsetAsync(noalloc scratch)");
     if (kr == PtrKind::kDevice) {
         e = launch_trace(da, rays, n, hits, nullptr, err, lp, s);
@@ -114,14 +123,14 @@ extern "C" int32_t ilm_intersect_closest_noalloc(ilm_context* ctx, ilm_accel_id 
     if (e != cudaSuccess) return cuda_fail(ctx, e, "trace launch");
     e = cudaMemcpyAsync(hits, d_hits, n * sizeof(ilm_hit), cudaMemcpyDeviceToHost, s);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaMemcpyAsync(hits)");
-    uint32_t flags = 0;
-    e = cudaMemcpyAsync(&flags, err, sizeof flags, cudaMemcpyDeviceToHost, s);
-    if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaMemcpyAsync(error word)");
     e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaStreamSynchronize");
-    if (flags) {
-        set_error(ctx, "ilm_intersect_closest_noalloc: traversal limit reached; affected records are marked");
-        return ILM_ERR_TRAVERSAL_LIMIT;
-    }
+    // This call's own limit hits are the records it marked (the error word
+    // also holds earlier calls' flags until ilm_device_errors resets it).
+    for (uint64_t i = 0; i < n; ++i)
+        if (hits[i].prim == kHitTraversalError) {
+            set_error(ctx, "ilm_intersect_closest_noalloc: traversal limit reached; affected records are marked");
+            return ILM_ERR_TRAVERSAL_LIMIT;
+        }
     return ILM_OK;
 }

@@ -1,6 +1,6 @@
 // Neural radiance cache: input encoding, a 5 x 64 ReLU MLP on the BF16
-// tensor cores (tcgen05.mma, FP32 accumulators in TMEM; the weight gradients
-// on mma.sync), relative-L2 loss and Adam.
+// tensor cores (tcgen05.mma, FP32 accumulators in TMEM), relative-L2 loss
+// and Adam.
 // No counterpart in the reference (a learned component added on top of the
 // path tracer); the method follows published neural radiance caching:
 //   inputs: position (12-frequency sin/cos per axis, 72), outgoing direction
@@ -18,12 +18,11 @@
 //                  also stores the encoding and the bf16 activations
 //   k_mlp_bwd_tc   loss gradient, then back through the layers the same way
 //                  (transposed weights), storing dOut
-//   k_wgrad_all    dW_l = dOut_l^T * in_l for all six layers: each CTA takes
-//                  64-row chunks (16-byte cp.async into padded shared tiles),
-//                  ldmatrix.trans gives both operands' fragments, warps own
-//                  output tiles; one FP32 partial sum per CTA, no atomics.
-//                  A split-K over the batch rows with 64 x 64 outputs: about
-//                  1 GFLOP per step, bound by latency, not by the MMAs
+//   k_wgrad_tc     dW_l = dOut_l^T * in_l for all six layers on tcgen05
+//                  (M = outputs, N = inputs, K = batch rows, both operands
+//                  MN-major as the rows are stored, staged by 16-byte
+//                  cp.async into two buffers); split-K over the rows, one FP32
+//                  partial per CTA, no atomics
 //   k_reduce_adam  sums the CTA partials, Adam on the FP32 master weights,
 //                  bf16 weight packs and the inference moving average
 //   k_nrc_encode   the encoding alone (for inspection)
@@ -69,8 +68,7 @@ __host__ __device__ constexpr int tcb_index(int l, int o, int i) {
 }
 constexpr int kTcbElems = 4 * kHid * kHid + kHid * kOut;   // 17408
 constexpr float kLossEps = 0.01f;
-constexpr int kMaxPartials = 148;   // CTAs of k_wgrad_all (one FP32 partial gradient each)
-constexpr int kChunk = 64;          // rows per k_wgrad_all staging step
+constexpr int kMaxPartials = 148;   // CTAs of k_wgrad_tc (one FP32 partial gradient each)
 
 struct Enc {   // position normalisation: q = (p - origin) * scale
     float x0, y0, z0, sx, sy, sz;
@@ -96,22 +94,6 @@ __device__ __forceinline__ uint32_t rows_of(const NrcCount& c) {
     }
     if (c.batches > 1) n = n > c.batch ? (n - c.batch + c.batches - 1) / c.batches : 0u;
     return n;
-}
-
-__device__ __forceinline__ void mma(float (&d)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
-    asm volatile(
-        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
-        "{%0,%1,%2,%3};\n"
-        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
-        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
-}
-
-// Four transposed 8x8 bf16 tiles; lane l addresses row (l & 7) of tile l >> 3.
-__device__ __forceinline__ void ldsm_x4_t(uint32_t (&r)[4], const __nv_bfloat16* p) {
-    uint32_t a = (uint32_t)__cvta_generic_to_shared(p);
-    asm volatile("ldmatrix.sync.aligned.m8n8.x4.trans.shared.b16 {%0,%1,%2,%3}, [%4];\n"
-                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
-                 : "r"(a));
 }
 
 // 16-byte global -> shared copy; zero-filled when !ok.
@@ -233,6 +215,7 @@ constexpr int kTcWBytes = kParams * 2;                         // 61,440
 constexpr int kTcSmem = kTcWBytes + kTcGroups * kTcABytes;     // 176,128 at 4 warpgroups
 constexpr uint32_t kErrMlpTimeout = 4u;
 constexpr uint32_t kTcWaitCap = 1u << 22;   // try_wait polls before a wait gives up
+constexpr uint32_t kTcDrainCap = 1u << 26;  // further polls for a batch whose wait gave up
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -374,12 +357,23 @@ __device__ __forceinline__ void tc_setup(uint64_t* mbar, int* fail, uint32_t* tm
     tc_fence_after();
 }
 
-// Reports a timed-out wait and frees the TMEM (every warpgroup has stopped
-// issuing by then: its last batch was committed and waited for, or it gave up
-// waiting, and the CTA barrier below follows every warpgroup's exit).
-__device__ __forceinline__ void tc_teardown(const int* fail, uint32_t tmem_base, uint32_t* err) {
+// Reports a timed-out wait and frees the TMEM.  Every warpgroup has stopped
+// issuing by then: its last batch was committed and waited for, or its wait
+// gave up.  A warpgroup whose wait gave up first drains that batch: its issuing
+// thread waits again, up to kTcDrainCap more polls, on the same mbarrier phase
+// (the parity before mma_batch's flip, phase ^ 1), so tcgen05.dealloc does not
+// free columns an MMA may still write.  If the drain runs out too, the columns
+// are freed all the same -- a CTA that kept them would leave the tcgen05.alloc
+// of later CTAs on its SM waiting -- and the error word marks the launch's
+// results as invalid.  The CTA barrier below follows every warpgroup's exit.
+__device__ __forceinline__ void tc_teardown(const int* fail, uint32_t tmem_base, uint32_t* err, uint32_t mbar,
+                                            uint32_t phase) {
     const int g = threadIdx.x >> 7;
-    if ((threadIdx.x & 127) == 0 && fail[g]) atomicOr(err, kErrMlpTimeout);
+    if ((threadIdx.x & 127) == 0 && fail[g]) {
+        uint32_t it = 0;
+        while (!mbar_try_wait(mbar, phase ^ 1u) && ++it < kTcDrainCap) {}
+        atomicOr(err, kErrMlpTimeout);
+    }
     tc_fence_before();
     __syncthreads();
     if ((threadIdx.x >> 5) == 0) {
@@ -448,7 +442,7 @@ __global__ void __launch_bounds__(128 * kTcGroups, 1) k_mlp_fwd_tc(const float* 
             out[3 * (size_t)row + 2] = o[2];
         }
     }
-    tc_teardown(fail, tmem_base, err);
+    tc_teardown(fail, tmem_base, err, mb, phase);
 }
 
 // ---------------------------------------------------------------- backward on tcgen05
@@ -552,95 +546,182 @@ __global__ void __launch_bounds__(128 * kTcGroups, 1) k_mlp_bwd_tc(const float* 
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) loss += __shfl_xor_sync(0xFFFFFFFFu, loss, o);
     if ((threadIdx.x & 31) == 0 && loss != 0.0f) atomicAdd(loss_sum, loss);
-    tc_teardown(fail, tmem_base, err);
+    tc_teardown(fail, tmem_base, err, mb, phase);
 }
 
-// ---------------------------------------------------------------- weight gradient
-// Partial dW[o][i] = sum over this CTA's chunks of dOut[r][o] * in[r][i].
-// A (16 x 16: o x r) and B (16 x 8: r x i) fragments come from the row-major
-// [r][o] / [r][i] shared tiles through ldmatrix.trans; each warp owns
-// (16-row o tile, 16-column i pair) items.
-template <int OUT, int IN>
-__device__ __forceinline__ void wgrad_layer(const __nv_bfloat16* __restrict__ dout,
-                                            const __nv_bfloat16* __restrict__ in, uint32_t n, __nv_bfloat16* sD,
-                                            __nv_bfloat16* sI, float* __restrict__ part) {
-    constexpr int SD = OUT + 8, SI = IN + 8;
-    constexpr int kIP = IN / 16, kItems = (OUT / 16) * kIP, kPer = (kItems + 7) / 8;
-    constexpr int kVecD = OUT / 8, kVecI = IN / 8;   // 16-byte vectors per row
-    const unsigned lane = threadIdx.x & 31u, warp = threadIdx.x >> 5, g = lane >> 2, t = lane & 3u;
-    const unsigned li = lane >> 3, lj = lane & 7u;
-    float acc[kPer][2][4];
-#pragma unroll
-    for (int k = 0; k < kPer; ++k)
-#pragma unroll
-        for (int h = 0; h < 2; ++h)
-#pragma unroll
-            for (int q = 0; q < 4; ++q) acc[k][h][q] = 0.0f;
-    const uint32_t chunks = (n + kChunk - 1) / kChunk;
-    for (uint32_t ch = blockIdx.x; ch < chunks; ch += gridDim.x) {
-        const uint32_t base = ch * kChunk;
-        __syncthreads();   // the previous chunk's fragments have been read
-        for (int e = threadIdx.x; e < kChunk * kVecD; e += blockDim.x) {
-            int r = e / kVecD, c = e - r * kVecD;
-            bool ok = base + r < n;
-            cp_async16(sD + r * SD + c * 8, dout + (size_t)(ok ? base + r : 0) * OUT + c * 8, ok);
-        }
-        for (int e = threadIdx.x; e < kChunk * kVecI; e += blockDim.x) {
-            int r = e / kVecI, c = e - r * kVecI;
-            bool ok = base + r < n;
-            cp_async16(sI + r * SI + c * 8, in + (size_t)(ok ? base + r : 0) * IN + c * 8, ok);
-        }
-        cp_async_wait_all();
-        __syncthreads();
-#pragma unroll
-        for (int ks = 0; ks < kChunk / 16; ++ks)
-#pragma unroll
-            for (int k = 0; k < kPer; ++k) {
-                const int item = warp + 8 * k;
-                if (item < kItems) {
-                    const int mt = item / kIP, np = item % kIP;
-                    uint32_t a[4], b[4];
-                    ldsm_x4_t(a, sD + (ks * 16 + lj + ((li & 2) ? 8 : 0)) * SD + mt * 16 + ((li & 1) ? 8 : 0));
-                    ldsm_x4_t(b, sI + (ks * 16 + lj + ((li & 1) ? 8 : 0)) * SI + np * 16 + ((li & 2) ? 8 : 0));
-                    mma(acc[k][0], a, b[0], b[1]);
-                    mma(acc[k][1], a, b[2], b[3]);
-                }
-            }
+// ---------------------------------------------------------------- weight gradient on tcgen05
+// k_wgrad_tc: dW_l[o][i] = sum over rows r of dOut_l[r][o] * in_l[r][i], all six
+// layers, split over the batch rows: CTA c takes rows [c * R, (c + 1) * R) and
+// writes one FP32 partial of all 30,720 weights (k_reduce_adam sums them).
+// One warpgroup per CTA; per layer D = A * B with M = o, N = i (208 or 64),
+// K = rows, FP32 D in TMEM (256 columns).
+// Both operands are MN-major without swizzle, which is how the rows are stored
+// (features contiguous): a core matrix is 8 consecutive rows (K) x 8 features
+// (MN), 16 contiguous bytes per row, so staging is one 16-byte cp.async per
+// (row, 8 features), no transpose.
+//   A (dOut_l^T): core matrix (o/8, r/8) at (r/8) * LBO_A + (o/8) * 128,
+//                 LBO_A = O * 16 (an 8-row group of all O outputs), SBO = 128;
+//   B (in_l):     core matrix (i/8, r/8) at (r/8) * LBO_B + (i/8) * 128,
+//                 LBO_B = I * 16, SBO = 128.
+// The MMA has M = 128 and the layer O = 64 or 16 real rows: the descriptor's
+// MN groups past O/8 read the bytes that follow (the next 8-row groups, and up
+// to kWgPad bytes past the tile, reserved), and the D rows they give are never
+// read.  Rows are staged kWgRows at a time into two buffers: one buffer's MMAs
+// run while the other fills.  Waits are bounded as in the forward kernel.
+constexpr int kWgRows = 64;                                   // rows per staging step (4 MMAs of K = 16)
+constexpr int kWgPad = 2048;                                  // bytes past an A tile its descriptor reads
+constexpr int kWgABytes = kWgRows / 8 * kHid * 16 + kWgPad;   // 10,240
+constexpr int kWgBBytes = kWgRows / 8 * kIn * 16;             // 26,624
+constexpr int kWgBuf = kWgABytes + kWgBBytes;                 // 36,864
+constexpr int kWgSmem = 2 * kWgBuf;                           // 73,728
+constexpr int kWgMinRows = 256;                               // rows per CTA, at least
+
+__device__ __forceinline__ uint32_t idesc_bf16_mn(int m, int n) {
+    return idesc_bf16(m, n) | (1u << 15) | (1u << 16);        // A and B MN-major
+}
+
+// Layer l's operand tiles for rows r0 .. r0 + kWgRows - 1 (zeros past n).
+__device__ __forceinline__ void wg_stage(uint8_t* buf, int l, uint32_t r0, uint32_t n, uint32_t ld,
+                                         const __nv_bfloat16* __restrict__ enc, const __nv_bfloat16* __restrict__ acts,
+                                         const __nv_bfloat16* __restrict__ douts) {
+    const int O = out_dim(l), I = in_dim(l);
+    const __nv_bfloat16* dsrc = douts + (size_t)l * ld * kHid;
+    const __nv_bfloat16* isrc = l == 0 ? enc : acts + (size_t)(l - 1) * ld * kHid;
+    const int oc = O / 8, ic = I / 8;
+    uint8_t* a = buf;
+    uint8_t* b = buf + kWgABytes;
+    for (int e = threadIdx.x; e < kWgRows * (oc + ic); e += blockDim.x) {
+        const int r = e / (oc + ic), c = e - r * (oc + ic);
+        const uint32_t row = r0 + (uint32_t)r;
+        const bool ok = row < n;
+        const size_t src_row = ok ? row : 0;
+        if (c < oc)
+            cp_async16(a + (r >> 3) * (O * 16) + c * 128 + (r & 7) * 16, dsrc + src_row * O + c * 8, ok);
+        else
+            cp_async16(b + (r >> 3) * (I * 16) + (c - oc) * 128 + (r & 7) * 16, isrc + src_row * I + (c - oc) * 8, ok);
     }
-#pragma unroll
-    for (int k = 0; k < kPer; ++k) {
-        const int item = warp + 8 * k;
-        if (item < kItems) {
-            const int mt = item / kIP, np = item % kIP;
-#pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                const int o0 = mt * 16 + g, i0 = (2 * np + h) * 8 + 2 * t;
-                *reinterpret_cast<float2*>(part + o0 * IN + i0) = make_float2(acc[k][h][0], acc[k][h][1]);
-                *reinterpret_cast<float2*>(part + (o0 + 8) * IN + i0) = make_float2(acc[k][h][2], acc[k][h][3]);
-            }
-        }
-    }
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+
+// Bounded wait of the issuing thread on an mbarrier phase; false on a timeout.
+__device__ __forceinline__ bool wg_wait(uint32_t mbar, uint32_t parity) {
+    uint32_t it = 0;
+    while (!mbar_try_wait(mbar, parity) && ++it < kTcWaitCap) {}
+    return it < kTcWaitCap;
 }
 
 // Also advances the step counters (read by k_reduce_adam, which follows).
-__global__ void __launch_bounds__(256) k_wgrad_all(NrcCount cnt, uint32_t ld, const __nv_bfloat16* __restrict__ enc,
-                                                   const __nv_bfloat16* __restrict__ acts,
-                                                   const __nv_bfloat16* __restrict__ douts,
-                                                   float* __restrict__ partial, StepState* st, int do_step) {
-    __shared__ __align__(16) __nv_bfloat16 sD[kChunk * (kHid + 8)];
-    __shared__ __align__(16) __nv_bfloat16 sI[kChunk * (kIn + 8)];
+__global__ void __launch_bounds__(128, 1) k_wgrad_tc(NrcCount cnt, uint32_t ld, uint32_t rows_per_cta,
+                                                     const __nv_bfloat16* __restrict__ enc,
+                                                     const __nv_bfloat16* __restrict__ acts,
+                                                     const __nv_bfloat16* __restrict__ douts,
+                                                     float* __restrict__ partial, StepState* st, int do_step,
+                                                     uint32_t* err) {
+    extern __shared__ __align__(1024) uint8_t wg_smem[];
+    __shared__ __align__(8) uint64_t mbar[2];
+    __shared__ int fail[1];
+    __shared__ uint32_t tmem_base;
     const uint32_t n = rows_of(cnt);
     if (do_step && n > 0 && blockIdx.x == 0 && threadIdx.x == 0) {   // an empty batch takes no step
         st->step += 1;
         st->ema_steps += 1;
     }
+    const int t = threadIdx.x, warp = t >> 5;
+    if (t < 2) mbar_init(smem_u32(&mbar[t]));
+    if (t == 0) fail[0] = 0;
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base)),
+                     "r"(256u));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem_d = tmem_base;
+    const uint32_t row0 = blockIdx.x * rows_per_cta;
+    const int per_layer = (int)(rows_per_cta / kWgRows);
+    const int steps = kLayers * per_layer;
     float* part = partial + (size_t)blockIdx.x * kParams;
-    const size_t layer = (size_t)ld * kHid;
-    wgrad_layer<kHid, kIn>(douts, enc, n, sD, sI, part + param_off(0));
+    bool ok = true;
+    // the issuing thread's last commit (barrier and phase parity): a later
+    // commit covers every earlier MMA, so a drain waits on this one
+    uint32_t last_bar = 0, last_parity = 0;
+    wg_stage(wg_smem, 0, row0, n, ld, enc, acts, douts);
+    for (int s = 0; s < steps && ok; ++s) {
+        const int l = s / per_layer, j = s - l * per_layer;
+        const int b = s & 1;
+        uint8_t* buf = wg_smem + b * kWgBuf;
+        asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+        fence_proxy_async();        // this thread's copies, visible to the tensor core
+        tc_fence_before();
+        __syncthreads();
+        if (t == 0) {
+            tc_fence_after();
+            const int O = out_dim(l), I = in_dim(l);
+            const uint32_t a0 = smem_u32(buf), b0 = smem_u32(buf + kWgABytes);
+            const uint32_t idesc = idesc_bf16_mn(128, I);
 #pragma unroll 1
-    for (int l = 1; l <= 4; ++l)
-        wgrad_layer<kHid, kHid>(douts + l * layer, acts + (l - 1) * layer, n, sD, sI, part + param_off(l));
-    wgrad_layer<kOut, kHid>(douts + 5 * layer, acts + 4 * layer, n, sD, sI, part + param_off(5));
+            for (int ks = 0; ks < kWgRows / 16; ++ks) {
+                const uint64_t da = umma_desc(a0 + (uint32_t)(ks * 2 * O * 16), (uint32_t)(O * 16), 128u);
+                const uint64_t db = umma_desc(b0 + (uint32_t)(ks * 2 * I * 16), (uint32_t)(I * 16), 128u);
+                umma(tmem_d, da, db, idesc, (j > 0 || ks > 0) ? 1u : 0u);
+            }
+            umma_commit(smem_u32(&mbar[b]));
+            last_bar = smem_u32(&mbar[b]);
+            last_parity = (uint32_t)(s >> 1) & 1u;
+        }
+        // refill the other buffer with step s + 1 once step s - 1's MMAs (its
+        // last reader) are done
+        if (s + 1 < steps) {
+            if (s >= 1) {
+                if (t == 0 && !wg_wait(smem_u32(&mbar[b ^ 1]), ((s - 1) >> 1) & 1)) fail[0] = 1;
+                __syncthreads();
+                if (fail[0]) { ok = false; break; }
+            }
+            const int l1 = (s + 1) / per_layer, j1 = (s + 1) - l1 * per_layer;
+            wg_stage(wg_smem + (b ^ 1) * kWgBuf, l1, row0 + (uint32_t)(j1 * kWgRows), n, ld, enc, acts, douts);
+        }
+        if (j == per_layer - 1) {
+            // layer l complete: D rows o < O to this CTA's partial
+            if (t == 0 && !wg_wait(smem_u32(&mbar[b]), (s >> 1) & 1)) fail[0] = 1;
+            __syncthreads();
+            if (fail[0]) { ok = false; break; }
+            tc_fence_after();
+            const int O = out_dim(l), I = in_dim(l);
+            if (warp * 32 < O) {
+                float* dst = part + param_off(l) + (size_t)(warp * 32 + (t & 31)) * I;
+                const bool real = warp * 32 + (t & 31) < O;
+                for (int c0 = 0; c0 < I; c0 += 16) {
+                    float v[16];
+                    tmem_ld16(tmem_d + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
+                    if (real) {
+                        float4* d4 = reinterpret_cast<float4*>(dst + c0);
+                        d4[0] = make_float4(v[0], v[1], v[2], v[3]);
+                        d4[1] = make_float4(v[4], v[5], v[6], v[7]);
+                        d4[2] = make_float4(v[8], v[9], v[10], v[11]);
+                        d4[3] = make_float4(v[12], v[13], v[14], v[15]);
+                    }
+                }
+            }
+            tc_fence_before();      // the reads above, before the next layer's MMAs
+            __syncthreads();
+        }
+    }
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+    // a wait that gave up: drain the last commit before the TMEM is freed
+    // (as tc_teardown does), then report
+    if (t == 0 && fail[0]) {
+        uint32_t it = 0;
+        while (!mbar_try_wait(last_bar, last_parity) && ++it < kTcDrainCap) {}
+        atomicOr(err, kErrMlpTimeout);
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base), "r"(256u));
+    }
 }
 
 // ---------------------------------------------------------------- optimiser
@@ -723,7 +804,7 @@ struct ilm_nrc {
     DeviceBuffer state;                          // StepState
     DeviceBuffer w, m, v, grad, wtc, wtcb;       // params and their training packs
     DeviceBuffer ema, winf;                      // moving average and its inference pack
-    DeviceBuffer partial;                        // k_wgrad_all partial sums
+    DeviceBuffer partial;                        // k_wgrad_tc partial sums
     DeviceBuffer err;                            // device error word (kErrMlpTimeout)
     DeviceBuffer raw, enc, out, target, acts, douts, loss;
     cudaStream_t stream = nullptr;
@@ -811,10 +892,15 @@ cudaError_t train_rows(ilm_nrc* h, const float* raw, const float* target, NrcCou
         pred, target, cnt, cap, acts, static_cast<const __nv_bfloat16*>(h->wtcb.ptr), douts,
         static_cast<float*>(h->loss.ptr), static_cast<uint32_t*>(h->err.ptr));
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    int n_part = (int)std::min<uint32_t>(kMaxPartials, std::max<uint32_t>(1, (cap + kChunk - 1) / kChunk));
+    // split-K over the rows: kWgMinRows or more per CTA (a multiple of
+    // kWgRows), at most kMaxPartials CTAs
+    uint32_t per_cta = (cap + kMaxPartials - 1) / kMaxPartials;
+    per_cta = std::max<uint32_t>(kWgMinRows, (per_cta + kWgRows - 1) / kWgRows * kWgRows);
+    const int n_part = (int)std::max<uint32_t>(1, (cap + per_cta - 1) / per_cta);
     StepState* st = static_cast<StepState*>(h->state.ptr);
-    k_wgrad_all<<<n_part, 256, 0, s>>>(cnt, cap, static_cast<const __nv_bfloat16*>(h->enc.ptr), acts, douts,
-                                       static_cast<float*>(h->partial.ptr), st, do_step);
+    k_wgrad_tc<<<n_part, 128, kWgSmem, s>>>(cnt, cap, per_cta, static_cast<const __nv_bfloat16*>(h->enc.ptr), acts,
+                                            douts, static_cast<float*>(h->partial.ptr), st, do_step,
+                                            static_cast<uint32_t*>(h->err.ptr));
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     AdamArgs ar{h->cfg.lr, h->cfg.beta1, h->cfg.beta2, h->cfg.eps,
                 h->cfg.ema > 0.0f && h->cfg.ema < 1.0f ? h->cfg.ema : 0.0f};
@@ -894,6 +980,7 @@ int32_t ilm_nrc_create(ilm_context* ctx, const ilm_nrc_config* cfg, ilm_nrc** ou
     cudaFuncSetAttribute(k_mlp_fwd_tc<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem);
     cudaFuncSetAttribute(k_mlp_fwd_tc<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem);
     cudaFuncSetAttribute(k_mlp_bwd_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcbSmem);
+    cudaFuncSetAttribute(k_wgrad_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kWgSmem);
     if ((e = pack(h.get(), h->stream)) != cudaSuccess) return cuda_fail(ctx, e, "nrc pack");
     if ((e = cudaStreamSynchronize(h->stream)) != cudaSuccess) return cuda_fail(ctx, e, "nrc");
     *out = h.release();

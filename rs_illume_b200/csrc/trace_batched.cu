@@ -1,5 +1,5 @@
 // Batched ray queries: many scenes, each with its own ray batch of any size,
-// in one persistent launch per BVH width.
+// in one persistent launch per BVH width (2, 4 or 8).
 //
 // The batches are concatenated into one index space.  Warps claim rays 64 at a
 // time from a device counter as in the single-scene persistent kernel; each
@@ -148,17 +148,17 @@ cudaError_t launch_batched(const BatchTable& t, bool any, bool analytic, cudaStr
 
 using namespace ilm;
 
-// A captured batch: one sub-table per BVH width present.
+// A captured batch: one sub-table per (BVH width, stack depth) present.
 struct ilm_batch_plan {
     struct Group {
         int width;
+        bool deep = true;        // 64-entry stack (else 32); binary nodes always 64
         bool analytic = false;   // some accel holds quadric or curve records
         DeviceBuffer table, counter;
         BatchTable t;
     };
     std::vector<std::unique_ptr<Group>> groups;
     bool any = false;
-    int stack_depth = 64;
     cudaStream_t capture = nullptr;
     cudaGraphExec_t exec = nullptr;
     uint64_t total_rays = 0;
@@ -173,12 +173,14 @@ namespace {
 cudaError_t launch_plan(const ilm_batch_plan& p, cudaStream_t s) {
     for (const auto& g : p.groups) {
         cudaError_t e;
-        bool deep = p.stack_depth > 32;
+        const bool deep = g->deep;
         const bool an = g->analytic;
         if (g->width == 8)
             e = deep ? launch_batched<8, 64>(g->t, p.any, an, s) : launch_batched<8, 32>(g->t, p.any, an, s);
-        else
+        else if (g->width == 4)
             e = deep ? launch_batched<4, 64>(g->t, p.any, an, s) : launch_batched<4, 32>(g->t, p.any, an, s);
+        else   // binary nodes: the reference's 64-entry stack
+            e = launch_batched<2, 64>(g->t, p.any, an, s);
         if (e != cudaSuccess) return e;
     }
     return cudaSuccess;
@@ -188,15 +190,17 @@ int32_t build_plan(ilm_context* ctx, const ilm_batch_desc* batches, uint32_t n, 
                    std::unique_ptr<ilm_batch_plan>& out) {
     auto plan = std::make_unique<ilm_batch_plan>();
     plan->any = any_hit != 0;
-    plan->stack_depth = ctx->stack_depth;
-    std::vector<BatchEntry> per_width[2];   // [0] width 4, [1] width 8
+    // sub-tables by width (2, 4, 8) and stack depth (32, 64): an accel's own
+    // stack depth (ilm_accel_set_launch, ilm_autotune), else the context's
+    const int widths[3] = {2, 4, 8};
+    std::vector<BatchEntry> per_width[3][2];
     for (uint32_t i = 0; i < n; ++i) {
         const ilm_batch_desc& b = batches[i];
         Accel* a = find_accel(ctx, b.accel);
         if (!a) { set_error(ctx, "batched: unknown accel id"); return ILM_ERR_NOT_FOUND; }
         int w = a->host.width;
-        if (w != 4 && w != 8) {
-            set_error(ctx, "batched: accels must have width 4 or 8");
+        if (w != 2 && w != 4 && w != 8) {
+            set_error(ctx, "batched: accels must be BVHs of width 2, 4 or 8 (not kd-trees)");
             return ILM_ERR_INVALID_ARGUMENT;
         }
         void* out_ptr = plan->any ? (void*)b.occluded : (void*)b.hits;
@@ -219,15 +223,17 @@ int32_t build_plan(ilm_context* ctx, const ilm_batch_desc* batches, uint32_t n, 
         e.n_nodes = da.n_nodes;
         e.pad = 0;
         for (int k = 0; k < 6; ++k) e.bound[k] = da.bound[k];
-        per_width[w == 8].push_back(e);
+        const int depth = a->stack_depth > 0 ? a->stack_depth : ctx->stack_depth;
+        per_width[w == 2 ? 0 : (w == 4 ? 1 : 2)][w == 2 || depth > 32].push_back(e);
     }
-    for (int k = 0; k < 2; ++k) {
-        auto& v = per_width[k];
+    for (int k = 0; k < 6; ++k) {
+        auto& v = per_width[k / 2][k % 2];
         if (v.empty()) continue;
         unsigned long long first = 0;
         for (auto& e : v) { e.first = first; first += e.n; }
         auto g = std::make_unique<ilm_batch_plan::Group>();
-        g->width = k ? 8 : 4;
+        g->width = widths[k / 2];
+        g->deep = (k % 2) != 0;
         for (const auto& e : v) g->analytic = g->analytic || e.spheres != nullptr;
         cudaError_t ce = g->table.reserve(v.size() * sizeof(BatchEntry));
         if (ce == cudaSuccess) ce = g->counter.reserve(sizeof(unsigned long long));

@@ -57,3 +57,21 @@ def test_gpu_matches_golden_queries(ctx, name, width):
     hits = acc.intersect_batch(rays)
     compare_closest(hits, G[f"{name}_hits"], tol_uv=1e-5 if name == "spheres" else 0.0, label=f"{name} w{width}")
     assert np.array_equal(acc.intersect_p_batch(rays).astype(np.uint8), G[f"{name}_occ"])
+
+
+def test_oracle_generators_equal_the_products():
+    """The CPU reference leg of the benchmark builds its inputs with the
+    oracle's own generators (oracle/workloads.cpp), so it never loads the
+    product library; they must give the product generators' bytes."""
+    from rs_illume_b200 import workloads as wl
+    for a, b in zip(oracle.incoherent_workload(), wl.incoherent_workload()):
+        assert a.tobytes() == b.tobytes()
+    for a, b in zip(oracle.coherent_workload(), wl.coherent_workload()):
+        assert a.tobytes() == b.tobytes()
+    for a, b in zip(oracle.icosphere(5, 1021, 0.05, 0.2, (0.66, 0.52, 0.33)),
+                    wl.icosphere(5, 1021, 0.05, 0.2, (0.66, 0.52, 0.33))):
+        assert a.tobytes() == b.tobytes()
+    assert oracle.ball_rays(9, 3, 5000, 1700, 1.5, 0.2, 2.0).tobytes() == \
+        wl.ball_rays(9, 3, 5000, 1700, 1.5, 0.2, 2.0).tobytes()
+    assert oracle.camera_rays(33, 17, (0.1, 0.2, -3.0), 60.0).tobytes() == \
+        wl.camera_rays(33, 17, (0.1, 0.2, -3.0), 60.0).tobytes()

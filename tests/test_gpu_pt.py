@@ -138,3 +138,36 @@ def test_filtered_film_matches_oracle_statistically():
     np.testing.assert_allclose(b, d, rtol=1e-5, atol=1e-6)
     assert np.all(np.isfinite(b_general))
     ctx.close()
+
+
+def test_full_frame_matches_oracle_centre_tile():
+    """The path-tracer workload as measured: Cornell box with the level-6
+    icosphere (81,920 + 34 triangles), 1024x1024, 64 spp, depth 8, Russian
+    roulette from depth 3.  The GPU renders the whole frame twice (two seeds);
+    the oracle renders its 256x256 centre tile, the sample of the frame that
+    the CPU baseline times.  Statistical parity on the tile as above."""
+    xyz, idx, mat, alb, emi = wl.cornell(6, 3)
+    cam = wl.CORNELL_CAMERA
+    ctx = rb.Context(0)
+    acc = rb.GpuBVHAccel(ctx, [rb.TriangleMesh(ctx, xyz, idx)], width=8)
+    pt = rb.PathTracer(acc, mat, alb, emi, cam["eye"], cam["fov_deg"], 1024, 1024)
+    g1, _ = pt.render(64, seed=21)
+    g2, _ = pt.render(64, seed=22)
+    ctx.close()
+    sc = oracle.Scene(xyz, idx)
+    o, _ = oracle.render_pt(sc, xyz, idx, mat, alb, emi, cam["eye"], cam["fov_deg"], 1024, 1024, 64, 8, 3, 3,
+                            window=(384, 384, 640, 640), threads=0)
+    t1, t2 = g1[384:640, 384:640], g2[384:640, 384:640]
+    assert np.all(np.isfinite(g1)) and g1.min() >= 0.0
+    r_go, r_gg = relmse(t1, o), relmse(t1, t2)
+    assert 0.75 < r_go / r_gg < 1.33, (r_go, r_gg)
+    se = (t1 - t2).reshape(-1, 3).std(axis=0) / np.sqrt(t1.size // 3)
+    diff = t1.reshape(-1, 3).mean(axis=0) - o.reshape(-1, 3).mean(axis=0)
+    assert np.all(np.abs(diff) < 5 * se + 1e-6), (diff, se)
+
+    def blocks(x):
+        return x.reshape(256 // 8, 8, 256 // 8, 8, 3).mean(axis=(1, 3))
+    dg = blocks(t1) - blocks(o)
+    sb = np.sqrt(blocks((t1 - t2) ** 2) / 2.0 / 64.0) + 1e-4
+    z = np.abs(dg) / (np.sqrt(2.0) * sb)
+    assert np.mean(z > 5.0) < 0.01

@@ -121,6 +121,37 @@ def test_incoherent_full_size_properties(ctx, incoherent):
     assert ctx.device_errors() == 0
 
 
+def test_bench_launch_full_size_against_oracle(incoherent):
+    """The exact launch the headline measures: a high-occupancy context
+    (persistent schedule, 8 resident blocks per SM, 64-entry stack), width 8,
+    device-resident rays and results on a stream of the caller.  Every one of
+    the 2,097,152 closest-hit and 2,097,152 any-hit answers is checked against
+    the oracle (BVHAccel::intersect / intersect_p, accelerators/bvh.rs:563-662)."""
+    import torch
+    xyz, idx, rays, sc = incoherent
+    ctx = rb.Context(0, high_occupancy=True, stack_depth=64)
+    acc = rb.GpuBVHAccel(ctx, [rb.TriangleMesh(ctx, xyz, idx)], width=8)
+    half = len(rays) // 2
+    closest = np.ascontiguousarray(rays[:half])
+    shadow = np.ascontiguousarray(rays[half:])
+    d_closest = torch.from_numpy(closest.view(np.uint8)).cuda()
+    d_shadow = torch.from_numpy(shadow.view(np.uint8)).cuda()
+    d_hits = torch.empty(half * 16, dtype=torch.uint8, device="cuda")
+    d_occ = torch.empty(half, dtype=torch.int32, device="cuda")
+    s = torch.cuda.Stream()
+    torch.cuda.synchronize()
+    for _ in range(2):     # a relaunch reuses the stream's work counter
+        acc.intersect_batch(d_closest, d_hits, stream=s)
+        acc.intersect_p_batch(d_shadow, d_occ, stream=s)
+    s.synchronize()
+    g = d_hits.cpu().numpy().view(HIT_DTYPE)
+    ties = compare_closest(g, sc.intersect(closest), label="bench launch, closest")
+    assert ties <= 8, ties
+    assert np.array_equal(d_occ.cpu().numpy().view(np.uint32).astype(np.uint8), sc.intersect_p(shadow))
+    assert ctx.device_errors() == 0
+    ctx.close()
+
+
 @pytest.mark.parametrize("width", [4, 8])
 def test_persistent_and_grid_schedules_agree(incoherent, width):
     """The persistent schedule (work counter, lane refill) and one thread per
