@@ -83,6 +83,22 @@ def test_gradients_match_bf16_emulation(cache):
     assert np.all(g5[3:] == 0)
 
 
+def test_gradients_of_a_large_batch_match_bf16_emulation(cache):
+    """40,000 rows: the weight-gradient split-K over many CTAs, each with a
+    row range that is not a multiple of its staging step at the end."""
+    x, y = random_inputs(40000, 7)
+    grad, loss = cache.gradients(x, y)
+    enc = cache.encode(x)
+    pred, rloss, rgrads = ref.forward_backward(enc, cache.params(), y)
+    assert loss == pytest.approx(rloss, rel=2e-3)
+    off = 0
+    for l, (o, i) in enumerate(LAYERS):
+        g = grad[off: off + o * i].reshape(o, i)
+        off += o * i
+        err = np.linalg.norm(g - rgrads[l]) / max(np.linalg.norm(rgrads[l]), 1e-30)
+        assert err < 2e-2, (l, err)
+
+
 def test_gradients_close_to_fp32_autograd(cache):
     torch = pytest.importorskip("torch")
     x, y = random_inputs(2048, 3)
