@@ -22,6 +22,14 @@ from ._lib import ilm_batch_desc, ilm_launch_opts, ilm_tune_result, ptr
 from .primitive import Context, GpuBVHAccel
 
 
+def _ray_count(rays) -> int:
+    """32-byte ray records in a RAY_DTYPE numpy array or a torch tensor (the
+    C ABI refuses host buffers; they are counted so that it can)."""
+    if hasattr(rays, "numel"):
+        return rays.numel() * rays.element_size() // 32
+    return rays.nbytes // 32
+
+
 class BatchPlan:
     """entries: sequence of (GpuBVHAccel, device rays, device output) where the
     output holds 16-byte hits (closest) or uint32 flags (any_hit)."""
@@ -32,7 +40,7 @@ class BatchPlan:
         descs = (ilm_batch_desc * len(entries))()
         self.total_rays = 0
         for k, (acc, rays, out) in enumerate(entries):
-            n = rays.numel() * rays.element_size() // 32
+            n = _ray_count(rays)
             descs[k].accel = acc.id
             descs[k].rays = ptr(rays)
             descs[k].n = n

@@ -467,11 +467,9 @@ float biased_origin(float mn, float s) {
 // Every child plane of one axis rounded outward on the grid (scale s, biased
 // origin b), checked with the kernel's arithmetic; false when 255 steps do not
 // reach a plane.
-bool quantize_axis(float b, float s, const std::vector<Entry>& ch, const std::vector<bool>& present, int axis,
-                   uint8_t* qlo, uint8_t* qhi) {
+bool quantize_axis(float b, float s, const std::vector<Entry>& ch, int axis, uint8_t* qlo, uint8_t* qhi) {
     const double base = (double)dequant(0, s, b);
     for (size_t c = 0; c < ch.size(); ++c) {
-        if (!present[c]) continue;
         float lo = ch[c].box.mn[axis], hi = ch[c].box.mx[axis];
         double fl = std::floor(((double)lo - base) / (double)s);
         double fh = std::ceil(((double)hi - base) / (double)s);
@@ -484,44 +482,6 @@ bool quantize_axis(float b, float s, const std::vector<Entry>& ch, const std::ve
         qhi[c] = (uint8_t)qh;
     }
     return true;
-}
-
-// Children of an 8-wide node placed in octant slots (Ylitie, Karras and Laine,
-// "Efficient Incoherent Ray Traversal on GPUs Through Compressed Wide BVHs",
-// HPG 2017): slot s takes the child that a ray whose direction has sign bits s
-// (bit 0 = x < 0, bit 1 = y < 0, bit 2 = z < 0) meets first, i.e. the child
-// whose centroid offset from the node's centre has the smallest projection on
-// the octant's diagonal (+-1, +-1, +-1).  Pairs are assigned greedily in order
-// of cost.  A ray of octant o then visits slots in the order o ^ 0, o ^ 1, ...,
-// o ^ 7, an approximate near-to-far order with no sorting.  Unused slots hold
-// an empty entry (present = false).
-std::vector<Entry> octant_slots(const std::vector<Entry>& ch, const Box& node, std::vector<bool>& present) {
-    const int n = (int)ch.size();
-    float cost[8][8];
-    for (int i = 0; i < n; ++i)
-        for (int sl = 0; sl < 8; ++sl) {
-            float c = 0.0f;
-            for (int a = 0; a < 3; ++a) {
-                float off = 0.5f * (ch[i].box.mn[a] + ch[i].box.mx[a]) - 0.5f * (node.mn[a] + node.mx[a]);
-                c += ((sl >> a) & 1) ? -off : off;
-            }
-            cost[i][sl] = c;
-        }
-    std::vector<Entry> out(8);
-    present.assign(8, false);
-    bool used[8] = {false, false, false, false, false, false, false, false};
-    for (int k = 0; k < n; ++k) {
-        int bi = -1, bs = -1;
-        for (int i = 0; i < n; ++i) {
-            if (used[i]) continue;
-            for (int sl = 0; sl < 8; ++sl)
-                if (!present[sl] && (bi < 0 || cost[i][sl] < cost[bi][bs])) { bi = i; bs = sl; }
-        }
-        used[bi] = true;
-        present[bs] = true;
-        out[bs] = ch[bi];
-    }
-    return out;
 }
 
 }  // namespace
@@ -545,18 +505,12 @@ void collapse_wide(const std::vector<BinNode>& bin, const std::vector<BuildPrim>
         // node bounds = union of children
         Box nbx = empty_box();
         for (auto& c : ch) box_union(nbx, c.box);
-        // 8-wide nodes: children in octant slots; interior children and leaf
-        // records are numbered in slot order (a child's index is child_base +
-        // the number of interior children in lower slots)
-        std::vector<bool> present(ch.size(), true);
-        if (width == 8) ch = octant_slots(ch, nbx, present);
         uint8_t meta[8] = {0}, qlo[3][8] = {{0}}, qhi[3][8] = {{0}}, ex[3];
         uint32_t imask = 0;
         uint32_t child_base = (uint32_t)queue.size();
         uint32_t prim_base = (uint32_t)record_order.size();
         uint32_t n_int = 0, prim_off = 0;
         for (size_t c = 0; c < ch.size(); ++c) {
-            if (!present[c]) continue;
             if (Collapser::expandable(ch[c])) {
                 meta[c] = (uint8_t)((1u << 5) | n_int);
                 imask |= 1u << c;
@@ -582,7 +536,7 @@ void collapse_wide(const std::vector<BinNode>& bin, const std::vector<BuildPrim>
             for (;;) {
                 float sc = std::ldexp(1.0f, e2);
                 origin[a] = biased_origin(nbx.mn[a], sc);
-                if (std::isfinite(origin[a]) && quantize_axis(origin[a], sc, ch, present, a, qlo[a], qhi[a])) break;
+                if (std::isfinite(origin[a]) && quantize_axis(origin[a], sc, ch, a, qlo[a], qhi[a])) break;
                 if (++e2 > 104) throw std::runtime_error("cannot quantise node bounds");
             }
             ex[a] = (uint8_t)(e2 + 127);

@@ -550,11 +550,11 @@ __global__ void __launch_bounds__(128 * kTcGroups, 1) k_mlp_bwd_tc(const float* 
 }
 
 // ---------------------------------------------------------------- weight gradient on tcgen05
-// k_wgrad_tc: dW_l[o][i] = sum over rows r of dOut_l[r][o] * in_l[r][i], all six
-// layers, split over the batch rows: CTA c takes rows [c * R, (c + 1) * R) and
-// writes one FP32 partial of all 30,720 weights (k_reduce_adam sums them).
-// One warpgroup per CTA; per layer D = A * B with M = o, N = i (208 or 64),
-// K = rows, FP32 D in TMEM (256 columns).
+// k_wgrad_tc: dW_l[o][i] = sum over rows r of dOut_l[r][o] * in_l[r][i], split
+// over the batch rows and the six layers: CTA (c, l) takes layer l's rows
+// [c * R, (c + 1) * R) and writes layer l's slice of partial c (k_reduce_adam
+// sums the partials).  One warpgroup per CTA; D = A * B with M = o, N = i
+// (208 or 64), K = rows, FP32 D in TMEM (256 or 64 columns).
 // Both operands are MN-major without swizzle, which is how the rows are stored
 // (features contiguous): a core matrix is 8 consecutive rows (K) x 8 features
 // (MN), 16 contiguous bytes per row, so staging is one 16-byte cp.async per
@@ -622,16 +622,18 @@ __global__ void __launch_bounds__(128, 1) k_wgrad_tc(NrcCount cnt, uint32_t ld, 
     __shared__ int fail[1];
     __shared__ uint32_t tmem_base;
     const uint32_t n = rows_of(cnt);
-    if (do_step && n > 0 && blockIdx.x == 0 && threadIdx.x == 0) {   // an empty batch takes no step
+    if (do_step && n > 0 && blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) {   // an empty batch takes no step
         st->step += 1;
         st->ema_steps += 1;
     }
     const int t = threadIdx.x, warp = t >> 5;
+    const int l = blockIdx.y;                        // this CTA's layer
+    const uint32_t cols = l == 0 ? 256u : 64u;       // TMEM columns: N = 208 or 64, a power of two
     if (t < 2) mbar_init(smem_u32(&mbar[t]));
     if (t == 0) fail[0] = 0;
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base)),
-                     "r"(256u));
+                     "r"(cols));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -640,16 +642,14 @@ __global__ void __launch_bounds__(128, 1) k_wgrad_tc(NrcCount cnt, uint32_t ld, 
     tc_fence_after();
     const uint32_t tmem_d = tmem_base;
     const uint32_t row0 = blockIdx.x * rows_per_cta;
-    const int per_layer = (int)(rows_per_cta / kWgRows);
-    const int steps = kLayers * per_layer;
+    const int steps = (int)(rows_per_cta / kWgRows);
     float* part = partial + (size_t)blockIdx.x * kParams;
     bool ok = true;
     // the issuing thread's last commit (barrier and phase parity): a later
     // commit covers every earlier MMA, so a drain waits on this one
     uint32_t last_bar = 0, last_parity = 0;
-    wg_stage(wg_smem, 0, row0, n, ld, enc, acts, douts);
+    wg_stage(wg_smem, l, row0, n, ld, enc, acts, douts);
     for (int s = 0; s < steps && ok; ++s) {
-        const int l = s / per_layer, j = s - l * per_layer;
         const int b = s & 1;
         uint8_t* buf = wg_smem + b * kWgBuf;
         asm volatile("cp.async.wait_group 0;\n" ::: "memory");
@@ -665,7 +665,7 @@ __global__ void __launch_bounds__(128, 1) k_wgrad_tc(NrcCount cnt, uint32_t ld, 
             for (int ks = 0; ks < kWgRows / 16; ++ks) {
                 const uint64_t da = umma_desc(a0 + (uint32_t)(ks * 2 * O * 16), (uint32_t)(O * 16), 128u);
                 const uint64_t db = umma_desc(b0 + (uint32_t)(ks * 2 * I * 16), (uint32_t)(I * 16), 128u);
-                umma(tmem_d, da, db, idesc, (j > 0 || ks > 0) ? 1u : 0u);
+                umma(tmem_d, da, db, idesc, (s > 0 || ks > 0) ? 1u : 0u);
             }
             umma_commit(smem_u32(&mbar[b]));
             last_bar = smem_u32(&mbar[b]);
@@ -679,10 +679,9 @@ __global__ void __launch_bounds__(128, 1) k_wgrad_tc(NrcCount cnt, uint32_t ld, 
                 __syncthreads();
                 if (fail[0]) { ok = false; break; }
             }
-            const int l1 = (s + 1) / per_layer, j1 = (s + 1) - l1 * per_layer;
-            wg_stage(wg_smem + (b ^ 1) * kWgBuf, l1, row0 + (uint32_t)(j1 * kWgRows), n, ld, enc, acts, douts);
+            wg_stage(wg_smem + (b ^ 1) * kWgBuf, l, row0 + (uint32_t)((s + 1) * kWgRows), n, ld, enc, acts, douts);
         }
-        if (j == per_layer - 1) {
+        if (s == steps - 1) {
             // layer l complete: D rows o < O to this CTA's partial
             if (t == 0 && !wg_wait(smem_u32(&mbar[b]), (s >> 1) & 1)) fail[0] = 1;
             __syncthreads();
@@ -704,8 +703,6 @@ __global__ void __launch_bounds__(128, 1) k_wgrad_tc(NrcCount cnt, uint32_t ld, 
                     }
                 }
             }
-            tc_fence_before();      // the reads above, before the next layer's MMAs
-            __syncthreads();
         }
     }
     asm volatile("cp.async.wait_group 0;\n" ::: "memory");
@@ -720,7 +717,7 @@ __global__ void __launch_bounds__(128, 1) k_wgrad_tc(NrcCount cnt, uint32_t ld, 
     __syncthreads();
     if (warp == 0) {
         tc_fence_after();
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base), "r"(256u));
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base), "r"(cols));
     }
 }
 
@@ -898,7 +895,7 @@ cudaError_t train_rows(ilm_nrc* h, const float* raw, const float* target, NrcCou
     per_cta = std::max<uint32_t>(kWgMinRows, (per_cta + kWgRows - 1) / kWgRows * kWgRows);
     const int n_part = (int)std::max<uint32_t>(1, (cap + per_cta - 1) / per_cta);
     StepState* st = static_cast<StepState*>(h->state.ptr);
-    k_wgrad_tc<<<n_part, 128, kWgSmem, s>>>(cnt, cap, per_cta, static_cast<const __nv_bfloat16*>(h->enc.ptr), acts,
+    k_wgrad_tc<<<dim3(n_part, kLayers), 128, kWgSmem, s>>>(cnt, cap, per_cta, static_cast<const __nv_bfloat16*>(h->enc.ptr), acts,
                                             douts, static_cast<float*>(h->partial.ptr), st, do_step,
                                             static_cast<uint32_t*>(h->err.ptr));
     if ((e = cudaGetLastError()) != cudaSuccess) return e;

@@ -125,9 +125,9 @@ __device__ __forceinline__ void sort_keys(uint32_t* k) {
     }
 }
 
-// Per-lane traversal state of one ray, 4-wide nodes: hit children sorted by
-// entry distance and pushed far-to-near, one stack entry (node or leaf, with
-// its entry distance) per child.
+// Per-lane traversal state of one ray over 4- or 8-wide nodes: hit children
+// sorted by entry distance and pushed far-to-near, one stack entry (node or
+// leaf, with its entry distance) per child.
 template <int W, int kStack, bool kAny, bool kAnalytic = true>
 struct WideTracerSorted {
     RayIn ray;
@@ -249,186 +249,6 @@ struct WideTracerSorted {
 };
 
 
-// Per-lane traversal state of one ray, 8-wide nodes whose children sit in
-// octant slots (the builder's octant_slots): a ray of octant `oct` (sign bits
-// of its direction) visits a node's children in slot order oct ^ 0, oct ^ 1,
-// ..., oct ^ 7, so no sorting is needed.
-//
-// A node expansion yields two groups (Ylitie, Karras and Laine, HPG 2017):
-//  * a node group: the node's first interior child, its interior-child mask
-//    and the bits of the interior children hit, in visiting order (bit k =
-//    slot oct ^ k);
-//  * a triangle group: the node's first primitive record and one bit per
-//    record of the leaf children hit.
-// Each step tests one record of the triangle group, or, when that is empty,
-// takes the next child of the node group and expands it; what is left of the
-// node group goes on the stack as one 8-byte entry (so a node costs at most
-// one push).  For closest hit an entry keeps the smallest entry distance of
-// its remaining children (truncated to its upper 16 bits, i.e. rounded toward
-// zero), and a popped entry at or beyond the current hit is dropped.
-// The first kShared stack entries live in shared memory, [entry][thread], the
-// rest in local memory.
-// Shared-memory stack entries per thread of the 8-wide tracer, and the
-// block's shared stack (blocks of 128 threads), [entry][thread]: a warp's
-// pushes at one depth are 32 consecutive 8-byte words.  Kernels whose tracer
-// never pushes to it do not allocate it.
-constexpr int kSharedStack = 8;
-static __shared__ uint2 g_block_stack[kSharedStack * 128];
-
-template <int kStack, bool kAny, bool kAnalytic = true>
-struct WideTracerOct {
-    static constexpr int kSpill = kStack > kSharedStack ? kStack - kSharedStack : 1;
-    RayIn ray;
-    float ix, iy, iz;
-    bool tr_ready, occluded;
-    TriRay tr;
-    float best_t, bu, bv;
-    uint32_t best, status, iter, oct;
-    // node group: first interior child, hits (bits 0-7, visiting order) |
-    // interior mask (bits 8-15, slot order); entry-distance bounds of all of
-    // its children and of all but the first
-    uint32_t g_base, g_bits;
-    float g_t, g_t_rest;
-    // triangle group: first record, one bit per record
-    uint32_t t_base, t_bits;
-    int sp;
-    uint2 spill[kSpill];
-
-    __device__ __forceinline__ void init(const RayIn& r) {
-        ray = r;
-        best_t = r.tmax; bu = 0.0f; bv = 0.0f;
-        best = ILM_MISS;
-        occluded = false;
-        status = 0;
-        ix = __frcp_rn(r.dx); iy = __frcp_rn(r.dy); iz = __frcp_rn(r.dz);   // == 1/d exactly
-        oct = (ix < 0.0f ? 1u : 0u) | (iy < 0.0f ? 2u : 0u) | (iz < 0.0f ? 4u : 0u);
-        tr_ready = false;
-        iter = 0; sp = 0;
-        // the root as a one-child node group: slot 0, interior
-        g_base = 0u;
-        g_bits = (1u << oct) | (1u << 8);
-        g_t = g_t_rest = -INFINITY;
-        t_base = 0u; t_bits = 0u;
-    }
-
-    __device__ __forceinline__ bool enters(const float* b) const {
-        return box_intersect_p(b[0], b[1], b[2], b[3], b[4], b[5], ray, ix, iy, iz, oct & 1u, oct & 2u, oct & 4u,
-                               ray.tmax);
-    }
-
-    __device__ __forceinline__ void push(uint2 e) {
-        if (sp < kSharedStack) g_block_stack[sp * 128 + threadIdx.x] = e;
-        else spill[sp - kSharedStack] = e;
-        ++sp;
-    }
-
-    // Next stacked node group still nearer than the current hit; false when none.
-    __device__ __forceinline__ bool pop() {
-        while (sp > 0) {
-            --sp;
-            uint2 e = sp < kSharedStack ? g_block_stack[sp * 128 + threadIdx.x] : spill[sp - kSharedStack];
-            float t = __uint_as_float(e.y & 0xFFFF0000u);
-            if (kAny || t < best_t) {
-                g_base = e.x;
-                g_bits = e.y & 0xFFFFu;
-                g_t = g_t_rest = t;
-                return true;
-            }
-        }
-        return false;
-    }
-
-    // Tests node `idx`'s children and makes its node and triangle groups.
-    __device__ __forceinline__ void expand(const uint4* __restrict__ nodes, uint32_t idx) {
-        WideView<8> nv = load_wide<8>(nodes, idx, oct & 1u, oct & 2u, oct & 4u);
-        const float lim = kAny ? ray.tmax : best_t;
-        uint32_t hits = 0u, tris = 0u;
-        // closest hit: the two smallest entry distances of the interior
-        // children hit, and the distance of the first one in visiting order
-        float min1 = INFINITY, min2 = INFINITY, t_first = INFINITY;
-        uint32_t r_first = 8u;
-#pragma unroll
-        for (int c = 0; c < 8; ++c) {
-            float tn;
-            const bool h = child_hit<8>(nv, c, ray, ix, iy, iz, lim, tn);
-            const uint32_t m = byte_of(nv.meta[0], nv.meta[1], c);
-            const uint32_t r = (uint32_t)c ^ oct;
-            if (h && ((nv.imask >> c) & 1u)) {
-                hits |= 1u << r;
-                if (!kAny) {
-                    tn = fmaxf(tn, 0.0f);
-                    if (r < r_first) { r_first = r; t_first = tn; }
-                    if (tn < min1) { min2 = min1; min1 = tn; }
-                    else if (tn < min2) { min2 = tn; }
-                }
-            } else if (h) {
-                tris |= ((1u << (m >> 5)) - 1u) << (m & 31u);
-            }
-        }
-        g_base = nv.child_base;
-        g_bits = hits | (nv.imask << 8);
-        t_base = nv.prim_base;
-        t_bits = tris;
-        if (!kAny) {
-            g_t = min1;
-            g_t_rest = t_first == min1 ? min2 : min1;
-        }
-    }
-
-    __device__ __forceinline__ void test_record(const PrimRec* __restrict__ prims,
-                                                const SphereRec* __restrict__ spheres) {
-        const uint32_t k = (uint32_t)(__ffs(t_bits) - 1);
-        t_bits &= t_bits - 1u;
-        float t, u, v;
-        uint32_t pid;
-        if (kAny) {
-            if (prim_test<false, kAnalytic>(prims, spheres, t_base + k, tr, tr_ready, ray, ray.tmax, t, u, v, pid))
-                occluded = true;
-        } else if (prim_test<true, kAnalytic>(prims, spheres, t_base + k, tr, tr_ready, ray, best_t, t, u, v, pid) &&
-                   (t < best_t || (t == best_t && pid < best))) {
-            best_t = t; best = pid; bu = u; bv = v;
-        }
-    }
-
-    // Advances by one record test or one node expansion; true when the ray
-    // is finished.
-    __device__ __forceinline__ bool step(const TraceArgs& a) {
-        if (++iter > a.max_iter) { status = kErrIterationCap; return true; }
-        if (t_bits) {
-            test_record(a.prims, a.spheres);
-            if (kAny && occluded) return true;
-        } else {
-            // the node group has a child left here (else it was dropped below)
-            const uint32_t k = (uint32_t)(__ffs(g_bits & 0xFFu) - 1);
-            const uint32_t slot = k ^ oct;
-            const uint32_t imask = g_bits >> 8;
-            const uint32_t child = g_base + (uint32_t)__popc(imask & ((1u << slot) - 1u));
-            const uint32_t rest = (g_bits & 0xFFu) & ~(1u << k);
-            if (rest) {
-                if (sp >= kStack) { status = kErrStackOverflow; return true; }
-                const uint32_t tq = __float_as_uint(fmaxf(g_t_rest, 0.0f)) & 0xFFFF0000u;
-                push(make_uint2(g_base, rest | (imask << 8) | tq));
-            }
-            expand(static_cast<const uint4*>(a.nodes), child);
-        }
-        // next work: this group's records, then its nodes (unless all of them
-        // lie at or beyond the current hit), then the stack
-        if (t_bits) return false;
-        if ((g_bits & 0xFFu) && (kAny || g_t < best_t)) return false;
-        return !pop();
-    }
-
-    __device__ __forceinline__ void write(uint64_t i, const TraceArgs& a) const {
-        if (status) atomicOr(a.err, status);
-        if (kAny) {
-            a.occ[i] = status ? kHitTraversalError : (occluded ? 1u : 0u);
-        } else {
-            if (status) store_hit(a.hits, i, kHitTraversalError, ray.tmax, 0.0f, 0.0f);
-            else store_hit(a.hits, i, best, best == ILM_MISS ? ray.tmax : best_t, bu, bv);
-        }
-    }
-};
-
 // Per-lane traversal state of one ray over the binary layout (the reference's
 // 32-byte LinearBVHNode, accelerators/bvh.rs:665-673): the ordered traversal of
 // BVHAccel::intersect / intersect_p (bvh.rs:563-662, the far child pushed on
@@ -513,15 +333,12 @@ struct BinTracer {
     }
 };
 
-// The tracer of a width: octant-ordered groups for 8-wide nodes, sorted
-// children for 4-wide nodes, the reference's ordered traversal for binary
-// nodes.
+// The tracer of a width: sorted children for 4- and 8-wide nodes, the
+// reference's ordered traversal for binary nodes.
 template <int W, int kStack, bool kAny, bool kAnalytic>
 struct TracerOf { using type = WideTracerSorted<W, kStack, kAny, kAnalytic>; };
 template <int kStack, bool kAny, bool kAnalytic>
 struct TracerOf<2, kStack, kAny, kAnalytic> { using type = BinTracer<kAny, kAnalytic>; };
-template <int kStack, bool kAny, bool kAnalytic>
-struct TracerOf<8, kStack, kAny, kAnalytic> { using type = WideTracerOct<kStack, kAny, kAnalytic>; };
 template <int W, int kStack, bool kAny, bool kAnalytic = true>
 using WideTracer = typename TracerOf<W, kStack, kAny, kAnalytic>::type;
 
