@@ -294,8 +294,9 @@ def neural_cache_leg(rb, wl, ctx, torch, dev):
             "ms_per_frame": worst["ms_per_frame"], "plain_ms_per_spp": round(1e3 * t_spp, 3),
             "queries_per_path": worst["queries_per_path"], "warm_frames": 200, "repeats": reps,
             "mlp": mlp,
-            "config": f"Cornell box, 1024x1024, 1-spp frames, spread c 0.01, 16384 training paths and "
-                      f"4 x 16384 samples per frame, one-vertex self-training suffix, reference {REF_SPP} spp"}
+            "config": f"Cornell box, 1024x1024, 1-spp frames, spread c 0.003, 16384 training paths and "
+                      f"2 Adam steps x 32768 samples per frame, one-vertex self-training suffix, "
+                      f"reference {REF_SPP} spp"}
 
 
 def nrc_frame_leg(rb, wl, ctx):

@@ -419,8 +419,8 @@ class PathTracer:
                      "waves": st.waves}
 
     def render_nrc(self, cache, frames: int = 0, spp_per_frame: int = 1, max_depth: int = 8, rr_depth: int = 3,
-                   seed: int = 3, spread_c: float = 0.01, train_paths: int = 16384, train_samples: int = 65536,
-                   time_budget_s: float = 0.0, train: bool = True, train_steps: int = 4, train_suffix: int = 1,
+                   seed: int = 3, spread_c: float = 0.003, train_paths: int = 16384, train_samples: int = 65536,
+                   time_budget_s: float = 0.0, train: bool = True, train_steps: int = 2, train_suffix: int = 1,
                    out=None):
         """Path tracing with a RadianceCache (ilm_render_nrc): frames of
         spp_per_frame samples, the cache answering paths whose spread has

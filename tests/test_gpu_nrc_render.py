@@ -101,21 +101,22 @@ def test_equal_time_relmse_beats_plain_tracer():
     _, sp = pt.render(16, seed=4)
     t_spp = sp["seconds"] / 16
     r1 = np.mean([rel(pt.render(1, seed=10 + k)[0]) for k in range(4)])
-    cache = RadianceCache(ctx, bound, seed=4)
-    pt.render_nrc(cache, frames=200, seed=9)                 # online training over earlier frames
-    rs, ts = [], []
-    for k in range(6):
-        img, st = pt.render_nrc(cache, frames=1, seed=100 + k)
-        assert np.all(np.isfinite(img))
-        rs.append(rel(img))
-        ts.append(st["seconds"])
-    r_nrc, t_frame = float(np.mean(rs)), float(np.median(ts))
-    r_plain = r1 * t_spp / t_frame
-    gain = r_plain / r_nrc
-    print(f"\nframe {t_frame * 1e3:.2f} ms (plain {t_spp * 1e3:.2f} ms/spp): relMSE cache {r_nrc:.4f}, "
-          f"plain at equal time {r_plain:.4f}: gain {gain:.2f}x")
-    # measured about 2x on B200 (1-spp frames at 1024^2); the bar keeps a
-    # margin for frame-time and noise variation between runs
-    assert gain > 1.5, gain
-    cache.close()
+    gains = []
+    for rep in range(3):          # independent runs: a fresh cache each
+        cache = RadianceCache(ctx, bound, seed=4 + rep)
+        pt.render_nrc(cache, frames=200, seed=9 + 1000 * rep)      # online training over earlier frames
+        rs, ts = [], []
+        for k in range(6):
+            img, st = pt.render_nrc(cache, frames=1, seed=100 + 1000 * rep + k)
+            assert np.all(np.isfinite(img))
+            rs.append(rel(img))
+            ts.append(st["seconds"])
+        cache.close()
+        r_nrc, t_frame = float(np.mean(rs)), float(np.median(ts))
+        gains.append(r1 * t_spp / t_frame / r_nrc)
+    print(f"\nplain {t_spp * 1e3:.2f} ms/spp, relMSE(1 spp) {r1:.4f}; equal-time gains {np.round(gains, 3)}")
+    # at least 2x lower relMSE than the plain tracer at
+    # equal time, on average over the runs (measured 2.1-2.2 on B200 with the
+    # default settings: spread threshold 0.003, 2 Adam steps of 32,768 rows)
+    assert np.mean(gains) > 2.0, gains
     ctx.close()
