@@ -126,6 +126,7 @@ struct RowIn {
     float q[3];     // normalised position
     float u[4];     // theta/pi, phi/2pi of the direction, then of the normal
     float alb[3];
+    float ps[3], pc[3];   // encoding state: the last octave's (sin, cos) per axis
 };
 
 __device__ __forceinline__ RowIn load_row(const float* __restrict__ raw, uint32_t r, const Enc& e) {
@@ -146,39 +147,75 @@ __device__ __forceinline__ RowIn load_row(const float* __restrict__ raw, uint32_
     return v;
 }
 
-// Features F + 2t and F + 2t + 1 as a bf16 pair; F is a multiple of 8, so the
-// eight features F..F+7 lie in one block of the layout:
-//   [0, 72)    axis F/24, octave k = (f % 24) / 2: (sin, cos)(2^k pi q)
+// The eight features 8 KC .. 8 KC + 7 of a row as four bf16 pairs (pair t =
+// features 8 KC + 2t, 8 KC + 2t + 1).  The layout:
+//   [0, 72)    axis f / 24, octave k = (f % 24) / 2: (sin, cos)(2^k pi q)
 //   [72, 200)  one-blob of u[(f - 72) / 32], bin j = (f - 72) % 32:
 //              exp(-((u - (j + 1/2)/32) * 32)^2 / 2)
 //   200..202   albedo, then zeros
-template <int F>
-__device__ __forceinline__ uint32_t feat2(const RowIn& v, int t) {
+// Groups are evaluated in order (KC = 0, 1, ... 25), and two recurrences cut
+// the special-function work:
+//   * octaves: one sincospi per axis at octave 0, then the double angle,
+//     sin 2x = 2 sin x cos x, cos 2x = (cos x - sin x)(cos x + sin x); the
+//     error doubles per octave, about 2^11 float ulps at octave 11, far below
+//     a bf16 ulp; the last octave of a group is kept in the row state;
+//   * one-blob bins: two exps per group of 8 bins, g_j = exp(-d_j^2 / 2) and
+//     the ratio r_j = g_{j+1} / g_j = exp(d_j - 1/2) (d_{j+1} = d_j - 1), then
+//     g_{j+1} = g_j r_j and r_{j+1} = r_j / e; relative error grows by a few
+//     ulps per step.
+template <int KC>
+__device__ __forceinline__ uint4 feature_group(RowIn& v) {
+    constexpr int F = 8 * KC;
+    uint4 q;
     if constexpr (F < 72) {
-        constexpr int a = F / 24;
-        const int oct = ((F % 24) >> 1) + t;
+        constexpr int a = F / 24, o0 = (F % 24) >> 1;
         float s, c;
-        sincospif(v.q[a] * (float)(1 << oct), &s, &c);
-        return pack(s, c);
+        if constexpr (o0 == 0) {
+            sincospif(v.q[a], &s, &c);
+        } else {
+            s = 2.0f * v.ps[a] * v.pc[a];
+            c = (v.pc[a] - v.ps[a]) * (v.pc[a] + v.ps[a]);
+        }
+        uint32_t w[4];
+#pragma unroll
+        for (int t = 0; t < 4; ++t) {
+            w[t] = pack(s, c);
+            if (t < 3) {
+                const float s2 = 2.0f * s * c, c2 = (c - s) * (c + s);
+                s = s2;
+                c = c2;
+            }
+        }
+        v.ps[a] = s;
+        v.pc[a] = c;
+        q = make_uint4(w[0], w[1], w[2], w[3]);
     } else if constexpr (F < 200) {
-        constexpr int ui = (F - 72) >> 5;
-        const int j = ((F - 72) & 31) + 2 * t;
-        const float u = v.u[ui];
-        float d0 = (u - (j + 0.5f) * (1.0f / 32.0f)) * 32.0f;
-        float d1 = (u - (j + 1.5f) * (1.0f / 32.0f)) * 32.0f;
-        return pack(__expf(-0.5f * d0 * d0), __expf(-0.5f * d1 * d1));
+        constexpr int ui = (F - 72) >> 5, j0 = (F - 72) & 31;
+        constexpr float kInvE = 0.36787944117144233f;   // e^-1
+        const float d = (v.u[ui] - (j0 + 0.5f) * (1.0f / 32.0f)) * 32.0f;
+        float g = __expf(-0.5f * d * d), r = __expf(d - 0.5f);
+        float gv[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            gv[k] = g;
+            g *= r;
+            r *= kInvE;
+        }
+        q = make_uint4(pack(gv[0], gv[1]), pack(gv[2], gv[3]), pack(gv[4], gv[5]), pack(gv[6], gv[7]));
     } else {
-        if (t == 0) return pack(v.alb[0], v.alb[1]);
-        if (t == 1) return pack(v.alb[2], 0.0f);
-        return 0u;
+        q = make_uint4(pack(v.alb[0], v.alb[1]), pack(v.alb[2], 0.0f), 0u, 0u);
     }
+    return q;
 }
 
 // Whole-row encoder (104 words) for k_nrc_encode.
 template <int B>
-__device__ __forceinline__ void encode_row(const RowIn& v, uint32_t* out) {
-#pragma unroll
-    for (int t = 0; t < 4; ++t) out[4 * B + t] = feat2<8 * B>(v, t);
+__device__ __forceinline__ void encode_row(RowIn& v, uint32_t* out) {
+    const uint4 q = feature_group<B>(v);
+    out[4 * B] = q.x;
+    out[4 * B + 1] = q.y;
+    out[4 * B + 2] = q.z;
+    out[4 * B + 3] = q.w;
     if constexpr (B + 1 < kIn / 8) encode_row<B + 1>(v, out);
 }
 
@@ -273,17 +310,13 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
 // Row t's 8 features F..F+7 (F = 8 * KC) into core-matrix column c of an A
 // buffer, and into the row's stored encoding when genc is set.
 template <int KC>
-__device__ __forceinline__ void put_features(uint8_t* a, int c, int row, const RowIn& v, uint4* genc) {
-    uint4 q;
-    q.x = feat2<8 * KC>(v, 0);
-    q.y = feat2<8 * KC>(v, 1);
-    q.z = feat2<8 * KC>(v, 2);
-    q.w = feat2<8 * KC>(v, 3);
+__device__ __forceinline__ void put_features(uint8_t* a, int c, int row, RowIn& v, uint4* genc) {
+    const uint4 q = feature_group<KC>(v);
     *reinterpret_cast<uint4*>(a + ((row >> 3) * kTcHalfCols + c) * 128 + (row & 7) * 16) = q;
     if (genc) genc[KC] = q;
 }
 template <int KC, int KEND>
-__device__ __forceinline__ void encode_cols(uint8_t* a, int c0, int row, const RowIn& v, uint4* genc) {
+__device__ __forceinline__ void encode_cols(uint8_t* a, int c0, int row, RowIn& v, uint4* genc) {
     put_features<KC>(a, KC - c0, row, v, genc);
     if constexpr (KC + 1 < KEND) encode_cols<KC + 1, KEND>(a, c0, row, v, genc);
 }
