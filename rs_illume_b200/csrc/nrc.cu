@@ -31,6 +31,7 @@
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <memory>
@@ -478,6 +479,180 @@ __global__ void __launch_bounds__(128 * kTcGroups, 1) k_mlp_fwd_tc(const float* 
     tc_teardown(fail, tmem_base, err, mb, phase);
 }
 
+// ---------------------------------------------------------------- inference on tcgen05, two tiles per warpgroup
+// k_mlp_infer_tc: the inference forward with two 128-row tiles in flight per
+// warpgroup.  Each tile (slot) has its own A buffer (128 rows x 64 features,
+// 16 KB), its own 64 TMEM columns and its own mbarrier; the warpgroup
+// alternates between its slots, so while one slot's MMAs run the threads
+// produce the other slot's next A operand (encoding or accumulator -> ReLU ->
+// bf16).  Layer 0 is issued in four parts of K = 64, 64, 64 and 16 features
+// (features 0-63, 64-127, 128-191, 192-207), so an A buffer holds 64
+// features; a tile takes nine MMA batches (four layer-0 parts, five layers).
+// With 4 warpgroups per CTA, 8 tiles are in flight per SM (192,512 bytes of
+// shared memory, all 512 TMEM columns).  Waits are bounded; a warpgroup
+// whose wait gives up drains both slots' last commits before the TMEM is
+// freed.
+constexpr int kInfABytes = 128 / 8 * 8 * 128;                        // 16,384
+constexpr int kInfSmem = kTcWBytes + kTcGroups * 2 * kInfABytes;      // 192,512
+
+// The features of layer-0 part p (groups 8p .. 8p + 7, at most 25) into
+// columns 0.. of an A buffer (8 core-matrix columns, SBO 1024).
+template <int KC, int KEND>
+__device__ __forceinline__ void encode_part(uint8_t* a, int c0, int row, RowIn& v) {
+    const uint4 q = feature_group<KC>(v);
+    *reinterpret_cast<uint4*>(a + ((row >> 3) * 8 + (KC - c0)) * 128 + (row & 7) * 16) = q;
+    if constexpr (KC + 1 < KEND) encode_part<KC + 1, KEND>(a, c0, row, v);
+}
+
+// Issues one batch (no wait): fences, group barrier, one thread issues and
+// commits to the slot's mbarrier.
+__device__ __forceinline__ void inf_issue(int g, int t, uint32_t tmem_d, uint32_t a_base, uint32_t a_sbo,
+                                          uint32_t w_base, uint32_t w_sbo, int k0, int ksteps, int n_out,
+                                          bool accumulate, uint32_t mbar) {
+    fence_proxy_async();
+    tc_fence_before();
+    group_sync(g);
+    if (t == 0) {
+        tc_fence_after();
+        const uint32_t idesc = idesc_bf16(128, n_out);
+        for (int k = 0; k < ksteps; ++k) {
+            const uint64_t da = umma_desc(a_base + (uint32_t)k * 256u, 128u, a_sbo);
+            const uint64_t db = umma_desc(w_base + (uint32_t)(k0 + k) * 256u, 128u, w_sbo);
+            umma(tmem_d, da, db, idesc, (accumulate || k > 0) ? 1u : 0u);
+        }
+        umma_commit(mbar);
+    }
+}
+
+// Waits for the slot's last batch (issuing thread, bounded); false on a timeout.
+__device__ __forceinline__ bool inf_wait(int g, int t, uint32_t mbar, uint32_t& phase, volatile int* fail) {
+    if (t == 0) {
+        uint32_t it = 0;
+        while (!mbar_try_wait(mbar, phase) && ++it < kTcWaitCap) {}
+        if (it >= kTcWaitCap) *fail = 1;
+    }
+    phase ^= 1u;
+    group_sync(g);
+    tc_fence_after();
+    return *fail == 0;
+}
+
+// Batch k (0-8) of the slot's tile: its A operand, then the issue.
+__device__ __forceinline__ void inf_step(int k, int g, int t, uint8_t* a, uint32_t a_base, uint32_t w_base,
+                                         uint32_t tmem_d, uint32_t tmem_row, RowIn& v, uint32_t mbar) {
+    if (k < 4) {
+        switch (k) {
+            case 0: encode_part<0, 8>(a, 0, t, v); break;
+            case 1: encode_part<8, 16>(a, 8, t, v); break;
+            case 2: encode_part<16, 24>(a, 16, t, v); break;
+            default: encode_part<24, 26>(a, 24, t, v); break;
+        }
+        inf_issue(g, t, tmem_d, a_base, 8 * 128, w_base + 2 * param_off(0), 26 * 128, 4 * k, k < 3 ? 4 : 1, 64,
+                  k > 0, mbar);
+    } else {
+        const int l = k - 3;
+        acc_to_a(tmem_row, a, t, nullptr);
+        inf_issue(g, t, tmem_d, a_base, 8 * 128, w_base + 2 * param_off(l), 8 * 128, 0, 4, l == 5 ? 16 : 64, false,
+                  mbar);
+    }
+}
+
+__global__ void __launch_bounds__(128 * kTcGroups, 1) k_mlp_infer_tc(const float* __restrict__ raw, NrcCount cnt,
+                                                                     Enc ec, const __nv_bfloat16* __restrict__ wtc,
+                                                                     float* __restrict__ out, uint32_t* err) {
+    extern __shared__ __align__(1024) uint8_t tc_smem[];
+    __shared__ __align__(8) uint64_t mbar[2 * kTcGroups];
+    __shared__ int fail[kTcGroups];
+    __shared__ uint32_t tmem_base;
+    const int warp = threadIdx.x >> 5, g = warp >> 2, t = threadIdx.x & 127;
+    const uint32_t groups = blockDim.x >> 7;
+    {
+        const uint4* src = reinterpret_cast<const uint4*>(wtc);
+        uint4* dst = reinterpret_cast<uint4*>(tc_smem);
+        for (int k = threadIdx.x; k < kTcWBytes / 16; k += blockDim.x) dst[k] = src[k];
+    }
+    if (threadIdx.x < 2 * groups) mbar_init(smem_u32(&mbar[threadIdx.x]));
+    if (threadIdx.x < groups) fail[threadIdx.x] = 0;
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base)),
+                     "r"(128u * groups));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    fence_proxy_async();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t n = rows_of(cnt);
+    const uint32_t w_base = smem_u32(tc_smem);
+    // per slot: A buffer, TMEM columns (and this warp's lanes), mbarrier
+    auto a_of = [&](int sl) { return tc_smem + kTcWBytes + (2 * g + sl) * kInfABytes; };
+    auto tmem_of = [&](int sl) { return tmem_base + 64u * (2u * g + sl); };
+    auto lanes_of = [&](int sl) { return tmem_of(sl) + ((uint32_t)(32 * (warp & 3)) << 16); };
+    auto mb_of = [&](int sl) { return smem_u32(&mbar[2 * g + sl]); };
+    uint32_t phase[2] = {0u, 0u};
+    // a committed batch not yet waited for, and its phase parity
+    bool pending[2] = {false, false};
+    uint32_t pend_par[2] = {0u, 0u};
+    const uint32_t tiles = (n + 127) / 128, pairs = (tiles + 1) / 2;
+    bool ok = true;
+    for (uint32_t pr = blockIdx.x * groups + g; pr < pairs && ok; pr += gridDim.x * groups) {
+        RowIn v[2];
+#pragma unroll
+        for (int sl = 0; sl < 2; ++sl) {
+            const uint32_t row = (2 * pr + sl) * 128 + t;
+            v[sl] = RowIn{};
+            if (row < n) v[sl] = load_row(raw, row, ec);
+        }
+        for (int k = 0; k < 9 && ok; ++k) {
+#pragma unroll
+            for (int sl = 0; sl < 2; ++sl) {
+                if (k > 0) {
+                    ok = inf_wait(g, t, mb_of(sl), phase[sl], &fail[g]);
+                    if (!ok) break;
+                    pending[sl] = false;
+                }
+                pend_par[sl] = phase[sl];
+                uint8_t* buf = a_of(sl);
+                inf_step(k, g, t, buf, smem_u32(buf), w_base, tmem_of(sl), lanes_of(sl), v[sl], mb_of(sl));
+                pending[sl] = true;
+            }
+        }
+        if (!ok) break;
+#pragma unroll
+        for (int sl = 0; sl < 2; ++sl) {
+            ok = ok && inf_wait(g, t, mb_of(sl), phase[sl], &fail[g]);
+            if (!ok) break;
+            pending[sl] = false;
+            float o[16];
+            tmem_ld16(lanes_of(sl), o);
+            const uint32_t row = (2 * pr + sl) * 128 + t;
+            if (row < n) {
+                out[3 * (size_t)row] = o[0];
+                out[3 * (size_t)row + 1] = o[1];
+                out[3 * (size_t)row + 2] = o[2];
+            }
+        }
+    }
+    // a wait that gave up: drain both slots' outstanding commits, then
+    // report; see tc_teardown
+    if (t == 0 && fail[g]) {
+#pragma unroll
+        for (int sl = 0; sl < 2; ++sl) {
+            if (!pending[sl]) continue;
+            uint32_t it = 0;
+            while (!mbar_try_wait(mb_of(sl), pend_par[sl]) && ++it < kTcDrainCap) {}
+        }
+        atomicOr(err, kErrMlpTimeout);
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base), "r"(128u * groups));
+    }
+}
+
 // ---------------------------------------------------------------- backward on tcgen05
 // k_mlp_bwd_tc: loss gradient (mean over the n rows and 3 channels), then
 // dOut of every layer back to the input (layer l at douts + l * ld * 64:
@@ -899,9 +1074,13 @@ cudaError_t forward(ilm_nrc* h, const float* raw, NrcCount cnt, bool train, floa
         k_mlp_fwd_tc<true><<<L.grid, L.threads, L.smem, s>>>(
             raw, cnt, enc_params(h), static_cast<const __nv_bfloat16*>(h->wtc.ptr), out, err, rows,
             static_cast<__nv_bfloat16*>(h->acts.ptr), static_cast<__nv_bfloat16*>(h->enc.ptr));
-    else
-        k_mlp_fwd_tc<false><<<L.grid, L.threads, L.smem, s>>>(
-            raw, cnt, enc_params(h), static_cast<const __nv_bfloat16*>(h->winf.ptr), out, err, 0u, nullptr, nullptr);
+    else {
+        // inference: two tiles per warpgroup, 4 warpgroups per CTA, one CTA per SM
+        const uint32_t pairs = (rows + 255) / 256;   // two 128-row tiles per pair
+        const uint32_t grid = std::max<uint32_t>(1, std::min<uint32_t>(148, (pairs + kTcGroups - 1) / kTcGroups));
+        k_mlp_infer_tc<<<grid, 128 * kTcGroups, kInfSmem, s>>>(
+            raw, cnt, enc_params(h), static_cast<const __nv_bfloat16*>(h->winf.ptr), out, err);
+    }
     return cudaGetLastError();
 }
 
@@ -1011,6 +1190,7 @@ int32_t ilm_nrc_create(ilm_context* ctx, const ilm_nrc_config* cfg, ilm_nrc** ou
     cudaFuncSetAttribute(k_mlp_fwd_tc<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem);
     cudaFuncSetAttribute(k_mlp_bwd_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcbSmem);
     cudaFuncSetAttribute(k_wgrad_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kWgSmem);
+    cudaFuncSetAttribute(k_mlp_infer_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kInfSmem);
     if ((e = pack(h.get(), h->stream)) != cudaSuccess) return cuda_fail(ctx, e, "nrc pack");
     if ((e = cudaStreamSynchronize(h->stream)) != cudaSuccess) return cuda_fail(ctx, e, "nrc");
     *out = h.release();

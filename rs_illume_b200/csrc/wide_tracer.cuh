@@ -125,17 +125,6 @@ __device__ __forceinline__ void sort_keys(uint32_t* k) {
     }
 }
 
-// Stack entries per lane kept in shared memory ([entry][thread], blocks of 128
-// threads): the top kStackTop entries live there as a ring, deeper ones in
-// local memory (a push past the ring moves the ring's oldest entry down, a pop
-// brings it back).  0 keeps the whole stack in local memory.
-#ifndef ILM_STACK_TOP
-#define ILM_STACK_TOP 0
-#endif
-constexpr int kStackTop = ILM_STACK_TOP;
-static_assert((kStackTop & (kStackTop - 1)) == 0, "the ring size is a power of two");
-static __shared__ uint2 g_stack_top[kStackTop > 0 ? kStackTop * 128 : 1];
-
 // Per-lane traversal state of one ray over 4- or 8-wide nodes: hit children
 // sorted by entry distance and pushed far-to-near, one stack entry (node or
 // leaf, with its entry distance) per child.
@@ -168,24 +157,8 @@ struct WideTracerSorted {
         return box_intersect_p(b[0], b[1], b[2], b[3], b[4], b[5], ray, ix, iy, iz, negx, negy, negz, ray.tmax);
     }
 
-    __device__ __forceinline__ void push(uint2 e) {
-        if constexpr (kStackTop == 0) {
-            stack[sp++] = e;
-            return;
-        }
-        uint2& slot = g_stack_top[(sp & (kStackTop - 1)) * 128 + threadIdx.x];
-        if (sp >= kStackTop) stack[sp - kStackTop] = slot;
-        slot = e;
-        ++sp;
-    }
-    __device__ __forceinline__ uint2 pop_one() {
-        if constexpr (kStackTop == 0) return stack[--sp];
-        --sp;
-        uint2& slot = g_stack_top[(sp & (kStackTop - 1)) * 128 + threadIdx.x];
-        const uint2 e = slot;
-        if (sp >= kStackTop) slot = stack[sp - kStackTop];
-        return e;
-    }
+    __device__ __forceinline__ void push(uint2 e) { stack[sp++] = e; }
+    __device__ __forceinline__ uint2 pop_one() { return stack[--sp]; }
 
     // Next stacked entry still nearer than the current hit; false when none.
     __device__ __forceinline__ bool pop() {

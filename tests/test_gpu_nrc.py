@@ -134,6 +134,19 @@ def test_inference_matches_emulation(cache):
     np.testing.assert_allclose(out, pred, rtol=2e-2, atol=1e-2)
 
 
+@pytest.mark.parametrize("rows", [1, 129, 256, 300, 5000])
+def test_inference_tile_pairs(cache, rows):
+    """The inference kernel runs 128-row tiles two at a time per warpgroup:
+    one row, a partial second tile, an exact pair, a partial pair and many
+    pairs all give the emulation's outputs."""
+    x, y = random_inputs(rows, 40 + rows)
+    out = cache.infer(x)
+    pred, _, _ = ref.forward_backward(cache.encode(x), cache.params(), y)
+    close = np.abs(out - pred) <= 1e-4 + 1e-4 * np.abs(pred)
+    assert close.mean() > 0.98
+    np.testing.assert_allclose(out, pred, rtol=2e-2, atol=1e-2)
+
+
 def test_adam_step_and_training_converges(cache):
     x, y = random_inputs(16384, 5)
     w0 = cache.params()
