@@ -357,9 +357,9 @@ def mlp_leg(rb, ctx, torch, dev, cache=None):
             "infer_frac": round(inf_tf / peak, 4), "train_step_ms_16384": round(1e3 * t_train, 4),
             "train_tflops": round(3 * 16384 * flops_row / t_train / 1e12, 2),
             "peak_tflops": peak, "flop_per_row_forward": flops_row,
-            "kernels": "inference and the training forward / backward: tcgen05.mma kind::f16 (bf16, FP32 "
-                       "accumulators in TMEM), M 128 N 64 K 16; weight gradients: tcgen05.mma kind::f16, "
-                       "MN-major operands, M 128 N 208/64, split-K over the batch rows"}
+            "kernels": "inference (two 128-row tiles per warpgroup), training forward and backward: tcgen05.mma "
+                       "kind::f16 (bf16, FP32 accumulators in TMEM), M 128 N 64 K 16; weight gradients: "
+                       "tcgen05.mma kind::f16, MN-major operands, M 128 N 208/64, split-K over the batch rows"}
 
 
 # Oracle (binary SAH BVH) node visits / triangle tests per ray over all
