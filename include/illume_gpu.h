@@ -105,6 +105,11 @@ typedef struct {
 /* Persistent schedule compiled for 8 resident blocks per SM (64 registers per
  * thread) instead of the compiler's register choice. */
 #define ILM_FLAG_HIGH_OCCUPANCY 4
+/* Persistent schedule: each idle lane tests its own claimed rays against the
+ * scene's root box instead of the whole warp testing each claimed chunk and
+ * pooling the rays that enter.  Only worth it when nearly every ray enters
+ * the scene (the answers are the same either way). */
+#define ILM_FLAG_LANE_REFILL 8
 
 typedef struct {
     int32_t width;             /* 2 (the reference's binary layout), 4 or 8 */

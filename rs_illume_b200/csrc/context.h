@@ -152,7 +152,7 @@ inline LaunchParams accel_launch(const ilm_context* ctx, const Accel* a) {
     const int persistent = a->schedule >= 0 ? (a->schedule == 0) : !(ctx->flags & ILM_FLAG_GRID_SCHEDULE);
     const int high_occ = a->high_occupancy >= 0 ? a->high_occupancy : (ctx->flags & ILM_FLAG_HIGH_OCCUPANCY) != 0;
     return LaunchParams{a->stack_depth > 0 ? a->stack_depth : ctx->stack_depth, ctx->block_size, ctx->max_iter,
-                        persistent, nullptr, high_occ ? 8 : 0};
+                        persistent, nullptr, high_occ ? 8 : 0, (ctx->flags & ILM_FLAG_LANE_REFILL) ? 0 : 1};
 }
 
 // ILM_FLAG_VALIDATE_RAYS on host rays: ILM_OK, or ILM_ERR_INVALID_ARGUMENT with

@@ -27,6 +27,9 @@ struct LaunchParams {
     int persistent;            // wide layouts: persistent schedule (needs `counter`)
     unsigned long long* counter;   // device work counter, private to the launch's stream
     int min_blocks;            // persistent kernel occupancy hint (8 = 64-register variant)
+    int root_pool;             // persistent schedule: claimed chunks tested against the root box by the
+                               // whole warp, entering rays pooled per warp (1), or each idle lane
+                               // testing its own claims (0)
 };
 
 // Everything a trace kernel reads, passed by value.

@@ -710,7 +710,8 @@ int32_t setup_render(ilm_context* ctx, PtScene& sc, uint32_t spp, uint32_t max_d
     unsigned long long* counter = ctx->counter_for(r.s);
     if (!counter) return ILM_ERR_OUT_OF_MEMORY;
     r.lp = LaunchParams{ctx->stack_depth, ctx->block_size, ctx->max_iter, 1, counter,
-                        (ctx->flags & ILM_FLAG_HIGH_OCCUPANCY) ? 8 : 0};
+                        (ctx->flags & ILM_FLAG_HIGH_OCCUPANCY) ? 8 : 0,
+                        0};   // path-queue rays almost all enter the scene: lanes refill one by one
     r.err = static_cast<uint32_t*>(ctx->err_word.ptr);
     int dev_sms = 148;
     cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, ctx->device);

@@ -100,4 +100,13 @@ __device__ __forceinline__ bool box_intersect_p(float minx, float miny, float mi
     return (t_min < tmax) && (t_max > 0.0f);
 }
 
+// The root box test a tracer's enters() performs (Bounds3::intersect_p on the
+// world bound with the ray's own tmax), for rays not yet in a tracer.
+__device__ __forceinline__ bool root_enters(const RayIn& r, const float* b) {
+    const float ix = __frcp_rn(r.dx), iy = __frcp_rn(r.dy), iz = __frcp_rn(r.dz);   // == 1/d exactly
+    return box_intersect_p(b[0], b[1], b[2], b[3], b[4], b[5], r, ix, iy, iz, ix < 0.0f, iy < 0.0f, iz < 0.0f,
+                           r.tmax);
+}
+
+
 }  // namespace ilm

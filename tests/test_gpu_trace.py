@@ -152,6 +152,38 @@ def test_bench_launch_full_size_against_oracle(incoherent):
     ctx.close()
 
 
+@pytest.mark.parametrize("width,n", [(8, 1000003), (4, 600001), (8, 40000)])
+def test_pooled_lane_refill_and_grid_schedules_agree(incoherent, width, n):
+    """Device buffers: the persistent schedule with warp-filtered chunks and a
+    per-warp pool (the default), with per-lane refill, and one thread per
+    ray give byte-identical records for closest and any hit.  The counts are
+    not multiples of a chunk, and 40,000 rays is a short queue (one ray per
+    lane per claim).  Outputs start as a fill pattern, so a ray handed out
+    twice or never would show."""
+    import torch
+    xyz, idx, rays, sc = incoherent
+    half = len(rays) // 2                                       # closest (tmax = inf) and shadow rays mixed
+    sub = np.ascontiguousarray(np.concatenate([rays[:n // 2], rays[half:half + n - n // 2]]))
+    d_rays = torch.from_numpy(sub.view(np.uint8)).cuda()
+    out = []
+    for kw in ({"high_occupancy": True}, {"high_occupancy": True, "lane_refill": True}, {"grid_schedule": True}):
+        ctx = rb.Context(0, **kw)
+        acc = rb.GpuBVHAccel(ctx, [rb.TriangleMesh(ctx, xyz, idx)], width=width)
+        d_hits = torch.full((n * 16,), 0xAB, dtype=torch.uint8, device="cuda")
+        d_occ = torch.full((n * 4,), 0xAB, dtype=torch.uint8, device="cuda")
+        acc.intersect_batch(d_rays, d_hits)
+        acc.intersect_p_batch(d_rays, d_occ)
+        torch.cuda.synchronize()
+        out.append((d_hits.cpu().numpy().tobytes(), d_occ.cpu().numpy().tobytes()))
+        assert ctx.device_errors() == 0
+        ctx.close()
+    assert out[0] == out[1] == out[2]
+    assert np.all(np.frombuffer(out[0][1], np.uint32) <= 1)
+    pick = np.sort(np.random.default_rng(n).choice(n, 20000, replace=False))
+    g = np.frombuffer(out[0][0], HIT_DTYPE)[pick]
+    compare_closest(g, sc.intersect(np.ascontiguousarray(sub[pick])), label="pooled")
+
+
 @pytest.mark.parametrize("width", [4, 8])
 def test_persistent_and_grid_schedules_agree(incoherent, width):
     """The persistent schedule (work counter, lane refill) and one thread per
