@@ -75,44 +75,67 @@ __device__ __forceinline__ TraceArgs args_of(const BatchTable& t, uint32_t b) {
     return a;
 }
 
+// Rays are claimed from the concatenation 64 at a time.  The whole warp
+// tests each claimed chunk against the root boxes of the rays' scenes (two
+// rays per lane), answers the misses at full width and keeps the rays that
+// enter in a per-warp pool in shared memory, from which idle lanes take rays
+// (the single-scene kernel's kPool schedule).
 template <int W, int kStack, bool kAny, bool kAnalytic>
 __global__ void __launch_bounds__(128, 8) k_trace_batched(BatchTable tab) {
     const unsigned lane = threadIdx.x & 31u;
     const unsigned below = (1u << lane) - 1u;
+    __shared__ uint32_t s_pool[4][kChunk];              // per warp: offsets of the pooled rays in their chunk
+    uint32_t* pool = s_pool[threadIdx.x >> 5];
+    unsigned pool_n = 0;                                // warp-uniform
+    unsigned long long pool_base = 0;                   // warp-uniform
     WideTracer<W, kStack, kAny, kAnalytic> T;
     TraceArgs a;
     bool active = false;
     uint64_t id = 0;
-    unsigned long long chunk_next = 0, chunk_end = 0;   // warp-uniform
     bool exhausted = false;                             // warp-uniform
     const unsigned long long n = tab.total;
     for (;;) {
         unsigned need = __ballot_sync(0xFFFFFFFFu, !active);
-        while (need != 0u && !exhausted) {
-            if (chunk_next == chunk_end) {
+        while (need != 0u) {
+            if (pool_n == 0) {
+                if (exhausted) break;
                 unsigned long long b = 0;
                 if (lane == 0) b = atomicAdd(tab.counter, (unsigned long long)kChunk);
                 b = __shfl_sync(0xFFFFFFFFu, b, 0);
                 if (b >= n) { exhausted = true; break; }
-                chunk_next = b;
-                chunk_end = b + kChunk < n ? b + kChunk : n;
+                for (unsigned k = 0; k < kChunk; k += 32u) {
+                    const unsigned long long g = b + k + lane;
+                    bool enter = false;
+                    if (g < n) {
+                        const BatchEntry& e = tab.entries[find_batch(tab, g)];
+                        const uint64_t rid = g - e.first;
+                        const RayIn r = load_ray(e.rays, rid);
+                        enter = e.n_nodes != 0 && root_enters(r, e.bound);
+                        if (!enter) write_miss(rid, r, e.hits, e.occ);
+                    }
+                    const unsigned m = __ballot_sync(0xFFFFFFFFu, enter);
+                    if (enter) pool[pool_n + __popc(m & below)] = k + lane;
+                    pool_n += __popc(m);
+                }
+                __syncwarp();
+                pool_base = b;
+                continue;
             }
-            unsigned avail = (unsigned)(chunk_end - chunk_next);
-            unsigned rank = __popc(need & below);
-            if (((need >> lane) & 1u) && rank < avail) {
-                unsigned long long g = chunk_next + rank;
-                uint32_t b = find_batch(tab, g);
-                a = args_of(tab, b);
-                id = g - tab.entries[b].first;
-                RayIn r = load_ray(a.rays, id);
-                T.init(r);
-                if (a.n_nodes != 0 && T.enters(a.bound)) active = true;
-                else write_miss(id, r, a.hits, a.occ);
+            const unsigned rank = __popc(need & below);
+            const unsigned take = min((unsigned)__popc(need), pool_n);
+            if (((need >> lane) & 1u) && rank < take) {
+                const unsigned long long g = pool_base + pool[pool_n - 1u - rank];
+                const uint32_t bi = find_batch(tab, g);
+                a = args_of(tab, bi);
+                id = g - tab.entries[bi].first;
+                T.init(load_ray(a.rays, id));
+                active = true;
             }
-            chunk_next += min((unsigned)__popc(need), avail);
+            pool_n -= take;
+            __syncwarp();
             need = __ballot_sync(0xFFFFFFFFu, !active);
         }
-        if (!__any_sync(0xFFFFFFFFu, active)) break;   // only reached once exhausted
+        if (!__any_sync(0xFFFFFFFFu, active)) break;   // only once exhausted with an empty pool
         if (active && T.step(a)) {
             T.write(id, a);
             active = false;

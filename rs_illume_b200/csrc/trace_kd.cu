@@ -154,7 +154,10 @@ __global__ void __launch_bounds__(kKdBlock) k_trace_kd(TraceArgs a) {
     T.write(i, a);
 }
 
-template <bool kAny, int kMinBlocks, bool kAnalytic>
+// kPool: as in the wide kernel, the whole warp tests each claimed chunk
+// against the tree's bound and pools the rays that enter (true), or each
+// idle lane tests its own claims (false).
+template <bool kAny, int kMinBlocks, bool kAnalytic, bool kPool>
 __global__ void __launch_bounds__(kKdBlock, kMinBlocks) k_trace_kd_persistent(TraceArgs a) {
     const uint64_t n = ray_count(a);
     const unsigned chunk = n < 2ull * gridDim.x * blockDim.x ? 32u : kChunk;
@@ -163,8 +166,59 @@ __global__ void __launch_bounds__(kKdBlock, kMinBlocks) k_trace_kd_persistent(Tr
     KdTracer<kAny, kAnalytic> T;
     bool active = false;
     uint64_t id = 0;
-    unsigned long long chunk_next = 0, chunk_end = 0;   // warp-uniform
     bool exhausted = false;                             // warp-uniform
+    if constexpr (kPool) {
+        __shared__ uint32_t s_pool[kKdBlock / 32][kChunk];   // per warp: offsets of the pooled rays
+        uint32_t* pool = s_pool[threadIdx.x >> 5];
+        unsigned pool_n = 0;                            // warp-uniform
+        unsigned long long pool_base = 0;               // warp-uniform
+        for (;;) {
+            unsigned need = __ballot_sync(0xFFFFFFFFu, !active);
+            while (need != 0u) {
+                if (pool_n == 0) {
+                    if (exhausted) break;
+                    unsigned long long b = 0;
+                    if (lane == 0) b = atomicAdd(a.counter, (unsigned long long)chunk);
+                    b = __shfl_sync(0xFFFFFFFFu, b, 0);
+                    if (b >= n) { exhausted = true; break; }
+                    for (unsigned k = 0; k < chunk; k += 32u) {
+                        const uint64_t rid = b + k + lane;
+                        bool enter = false;
+                        if (rid < n) {
+                            const RayIn r = load_ray(a.rays, rid);
+                            KdTracer<kAny, kAnalytic> probe;
+                            probe.init(r);
+                            enter = a.n_nodes != 0 && probe.enters(a.bound);
+                            if (!enter) write_miss(rid, r, a.hits, a.occ);
+                        }
+                        const unsigned m = __ballot_sync(0xFFFFFFFFu, enter);
+                        if (enter) pool[pool_n + __popc(m & below)] = k + lane;
+                        pool_n += __popc(m);
+                    }
+                    __syncwarp();
+                    pool_base = b;
+                    continue;
+                }
+                const unsigned rank = __popc(need & below);
+                const unsigned take = min((unsigned)__popc(need), pool_n);
+                if (((need >> lane) & 1u) && rank < take) {
+                    id = pool_base + pool[pool_n - 1u - rank];
+                    T.init(load_ray(a.rays, id));
+                    active = T.enters(a.bound);   // true: the probe passed; sets the clip range
+                }
+                pool_n -= take;
+                __syncwarp();
+                need = __ballot_sync(0xFFFFFFFFu, !active);
+            }
+            if (!__any_sync(0xFFFFFFFFu, active)) break;
+            if (active && T.step(a)) {
+                T.write(id, a);
+                active = false;
+            }
+        }
+        return;
+    }
+    unsigned long long chunk_next = 0, chunk_end = 0;   // warp-uniform
     for (;;) {
         unsigned need = __ballot_sync(0xFFFFFFFFu, !active);
         // Hand rays to idle lanes; rays missing the tree's bound are answered
@@ -198,11 +252,11 @@ __global__ void __launch_bounds__(kKdBlock, kMinBlocks) k_trace_kd_persistent(Tr
     }
 }
 
-template <int kMinBlocks, bool kAnalytic>
+template <int kMinBlocks, bool kAnalytic, bool kPool>
 cudaError_t launch_persistent(const TraceArgs& t, cudaStream_t s) {
     const unsigned block = kKdBlock;
-    auto kc = k_trace_kd_persistent<false, kMinBlocks, kAnalytic>;
-    auto ka = k_trace_kd_persistent<true, kMinBlocks, kAnalytic>;
+    auto kc = k_trace_kd_persistent<false, kMinBlocks, kAnalytic, kPool>;
+    auto ka = k_trace_kd_persistent<true, kMinBlocks, kAnalytic, kPool>;
     uint64_t grid = resident_blocks(t.occ ? (const void*)ka : (const void*)kc, (int)block);
     if (grid == 0) return cudaErrorInvalidConfiguration;
     const uint64_t need_blocks = (t.n + block - 1) / block;
@@ -216,8 +270,13 @@ cudaError_t launch_persistent(const TraceArgs& t, cudaStream_t s) {
 
 template <bool kAnalytic>
 cudaError_t launch_kd(const TraceArgs& t, const LaunchParams& lp, cudaStream_t s) {
-    if (lp.persistent && t.counter)
-        return lp.min_blocks >= 8 ? launch_persistent<8, kAnalytic>(t, s) : launch_persistent<1, kAnalytic>(t, s);
+    if (lp.persistent && t.counter) {
+        if (lp.root_pool)
+            return lp.min_blocks >= 8 ? launch_persistent<8, kAnalytic, true>(t, s)
+                                      : launch_persistent<1, kAnalytic, true>(t, s);
+        return lp.min_blocks >= 8 ? launch_persistent<8, kAnalytic, false>(t, s)
+                                  : launch_persistent<1, kAnalytic, false>(t, s);
+    }
     const unsigned block = kKdBlock;
     unsigned grid = (unsigned)((t.n + block - 1) / block);
     if (t.occ) k_trace_kd<true, kAnalytic><<<grid, block, 0, s>>>(t);
