@@ -88,7 +88,9 @@ __global__ void __launch_bounds__(128, 8) k_trace_batched(BatchTable tab) {
     uint32_t* pool = s_pool[threadIdx.x >> 5];
     unsigned pool_n = 0;                                // warp-uniform
     unsigned long long pool_base = 0;                   // warp-uniform
-    WideTracer<W, kStack, kAny, kAnalytic> T;
+    using Tracer = WideTracer<W, kStack, kAny, kAnalytic>;
+    typename Tracer::Entry stk[Tracer::kDepth];
+    Tracer T(stk);
     TraceArgs a;
     bool active = false;
     uint64_t id = 0;

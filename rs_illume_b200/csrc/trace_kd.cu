@@ -60,7 +60,10 @@ struct KdTracer {
     int sp;
     bool tr_ready, occluded;
     TriRay tr;
-    uint2 stack[kKdMaxDepth];        // (node, t_min bits)
+    uint2* stack;                    // (node, t_min bits): the launching kernel's array of kKdMaxDepth
+
+    // The stack stays outside the struct, for the reason WideTracerSorted's does.
+    __device__ __forceinline__ explicit KdTracer(uint2* s) : stack(s) {}
 
     __device__ __forceinline__ void init(const RayIn& r) {
         ray = r;
@@ -147,7 +150,8 @@ __global__ void __launch_bounds__(kKdBlock) k_trace_kd(TraceArgs a) {
     uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= ray_count(a)) return;
     RayIn r = load_ray(a.rays, i);
-    KdTracer<kAny, kAnalytic> T;
+    uint2 stk[kKdMaxDepth];
+    KdTracer<kAny, kAnalytic> T(stk);
     T.init(r);
     if (a.n_nodes == 0 || !T.enters(a.bound)) { write_miss(i, r, a.hits, a.occ); return; }
     while (!T.step(a)) {}
@@ -163,7 +167,8 @@ __global__ void __launch_bounds__(kKdBlock, kMinBlocks) k_trace_kd_persistent(Tr
     const unsigned chunk = n < 2ull * gridDim.x * blockDim.x ? 32u : kChunk;
     const unsigned lane = threadIdx.x & 31u;
     const unsigned below = (1u << lane) - 1u;
-    KdTracer<kAny, kAnalytic> T;
+    uint2 stk[kKdMaxDepth];
+    KdTracer<kAny, kAnalytic> T(stk);
     bool active = false;
     uint64_t id = 0;
     bool exhausted = false;                             // warp-uniform
@@ -186,7 +191,7 @@ __global__ void __launch_bounds__(kKdBlock, kMinBlocks) k_trace_kd_persistent(Tr
                         bool enter = false;
                         if (rid < n) {
                             const RayIn r = load_ray(a.rays, rid);
-                            KdTracer<kAny, kAnalytic> probe;
+                            KdTracer<kAny, kAnalytic> probe(nullptr);   // root clip only: no stack
                             probe.init(r);
                             enter = a.n_nodes != 0 && probe.enters(a.bound);
                             if (!enter) write_miss(rid, r, a.hits, a.occ);

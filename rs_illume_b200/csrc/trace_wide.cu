@@ -22,7 +22,9 @@ __global__ void __launch_bounds__(128) k_trace_wide(TraceArgs a) {
     uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= ray_count(a)) return;
     RayIn r = load_ray(a.rays, i);
-    WideTracer<W, kStack, kAny, kAnalytic> T;
+    using Tracer = WideTracer<W, kStack, kAny, kAnalytic>;
+    typename Tracer::Entry stk[Tracer::kDepth];
+    Tracer T(stk);
     T.init(r);
     if (a.n_nodes == 0 || !T.enters(a.bound)) { write_miss(i, r, a.hits, a.occ); return; }
     while (!T.step(a)) {}
@@ -50,7 +52,9 @@ __global__ void __launch_bounds__(128, kMinBlocks) k_trace_wide_persistent(Trace
     const unsigned chunk = n < 2ull * gridDim.x * blockDim.x ? 32u : kChunk;
     const unsigned lane = threadIdx.x & 31u;
     const unsigned below = (1u << lane) - 1u;
-    WideTracer<W, kStack, kAny, kAnalytic> T;
+    using Tracer = WideTracer<W, kStack, kAny, kAnalytic>;
+    typename Tracer::Entry stk[Tracer::kDepth];
+    Tracer T(stk);
     bool active = false;
     uint64_t id = 0;
     bool exhausted = false;                             // warp-uniform

@@ -128,8 +128,16 @@ __device__ __forceinline__ void sort_keys(uint32_t* k) {
 // Per-lane traversal state of one ray over 4- or 8-wide nodes: hit children
 // sorted by entry distance and pushed far-to-near, one stack entry (node or
 // leaf, with its entry distance) per child.
+//
+// The stack is a local array of the launching kernel (Entry stk[kDepth]),
+// handed to the constructor, never a member: a struct that holds a
+// dynamically indexed array is kept whole in local memory, and every scalar
+// of the traversal state (ray, current node, best hit) would be loaded from
+// and stored to local memory at each step beside it.
 template <int W, int kStack, bool kAny, bool kAnalytic = true>
 struct WideTracerSorted {
+    using Entry = uint2;
+    static constexpr int kDepth = kStack;
     RayIn ray;
     float ix, iy, iz;
     bool negx, negy, negz, tr_ready, occluded;
@@ -137,7 +145,9 @@ struct WideTracerSorted {
     float best_t, bu, bv;
     uint32_t best, status, cur, iter;
     int sp;
-    uint2 stack[kStack];
+    uint2* stack;
+
+    __device__ __forceinline__ explicit WideTracerSorted(uint2* s) : stack(s) {}
 
     __device__ __forceinline__ void init(const RayIn& r) {
         ray = r;
@@ -257,9 +267,12 @@ struct WideTracerSorted {
 // BVHAccel::intersect / intersect_p (bvh.rs:563-662, the far child pushed on
 // both branches), one node visit per step, exactly as k_trace_bin runs it, so
 // the records (and which rays reach a limit) are the same.  The stack has the
-// reference's 64 entries (bvh.rs:573) whatever the caller's depth.
+// reference's 64 entries (bvh.rs:573) whatever the caller's depth; like
+// WideTracerSorted's, it is the launching kernel's array.
 template <bool kAny, bool kAnalytic = true>
 struct BinTracer {
+    using Entry = uint32_t;
+    static constexpr int kDepth = 64;
     RayIn ray;
     float ix, iy, iz;
     bool negx, negy, negz, tr_ready, occluded;
@@ -267,7 +280,9 @@ struct BinTracer {
     float best_t, bu, bv;
     uint32_t best, status, cur, iter;
     int sp;
-    uint32_t stack[64];
+    uint32_t* stack;
+
+    __device__ __forceinline__ explicit BinTracer(uint32_t* s) : stack(s) {}
 
     __device__ __forceinline__ void init(const RayIn& r) {
         ray = r;
