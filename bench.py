@@ -68,7 +68,7 @@ BYTES_PER_RAY_ANY = 32 + 4 + 32 * N_NODE_ANY + 36 * N_TRI_ANY
 # (width, schedule, occupancy, stack depth): dram__bytes_read.sum +
 # dram__bytes_write.sum from an ncu capture of one timed launch after three
 # warm-ups (a constant of that capture, not measured by this script).
-DRAM_TRAFFIC = {(8, "persistent", "high", 64): 208514560}
+DRAM_TRAFFIC = {(8, "persistent", "high", 64): 219392256}
 TRAFFIC_SOURCE = "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch (captured constant)"
 WORKLOAD = ("incoherent closest-hit: displaced icosphere level 8 (1,310,720 tris, seed 2), "
             "2,097,152 closest rays of 4,194,304 ball rays (radius 3, uniform directions)")

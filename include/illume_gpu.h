@@ -110,6 +110,13 @@ typedef struct {
  * pooling the rays that enter.  Only worth it when nearly every ray enters
  * the scene (the answers are the same either way). */
 #define ILM_FLAG_LANE_REFILL 8
+/* Pooled persistent schedule: once every ray of the query has been claimed,
+ * idle lanes no longer help their warp's unfinished rays by taking subtrees
+ * from their traversal stacks (the split tail, on by default; the answers are
+ * the same either way).  The split tail is also off whenever max_iterations
+ * is below its default of 2^20, so that which rays reach a lowered cap does
+ * not depend on which lanes traversed them. */
+#define ILM_FLAG_NO_TAIL_SPLIT 16
 
 typedef struct {
     int32_t width;             /* 2 (the reference's binary layout), 4 or 8 */

@@ -26,6 +26,7 @@ ILM_FLAG_VALIDATE_RAYS = 1
 ILM_FLAG_GRID_SCHEDULE = 2
 ILM_FLAG_HIGH_OCCUPANCY = 4
 ILM_FLAG_LANE_REFILL = 8
+ILM_FLAG_NO_TAIL_SPLIT = 16
 ILM_MISS = 0xFFFFFFFF
 # cudaStreamLegacy: the explicit handle of the legacy default stream (a NULL
 # stream argument selects the context's own stream instead)

@@ -106,7 +106,7 @@ struct ilm_context {
     int stack_depth = 64;
     int block_size = 128;
     int flags = 0;
-    uint32_t max_iter = 1u << 20;
+    uint32_t max_iter = 1u << 20;   // kDefaultMaxIter
     cudaStream_t stream = nullptr;
     cudaStream_t pipe[ilm::kPipeStreams] = {nullptr, nullptr};
     cudaEvent_t fence = nullptr;
@@ -145,14 +145,24 @@ int32_t cuda_fail(ilm_context* ctx, cudaError_t e, const char* what);
 PtrKind classify(const void* p);
 Accel* find_accel(ilm_context* ctx, ilm_accel_id id);
 
+// Default per-ray traversal loop cap (ilm_config.max_iterations = 0).
+constexpr uint32_t kDefaultMaxIter = 1u << 20;
+
+// Whether the pooled persistent schedule splits its tail (ILM_FLAG_NO_TAIL_SPLIT).
+inline int split_tail_of(const ilm_context* ctx) {
+    return !(ctx->flags & ILM_FLAG_NO_TAIL_SPLIT) && ctx->max_iter >= kDefaultMaxIter;
+}
+
 // Launch choices of a query on accel `a`: the accel's own (ilm_accel_set_launch,
 // ilm_autotune) where it has them, else the context's.  The work counter is
 // left null for the caller to supply.
 inline LaunchParams accel_launch(const ilm_context* ctx, const Accel* a) {
     const int persistent = a->schedule >= 0 ? (a->schedule == 0) : !(ctx->flags & ILM_FLAG_GRID_SCHEDULE);
     const int high_occ = a->high_occupancy >= 0 ? a->high_occupancy : (ctx->flags & ILM_FLAG_HIGH_OCCUPANCY) != 0;
-    return LaunchParams{a->stack_depth > 0 ? a->stack_depth : ctx->stack_depth, ctx->block_size, ctx->max_iter,
-                        persistent, nullptr, high_occ ? 8 : 0, (ctx->flags & ILM_FLAG_LANE_REFILL) ? 0 : 1};
+    LaunchParams lp{a->stack_depth > 0 ? a->stack_depth : ctx->stack_depth, ctx->block_size, ctx->max_iter,
+                    persistent, nullptr, high_occ ? 8 : 0, (ctx->flags & ILM_FLAG_LANE_REFILL) ? 0 : 1};
+    lp.split_tail = split_tail_of(ctx);
+    return lp;
 }
 
 // ILM_FLAG_VALIDATE_RAYS on host rays: ILM_OK, or ILM_ERR_INVALID_ARGUMENT with

@@ -30,6 +30,8 @@ struct LaunchParams {
     int root_pool;             // persistent schedule: claimed chunks tested against the root box by the
                                // whole warp, entering rays pooled per warp (1), or each idle lane
                                // testing its own claims (0)
+    int split_tail = 0;        // pooled persistent schedule: once the work counter has run out, idle
+                               // lanes take stacked subtrees of their warp's unfinished rays
 };
 
 // Everything a trace kernel reads, passed by value.
@@ -48,6 +50,7 @@ struct TraceArgs {
     unsigned long long* counter;       // persistent-schedule work counter
     float bound[6];
     const uint32_t* kd_index;          // kd-tree leaf runs
+    uint32_t split_tail = 0;           // LaunchParams::split_tail
 };
 
 // occ == nullptr: closest hit into `hits`; otherwise any-hit into `occ`.

@@ -50,6 +50,7 @@ cudaError_t launch_trace(const DeviceAccel& a, const ilm_ray* rays, uint64_t n, 
     t.counter = lp.counter;
     for (int k = 0; k < 6; ++k) t.bound[k] = a.bound[k];
     t.kd_index = a.kd_index;
+    t.split_tail = lp.split_tail ? 1u : 0u;
     if (a.width == kLayoutKdTree) return launch_trace_kd(t, lp, s);
     if (a.width == 2) return launch_trace_binary(t, s);
     return launch_trace_wide(a.width, t, lp, s);

@@ -55,59 +55,82 @@ __global__ void __launch_bounds__(128, kMinBlocks) k_trace_wide_persistent(Trace
     using Tracer = WideTracer<W, kStack, kAny, kAnalytic>;
     typename Tracer::Entry stk[Tracer::kDepth];
     Tracer T(stk);
-    bool active = false;
-    uint64_t id = 0;
     bool exhausted = false;                             // warp-uniform
     if constexpr (kPool) {
-        __shared__ uint32_t s_pool[4][kChunk];          // per warp: offsets of the pooled rays in their chunk
-        uint32_t* pool = s_pool[threadIdx.x >> 5];
+        __shared__ __align__(16) uint32_t s_warp[4][kWarpWords];
+        uint32_t* warp_words = s_warp[threadIdx.x >> 5];
+        uint32_t* pool = warp_words;                    // offsets of the pooled rays in their chunk
+        uint32_t* ids = warp_words + kPoolWords;        // each lane's ray id (owners)
         unsigned pool_n = 0;                            // warp-uniform
         unsigned long long pool_base = 0;               // warp-uniform: the pooled rays' chunk
+        uint32_t st = kFree | (lane << 2);
         for (;;) {
-            unsigned need = __ballot_sync(0xFFFFFFFFu, !active);
-            // Every pass either hands out pooled rays or claims and filters a
-            // chunk (claims are only made with an empty pool), so the loop ends.
-            while (need != 0u) {
-                if (pool_n == 0) {
-                    if (exhausted) break;
-                    unsigned long long b = 0;
-                    if (lane == 0) b = atomicAdd(a.counter, (unsigned long long)chunk);
-                    b = __shfl_sync(0xFFFFFFFFu, b, 0);
-                    if (b >= n) { exhausted = true; break; }
-                    for (unsigned k = 0; k < chunk; k += 32u) {
-                        const uint64_t rid = b + k + lane;
-                        bool enter = false;
-                        if (rid < n) {
-                            const RayIn r = load_ray(a.rays, rid);
-                            enter = a.n_nodes != 0 && root_enters(r, a.bound);
-                            if (!enter) write_miss(rid, r, a.hits, a.occ);
+            if (!exhausted) {
+                unsigned need = __ballot_sync(0xFFFFFFFFu, role_of(st) == kFree);
+                // Every pass either hands out pooled rays or claims and filters
+                // a chunk (claims are only made with an empty pool), so the
+                // loop ends.
+                while (need != 0u) {
+                    if (pool_n == 0) {
+                        unsigned long long b = 0;
+                        if (lane == 0) b = atomicAdd(a.counter, (unsigned long long)chunk);
+                        b = __shfl_sync(0xFFFFFFFFu, b, 0);
+                        if (b >= n) { exhausted = true; break; }
+                        for (unsigned k = 0; k < chunk; k += 32u) {
+                            const uint64_t rid = b + k + lane;
+                            bool enter = false;
+                            if (rid < n) {
+                                const RayIn r = load_ray(a.rays, rid);
+                                enter = a.n_nodes != 0 && root_enters(r, a.bound);
+                                if (!enter) write_miss(rid, r, a.hits, a.occ);
+                            }
+                            const unsigned m = __ballot_sync(0xFFFFFFFFu, enter);
+                            if (enter) pool[pool_n + __popc(m & below)] = k + lane;
+                            pool_n += __popc(m);
                         }
-                        const unsigned m = __ballot_sync(0xFFFFFFFFu, enter);
-                        if (enter) pool[pool_n + __popc(m & below)] = k + lane;
-                        pool_n += __popc(m);
+                        __syncwarp();
+                        pool_base = b;
+                        continue;
                     }
+                    const unsigned rank = __popc(need & below);
+                    const unsigned take = min((unsigned)__popc(need), pool_n);
+                    if (((need >> lane) & 1u) && rank < take) {
+                        const uint64_t id = pool_base + pool[pool_n - 1u - rank];
+                        ids[2 * lane] = (uint32_t)id;
+                        ids[2 * lane + 1] = (uint32_t)(id >> 32);
+                        T.init(load_ray(a.rays, id));
+                        st = kOwner | (lane << 2);
+                    }
+                    pool_n -= take;
                     __syncwarp();
-                    pool_base = b;
-                    continue;
+                    need = __ballot_sync(0xFFFFFFFFu, role_of(st) == kFree);
                 }
-                const unsigned rank = __popc(need & below);
-                const unsigned take = min((unsigned)__popc(need), pool_n);
-                if (((need >> lane) & 1u) && rank < take) {
-                    id = pool_base + pool[pool_n - 1u - rank];
-                    T.init(load_ray(a.rays, id));
-                    active = true;
-                }
-                pool_n -= take;
-                __syncwarp();
-                need = __ballot_sync(0xFFFFFFFFu, !active);
             }
-            if (!__any_sync(0xFFFFFFFFu, active)) break;   // only once exhausted with an empty pool
-            if (active && T.step(a)) {
-                T.write(id, a);
-                active = false;
+            // A helper of an occluded any-hit ray has nothing left to find.
+            bool owner_occluded = kAny && __shfl_sync(0xFFFFFFFFu, (int)T.occluded, owner_of(st));
+            if (exhausted && a.split_tail) {
+                share_subtrees<Tracer, kAny>(T, st, owner_occluded, warp_words);
+                // Lanes that just took a subtree have a new owner.
+                if (kAny) owner_occluded = __shfl_sync(0xFFFFFFFFu, (int)T.occluded, owner_of(st));
+            }
+            if (!__any_sync(0xFFFFFFFFu, role_of(st) != kFree)) break;   // only once exhausted
+            const uint32_t role = role_of(st);
+            bool done = false;
+            // An any-hit ray one of its helpers found occluded is finished.
+            if ((role == kOwner || role == kHelper) && owner_occluded) done = true;
+            else if (role == kOwner || role == kHelper) done = T.step(a);
+            const unsigned fin = __ballot_sync(0xFFFFFFFFu, role == kHelper && done);
+            if (fin) merge_helpers<Tracer, kAny>(T, st, fin);
+            if (role == kHelper && done) st = kFree | (lane << 2);
+            if (role == kOwner && done) st = (st & ~3u) | kWaiting;
+            if (role_of(st) == kWaiting && (st >> 8) == 0u) {
+                T.write((uint64_t)ids[2 * lane] | ((uint64_t)ids[2 * lane + 1] << 32), a);
+                st = kFree | (lane << 2);
             }
         }
     } else {
+        bool active = false;
+        uint64_t id = 0;
         unsigned long long chunk_next = 0, chunk_end = 0;   // warp-uniform
         for (;;) {
             unsigned need = __ballot_sync(0xFFFFFFFFu, !active);

@@ -167,6 +167,21 @@ struct WideTracerSorted {
         return box_intersect_p(b[0], b[1], b[2], b[3], b[4], b[5], ray, ix, iy, iz, negx, negy, negz, ray.tmax);
     }
 
+    // Starts on subtree `node` of a ray another lane is tracing, with that
+    // lane's reciprocal directions and `bound` (its best distance so far) as
+    // the limit; the hit found, if any, is this lane's own.
+    __device__ __forceinline__ void adopt(const RayIn& r, float rx, float ry, float rz, float bound, uint32_t node) {
+        ray = r;
+        ix = rx; iy = ry; iz = rz;
+        negx = ix < 0.0f; negy = iy < 0.0f; negz = iz < 0.0f;
+        best_t = bound; bu = 0.0f; bv = 0.0f;
+        best = ILM_MISS;
+        occluded = false;
+        status = 0;
+        tr_ready = false;
+        cur = node; iter = 0; sp = 0;
+    }
+
     __device__ __forceinline__ void push(uint2 e) { stack[sp++] = e; }
     __device__ __forceinline__ uint2 pop_one() { return stack[--sp]; }
 
@@ -359,6 +374,126 @@ template <int kStack, bool kAny, bool kAnalytic>
 struct TracerOf<2, kStack, kAny, kAnalytic> { using type = BinTracer<kAny, kAnalytic>; };
 template <int W, int kStack, bool kAny, bool kAnalytic = true>
 using WideTracer = typename TracerOf<W, kStack, kAny, kAnalytic>::type;
+
+// Split tail of the pooled persistent schedule (k_trace_wide_persistent).
+// Once the work counter has run out, a warp's last rays finish with its idle
+// lanes helping them; without help the launch lasts as long as its longest
+// rays, which make ten times the median number of node visits.  A ray's lane
+// (its owner) keeps traversing; each pass, every idle lane takes the top stack
+// entry of a lane that has one (owner or helper) and traverses that subtree
+// with a copy of the ray, bounded by the donor's best distance so far.  A
+// helper that finishes hands its best hit to the owner, which keeps the
+// smaller (t, primitive id), the tie rule of every traversal here: the nearest
+// hit is the nearest whichever lane tests it, and culling only skips subtrees
+// that cannot hold a nearer hit, so the records are the lone traversal's --
+// except that of two hits at exactly the same t the split keeps the smaller
+// primitive id where the lone traversal may keep the first it found.  Any-hit
+// owners stop at the first occlusion any of their lanes finds, and their
+// helpers stop with them.  An owner writes its record once its own traversal
+// and all its helpers are done.  Nothing waits on another warp; every lane's
+// traversal is bounded by the iteration cap.
+//
+// Lane roles, packed with the owner lane (bits 2-6) and an owner's count of
+// helpers (bits 8-13) in one word.
+enum : uint32_t { kFree = 0, kOwner = 1, kWaiting = 2, kHelper = 3 };
+__device__ __forceinline__ uint32_t role_of(uint32_t st) { return st & 3u; }
+__device__ __forceinline__ uint32_t owner_of(uint32_t st) { return (st >> 2) & 31u; }
+
+// A staged subtree the donor's own pop would have culled (no node or leaf
+// entry has all bits set: that would be a leaf of 8 records at 2^28 - 1).
+constexpr uint32_t kNoEntry = 0xFFFFFFFFu;
+
+// Words of the per-warp shared area of the pooled schedule: the pool of
+// entering rays' offsets, each lane's ray id, 16 staging slots of 12 words
+// for handed-over subtrees and their z reciprocals.
+constexpr int kPoolWords = 64;
+constexpr int kIdWords = 64;
+constexpr int kSplitSlots = 16;
+constexpr int kWarpWords = kPoolWords + kIdWords + kSplitSlots * 13;
+
+// Idle lanes take stacked subtrees: the j-th lane holding an entry stages its
+// top entry (with the ray, its reciprocals, its best distance and its owner)
+// in slot j, and the j-th idle lane adopts slot j.  Helpers first lower their
+// bound to their owner's best distance when that is nearer.
+template <class Tracer, bool kAny>
+__device__ __forceinline__ void share_subtrees(Tracer& T, uint32_t& st, bool owner_occluded, uint32_t* warp_words) {
+    const unsigned lane = threadIdx.x & 31u;
+    if (!kAny) {
+        const float ob = __shfl_sync(0xFFFFFFFFu, T.best_t, owner_of(st));
+        if (role_of(st) == kHelper && ob < T.best_t) { T.best_t = ob; T.best = ILM_MISS; }
+    }
+    const uint32_t role = role_of(st);
+    const unsigned idle = __ballot_sync(0xFFFFFFFFu, role == kFree);
+    const unsigned don = __ballot_sync(0xFFFFFFFFu, (role == kOwner || role == kHelper) && T.sp > 0 &&
+                                                        !T.status && !(kAny && owner_occluded));
+    const unsigned pairs = min(__popc(idle), __popc(don));
+    if (pairs == 0u) return;
+    const unsigned below = (1u << lane) - 1u;
+    const unsigned irank = __popc(idle & below), drank = __popc(don & below);
+    uint4* stage = reinterpret_cast<uint4*>(warp_words + kPoolWords + kIdWords);
+    uint32_t* stage_iz = warp_words + kPoolWords + kIdWords + kSplitSlots * 12;
+    if (((don >> lane) & 1u) && drank < pairs) {
+        const uint2 e = T.pop_one();
+        const bool live = kAny || __uint_as_float(e.y) < T.best_t;
+        stage[3 * drank] = make_uint4(live ? e.x : kNoEntry, __float_as_uint(T.ray.tmax),
+                                      __float_as_uint(T.best_t), owner_of(st));
+        stage[3 * drank + 1] = make_uint4(__float_as_uint(T.ray.ox), __float_as_uint(T.ray.oy),
+                                          __float_as_uint(T.ray.oz), __float_as_uint(T.ix));
+        stage[3 * drank + 2] = make_uint4(__float_as_uint(T.ray.dx), __float_as_uint(T.ray.dy),
+                                          __float_as_uint(T.ray.dz), __float_as_uint(T.iy));
+        stage_iz[drank] = __float_as_uint(T.iz);
+    }
+    __syncwarp();
+    bool take = false;
+    uint32_t o = 0;
+    if (role == kFree && irank < pairs) {
+        const uint4 h = stage[3 * irank];
+        take = h.x != kNoEntry;
+        if (take) {
+            const uint4 r0 = stage[3 * irank + 1], r1 = stage[3 * irank + 2];
+            T.adopt(RayIn{__uint_as_float(r0.x), __uint_as_float(r0.y), __uint_as_float(r0.z),
+                          __uint_as_float(r1.x), __uint_as_float(r1.y), __uint_as_float(r1.z),
+                          __uint_as_float(h.y)},
+                    __uint_as_float(r0.w), __uint_as_float(r1.w), __uint_as_float(stage_iz[irank]),
+                    __uint_as_float(h.z), h.x);
+            o = h.w;
+            st = kHelper | (o << 2);
+        }
+    }
+    __syncwarp();
+    unsigned fresh = __ballot_sync(0xFFFFFFFFu, take);
+    while (fresh != 0u) {
+        const int k = __ffs(fresh) - 1;
+        fresh &= fresh - 1u;
+        if (lane == __shfl_sync(0xFFFFFFFFu, o, k)) st += 1u << 8;
+    }
+}
+
+// Helpers that finished this pass report to their owners, one at a time.
+template <class Tracer, bool kAny>
+__device__ __forceinline__ void merge_helpers(Tracer& T, uint32_t& st, unsigned fin) {
+    const unsigned lane = threadIdx.x & 31u;
+    while (fin != 0u) {
+        const int k = __ffs(fin) - 1;
+        fin &= fin - 1u;
+        const unsigned o = __shfl_sync(0xFFFFFFFFu, owner_of(st), k);
+        const float t = __shfl_sync(0xFFFFFFFFu, T.best_t, k);
+        const uint32_t p = __shfl_sync(0xFFFFFFFFu, T.best, k);
+        const float u = __shfl_sync(0xFFFFFFFFu, T.bu, k);
+        const float v = __shfl_sync(0xFFFFFFFFu, T.bv, k);
+        const uint32_t es = __shfl_sync(0xFFFFFFFFu, T.status, k);
+        const int oc = __shfl_sync(0xFFFFFFFFu, (int)T.occluded, k);
+        if (lane == o) {
+            T.status |= es;
+            if (kAny) {
+                T.occluded = T.occluded || oc;
+            } else if (p != ILM_MISS && (t < T.best_t || (t == T.best_t && p < T.best))) {
+                T.best_t = t; T.best = p; T.bu = u; T.bv = v;
+            }
+            st -= 1u << 8;
+        }
+    }
+}
 
 // Warp-level ray claiming of the persistent schedules: kChunk rays per
 // atomicAdd on a device counter.

@@ -70,12 +70,13 @@ class Context:
 
     def __init__(self, device: int = 0, stack_depth: int = 0, block_size: int = 0, validate_rays: bool = False,
                  max_iterations: int = 0, grid_schedule: bool = False, high_occupancy: bool = False,
-                 lane_refill: bool = False):
+                 lane_refill: bool = False, tail_split: bool = True):
         self._lib = _lib.load()
         flags = (_lib.ILM_FLAG_VALIDATE_RAYS if validate_rays else 0) | \
                 (_lib.ILM_FLAG_GRID_SCHEDULE if grid_schedule else 0) | \
                 (_lib.ILM_FLAG_HIGH_OCCUPANCY if high_occupancy else 0) | \
-                (_lib.ILM_FLAG_LANE_REFILL if lane_refill else 0)
+                (_lib.ILM_FLAG_LANE_REFILL if lane_refill else 0) | \
+                (0 if tail_split else _lib.ILM_FLAG_NO_TAIL_SPLIT)
         cfg = ilm_config(device, stack_depth, block_size, flags, max_iterations)
         h = ctypes.c_void_p()
         st = self._lib.ilm_context_create(ctypes.byref(h), ctypes.byref(cfg))

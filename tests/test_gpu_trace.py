@@ -155,18 +155,23 @@ def test_bench_launch_full_size_against_oracle(incoherent):
 @pytest.mark.parametrize("width,n", [(8, 1000003), (4, 600001), (8, 40000)])
 def test_pooled_lane_refill_and_grid_schedules_agree(incoherent, width, n):
     """Device buffers: the persistent schedule with warp-filtered chunks and a
-    per-warp pool (the default), with per-lane refill, and one thread per
-    ray give byte-identical records for closest and any hit.  The counts are
-    not multiples of a chunk, and 40,000 rays is a short queue (one ray per
-    lane per claim).  Outputs start as a fill pattern, so a ray handed out
-    twice or never would show."""
+    per-warp pool, with per-lane refill, and one thread per ray give
+    byte-identical records for closest and any hit.  The pooled schedule's
+    split tail (the default: idle lanes take subtrees of their warp's last
+    rays) gives the same any-hit flags and the same closest hits up to exact
+    ties in t, where the lone traversal keeps the first hit it found and the
+    split keeps the smaller primitive id.  The counts are not multiples of a
+    chunk, and 40,000 rays is a short queue (one ray per lane per claim).
+    Outputs start as a fill pattern, so a ray handed out twice or never
+    would show."""
     import torch
     xyz, idx, rays, sc = incoherent
     half = len(rays) // 2                                       # closest (tmax = inf) and shadow rays mixed
     sub = np.ascontiguousarray(np.concatenate([rays[:n // 2], rays[half:half + n - n // 2]]))
     d_rays = torch.from_numpy(sub.view(np.uint8)).cuda()
     out = []
-    for kw in ({"high_occupancy": True}, {"high_occupancy": True, "lane_refill": True}, {"grid_schedule": True}):
+    for kw in ({"high_occupancy": True, "tail_split": False}, {"high_occupancy": True, "lane_refill": True},
+               {"grid_schedule": True}, {"high_occupancy": True}, {}):
         ctx = rb.Context(0, **kw)
         acc = rb.GpuBVHAccel(ctx, [rb.TriangleMesh(ctx, xyz, idx)], width=width)
         d_hits = torch.full((n * 16,), 0xAB, dtype=torch.uint8, device="cuda")
@@ -179,6 +184,11 @@ def test_pooled_lane_refill_and_grid_schedules_agree(incoherent, width, n):
         ctx.close()
     assert out[0] == out[1] == out[2]
     assert np.all(np.frombuffer(out[0][1], np.uint32) <= 1)
+    for split in out[3:]:                                       # split tail, 8 blocks per SM and default
+        assert split[1] == out[0][1]
+        ties = compare_closest(np.frombuffer(split[0], HIT_DTYPE), np.frombuffer(out[0][0], HIT_DTYPE),
+                               label="split tail")
+        assert ties <= 16
     pick = np.sort(np.random.default_rng(n).choice(n, 20000, replace=False))
     g = np.frombuffer(out[0][0], HIT_DTYPE)[pick]
     compare_closest(g, sc.intersect(np.ascontiguousarray(sub[pick])), label="pooled")
