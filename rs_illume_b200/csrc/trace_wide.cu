@@ -106,9 +106,15 @@ __global__ void __launch_bounds__(128, kMinBlocks) k_trace_wide_persistent(Trace
                     need = __ballot_sync(0xFFFFFFFFu, role_of(st) == kFree);
                 }
             }
+            // Subtrees are shared once the counter has run out (warp-uniform).
+            // Before that every busy lane is an owner, and the closest-hit
+            // kernel skips the helpers' bookkeeping (measured 1 % faster); the
+            // any-hit kernel keeps it throughout (2 % faster that way).
+            const bool split_now = exhausted && a.split_tail;
+            const bool tail = kAny || split_now;
             // A helper of an occluded any-hit ray has nothing left to find.
             bool owner_occluded = kAny && __shfl_sync(0xFFFFFFFFu, (int)T.occluded, owner_of(st));
-            if (exhausted && a.split_tail) {
+            if (split_now) {
                 share_subtrees<Tracer, kAny>(T, st, owner_occluded, warp_words);
                 // Lanes that just took a subtree have a new owner.
                 if (kAny) owner_occluded = __shfl_sync(0xFFFFFFFFu, (int)T.occluded, owner_of(st));
@@ -119,11 +125,16 @@ __global__ void __launch_bounds__(128, kMinBlocks) k_trace_wide_persistent(Trace
             // An any-hit ray one of its helpers found occluded is finished.
             if ((role == kOwner || role == kHelper) && owner_occluded) done = true;
             else if (role == kOwner || role == kHelper) done = T.step(a);
-            const unsigned fin = __ballot_sync(0xFFFFFFFFu, role == kHelper && done);
-            if (fin) merge_helpers<Tracer, kAny>(T, st, fin);
-            if (role == kHelper && done) st = kFree | (lane << 2);
-            if (role == kOwner && done) st = (st & ~3u) | kWaiting;
-            if (role_of(st) == kWaiting && (st >> 8) == 0u) {
+            if (tail) {
+                const unsigned fin = __ballot_sync(0xFFFFFFFFu, role == kHelper && done);
+                if (fin) merge_helpers<Tracer, kAny>(T, st, fin);
+                if (role == kHelper && done) st = kFree | (lane << 2);
+                if (role == kOwner && done) st = (st & ~3u) | kWaiting;
+                if (role_of(st) == kWaiting && (st >> 8) == 0u) {
+                    T.write((uint64_t)ids[2 * lane] | ((uint64_t)ids[2 * lane + 1] << 32), a);
+                    st = kFree | (lane << 2);
+                }
+            } else if (done) {
                 T.write((uint64_t)ids[2 * lane] | ((uint64_t)ids[2 * lane + 1] << 32), a);
                 st = kFree | (lane << 2);
             }
