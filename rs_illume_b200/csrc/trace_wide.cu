@@ -31,6 +31,52 @@ __global__ void __launch_bounds__(128) k_trace_wide(TraceArgs a) {
     T.write(i, a);
 }
 
+// One thread per ray with the split tail from the start: a lane whose ray
+// missed the scene's root box or has finished takes subtrees of its warp's
+// unfinished rays (share_subtrees).  A one-wave query is all tail: its
+// launch lasts as long as its longest rays.
+template <int W, int kStack, bool kAny, bool kAnalytic>
+__global__ void __launch_bounds__(128) k_trace_wide_split(TraceArgs a) {
+    const unsigned lane = threadIdx.x & 31u;
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    __shared__ __align__(16) uint32_t s_warp[4][kWarpWords];
+    uint32_t* warp_words = s_warp[threadIdx.x >> 5];
+    uint32_t* ids = warp_words + kPoolWords;
+    using Tracer = WideTracer<W, kStack, kAny, kAnalytic>;
+    typename Tracer::Entry stk[Tracer::kDepth];
+    Tracer T(stk);
+    uint32_t st = kFree | (lane << 2);
+    if (i < ray_count(a)) {
+        const RayIn r = load_ray(a.rays, i);
+        T.init(r);
+        if (a.n_nodes != 0 && T.enters(a.bound)) {
+            ids[2 * lane] = (uint32_t)i;
+            ids[2 * lane + 1] = (uint32_t)(i >> 32);
+            st = kOwner | (lane << 2);
+        } else {
+            write_miss(i, r, a.hits, a.occ);
+        }
+    }
+    for (;;) {
+        bool owner_occluded = kAny && __shfl_sync(0xFFFFFFFFu, (int)T.occluded, owner_of(st));
+        share_subtrees<Tracer, kAny>(T, st, owner_occluded, warp_words);
+        if (kAny) owner_occluded = __shfl_sync(0xFFFFFFFFu, (int)T.occluded, owner_of(st));
+        if (!__any_sync(0xFFFFFFFFu, role_of(st) != kFree)) break;
+        const uint32_t role = role_of(st);
+        bool done = false;
+        if ((role == kOwner || role == kHelper) && owner_occluded) done = true;
+        else if (role == kOwner || role == kHelper) done = T.step(a);
+        const unsigned fin = __ballot_sync(0xFFFFFFFFu, role == kHelper && done);
+        if (fin) merge_helpers<Tracer, kAny>(T, st, fin);
+        if (role == kHelper && done) st = kFree | (lane << 2);
+        if (role == kOwner && done) st = (st & ~3u) | kWaiting;
+        if (role_of(st) == kWaiting && (st >> 8) == 0u) {
+            T.write((uint64_t)ids[2 * lane] | ((uint64_t)ids[2 * lane + 1] << 32), a);
+            st = kFree | (lane << 2);
+        }
+    }
+}
+
 // kMinBlocks > 0 asks the compiler for that many resident 128-thread blocks
 // per SM (64 registers at 8), trading a few spills for more warps in flight.
 // kPool selects how claimed rays reach idle lanes:
@@ -206,6 +252,11 @@ cudaError_t launch_variant(const TraceArgs& t, const LaunchParams& lp, cudaStrea
         return lp.min_blocks >= 8 ? launch_pooled<W, kStack, 8, kAnalytic>(t, lp, s)
                                   : launch_pooled<W, kStack, 1, kAnalytic>(t, lp, s);
     unsigned grid = (unsigned)((t.n + block - 1) / block);
+    if (t.split_tail) {
+        if (t.occ) k_trace_wide_split<W, kStack, true, kAnalytic><<<grid, block, 0, s>>>(t);
+        else k_trace_wide_split<W, kStack, false, kAnalytic><<<grid, block, 0, s>>>(t);
+        return cudaGetLastError();
+    }
     if (t.occ) k_trace_wide<W, kStack, true, kAnalytic><<<grid, block, 0, s>>>(t);
     else k_trace_wide<W, kStack, false, kAnalytic><<<grid, block, 0, s>>>(t);
     return cudaGetLastError();

@@ -158,9 +158,10 @@ def test_pooled_lane_refill_and_grid_schedules_agree(incoherent, width, n):
     per-warp pool, with per-lane refill, and one thread per ray give
     byte-identical records for closest and any hit.  The pooled schedule's
     split tail (the default: idle lanes take subtrees of their warp's last
-    rays) gives the same any-hit flags and the same closest hits up to exact
-    ties in t, where the lone traversal keeps the first hit it found and the
-    split keeps the smaller primitive id.  The counts are not multiples of a
+    rays; in the one-thread-per-ray kernel, from the start) gives the same
+    any-hit flags and the same closest hits up to exact ties in t, where the
+    lone traversal keeps the first hit it found and the split keeps the
+    smaller primitive id.  The counts are not multiples of a
     chunk, and 40,000 rays is a short queue (one ray per lane per claim).
     Outputs start as a fill pattern, so a ray handed out twice or never
     would show."""
@@ -171,7 +172,7 @@ def test_pooled_lane_refill_and_grid_schedules_agree(incoherent, width, n):
     d_rays = torch.from_numpy(sub.view(np.uint8)).cuda()
     out = []
     for kw in ({"high_occupancy": True, "tail_split": False}, {"high_occupancy": True, "lane_refill": True},
-               {"grid_schedule": True}, {"high_occupancy": True}, {}):
+               {"grid_schedule": True, "tail_split": False}, {"high_occupancy": True}, {}, {"grid_schedule": True}):
         ctx = rb.Context(0, **kw)
         acc = rb.GpuBVHAccel(ctx, [rb.TriangleMesh(ctx, xyz, idx)], width=width)
         d_hits = torch.full((n * 16,), 0xAB, dtype=torch.uint8, device="cuda")
@@ -184,7 +185,7 @@ def test_pooled_lane_refill_and_grid_schedules_agree(incoherent, width, n):
         ctx.close()
     assert out[0] == out[1] == out[2]
     assert np.all(np.frombuffer(out[0][1], np.uint32) <= 1)
-    for split in out[3:]:                                       # split tail, 8 blocks per SM and default
+    for split in out[3:]:                       # split tail: pooled at 8 blocks per SM and default, grid
         assert split[1] == out[0][1]
         ties = compare_closest(np.frombuffer(split[0], HIT_DTYPE), np.frombuffer(out[0][0], HIT_DTYPE),
                                label="split tail")
