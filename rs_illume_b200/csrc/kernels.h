@@ -32,6 +32,10 @@ struct LaunchParams {
                                // testing its own claims (0)
     int split_tail = 0;        // pooled persistent schedule: once the work counter has run out, idle
                                // lanes take stacked subtrees of their warp's unfinished rays
+    int queue_split = 0;       // persistent queries with a device-side count (path queues): the
+                               // one-thread-per-ray split kernel is launched beside the persistent
+                               // one and answers counts of at most one wave; each kernel returns at
+                               // once when the count is the other's
 };
 
 // Everything a trace kernel reads, passed by value.
@@ -51,6 +55,8 @@ struct TraceArgs {
     float bound[6];
     const uint32_t* kd_index;          // kd-tree leaf runs
     uint32_t split_tail = 0;           // LaunchParams::split_tail
+    uint64_t small_max = 0;            // LaunchParams::queue_split: counts up to this go to the
+                                       // one-thread-per-ray kernel (0: no such split)
 };
 
 // occ == nullptr: closest hit into `hits`; otherwise any-hit into `occ`.

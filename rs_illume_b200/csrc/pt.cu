@@ -712,6 +712,10 @@ int32_t setup_render(ilm_context* ctx, PtScene& sc, uint32_t spp, uint32_t max_d
     r.lp = LaunchParams{ctx->stack_depth, ctx->block_size, ctx->max_iter, 1, counter,
                         (ctx->flags & ILM_FLAG_HIGH_OCCUPANCY) ? 8 : 0,
                         0};   // path-queue rays almost all enter the scene: lanes refill one by one
+    // Queues of at most one wave (late bounces, training suffixes) run one
+    // thread per ray with the split tail instead.
+    r.lp.split_tail = split_tail_of(ctx);
+    r.lp.queue_split = r.lp.split_tail;
     r.err = static_cast<uint32_t*>(ctx->err_word.ptr);
     int dev_sms = 148;
     cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, ctx->device);

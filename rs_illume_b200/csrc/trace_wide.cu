@@ -11,6 +11,8 @@
 //    the two ways of doing so).  Each loop iteration advances every busy lane
 //    by exactly one node or one leaf, then refills finished lanes, so a warp
 //    stays full while its rays differ in length.
+#include <algorithm>
+
 #include "wide_tracer.cuh"
 
 namespace ilm {
@@ -46,7 +48,9 @@ __global__ void __launch_bounds__(128) k_trace_wide_split(TraceArgs a) {
     typename Tracer::Entry stk[Tracer::kDepth];
     Tracer T(stk);
     uint32_t st = kFree | (lane << 2);
-    if (i < ray_count(a)) {
+    const uint64_t n = ray_count(a);
+    if (a.small_max && n > a.small_max) return;   // the persistent launch beside this one has it
+    if (i < n) {
         const RayIn r = load_ray(a.rays, i);
         T.init(r);
         if (a.n_nodes != 0 && T.enters(a.bound)) {
@@ -93,6 +97,7 @@ __global__ void __launch_bounds__(128) k_trace_wide_split(TraceArgs a) {
 template <int W, int kStack, bool kAny, int kMinBlocks, bool kAnalytic, bool kPool>
 __global__ void __launch_bounds__(128, kMinBlocks) k_trace_wide_persistent(TraceArgs a) {
     const uint64_t n = ray_count(a);
+    if (n <= a.small_max) return;                  // the one-thread-per-ray launch beside this one has it
     // A short queue (fewer than two rays per resident lane) is claimed one ray
     // per lane, so that its rays run side by side rather than two per lane.
     const unsigned chunk = n < 2ull * gridDim.x * blockDim.x ? 32u : kChunk;
@@ -248,9 +253,30 @@ cudaError_t launch_pooled(const TraceArgs& t, const LaunchParams& lp, cudaStream
 template <int W, int kStack, bool kAnalytic>
 cudaError_t launch_variant(const TraceArgs& t, const LaunchParams& lp, cudaStream_t s) {
     const unsigned block = 128;
-    if (lp.persistent && t.counter)
+    if (lp.persistent && t.counter) {
+        if (lp.queue_split && t.n_dev && t.split_tail) {
+            // A queue whose count is known on the device only: a count of at
+            // most one wave of the split kernel runs there (all of its rays
+            // resident at once, idle lanes helping from the start), a larger
+            // one on the persistent kernel.
+            auto kc = k_trace_wide_split<W, kStack, false, kAnalytic>;
+            auto ka = k_trace_wide_split<W, kStack, true, kAnalytic>;
+            const uint64_t wave_blocks = resident_blocks(t.occ ? (const void*)ka : (const void*)kc, (int)block);
+            const uint64_t blocks = std::min<uint64_t>(wave_blocks, (t.n + block - 1) / block);
+            if (blocks > 0) {
+                TraceArgs q = t;
+                q.small_max = blocks * block;
+                if (t.occ) ka<<<(unsigned)blocks, block, 0, s>>>(q);
+                else kc<<<(unsigned)blocks, block, 0, s>>>(q);
+                cudaError_t e = cudaGetLastError();
+                if (e != cudaSuccess) return e;
+                return lp.min_blocks >= 8 ? launch_pooled<W, kStack, 8, kAnalytic>(q, lp, s)
+                                          : launch_pooled<W, kStack, 1, kAnalytic>(q, lp, s);
+            }
+        }
         return lp.min_blocks >= 8 ? launch_pooled<W, kStack, 8, kAnalytic>(t, lp, s)
                                   : launch_pooled<W, kStack, 1, kAnalytic>(t, lp, s);
+    }
     unsigned grid = (unsigned)((t.n + block - 1) / block);
     if (t.split_tail) {
         if (t.occ) k_trace_wide_split<W, kStack, true, kAnalytic><<<grid, block, 0, s>>>(t);
