@@ -284,6 +284,18 @@ def neural_cache_leg(rb, wl, ctx, torch, dev):
                      "warm_ms_per_frame": round(1e3 * sw["seconds"] / sw["frames"], 3)})
         if rep + 1 < GAIN_REPEATS:
             cache.close()
+    # the last cache trained on to 800 frames: the per-frame relMSE rises
+    # over the first few hundred Adam steps and then holds (the gain after
+    # 200 frames is above this steady state)
+    pt.render_nrc(cache, frames=800 - 200 - 8, seed=50000)
+    rs, ts = [], []
+    for k in range(8):
+        img, st = pt.render_nrc(cache, frames=1, seed=60000 + k)
+        rs.append(rel(img))
+        ts.append(st["seconds"])
+    r_late, t_late = float(np.mean(rs)), float(np.median(ts))
+    steady = {"frames": 800, "gain": round(r1 * t_spp / t_late / r_late, 3), "relmse_cache_frame": round(r_late, 5),
+              "ms_per_frame": round(1e3 * t_late, 3)}
     mlp = mlp_leg(rb, ctx, torch, dev, cache)
     cache.close()
     worst = min(reps, key=lambda r: r["gain"])
@@ -293,6 +305,7 @@ def neural_cache_leg(rb, wl, ctx, torch, dev):
             "relmse_plain_equal_time": worst["relmse_plain_equal_time"], "relmse_plain_1spp": round(r1, 5),
             "ms_per_frame": worst["ms_per_frame"], "plain_ms_per_spp": round(1e3 * t_spp, 3),
             "queries_per_path": worst["queries_per_path"], "warm_frames": 200, "repeats": reps,
+            "steady_state": steady,
             "mlp": mlp,
             "config": f"Cornell box, 1024x1024, 1-spp frames, spread c 0.003, 16384 training paths and "
                       f"2 Adam steps x 32768 samples per frame, one-vertex self-training suffix, "
