@@ -79,6 +79,7 @@ CONFIG = {"workload": WORKLOAD, "accel": "SAH BVH, max_prims_in_node 4, 12 bucke
 METRIC = "closest-hit Mrays/s"
 REF_SPP = 16384   # plain-tracer reference of the radiance-cache comparison
 GAIN_REPEATS = 3  # independent radiance-cache runs; the smallest gain is reported
+NRC_WARM_FRAMES = 800  # frames of online training before a cache is measured
 UNIT = "Mrays/s"
 
 
@@ -264,51 +265,54 @@ def neural_cache_leg(rb, wl, ctx, torch, dev):
     t_spp = sp["seconds"] / 16
     r1 = float(np.mean([rel(pt.render(1, seed=20 + k)[0]) for k in range(4)]))
     # independent repeats: a fresh cache (its own initial weights and frame
-    # seeds) trained online over 200 frames, then 8 measured frames each;
-    # the reported gain is the smallest
-    reps = []
-    for rep in range(GAIN_REPEATS):
-        cache = RadianceCache(ctx, acc.world_bound(), seed=4 + rep)
-        _, sw = pt.render_nrc(cache, frames=200, seed=9 + 1000 * rep)
-        rs, ts, qs = [], [], []
+    # seeds) trained online; 8 frames measured after 200 frames and again
+    # after 800, where the per-frame relMSE has settled (it rises over the
+    # first few hundred Adam steps, then holds).  The reported gain is the
+    # smallest 800-frame gain; the mean-image bias against the reference is
+    # reported beside each measurement.
+    def measure(cache, seed0):
+        rs, ts, qs, mean = [], [], [], 0.0
         for k in range(8):
-            img, st = pt.render_nrc(cache, frames=1, seed=100 + 1000 * rep + k)
+            img, st = pt.render_nrc(cache, frames=1, seed=seed0 + k)
             rs.append(rel(img))
             ts.append(st["seconds"])
             qs.append(st["queries"])
+            mean += float(np.mean(img)) / 8
         r_nrc, t_frame = float(np.mean(rs)), float(np.median(ts))
         r_plain = r1 * t_spp / t_frame
-        reps.append({"gain": round(r_plain / r_nrc, 3), "relmse_cache_frame": round(r_nrc, 5),
-                     "relmse_plain_equal_time": round(r_plain, 5), "ms_per_frame": round(1e3 * t_frame, 3),
-                     "queries_per_path": round(float(np.mean(qs)) / res / res, 3),
-                     "warm_ms_per_frame": round(1e3 * sw["seconds"] / sw["frames"], 3)})
+        return {"gain": round(r_plain / r_nrc, 3), "relmse_cache_frame": round(r_nrc, 5),
+                "relmse_plain_equal_time": round(r_plain, 5), "ms_per_frame": round(1e3 * t_frame, 3),
+                "queries_per_path": round(float(np.mean(qs)) / res / res, 3),
+                "mean_bias": round(mean / float(np.mean(ref)) - 1.0, 4)}
+
+    reps, early = [], []
+    for rep in range(GAIN_REPEATS):
+        cache = RadianceCache(ctx, acc.world_bound(), seed=4 + rep)
+        pt.render_nrc(cache, frames=200, seed=9 + 1000 * rep)
+        early.append(measure(cache, 100 + 1000 * rep))
+        _, sw = pt.render_nrc(cache, frames=NRC_WARM_FRAMES - 208, seed=20000 + 1000 * rep)
+        m = measure(cache, 500 + 1000 * rep)
+        m["warm_ms_per_frame"] = round(1e3 * sw["seconds"] / sw["frames"], 3)
+        reps.append(m)
         if rep + 1 < GAIN_REPEATS:
             cache.close()
-    # the last cache trained on to 800 frames: the per-frame relMSE rises
-    # over the first few hundred Adam steps and then holds (the gain after
-    # 200 frames is above this steady state)
-    pt.render_nrc(cache, frames=800 - 200 - 8, seed=50000)
-    rs, ts = [], []
-    for k in range(8):
-        img, st = pt.render_nrc(cache, frames=1, seed=60000 + k)
-        rs.append(rel(img))
-        ts.append(st["seconds"])
-    r_late, t_late = float(np.mean(rs)), float(np.median(ts))
-    steady = {"frames": 800, "gain": round(r1 * t_spp / t_late / r_late, 3), "relmse_cache_frame": round(r_late, 5),
-              "ms_per_frame": round(1e3 * t_late, 3)}
     mlp = mlp_leg(rb, ctx, torch, dev, cache)
     cache.close()
     worst = min(reps, key=lambda r: r["gain"])
     return {"gain": worst["gain"], "gain_repeats": [r["gain"] for r in reps],
-            "gain_rule": f"smallest of {GAIN_REPEATS} independent repeats (fresh cache, 200 warm frames, 8 frames)",
+            "gain_rule": f"smallest of {GAIN_REPEATS} independent repeats (fresh cache trained online over "
+                         f"{NRC_WARM_FRAMES} frames, then 8 measured frames)",
             "relmse_cache_frame": worst["relmse_cache_frame"],
             "relmse_plain_equal_time": worst["relmse_plain_equal_time"], "relmse_plain_1spp": round(r1, 5),
             "ms_per_frame": worst["ms_per_frame"], "plain_ms_per_spp": round(1e3 * t_spp, 3),
-            "queries_per_path": worst["queries_per_path"], "warm_frames": 200, "repeats": reps,
-            "steady_state": steady,
+            "queries_per_path": worst["queries_per_path"], "warm_frames": NRC_WARM_FRAMES,
+            "mean_bias": [r["mean_bias"] for r in reps], "repeats": reps,
+            "after_200_frames": {"gain_repeats": [r["gain"] for r in early],
+                                 "mean_bias": [r["mean_bias"] for r in early]},
             "mlp": mlp,
             "config": f"Cornell box, 1024x1024, 1-spp frames, spread c 0.003, 16384 training paths and "
-                      f"2 Adam steps x 32768 samples per frame, one-vertex self-training suffix, "
+                      f"2 Adam steps x 32768 samples per frame (lr 1e-2, decoupled weight decay 1.0), "
+                      f"one-vertex self-training suffix, "
                       f"reference {REF_SPP} spp"}
 
 

@@ -454,6 +454,10 @@ typedef struct {
     float bound[6];                /* scene bound for the position encoding */
     float ema;                     /* inference uses a moving average of the weights over
                                       Adam steps with this decay (0.99); 0 = latest weights */
+    float weight_decay;            /* decoupled weight decay (AdamW): each step also subtracts
+                                      lr * weight_decay * w; 0 = none (1.0 in the benchmark,
+                                      where it keeps the online-trained cache smooth: steady
+                                      per-frame relMSE 0.30 against 0.345, mean image within 1%) */
 } ilm_nrc_config;
 typedef struct ilm_nrc ilm_nrc;
 #define ILM_NRC_PARAMS 30720       /* FP32 master weights: 64x208, 4 x 64x64, 16x64 (rows 3..15 zero) */

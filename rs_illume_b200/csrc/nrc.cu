@@ -78,6 +78,7 @@ struct Enc {   // position normalisation: q = (p - origin) * scale
 struct AdamArgs {
     float lr, b1, b2, eps;
     float ema_a;   // moving-average decay (0 = off)
+    float wd;      // decoupled weight decay (AdamW; 0 = none)
 };
 
 // Optimiser counters in device memory, so that a captured training step
@@ -966,7 +967,7 @@ __global__ void k_reduce_adam(const float* __restrict__ partial, int n_part, Nrc
         float vv = ar.b2 * v[p] + (1.0f - ar.b2) * gsum * gsum;
         m[p] = mm;
         v[p] = vv;
-        x -= ar.lr * (mm / c1) / (sqrtf(vv / c2) + ar.eps);
+        x -= ar.lr * ((mm / c1) / (sqrtf(vv / c2) + ar.eps) + ar.wd * x);
         w[p] = x;
     }
     __nv_bfloat16 h = __float2bfloat16_rn(x);
@@ -1112,7 +1113,7 @@ cudaError_t train_rows(ilm_nrc* h, const float* raw, const float* target, NrcCou
                                             static_cast<uint32_t*>(h->err.ptr));
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     AdamArgs ar{h->cfg.lr, h->cfg.beta1, h->cfg.beta2, h->cfg.eps,
-                h->cfg.ema > 0.0f && h->cfg.ema < 1.0f ? h->cfg.ema : 0.0f};
+                h->cfg.ema > 0.0f && h->cfg.ema < 1.0f ? h->cfg.ema : 0.0f, h->cfg.weight_decay};
     k_reduce_adam<<<(kParams + 255) / 256, 256, 0, s>>>(
         static_cast<const float*>(h->partial.ptr), n_part, cnt, static_cast<float*>(h->grad.ptr),
         static_cast<float*>(h->w.ptr), static_cast<float*>(h->m.ptr), static_cast<float*>(h->v.ptr), ar, st, do_step,
@@ -1151,6 +1152,10 @@ extern "C" {
 int32_t ilm_nrc_create(ilm_context* ctx, const ilm_nrc_config* cfg, ilm_nrc** out) {
     if (!ctx || !cfg || !out) return ILM_ERR_INVALID_ARGUMENT;
     *out = nullptr;
+    if (!(cfg->weight_decay >= 0.0f) || !std::isfinite(cfg->weight_decay) || !(cfg->weight_decay * cfg->lr < 1.0f)) {
+        set_error(ctx, "ilm_nrc_create: weight_decay must be finite, >= 0 and below 1 / lr");
+        return ILM_ERR_INVALID_ARGUMENT;
+    }
     if (cudaSetDevice(ctx->device) != cudaSuccess) return ILM_ERR_CUDA;
     auto h = std::make_unique<ilm_nrc>();
     h->cfg = *cfg;

@@ -20,7 +20,7 @@ LAYERS = [(64, 208), (64, 64), (64, 64), (64, 64), (64, 64), (16, 64)]   # (out,
 class ilm_nrc_config(ctypes.Structure):
     _fields_ = [("lr", ctypes.c_float), ("beta1", ctypes.c_float), ("beta2", ctypes.c_float),
                 ("eps", ctypes.c_float), ("seed", ctypes.c_uint64), ("bound", ctypes.c_float * 6),
-                ("ema", ctypes.c_float)]
+                ("ema", ctypes.c_float), ("weight_decay", ctypes.c_float)]
 
 
 def split_params(p: np.ndarray):
@@ -33,9 +33,13 @@ def split_params(p: np.ndarray):
 
 
 class RadianceCache:
-    def __init__(self, ctx: Context, bound, lr=1e-2, beta1=0.9, beta2=0.99, eps=1e-10, seed=4, ema=0.99):
+    def __init__(self, ctx: Context, bound, lr=1e-2, beta1=0.9, beta2=0.99, eps=1e-10, seed=4, ema=0.99,
+                 weight_decay=1.0):
         """`ema`: inference uses a moving average of the weights over Adam
-        steps with this decay (0 = the latest weights)."""
+        steps with this decay (0 = the latest weights).  `weight_decay`:
+        decoupled weight decay (AdamW), each step also subtracting
+        lr * weight_decay * w (0 = plain Adam); it keeps the online-trained
+        cache smooth."""
         self.ctx = ctx
         if hasattr(bound, "min") and hasattr(bound, "max"):      # Bounds3f
             bound = tuple(bound.min) + tuple(bound.max)
@@ -43,6 +47,7 @@ class RadianceCache:
         for k in range(6):
             c.bound[k] = bound[k]
         c.ema = ema
+        c.weight_decay = weight_decay
         h = ctypes.c_void_p()
         ctx.check(ctx._lib.ilm_nrc_create(ctx.handle, ctypes.addressof(c), ctypes.byref(h)), "ilm_nrc_create")
         self.handle = h

@@ -7,6 +7,7 @@ within 2% relative."""
 import numpy as np
 import pytest
 
+import rs_illume_b200 as rb
 from rs_illume_b200.nrc import LAYERS, RadianceCache
 from tests import nrc_reference as ref
 
@@ -31,14 +32,14 @@ def random_inputs(n, seed):
 
 @pytest.fixture
 def cache(ctx):
-    c = RadianceCache(ctx, BOUND, seed=7, ema=0.0)     # inference with the latest weights
+    c = RadianceCache(ctx, BOUND, seed=7, ema=0.0, weight_decay=0.0)   # latest weights, plain Adam
     yield c
     c.close()
 
 
 def test_inference_uses_the_weight_average(ctx):
     ema = 0.9
-    c = RadianceCache(ctx, BOUND, seed=7, ema=ema)
+    c = RadianceCache(ctx, BOUND, seed=7, ema=ema, weight_decay=0.0)
     x, y = random_inputs(4096, 8)
     avg = np.zeros(30720, np.float64)
     for k in range(1, 6):
@@ -163,3 +164,23 @@ def test_adam_step_and_training_converges(cache):
     pt = cache.infer(xt)
     rel = np.mean((pt - yt) ** 2 / (yt ** 2 + 0.01))
     assert rel < 0.1, rel
+
+
+def test_adam_step_with_decoupled_weight_decay(ctx):
+    """AdamW: the first step is lr * (g / (|g| + eps) + weight_decay * w0);
+    frozen weights (padded inputs, output rows 3-15) stay zero.  An invalid
+    decay (negative, or lr * decay >= 1) is refused at creation."""
+    wd = 1.0
+    c = RadianceCache(ctx, BOUND, seed=7, ema=0.0, weight_decay=wd)
+    x, y = random_inputs(16384, 5)
+    w0 = c.params()
+    g, _ = c.gradients(x, y)
+    c.train_step(x, y)
+    w1 = c.params()
+    with np.errstate(invalid="ignore", divide="ignore"):
+        want = w0 - 1e-2 * (g / (np.abs(g) + 1e-10) + wd * w0)
+    np.testing.assert_allclose(w1, want, atol=1e-5)
+    c.close()
+    for bad in (-1.0, 100.0, float("nan")):
+        with pytest.raises(rb.IllumeError):
+            RadianceCache(ctx, BOUND, seed=7, weight_decay=bad)
