@@ -143,6 +143,43 @@ struct KdTracer {
             else store_hit(a.hits, i, best, best == ILM_MISS ? ray.tmax : best_t, bu, bv);
         }
     }
+
+    // Split tail (share_subtrees): stages the top deferred entry for another
+    // lane with its range [its t_min, the t_min of the entry beneath or the
+    // root range's end], the ray, its reciprocals, the best distance and the
+    // owner lane; the donor's own ranges are unchanged, since the range it
+    // traverses already ends where the given one starts.  take() adopts a
+    // staging (false for an entry the donor's early exit would have skipped).
+    __device__ __forceinline__ void give(uint4* s, uint32_t owner) {
+        --sp;
+        const uint2 e = stack[sp];
+        const float lo = __uint_as_float(e.y);
+        const float hi = sp > 0 ? __uint_as_float(stack[sp - 1].y) : t_root;
+        const bool live = !((kAny ? ray.tmax : best_t) < lo);
+        s[0] = make_uint4(live ? e.x : kNoEntry, __float_as_uint(ray.tmax), __float_as_uint(best_t), owner);
+        s[1] = make_uint4(__float_as_uint(ray.ox), __float_as_uint(ray.oy), __float_as_uint(ray.oz),
+                          __float_as_uint(ix));
+        s[2] = make_uint4(__float_as_uint(ray.dx), __float_as_uint(ray.dy), __float_as_uint(ray.dz),
+                          __float_as_uint(iy));
+        s[3] = make_uint4(__float_as_uint(iz), __float_as_uint(lo), __float_as_uint(hi), 0u);
+    }
+    __device__ __forceinline__ bool take(const uint4* s, uint32_t& owner) {
+        const uint4 h = s[0];
+        if (h.x == kNoEntry) return false;
+        const uint4 r0 = s[1], r1 = s[2], r2 = s[3];
+        ray = RayIn{__uint_as_float(r0.x), __uint_as_float(r0.y), __uint_as_float(r0.z), __uint_as_float(r1.x),
+                    __uint_as_float(r1.y), __uint_as_float(r1.z), __uint_as_float(h.y)};
+        ix = __uint_as_float(r0.w); iy = __uint_as_float(r1.w); iz = __uint_as_float(r2.x);
+        best_t = __uint_as_float(h.z); bu = 0.0f; bv = 0.0f;
+        best = ILM_MISS;
+        status = 0; iter = 0; sp = 0;
+        tr_ready = false; occluded = false;
+        cur = h.x;
+        t_min = __uint_as_float(r2.y);
+        t_max = t_root = __uint_as_float(r2.z);
+        owner = h.w;
+        return true;
+    }
 };
 
 template <bool kAny, bool kAnalytic>
@@ -169,60 +206,89 @@ __global__ void __launch_bounds__(kKdBlock, kMinBlocks) k_trace_kd_persistent(Tr
     const unsigned below = (1u << lane) - 1u;
     uint2 stk[kKdMaxDepth];
     KdTracer<kAny, kAnalytic> T(stk);
-    bool active = false;
-    uint64_t id = 0;
     bool exhausted = false;                             // warp-uniform
     if constexpr (kPool) {
-        __shared__ uint32_t s_pool[kKdBlock / 32][kChunk];   // per warp: offsets of the pooled rays
-        uint32_t* pool = s_pool[threadIdx.x >> 5];
+        // The wide kernel's pooled schedule and split tail (share_subtrees,
+        // merge_helpers; the lane roles of wide_tracer.cuh).
+        __shared__ __align__(16) uint32_t s_warp[kKdBlock / 32][kWarpWords];
+        uint32_t* warp_words = s_warp[threadIdx.x >> 5];
+        uint32_t* pool = warp_words;                    // offsets of the pooled rays in their chunk
+        uint32_t* ids = warp_words + kPoolWords;        // each lane's ray id (owners)
         unsigned pool_n = 0;                            // warp-uniform
         unsigned long long pool_base = 0;               // warp-uniform
+        uint32_t st = kFree | (lane << 2);
         for (;;) {
-            unsigned need = __ballot_sync(0xFFFFFFFFu, !active);
-            while (need != 0u) {
-                if (pool_n == 0) {
-                    if (exhausted) break;
-                    unsigned long long b = 0;
-                    if (lane == 0) b = atomicAdd(a.counter, (unsigned long long)chunk);
-                    b = __shfl_sync(0xFFFFFFFFu, b, 0);
-                    if (b >= n) { exhausted = true; break; }
-                    for (unsigned k = 0; k < chunk; k += 32u) {
-                        const uint64_t rid = b + k + lane;
-                        bool enter = false;
-                        if (rid < n) {
-                            const RayIn r = load_ray(a.rays, rid);
-                            KdTracer<kAny, kAnalytic> probe(nullptr);   // root clip only: no stack
-                            probe.init(r);
-                            enter = a.n_nodes != 0 && probe.enters(a.bound);
-                            if (!enter) write_miss(rid, r, a.hits, a.occ);
+            if (!exhausted) {
+                unsigned need = __ballot_sync(0xFFFFFFFFu, role_of(st) == kFree);
+                while (need != 0u) {
+                    if (pool_n == 0) {
+                        unsigned long long b = 0;
+                        if (lane == 0) b = atomicAdd(a.counter, (unsigned long long)chunk);
+                        b = __shfl_sync(0xFFFFFFFFu, b, 0);
+                        if (b >= n) { exhausted = true; break; }
+                        for (unsigned k = 0; k < chunk; k += 32u) {
+                            const uint64_t rid = b + k + lane;
+                            bool enter = false;
+                            if (rid < n) {
+                                const RayIn r = load_ray(a.rays, rid);
+                                KdTracer<kAny, kAnalytic> probe(nullptr);   // root clip only: no stack
+                                probe.init(r);
+                                enter = a.n_nodes != 0 && probe.enters(a.bound);
+                                if (!enter) write_miss(rid, r, a.hits, a.occ);
+                            }
+                            const unsigned m = __ballot_sync(0xFFFFFFFFu, enter);
+                            if (enter) pool[pool_n + __popc(m & below)] = k + lane;
+                            pool_n += __popc(m);
                         }
-                        const unsigned m = __ballot_sync(0xFFFFFFFFu, enter);
-                        if (enter) pool[pool_n + __popc(m & below)] = k + lane;
-                        pool_n += __popc(m);
+                        __syncwarp();
+                        pool_base = b;
+                        continue;
                     }
+                    const unsigned rank = __popc(need & below);
+                    const unsigned take = min((unsigned)__popc(need), pool_n);
+                    if (((need >> lane) & 1u) && rank < take) {
+                        const uint64_t id = pool_base + pool[pool_n - 1u - rank];
+                        ids[2 * lane] = (uint32_t)id;
+                        ids[2 * lane + 1] = (uint32_t)(id >> 32);
+                        T.init(load_ray(a.rays, id));
+                        T.enters(a.bound);              // true: the probe passed; sets the clip range
+                        st = kOwner | (lane << 2);
+                    }
+                    pool_n -= take;
                     __syncwarp();
-                    pool_base = b;
-                    continue;
+                    need = __ballot_sync(0xFFFFFFFFu, role_of(st) == kFree);
                 }
-                const unsigned rank = __popc(need & below);
-                const unsigned take = min((unsigned)__popc(need), pool_n);
-                if (((need >> lane) & 1u) && rank < take) {
-                    id = pool_base + pool[pool_n - 1u - rank];
-                    T.init(load_ray(a.rays, id));
-                    active = T.enters(a.bound);   // true: the probe passed; sets the clip range
-                }
-                pool_n -= take;
-                __syncwarp();
-                need = __ballot_sync(0xFFFFFFFFu, !active);
             }
-            if (!__any_sync(0xFFFFFFFFu, active)) break;
-            if (active && T.step(a)) {
-                T.write(id, a);
-                active = false;
+            const bool tail = exhausted && a.split_tail;   // warp-uniform
+            bool owner_occluded = false;
+            if (tail) {
+                if (kAny) owner_occluded = __shfl_sync(0xFFFFFFFFu, (int)T.occluded, owner_of(st));
+                share_subtrees<KdTracer<kAny, kAnalytic>, kAny>(T, st, owner_occluded, warp_words);
+                if (kAny) owner_occluded = __shfl_sync(0xFFFFFFFFu, (int)T.occluded, owner_of(st));
+            }
+            if (!__any_sync(0xFFFFFFFFu, role_of(st) != kFree)) break;
+            const uint32_t role = role_of(st);
+            bool done = false;
+            if ((role == kOwner || role == kHelper) && owner_occluded) done = true;
+            else if (role == kOwner || role == kHelper) done = T.step(a);
+            if (tail) {
+                const unsigned fin = __ballot_sync(0xFFFFFFFFu, role == kHelper && done);
+                if (fin) merge_helpers<KdTracer<kAny, kAnalytic>, kAny>(T, st, fin);
+                if (role == kHelper && done) st = kFree | (lane << 2);
+                if (role == kOwner && done) st = (st & ~3u) | kWaiting;
+                if (role_of(st) == kWaiting && (st >> 8) == 0u) {
+                    T.write((uint64_t)ids[2 * lane] | ((uint64_t)ids[2 * lane + 1] << 32), a);
+                    st = kFree | (lane << 2);
+                }
+            } else if (done) {
+                T.write((uint64_t)ids[2 * lane] | ((uint64_t)ids[2 * lane + 1] << 32), a);
+                st = kFree | (lane << 2);
             }
         }
         return;
     }
+    bool active = false;
+    uint64_t id = 0;
     unsigned long long chunk_next = 0, chunk_end = 0;   // warp-uniform
     for (;;) {
         unsigned need = __ballot_sync(0xFFFFFFFFu, !active);

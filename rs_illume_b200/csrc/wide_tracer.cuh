@@ -125,6 +125,11 @@ __device__ __forceinline__ void sort_keys(uint32_t* k) {
     }
 }
 
+// A subtree handed to another lane that the donor's own pop would have culled
+// (no node or leaf entry has all bits set: that would be a leaf of 8 records
+// at 2^28 - 1; kd-tree node indices stay below 2^30).
+constexpr uint32_t kNoEntry = 0xFFFFFFFFu;
+
 // Per-lane traversal state of one ray over 4- or 8-wide nodes: hit children
 // sorted by entry distance and pushed far-to-near, one stack entry (node or
 // leaf, with its entry distance) per child.
@@ -180,6 +185,31 @@ struct WideTracerSorted {
         status = 0;
         tr_ready = false;
         cur = node; iter = 0; sp = 0;
+    }
+
+    // Split tail: stages the top stack entry for another lane (4 uint4: the
+    // entry, tmax, best distance, owner lane; the ray with its reciprocal
+    // directions), and adopts such a staging; take() is false for an entry
+    // the donor's pop would have culled.
+    __device__ __forceinline__ void give(uint4* s, uint32_t owner) {
+        const uint2 e = pop_one();
+        const bool live = kAny || __uint_as_float(e.y) < best_t;
+        s[0] = make_uint4(live ? e.x : kNoEntry, __float_as_uint(ray.tmax), __float_as_uint(best_t), owner);
+        s[1] = make_uint4(__float_as_uint(ray.ox), __float_as_uint(ray.oy), __float_as_uint(ray.oz),
+                          __float_as_uint(ix));
+        s[2] = make_uint4(__float_as_uint(ray.dx), __float_as_uint(ray.dy), __float_as_uint(ray.dz),
+                          __float_as_uint(iy));
+        s[3].x = __float_as_uint(iz);
+    }
+    __device__ __forceinline__ bool take(const uint4* s, uint32_t& owner) {
+        const uint4 h = s[0];
+        if (h.x == kNoEntry) return false;
+        const uint4 r0 = s[1], r1 = s[2];
+        adopt(RayIn{__uint_as_float(r0.x), __uint_as_float(r0.y), __uint_as_float(r0.z), __uint_as_float(r1.x),
+                    __uint_as_float(r1.y), __uint_as_float(r1.z), __uint_as_float(h.y)},
+              __uint_as_float(r0.w), __uint_as_float(r1.w), __uint_as_float(s[3].x), __uint_as_float(h.z), h.x);
+        owner = h.w;
+        return true;
     }
 
     __device__ __forceinline__ void push(uint2 e) { stack[sp++] = e; }
@@ -399,22 +429,19 @@ enum : uint32_t { kFree = 0, kOwner = 1, kWaiting = 2, kHelper = 3 };
 __device__ __forceinline__ uint32_t role_of(uint32_t st) { return st & 3u; }
 __device__ __forceinline__ uint32_t owner_of(uint32_t st) { return (st >> 2) & 31u; }
 
-// A staged subtree the donor's own pop would have culled (no node or leaf
-// entry has all bits set: that would be a leaf of 8 records at 2^28 - 1).
-constexpr uint32_t kNoEntry = 0xFFFFFFFFu;
-
 // Words of the per-warp shared area of the pooled schedule: the pool of
-// entering rays' offsets, each lane's ray id, 16 staging slots of 12 words
-// for handed-over subtrees and their z reciprocals.
+// entering rays' offsets, each lane's ray id, and 16 staging slots of 16
+// words for handed-over subtrees (a tracer's give / take).
 constexpr int kPoolWords = 64;
 constexpr int kIdWords = 64;
 constexpr int kSplitSlots = 16;
-constexpr int kWarpWords = kPoolWords + kIdWords + kSplitSlots * 13;
+constexpr int kWarpWords = kPoolWords + kIdWords + kSplitSlots * 16;
 
 // Idle lanes take stacked subtrees: the j-th lane holding an entry stages its
-// top entry (with the ray, its reciprocals, its best distance and its owner)
-// in slot j, and the j-th idle lane adopts slot j.  Helpers first lower their
-// bound to their owner's best distance when that is nearer.
+// top entry in slot j (the tracer's give: the entry with its range, the ray,
+// the donor's best distance and owner), and the j-th idle lane adopts slot j
+// (take).  Helpers first lower their bound to their owner's best distance when
+// that is nearer.
 template <class Tracer, bool kAny>
 __device__ __forceinline__ void share_subtrees(Tracer& T, uint32_t& st, bool owner_occluded, uint32_t* warp_words) {
     const unsigned lane = threadIdx.x & 31u;
@@ -431,34 +458,13 @@ __device__ __forceinline__ void share_subtrees(Tracer& T, uint32_t& st, bool own
     const unsigned below = (1u << lane) - 1u;
     const unsigned irank = __popc(idle & below), drank = __popc(don & below);
     uint4* stage = reinterpret_cast<uint4*>(warp_words + kPoolWords + kIdWords);
-    uint32_t* stage_iz = warp_words + kPoolWords + kIdWords + kSplitSlots * 12;
-    if (((don >> lane) & 1u) && drank < pairs) {
-        const uint2 e = T.pop_one();
-        const bool live = kAny || __uint_as_float(e.y) < T.best_t;
-        stage[3 * drank] = make_uint4(live ? e.x : kNoEntry, __float_as_uint(T.ray.tmax),
-                                      __float_as_uint(T.best_t), owner_of(st));
-        stage[3 * drank + 1] = make_uint4(__float_as_uint(T.ray.ox), __float_as_uint(T.ray.oy),
-                                          __float_as_uint(T.ray.oz), __float_as_uint(T.ix));
-        stage[3 * drank + 2] = make_uint4(__float_as_uint(T.ray.dx), __float_as_uint(T.ray.dy),
-                                          __float_as_uint(T.ray.dz), __float_as_uint(T.iy));
-        stage_iz[drank] = __float_as_uint(T.iz);
-    }
+    if (((don >> lane) & 1u) && drank < pairs) T.give(stage + 4 * drank, owner_of(st));
     __syncwarp();
     bool take = false;
     uint32_t o = 0;
     if (role == kFree && irank < pairs) {
-        const uint4 h = stage[3 * irank];
-        take = h.x != kNoEntry;
-        if (take) {
-            const uint4 r0 = stage[3 * irank + 1], r1 = stage[3 * irank + 2];
-            T.adopt(RayIn{__uint_as_float(r0.x), __uint_as_float(r0.y), __uint_as_float(r0.z),
-                          __uint_as_float(r1.x), __uint_as_float(r1.y), __uint_as_float(r1.z),
-                          __uint_as_float(h.y)},
-                    __uint_as_float(r0.w), __uint_as_float(r1.w), __uint_as_float(stage_iz[irank]),
-                    __uint_as_float(h.z), h.x);
-            o = h.w;
-            st = kHelper | (o << 2);
-        }
+        take = T.take(stage + 4 * irank, o);
+        if (take) st = kHelper | (o << 2);
     }
     __syncwarp();
     unsigned fresh = __ballot_sync(0xFFFFFFFFu, take);
