@@ -102,8 +102,9 @@ typedef struct {
  * (warps claim rays in chunks from a per-stream device counter and refill
  * finished lanes). */
 #define ILM_FLAG_GRID_SCHEDULE 2
-/* Persistent schedule compiled for 8 resident blocks per SM (64 registers per
- * thread) instead of the compiler's register choice. */
+/* Persistent schedule compiled for many resident blocks per SM instead of
+ * the compiler's register choice: 7 (up to 72 registers per thread) for the
+ * pooled kernel, 8 (64) for the lane-refill kernel. */
 #define ILM_FLAG_HIGH_OCCUPANCY 4
 /* Persistent schedule: each idle lane tests its own claimed rays against the
  * scene's root box instead of the whole warp testing each claimed chunk and

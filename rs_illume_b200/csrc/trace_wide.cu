@@ -246,7 +246,12 @@ cudaError_t launch_persistent(const TraceArgs& t, cudaStream_t s) {
 
 template <int W, int kStack, int kMinBlocks, bool kAnalytic>
 cudaError_t launch_pooled(const TraceArgs& t, const LaunchParams& lp, cudaStream_t s) {
-    return lp.root_pool ? launch_persistent<W, kStack, kMinBlocks, kAnalytic, true>(t, s)
+    // High occupancy: the pooled kernel at 7 resident blocks per SM (up to 72
+    // registers: its split tail's state fits without spills; 8,063-8,070
+    // against 7,699-7,704 Mrays/s closest hit at 8 blocks), the lane-refill
+    // kernel at 8 (64 registers, no spills).
+    constexpr int kPooledBlocks = kMinBlocks >= 8 ? 7 : kMinBlocks;
+    return lp.root_pool ? launch_persistent<W, kStack, kPooledBlocks, kAnalytic, true>(t, s)
                         : launch_persistent<W, kStack, kMinBlocks, kAnalytic, false>(t, s);
 }
 
