@@ -79,9 +79,11 @@ __device__ __forceinline__ TraceArgs args_of(const BatchTable& t, uint32_t b) {
 // tests each claimed chunk against the root boxes of the rays' scenes (two
 // rays per lane), answers the misses at full width and keeps the rays that
 // enter in a per-warp pool in shared memory, from which idle lanes take rays
-// (the single-scene kernel's kPool schedule).
+// (the single-scene kernel's kPool schedule).  7 resident blocks per SM (up
+// to 72 registers, no spills of the per-lane scene arguments): 4,880-4,896
+// against 4,806-4,810 Mrays/s at 8 blocks (64 registers) on the 32-scene set.
 template <int W, int kStack, bool kAny, bool kAnalytic>
-__global__ void __launch_bounds__(128, 8) k_trace_batched(BatchTable tab) {
+__global__ void __launch_bounds__(128, 7) k_trace_batched(BatchTable tab) {
     const unsigned lane = threadIdx.x & 31u;
     const unsigned below = (1u << lane) - 1u;
     __shared__ uint32_t s_pool[4][kChunk];              // per warp: offsets of the pooled rays in their chunk
