@@ -108,15 +108,18 @@ typedef struct {
 #define ILM_FLAG_HIGH_OCCUPANCY 4
 /* Persistent schedule: each idle lane tests its own claimed rays against the
  * scene's root box instead of the whole warp testing each claimed chunk and
- * pooling the rays that enter.  Only worth it when nearly every ray enters
- * the scene (the answers are the same either way). */
+ * pooling the rays that enter.  This kernel has no split tail.  The answers
+ * are the same either way, up to exact ties in t (see ILM_FLAG_NO_TAIL_SPLIT). */
 #define ILM_FLAG_LANE_REFILL 8
-/* Pooled persistent schedule: once every ray of the query has been claimed,
- * idle lanes no longer help their warp's unfinished rays by taking subtrees
- * from their traversal stacks (the split tail, on by default; the answers are
- * the same either way).  The split tail is also off whenever max_iterations
- * is below its default of 2^20, so that which rays reach a lowered cap does
- * not depend on which lanes traversed them. */
+/* Turns off the split tail, on by default: in the pooled persistent
+ * schedule once every ray of the query has been claimed, and in the
+ * one-thread-per-ray kernel throughout, idle lanes help their warp's
+ * unfinished rays by taking subtrees from their traversal stacks.  The
+ * answers are the same either way, except that of two hits at exactly the
+ * same t the split keeps the smaller primitive id where the lone traversal
+ * may keep the first it found.  The split tail is also off whenever
+ * max_iterations is below its default of 2^20, so that which rays reach a
+ * lowered cap does not depend on which lanes traversed them. */
 #define ILM_FLAG_NO_TAIL_SPLIT 16
 
 typedef struct {

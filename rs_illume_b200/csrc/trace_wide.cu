@@ -11,6 +11,10 @@
 //    the two ways of doing so).  Each loop iteration advances every busy lane
 //    by exactly one node or one leaf, then refills finished lanes, so a warp
 //    stays full while its rays differ in length.
+//  * split tail (pooled persistent kernel once every ray is claimed, and the
+//    one-thread-per-ray kernel k_trace_wide_split throughout): idle lanes
+//    take stacked subtrees of their warp's unfinished rays (share_subtrees in
+//    wide_tracer.cuh), so a launch does not wait on its longest rays alone.
 #include <algorithm>
 
 #include "wide_tracer.cuh"
@@ -82,7 +86,8 @@ __global__ void __launch_bounds__(128) k_trace_wide_split(TraceArgs a) {
 }
 
 // kMinBlocks > 0 asks the compiler for that many resident 128-thread blocks
-// per SM (64 registers at 8), trading a few spills for more warps in flight.
+// per SM (the high-occupancy build: 7 for the pooled kernel, up to 72
+// registers; 8 for the lane-refill kernel, 64 registers).
 // kPool selects how claimed rays reach idle lanes:
 //  * true: the whole warp tests each claimed chunk against the root box, two
 //    rays per lane, answers the misses at full width, and keeps the rays that
@@ -90,10 +95,9 @@ __global__ void __launch_bounds__(128) k_trace_wide_split(TraceArgs a) {
 //    pool.  For incoherent batches most rays miss the scene, and this keeps
 //    the lanes that are still traversing from waiting while a few idle lanes
 //    test misses one at a time (5,330 against 4,420 Mrays/s on the 2M-ray
-//    ball workload).
-//  * false: each idle lane tests its own claims, repeating until one enters;
-//    for queues whose rays nearly all enter the scene (the path tracer's) the
-//    pool's extra pass costs more than it saves.
+//    ball workload).  This kernel carries the split tail.
+//  * false: each idle lane tests its own claims, repeating until one enters
+//    (ILM_FLAG_LANE_REFILL); no split tail.
 template <int W, int kStack, bool kAny, int kMinBlocks, bool kAnalytic, bool kPool>
 __global__ void __launch_bounds__(128, kMinBlocks) k_trace_wide_persistent(TraceArgs a) {
     const uint64_t n = ray_count(a);

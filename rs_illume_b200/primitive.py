@@ -66,7 +66,9 @@ def rays_array(rays: Sequence[Ray]) -> np.ndarray:
 
 
 class Context:
-    """One ilm_context (device, streams, staging buffers, error word)."""
+    """One ilm_context (device, streams, staging buffers, error word).  The
+    keyword flags map to include/illume_gpu.h's ILM_FLAG_* (`tail_split=False`
+    is ILM_FLAG_NO_TAIL_SPLIT)."""
 
     def __init__(self, device: int = 0, stack_depth: int = 0, block_size: int = 0, validate_rays: bool = False,
                  max_iterations: int = 0, grid_schedule: bool = False, high_occupancy: bool = False,
