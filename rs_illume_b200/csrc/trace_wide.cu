@@ -44,7 +44,10 @@ __global__ void __launch_bounds__(128) k_trace_wide(TraceArgs a) {
 template <int W, int kStack, bool kAny, bool kAnalytic>
 __global__ void __launch_bounds__(128) k_trace_wide_split(TraceArgs a) {
     const unsigned lane = threadIdx.x & 31u;
-    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    // Lane `lane` < warp_rays of warp w starts on ray w * warp_rays + lane;
+    // the other lanes start idle and help from the first pass.
+    const uint64_t warp_id = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint64_t i = warp_id * a.warp_rays + lane;
     __shared__ __align__(16) uint32_t s_warp[4][kWarpWords];
     uint32_t* warp_words = s_warp[threadIdx.x >> 5];
     uint32_t* ids = warp_words + kPoolWords;
@@ -54,7 +57,7 @@ __global__ void __launch_bounds__(128) k_trace_wide_split(TraceArgs a) {
     uint32_t st = kFree | (lane << 2);
     const uint64_t n = ray_count(a);
     if (a.small_max && n > a.small_max) return;   // the persistent launch beside this one has it
-    if (i < n) {
+    if (lane < a.warp_rays && i < n) {
         const RayIn r = load_ray(a.rays, i);
         T.init(r);
         if (a.n_nodes != 0 && T.enters(a.bound)) {
@@ -288,8 +291,17 @@ cudaError_t launch_variant(const TraceArgs& t, const LaunchParams& lp, cudaStrea
     }
     unsigned grid = (unsigned)((t.n + block - 1) / block);
     if (t.split_tail) {
-        if (t.occ) k_trace_wide_split<W, kStack, true, kAnalytic><<<grid, block, 0, s>>>(t);
-        else k_trace_wide_split<W, kStack, false, kAnalytic><<<grid, block, 0, s>>>(t);
+        // A query that fits half a wave starts each warp with 16 rays, so
+        // that half its lanes help from the first pass.
+        auto kc = k_trace_wide_split<W, kStack, false, kAnalytic>;
+        auto ka = k_trace_wide_split<W, kStack, true, kAnalytic>;
+        const uint64_t wave = resident_blocks(t.occ ? (const void*)ka : (const void*)kc, (int)block) * block;
+        TraceArgs q = t;
+        q.warp_rays = 2 * t.n <= wave ? 16u : 32u;
+        const uint64_t rays_per_block = (uint64_t)q.warp_rays * (block / 32);
+        const unsigned g = (unsigned)((t.n + rays_per_block - 1) / rays_per_block);
+        if (t.occ) ka<<<g, block, 0, s>>>(q);
+        else kc<<<g, block, 0, s>>>(q);
         return cudaGetLastError();
     }
     if (t.occ) k_trace_wide<W, kStack, true, kAnalytic><<<grid, block, 0, s>>>(t);
