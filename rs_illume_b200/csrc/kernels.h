@@ -57,7 +57,8 @@ struct TraceArgs {
     uint32_t split_tail = 0;           // LaunchParams::split_tail
     uint64_t small_max = 0;            // LaunchParams::queue_split: counts up to this go to the
                                        // one-thread-per-ray kernel (0: no such split)
-    uint32_t warp_rays = 32;           // k_trace_wide_split: rays a warp starts with (16 or 32)
+    uint32_t warp_rays = 32;           // k_trace_wide_split: rays a warp starts with (16 or 32; 0: 16
+                                       // when the count fits half the launch, else 32)
 };
 
 // occ == nullptr: closest hit into `hits`; otherwise any-hit into `occ`.

@@ -46,8 +46,6 @@ __global__ void __launch_bounds__(128) k_trace_wide_split(TraceArgs a) {
     const unsigned lane = threadIdx.x & 31u;
     // Lane `lane` < warp_rays of warp w starts on ray w * warp_rays + lane;
     // the other lanes start idle and help from the first pass.
-    const uint64_t warp_id = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const uint64_t i = warp_id * a.warp_rays + lane;
     __shared__ __align__(16) uint32_t s_warp[4][kWarpWords];
     uint32_t* warp_words = s_warp[threadIdx.x >> 5];
     uint32_t* ids = warp_words + kPoolWords;
@@ -57,7 +55,11 @@ __global__ void __launch_bounds__(128) k_trace_wide_split(TraceArgs a) {
     uint32_t st = kFree | (lane << 2);
     const uint64_t n = ray_count(a);
     if (a.small_max && n > a.small_max) return;   // the persistent launch beside this one has it
-    if (lane < a.warp_rays && i < n) {
+    const uint32_t warp_rays = a.warp_rays ? a.warp_rays
+                                           : (2 * n <= (uint64_t)gridDim.x * blockDim.x ? 16u : 32u);
+    const uint64_t warp_id = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint64_t i = warp_id * warp_rays + lane;
+    if (lane < warp_rays && i < n) {
         const RayIn r = load_ray(a.rays, i);
         T.init(r);
         if (a.n_nodes != 0 && T.enters(a.bound)) {
@@ -278,6 +280,7 @@ cudaError_t launch_variant(const TraceArgs& t, const LaunchParams& lp, cudaStrea
             if (blocks > 0) {
                 TraceArgs q = t;
                 q.small_max = blocks * block;
+                q.warp_rays = 0;                    // 16 rays a warp when the count allows
                 if (t.occ) ka<<<(unsigned)blocks, block, 0, s>>>(q);
                 else kc<<<(unsigned)blocks, block, 0, s>>>(q);
                 cudaError_t e = cudaGetLastError();
