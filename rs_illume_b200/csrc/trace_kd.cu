@@ -22,7 +22,10 @@
 //
 // Schedules: one thread per ray (grid), or persistent warps that claim rays in
 // chunks and refill finished lanes (the wide BVH kernels' scheme); every loop
-// iteration advances a lane by one node or one leaf.
+// iteration advances a lane by one node or one leaf.  The pooled persistent
+// kernel also splits its tail as the wide one does: once every ray is claimed,
+// idle lanes take the top deferred entry of their warp's unfinished rays with
+// its range (KdTracer::give / take).
 #include "wide_tracer.cuh"
 
 namespace ilm {
