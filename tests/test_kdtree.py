@@ -232,6 +232,36 @@ def test_gpu_kdtree_matches_oracle(ctx, name):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("n", [40000, 700001])
+def test_gpu_kdtree_split_tail_agrees(n):
+    """The kd-tree's split tail (idle lanes take a deferred subtree with its
+    range) against the lone traversal, device buffers: any-hit flags equal,
+    closest hits equal up to exact ties in t.  700,001 rays run the pooled
+    persistent kernel well past its claims; 40,000 is a short queue."""
+    import torch
+    import rs_illume_b200 as rb
+    xyz, idx = wl.icosphere(6, 4)
+    rays = wl.ball_rays(6, 4, n, n // 2)
+    d_rays = torch.from_numpy(rays.view(np.uint8)).cuda()
+    out = []
+    for split in (False, True):
+        c = rb.Context(0, high_occupancy=True, tail_split=split)
+        kd = rb.GpuKdTreeAccel(c, [rb.TriangleMesh(c, xyz, idx)])
+        d_hits = torch.full((n * 16,), 0xAB, dtype=torch.uint8, device="cuda")
+        d_occ = torch.full((n * 4,), 0xAB, dtype=torch.uint8, device="cuda")
+        kd.intersect_batch(d_rays, d_hits)
+        kd.intersect_p_batch(d_rays, d_occ)
+        torch.cuda.synchronize()
+        out.append((d_hits.cpu().numpy().view(_lib.HIT_DTYPE), d_occ.cpu().numpy().view(np.uint32)))
+        assert c.device_errors() == 0
+        c.close()
+    assert np.array_equal(out[0][1], out[1][1])
+    assert np.all(out[1][1] <= 1)
+    compare(out[1][0], out[0][0], "kd split tail")
+    assert np.mean(out[0][0]["prim"] != MISS) > 0.05
+
+
+@pytest.mark.gpu
 def test_gpu_kdtree_device_buffers_noalloc_and_interactions(ctx):
     import torch
     import rs_illume_b200 as rb
